@@ -1,0 +1,191 @@
+// Device-side board primitives for the classic tablebase path (sm_100a).
+//
+// Board: 4x4 cells in a uint64, one log2 nibble per cell; nibble k is row
+// 3-k/4, column 3-k%4, so row 0 is the high 16 bits and column 0 the high
+// nibble of a row (native_core/include/BoardCodec.h:20-30). Nibble 0xF is the
+// 32768 tile, which never merges (native_core/include/BoardMover.h:31).
+#pragma once
+
+#include <cstdint>
+
+namespace egtb {
+
+constexpr int kMaxMasks = 32;
+
+// Pattern parameters handed to every kernel by value.
+struct DevSpec {
+    uint64_t masks[kMaxMasks];
+    int n_masks;
+    int symm;              // 0 identity, 1 full, 2 diagonal, 3 horizontal
+    uint64_t succ_hi;      // bit 4k+3 set for every success nibble k
+    uint64_t target_rep;   // target log2 replicated in every nibble
+    int has_success;       // 0: no success shifts -> everything is a success
+    int target;
+};
+
+// ---------------------------------------------------------------- moves ---
+
+// Row-move XOR deltas: low 16 bits move toward column 0, high 16 bits toward
+// column 3. Built on the host by egtb::host_row_tables().
+struct RowTables {
+    const uint32_t *delta;  // 65536 entries
+};
+
+__device__ __forceinline__ uint32_t row_delta(const uint32_t *__restrict__ tab, uint32_t row) {
+    return __ldg(tab + row);
+}
+
+// 4x4 nibble-matrix transpose: swap the off-diagonal 2x2 blocks (24-bit
+// shift), then the off-diagonal cells inside each block (12-bit shift).
+__device__ __forceinline__ uint64_t transpose(uint64_t b) {
+    uint64_t x =(b & 0xFF00FF0000FF00FFull) | ((b & 0x00FF00FF00000000ull) >> 24) |
+                 ((b & 0x00000000FF00FF00ull) << 24);
+    return (x & 0xF0F00F0FF0F00F0Full) | ((x & 0x0F0F00000F0F0000ull) >> 12) |
+           ((x & 0x0000F0F00000F0F0ull) << 12);
+}
+
+// Mirror columns: reverse the four nibbles of every 16-bit row.
+__device__ __forceinline__ uint64_t mirror_cols(uint64_t b) {
+    b = ((b & 0xFF00FF00FF00FF00ull) >> 8) | ((b & 0x00FF00FF00FF00FFull) << 8);
+    return ((b & 0xF0F0F0F0F0F0F0F0ull) >> 4) | ((b & 0x0F0F0F0F0F0F0F0Full) << 4);
+}
+
+// Mirror rows: reverse the four 16-bit rows.
+__device__ __forceinline__ uint64_t mirror_rows(uint64_t b) {
+    b = (b >> 32) | (b << 32);
+    return ((b & 0xFFFF0000FFFF0000ull) >> 16) | ((b & 0x0000FFFF0000FFFFull) << 16);
+}
+
+__device__ __forceinline__ uint64_t umin(uint64_t a, uint64_t b) { return a < b ? a : b; }
+
+// The eight symmetries, numbered like apply_sym_like
+// (native_core/include/SymmetryUtils.h:9-29): 1 mirror columns, 2 mirror rows,
+// 3 transpose, 4 anti-transpose, 5 half turn, 6 quarter turn
+// counter-clockwise, 7 quarter turn clockwise.
+__device__ __forceinline__ uint64_t apply_sym(uint64_t b, int idx) {
+    switch (idx) {
+        case 1: return mirror_cols(b);
+        case 2: return mirror_rows(b);
+        case 3: return transpose(b);
+        case 4: return mirror_cols(mirror_rows(transpose(b)));
+        case 5: return mirror_cols(mirror_rows(b));
+        case 6: return mirror_rows(transpose(b));
+        case 7: return mirror_cols(transpose(b));
+        default: return b;
+    }
+}
+
+// Minimum over the symmetry group (canonical_by_mode,
+// native_core/include/SymmetryUtils.h:31-49).
+__device__ __forceinline__ uint64_t canonical(uint64_t b, int symm) {
+    if (symm == 0) return b;
+    if (symm == 2) return umin(b, transpose(b));
+    if (symm == 3) return umin(b, mirror_cols(b));
+    // full group: b and its transpose, each with the four row/column mirrors
+    uint64_t t = transpose(b);
+    uint64_t m = umin(b, t);
+    uint64_t br = mirror_rows(b), tr = mirror_rows(t);
+    m = umin(m, umin(br, tr));
+    m = umin(m, umin(mirror_cols(b), mirror_cols(t)));
+    m = umin(m, umin(mirror_cols(br), mirror_cols(tr)));
+    return m;
+}
+
+// is_pattern (native_core/include/Formation.h:11-17)
+__device__ __forceinline__ bool is_pattern(uint64_t b, const DevSpec &s) {
+    if (s.n_masks == 0) return true;
+    for (int i = 0; i < s.n_masks; ++i)
+        if ((b & s.masks[i]) == s.masks[i]) return true;
+    return false;
+}
+
+// is_success_by_shifts (native_core/include/Formation.h:32-43) as a
+// zero-nibble test of b ^ target over the success nibbles.
+__device__ __forceinline__ bool is_success(uint64_t b, const DevSpec &s) {
+    if (!s.has_success) return true;
+    const uint64_t x = b ^ s.target_rep;
+    const uint64_t m7 = 0x7777777777777777ull;
+    const uint64_t zero_hi = ~(((x & m7) + m7) | x | m7);
+    return (zero_hi & s.succ_hi) != 0;
+}
+
+// The four moves of a board in the order left, right, up, down
+// (move_all_dir, native_core/include/CommonMover.h:136-139).
+__device__ __forceinline__ void move_all_dir(const uint32_t *__restrict__ tab, uint64_t b, uint64_t out[4]) {
+    uint64_t dl = 0, dr = 0, ul = 0, ur = 0;
+    const uint64_t t = transpose(b);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        uint32_t d = row_delta(tab, (uint32_t)(b >> (16 * r)) & 0xFFFFu);
+        dl |= (uint64_t)(d & 0xFFFFu) << (16 * r);
+        dr |= (uint64_t)(d >> 16) << (16 * r);
+        uint32_t e = row_delta(tab, (uint32_t)(t >> (16 * r)) & 0xFFFFu);
+        ul |= (uint64_t)(e & 0xFFFFu) << (16 * r);
+        ur |= (uint64_t)(e >> 16) << (16 * r);
+    }
+    out[0] = b ^ dl;
+    out[1] = b ^ dr;
+    out[2] = transpose(t ^ ul);
+    out[3] = transpose(t ^ ur);
+}
+
+// Per-parent move context: the parent's row deltas (for left/right) and the
+// transposed board's row deltas (for up/down). A spawn touches one row and
+// one column, so a child's four moves need only the deltas of the touched
+// row and column to be looked up again.
+struct MoveCtx {
+    uint64_t b, t;       // board and transpose
+    uint64_t dl, dr;     // left/right deltas of b, all rows
+    uint64_t ul, ur;     // left/right deltas of t, all rows (= up/down of b)
+};
+
+__device__ __forceinline__ void move_ctx_init(const uint32_t *__restrict__ tab, uint64_t b, MoveCtx &c) {
+    c.b = b;
+    c.t = transpose(b);
+    c.dl = c.dr = c.ul = c.ur = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        uint32_t d = row_delta(tab, (uint32_t)(b >> (16 * r)) & 0xFFFFu);
+        c.dl |= (uint64_t)(d & 0xFFFFu) << (16 * r);
+        c.dr |= (uint64_t)(d >> 16) << (16 * r);
+        uint32_t e = row_delta(tab, (uint32_t)(c.t >> (16 * r)) & 0xFFFFu);
+        c.ul |= (uint64_t)(e & 0xFFFFu) << (16 * r);
+        c.ur |= (uint64_t)(e >> 16) << (16 * r);
+    }
+}
+
+// Transposed nibble index of nibble k: (r, c) -> (c, r) keeps k/4 <-> k%4.
+__device__ __forceinline__ int transposed_nibble(int k) { return ((k & 3) << 2) | (k >> 2); }
+
+// Moves of s = parent | v << 4k (nibble k empty in the parent).
+__device__ __forceinline__ void spawn_moves(const uint32_t *__restrict__ tab, const MoveCtx &c, int k, uint64_t v,
+                                            uint64_t &s, uint64_t out[4]) {
+    s = c.b | (v << (4 * k));
+    const int row = k >> 2;
+    const uint64_t rmask = 0xFFFFull << (16 * row);
+    const uint32_t d = row_delta(tab, (uint32_t)(s >> (16 * row)) & 0xFFFFu);
+    out[0] = s ^ ((c.dl & ~rmask) | ((uint64_t)(d & 0xFFFFu) << (16 * row)));
+    out[1] = s ^ ((c.dr & ~rmask) | ((uint64_t)(d >> 16) << (16 * row)));
+    const int kt = transposed_nibble(k);
+    const uint64_t ts = c.t | (v << (4 * kt));
+    const int trow = kt >> 2;
+    const uint64_t tmask = 0xFFFFull << (16 * trow);
+    const uint32_t e = row_delta(tab, (uint32_t)(ts >> (16 * trow)) & 0xFFFFu);
+    out[2] = transpose(ts ^ ((c.ul & ~tmask) | ((uint64_t)(e & 0xFFFFu) << (16 * trow))));
+    out[3] = transpose(ts ^ ((c.ur & ~tmask) | ((uint64_t)(e >> 16) << (16 * trow))));
+}
+
+// Bit set in nibble k's low bit for every empty nibble of b.
+__device__ __forceinline__ uint64_t empty_nibbles(uint64_t b) {
+    uint64_t x = b | (b >> 1);
+    x |= x >> 2;
+    return ~x & 0x1111111111111111ull;
+}
+
+// Multiplicative hash for the device-side repeat filter (any hash works: the
+// filter only drops repeats, never a first occurrence).
+__device__ __forceinline__ uint64_t filter_slot(uint64_t key, int bits) {
+    return (key * 0x9E3779B97F4A7C15ull) >> (64 - bits);
+}
+
+}  // namespace egtb

@@ -1,0 +1,211 @@
+/*
+ * egtb_gpu.h — C ABI of libegtb_gpu.so, the B200 (sm_100a) implementation of
+ * the classic endgame-tablebase table build and book lookup of
+ * game-difficulty/2048EndgameTablebase.
+ *
+ * Plain C: fixed-size structs, pointers and sizes, int status codes. No
+ * CUDA, C++ or torch types cross this boundary. Every entry point returns
+ * EGTB_OK (0) or a negative EGTB_ERR_* code; egtb_last_error() gives the
+ * message of the calling thread's last failure.
+ *
+ * Each declaration names the reference interface it replaces (file:line in
+ * the reference project). The reference binds these from Python through
+ * nanobind (native_core/src/bindings_formation.cpp:46-241); this library is
+ * bound through ctypes by 2048endgametablebase_b200/native_core/formation_core.py.
+ *
+ * Threading: build entry points may run on any host thread; progress may be
+ * read from another thread while a build runs (relaxed atomics, as
+ * native_core/include/FormationRuntime.h:44-86). One device context is kept
+ * per device; builds on the same device are serialised inside the library.
+ */
+#ifndef EGTB_GPU_H
+#define EGTB_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status ---- */
+#define EGTB_OK 0
+#define EGTB_ERR_ARG (-1)          /* invalid argument */
+#define EGTB_ERR_CUDA (-2)         /* CUDA runtime error (no device, launch failure, ...) */
+#define EGTB_ERR_NOMEM (-3)        /* device or pinned-host allocation failed */
+#define EGTB_ERR_IO (-4)           /* file read/write failed */
+#define EGTB_ERR_CAPACITY (-5)     /* a layer outgrew the largest buffer the device can hold */
+#define EGTB_ERR_TIMEOUT (-6)      /* a bounded device wait gave up */
+#define EGTB_ERR_UNSUPPORTED (-7)  /* option outside the implemented path */
+
+/* ------------------------------------------------------------ types ----- */
+
+/* SymmMode, native_core/include/FormationRuntime.h:13 */
+enum egtb_symm_mode {
+    EGTB_SYMM_IDENTITY = 0,
+    EGTB_SYMM_FULL = 1,
+    EGTB_SYMM_DIAGONAL = 2,
+    EGTB_SYMM_HORIZONTAL = 3,
+    EGTB_SYMM_MIN33 = 4,
+    EGTB_SYMM_MIN24 = 5,
+    EGTB_SYMM_MIN34 = 6
+};
+
+/* success_rate_dtype names, native_core/include/FormationRuntime.h:243-255 */
+enum egtb_dtype {
+    EGTB_DTYPE_UINT32 = 0,
+    EGTB_DTYPE_UINT64 = 1,
+    EGTB_DTYPE_FLOAT32 = 2,
+    EGTB_DTYPE_FLOAT64 = 3,
+    EGTB_DTYPE_1_FLOAT32 = 4, /* stores success - 1 */
+    EGTB_DTYPE_1_FLOAT64 = 5
+};
+
+#define EGTB_MAX_MASKS 32
+#define EGTB_MAX_PATH 4096
+
+/* PatternSpec, native_core/include/FormationRuntime.h:17-22 */
+typedef struct egtb_pattern_spec {
+    char name[64];
+    uint64_t pattern_masks[EGTB_MAX_MASKS];
+    int32_t n_masks;
+    uint8_t success_shifts[16];
+    int32_t n_shifts;
+    int32_t symm_mode; /* enum egtb_symm_mode */
+} egtb_pattern_spec;
+
+/* RunOptions, native_core/include/FormationRuntime.h:24-42, plus device fields */
+typedef struct egtb_run_options {
+    int32_t target;       /* log2 of the target tile */
+    int32_t steps;
+    int32_t docheck_step;
+    char pathname[EGTB_MAX_PATH]; /* file prefix: layer t is <pathname><t>, book <pathname><t>.book */
+    int32_t is_free;
+    int32_t is_variant;
+    double spawn_rate4;
+    int32_t success_rate_dtype; /* enum egtb_dtype */
+    double deletion_threshold;
+    int32_t compress;
+    int32_t compress_temp_files;
+    int32_t optimal_branch_only;
+    int32_t chunked_solve;
+    int32_t num_threads;  /* host threads for file writing (0 = library default) */
+    int32_t direct_io;
+    int32_t direct_io_queue_depth;
+    int32_t direct_io_chunk_mib;
+    /* device fields (no reference counterpart) */
+    int32_t device;       /* CUDA device ordinal */
+    int32_t write_files;  /* egtb_build only: 0 keeps the books on the device (benchmarks) */
+} egtb_run_options;
+
+/* Per-build record filled by egtb_build / egtb_generate (no reference counterpart:
+ * the reference logs the same quantities through Config.logger). */
+typedef struct egtb_build_stats {
+    uint64_t raw_boards;       /* sum of raw layer sizes */
+    uint64_t book_entries;     /* sum of .book sizes (zero rates dropped) */
+    uint64_t max_layer;        /* largest raw layer */
+    uint64_t candidates;       /* children that reached the sort (after the device filter) */
+    uint64_t lookups;          /* exact searches done by the backward pass */
+    int32_t layers;            /* steps */
+    int32_t retries;           /* capacity regrowths */
+    double forward_ms;         /* device time */
+    double backward_ms;        /* device time */
+    double total_ms;           /* host wall time of the call */
+} egtb_build_stats;
+
+/* ------------------------------------------------------------ errors ---- */
+
+/* Message of the calling thread's last failure (empty when none). */
+int egtb_last_error(char *buf, size_t len);
+
+/* Library version string, e.g. "egtb_gpu 0.1 sm_100a". */
+const char *egtb_version(void);
+
+/* Number of visible CUDA devices (0 when none). */
+int egtb_device_count(void);
+
+/* ---------------------------------------------------------- progress ---- */
+
+/* get_build_progress / reset_build_progress,
+ * native_core/src/bindings_formation.cpp:140-155, FormationRuntime.h:57-84 */
+int egtb_get_build_progress(uint32_t *current, uint32_t *total);
+int egtb_reset_build_progress(uint32_t total);
+
+/* ------------------------------------------------------------ build ----- */
+
+/* run_pattern_build, native_core/src/BookSolver.cpp:823-832 (bound at
+ * bindings_formation.cpp:220-229): forward layer generation then backward
+ * solve, writing <pathname><t>.book for every layer and <pathname>stats.txt.
+ * With no layer files present the whole build stays in device memory and
+ * only books are written; with layer files present it resumes through
+ * egtb_generate + egtb_solve like the reference. stats may be NULL. */
+int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec *spec,
+               const egtb_run_options *options, egtb_build_stats *stats);
+
+/* run_pattern_generate, native_core/src/BookSolver.cpp:766-782 (bound at
+ * bindings_formation.cpp:200-208): writes raw layers <pathname>0 ..
+ * <pathname><steps-3> and the success-only books of layers steps-2 and
+ * steps-1 (final_steps, BookSolver.cpp:263-284). *started is 0 when every
+ * step was already on disk. */
+int egtb_generate(const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec *spec,
+                  const egtb_run_options *options, int32_t *started, egtb_build_stats *stats);
+
+/* run_pattern_solve, native_core/src/BookSolver.cpp:784-821 (bound at
+ * bindings_formation.cpp:210-218): backward pass from the raw layer files.
+ * d1/d2 are the packed book records of layers steps-2 and steps-1 (n1/n2
+ * records; may be empty, then they are read from their .book files). */
+int egtb_solve(const void *d1_records, size_t n1, const void *d2_records, size_t n2,
+               const egtb_pattern_spec *spec, const egtb_run_options *options, egtb_build_stats *stats);
+
+/* ------------------------------------------------------- primitives ----- */
+
+/* Batched board primitives on the device, host buffers in and out
+ * (move_all_dir native_core/include/CommonMover.h:136-139; canonical_by_mode
+ * SymmetryUtils.h:31-49; apply_sym_like SymmetryUtils.h:9-29). */
+int egtb_move_all_dir(int device, const uint64_t *boards, size_t n, uint64_t *out4);
+int egtb_canonical(int device, const uint64_t *boards, size_t n, int32_t symm_mode, uint64_t *out);
+int egtb_apply_sym(int device, const uint64_t *boards, size_t n, int32_t symm_index, uint64_t *out);
+
+/* ------------------------------------------------------------ books ----- */
+
+typedef struct egtb_book egtb_book;
+
+/* Open the books <dir>/<pattern_full>_<t>.book of one table and keep them
+ * resident in device memory as sorted keys + rates (the reader side of
+ * ClassicBookReader, native_core/src/ReaderRuntime.cpp:1050-1067).
+ * nums_adjust is the pattern's -(seed tile sum) (Config.py:265). Layers
+ * are loaded on first use; max_layers bounds the layer index scanned. */
+int egtb_book_open(const char *dir, const char *pattern_full, int32_t dtype, const egtb_pattern_spec *spec,
+                   int64_t nums_adjust, int32_t device, egtb_book **out);
+int egtb_book_close(egtb_book *book);
+
+/* Load every book layer of the table now (otherwise loaded on first lookup). */
+int egtb_book_load_all(egtb_book *book, int32_t *layers_loaded);
+
+/* Batched move_on_dic on encoded positions (encode_board_matrix,
+ * native_core/include/BoardCodec.h:20-30), host buffers, op order
+ * [last_op, 0..7] as evaluate_classic_result_candidates
+ * (ReaderRuntime.cpp:739-840). Per position writes 4 values in direction
+ * order up, right, down, left (kDirectionNames, ReaderRuntime.cpp:32) already
+ * normalised and rounded like maybe_round_value (:208-214), a validity mask
+ * (bit d set when direction d has a numeric value) and the operation index
+ * that matched (-1 when none; -2 when the layer index is negative; -3 when
+ * the layer's book file does not exist). */
+int egtb_book_lookup(egtb_book *book, const uint64_t *positions, size_t n, int32_t last_op,
+                     double *values4, uint8_t *valid_mask, int8_t *op_used);
+
+/* Same on device memory and a caller stream (cudaStream_t passed as void*),
+ * float32 values; used by the serving loop. Layers must be loaded. */
+int egtb_book_lookup_device(egtb_book *book, const uint64_t *d_positions, size_t n, int32_t last_op,
+                            float *d_values4, uint8_t *d_valid_mask, void *stream);
+
+/* find_classic_value, native_core/src/ReaderRuntime.cpp:1107-1133 (bound at
+ * bindings_formation.cpp:180-194): the normalised value of one key in one
+ * book file; *found = 0 when the file does not exist (value 0 then). */
+int egtb_find_classic_value(const char *pathname, const char *filename, uint64_t key, int32_t dtype,
+                            int32_t device, double *value, int32_t *found);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EGTB_GPU_H */

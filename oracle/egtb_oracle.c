@@ -1,0 +1,474 @@
+/*
+ * CPU oracle for the classic endgame-tablebase build/lookup path.
+ *
+ * TEST INFRASTRUCTURE ONLY — a plain-C restatement of the reference algorithm
+ * (game-difficulty/2048EndgameTablebase, native_core/). Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg use it, and only as
+ * the checker. Built with -ffp-contract=off so the one place the reference's
+ * -Ofast build contracts to FMA (the backward accumulation, see or_solve_layer)
+ * is written out explicitly with fma().
+ *
+ * Board layout (native_core/include/BoardCodec.h:20-30): 4x4 board packed in a
+ * uint64, one log2 nibble per cell; nibble k holds row 3-k/4, column 3-k%4, so
+ * row 0 is the high 16 bits and column 0 the high nibble of each row.
+ */
+#include "egtb_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ---------------------------------------------------------------- rows --- */
+
+static uint16_t g_left[65536], g_right[65536];
+static int g_tables_ready = 0;
+
+/* One row moved toward column 0 (reverse=0) or column 3 (reverse=1).
+ * Restates StandardMergePolicy::_internal_merge, native_core/include/BoardMover.h:6-55:
+ * slide non-empty cells, merge each adjacent equal pair once (first pair
+ * first), the 32768 tile (nibble 0xF) never merges. Works on log2 nibbles. */
+static uint16_t row_move(uint16_t row, int reverse) {
+    int line[4], nz[4], out[4] = {0, 0, 0, 0};
+    int n = 0, m = 0;
+    for (int i = 0; i < 4; ++i) line[i] = (row >> (4 * (3 - i))) & 0xF;
+    if (reverse) {
+        int t = line[0]; line[0] = line[3]; line[3] = t;
+        t = line[1]; line[1] = line[2]; line[2] = t;
+    }
+    for (int i = 0; i < 4; ++i)
+        if (line[i]) nz[n++] = line[i];
+    for (int i = 0; i < n; ++i) {
+        if (i + 1 < n && nz[i] == nz[i + 1] && nz[i] != 0xF) {
+            out[m++] = nz[i] + 1;
+            ++i;
+        } else {
+            out[m++] = nz[i];
+        }
+    }
+    if (reverse) {
+        int t = out[0]; out[0] = out[3]; out[3] = t;
+        t = out[1]; out[1] = out[2]; out[2] = t;
+    }
+    uint16_t r = 0;
+    for (int i = 0; i < 4; ++i) r |= (uint16_t)((out[i] & 0xF) << (4 * (3 - i)));
+    return r;
+}
+
+/* XOR-delta row tables, native_core/include/CommonMover.h:87-94 */
+static void init_tables(void) {
+    if (g_tables_ready) return;
+    for (uint32_t r = 0; r < 65536; ++r) {
+        g_left[r] = (uint16_t)(row_move((uint16_t)r, 0) ^ r);
+        g_right[r] = (uint16_t)(row_move((uint16_t)r, 1) ^ r);
+    }
+    g_tables_ready = 1;
+}
+
+void or_row_tables(uint16_t *left_xor, uint16_t *right_xor) {
+    init_tables();
+    memcpy(left_xor, g_left, sizeof g_left);
+    memcpy(right_xor, g_right, sizeof g_right);
+}
+
+/* ------------------------------------------------------------ symmetry --- */
+
+static inline int nib(uint64_t b, int r, int c) { return (int)((b >> (4 * ((3 - r) * 4 + (3 - c)))) & 0xF); }
+static inline uint64_t put(int v, int r, int c) { return (uint64_t)v << (4 * ((3 - r) * 4 + (3 - c))); }
+
+/* The eight symmetries of the square as cell maps (r,c) -> (r',c'),
+ * numbered as apply_sym_like, native_core/include/SymmetryUtils.h:9-29 /
+ * native_core/include/Calculator.h:28-78:
+ * 0 identity, 1 mirror columns, 2 mirror rows, 3 transpose, 4 anti-transpose,
+ * 5 half turn, 6 quarter turn counter-clockwise, 7 quarter turn clockwise. */
+uint64_t or_apply_sym(uint64_t b, int idx) {
+    uint64_t o = 0;
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            int v = nib(b, r, c), R = r, C = c;
+            switch (idx) {
+                case 1: C = 3 - c; break;
+                case 2: R = 3 - r; break;
+                case 3: R = c; C = r; break;
+                case 4: R = 3 - c; C = 3 - r; break;
+                case 5: R = 3 - r; C = 3 - c; break;
+                case 6: R = 3 - c; C = r; break;
+                case 7: R = c; C = 3 - r; break;
+                default: break;
+            }
+            o |= put(v, R, C);
+        }
+    return o;
+}
+
+/* canonical_by_mode, native_core/include/SymmetryUtils.h:31-49 with
+ * Calculator::canonical_{identity,full,diagonal,horizontal}
+ * (native_core/include/Calculator.h:80-97): the minimum over the group. */
+uint64_t or_canonical(uint64_t b, int mode) {
+    uint64_t m = b, t;
+    switch (mode) {
+        case OR_SYM_FULL:
+            for (int i = 1; i < 8; ++i) {
+                t = or_apply_sym(b, i);
+                if (t < m) m = t;
+            }
+            return m;
+        case OR_SYM_DIAGONAL:
+            t = or_apply_sym(b, 3);
+            return t < m ? t : m;
+        case OR_SYM_HORIZONTAL:
+            t = or_apply_sym(b, 1);
+            return t < m ? t : m;
+        default:
+            return b;
+    }
+}
+
+/* -------------------------------------------------------------- moves --- */
+
+/* transpose, the reference's reverse_board (native_core/include/CommonMover.h:33-37) */
+static inline uint64_t transpose(uint64_t b) { return or_apply_sym(b, 3); }
+
+static inline uint64_t rows_apply(uint64_t b, const uint16_t *tab) {
+    uint64_t o = b;
+    for (int r = 0; r < 4; ++r) o ^= (uint64_t)tab[(b >> (16 * r)) & 0xFFFF] << (16 * r);
+    return o;
+}
+
+/* move_all_dir: {left, right, up, down}, native_core/include/CommonMover.h:136-139 */
+void or_move_all_dir(uint64_t b, uint64_t out[4]) {
+    init_tables();
+    uint64_t t = transpose(b);
+    out[0] = rows_apply(b, g_left);
+    out[1] = rows_apply(b, g_right);
+    out[2] = transpose(rows_apply(t, g_left));
+    out[3] = transpose(rows_apply(t, g_right));
+}
+
+void or_move_all_dir_batch(const uint64_t *b, size_t n, uint64_t *out4) {
+    for (size_t i = 0; i < n; ++i) or_move_all_dir(b[i], out4 + 4 * i);
+}
+
+void or_canonical_batch(const uint64_t *b, size_t n, int mode, uint64_t *out) {
+    for (size_t i = 0; i < n; ++i) out[i] = or_canonical(b[i], mode);
+}
+
+/* is_pattern, native_core/include/Formation.h:11-17 */
+int or_is_pattern(uint64_t b, const or_spec *s) {
+    if (s->n_masks == 0) return 1;
+    for (int i = 0; i < s->n_masks; ++i)
+        if ((b & s->masks[i]) == s->masks[i]) return 1;
+    return 0;
+}
+
+/* is_success_by_shifts, native_core/include/Formation.h:32-43 */
+int or_is_success(uint64_t b, int target, const or_spec *s) {
+    if (s->n_shifts == 0) return 1;
+    for (int i = 0; i < s->n_shifts; ++i)
+        if (((b >> s->shifts[i]) & 0xF) == (uint64_t)target) return 1;
+    return 0;
+}
+
+/* ------------------------------------------------------------- forward --- */
+
+/* Children of one parent layer: for each parent (skipped when do_check and
+ * it is a success), each empty nibble i ascending, spawn 2 then 4, the four
+ * moves; a child is kept if it moved and matches the pattern, and is stored
+ * canonicalised. Restates gen_boards_simple / gen_boards_internal_naive,
+ * native_core/src/BookGenerator.cpp:717-760 and :472-589 (the lossy hash
+ * prefilter of :112-127,150-181 only drops repeats and is omitted). */
+size_t or_expand(const uint64_t *parents, size_t n, const or_spec *spec, int target, int do_check,
+                 uint64_t *out1, uint64_t *out2, size_t cap, size_t *n2) {
+    size_t c1 = 0, c2 = 0;
+    uint64_t mv[4];
+    for (size_t p = 0; p < n; ++p) {
+        uint64_t b = parents[p];
+        if (do_check && or_is_success(b, target, spec)) continue;
+        for (int i = 0; i < 16; ++i) {
+            if ((b >> (4 * i)) & 0xF) continue;
+            for (uint64_t v = 1; v <= 2; ++v) {
+                uint64_t s = b | (v << (4 * i));
+                or_move_all_dir(s, mv);
+                for (int d = 0; d < 4; ++d) {
+                    if (mv[d] == s || !or_is_pattern(mv[d], spec)) continue;
+                    uint64_t k = or_canonical(mv[d], spec->symm_mode);
+                    if (v == 1) {
+                        if (c1 < cap) out1[c1] = k;
+                        ++c1;
+                    } else {
+                        if (c2 < cap) out2[c2] = k;
+                        ++c2;
+                    }
+                }
+            }
+        }
+    }
+    *n2 = c2;
+    return c1;
+}
+
+/* LSD radix sort, 16-bit digits, then in-place unique. Any correct sort gives
+ * the reference's result: sort_array + parallel_unique
+ * (native_core/src/BookGeneratorUtils.cpp:138-158) leave a strictly
+ * ascending array. */
+static size_t sort_unique(uint64_t *a, size_t n) {
+    if (n < 2) return n;
+    uint64_t *tmp = (uint64_t *)malloc(n * sizeof(uint64_t));
+    size_t *cnt = (size_t *)malloc(65536 * sizeof(size_t));
+    uint64_t *src = a, *dst = tmp;
+    for (int pass = 0; pass < 4; ++pass) {
+        int sh = 16 * pass;
+        memset(cnt, 0, 65536 * sizeof(size_t));
+        for (size_t i = 0; i < n; ++i) cnt[(src[i] >> sh) & 0xFFFF]++;
+        size_t s = 0;
+        for (int d = 0; d < 65536; ++d) {
+            size_t c = cnt[d];
+            cnt[d] = s;
+            s += c;
+        }
+        for (size_t i = 0; i < n; ++i) dst[cnt[(src[i] >> sh) & 0xFFFF]++] = src[i];
+        uint64_t *t = src; src = dst; dst = t;
+    }
+    /* four passes: result is back in a */
+    size_t m = 1;
+    for (size_t i = 1; i < n; ++i)
+        if (a[i] != a[m - 1]) a[m++] = a[i];
+    free(tmp);
+    free(cnt);
+    return m;
+}
+
+struct or_build {
+    int steps;
+    uint64_t **keys;
+    size_t *len;
+    void **rates;
+    int dtype;
+    or_spec spec;
+    uint64_t *masks;
+    uint8_t *shifts;
+    int target, docheck;
+};
+
+/* The layer loop of generate_process, native_core/src/BookGenerator.cpp:963-1121:
+ * layer 0 = the seeds; for i = 1 .. steps-2 the parents are layer i-1, checked
+ * for success iff i > docheck_step (:991); layer i = unique(partial_i U spawn-2
+ * children) (:1059-1078); the spawn-4 children become partial_{i+1}. The last
+ * layer (steps-1) is left partial, as the reference leaves it (:978). */
+or_build *or_generate(const uint64_t *seeds, size_t n_seeds, const or_spec *spec,
+                      int target, int steps, int docheck_step) {
+    init_tables();
+    or_build *b = (or_build *)calloc(1, sizeof(or_build));
+    b->steps = steps;
+    b->keys = (uint64_t **)calloc((size_t)steps, sizeof(uint64_t *));
+    b->len = (size_t *)calloc((size_t)steps, sizeof(size_t));
+    b->rates = (void **)calloc((size_t)steps, sizeof(void *));
+    b->masks = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(spec->n_masks + 1));
+    b->shifts = (uint8_t *)malloc((size_t)spec->n_shifts + 1);
+    memcpy(b->masks, spec->masks, sizeof(uint64_t) * (size_t)spec->n_masks);
+    memcpy(b->shifts, spec->shifts, (size_t)spec->n_shifts);
+    b->spec = *spec;
+    b->spec.masks = b->masks;
+    b->spec.shifts = b->shifts;
+    b->target = target;
+    b->docheck = docheck_step;
+
+    b->keys[0] = (uint64_t *)malloc(sizeof(uint64_t) * (n_seeds + 1));
+    memcpy(b->keys[0], seeds, sizeof(uint64_t) * n_seeds);
+    b->len[0] = n_seeds; /* written as-is, BookGenerator.cpp:417-419 */
+
+    uint64_t *partial = NULL;
+    size_t npartial = 0;
+    for (int i = 1; i < steps - 1; ++i) {
+        const uint64_t *par = b->keys[i - 1];
+        size_t np = b->len[i - 1];
+        int do_check = i > docheck_step;
+        size_t cap = np * 64 + 16, n2 = 0;
+        uint64_t *s1 = (uint64_t *)malloc(sizeof(uint64_t) * (cap + npartial));
+        uint64_t *s2 = (uint64_t *)malloc(sizeof(uint64_t) * cap);
+        size_t n1 = or_expand(par, np, &b->spec, target, do_check, s1, s2, cap, &n2);
+        if (npartial) memcpy(s1 + n1, partial, sizeof(uint64_t) * npartial);
+        free(partial);
+        n1 = sort_unique(s1, n1 + npartial);
+        n2 = sort_unique(s2, n2);
+        b->keys[i] = s1;
+        b->len[i] = n1;
+        partial = s2;
+        npartial = n2;
+    }
+    if (steps >= 2) {
+        b->keys[steps - 1] = partial ? partial : (uint64_t *)malloc(8);
+        b->len[steps - 1] = npartial;
+    }
+    return b;
+}
+
+int or_num_layers(const or_build *b) { return b->steps; }
+size_t or_layer_len(const or_build *b, int t) { return b->len[t]; }
+const uint64_t *or_layer_keys(const or_build *b, int t) { return b->keys[t]; }
+const void *or_layer_rates(const or_build *b, int t) { return b->rates[t]; }
+
+void or_free(or_build *b) {
+    if (!b) return;
+    for (int t = 0; t < b->steps; ++t) {
+        free(b->keys[t]);
+        free(b->rates[t]);
+    }
+    free(b->keys);
+    free(b->len);
+    free(b->rates);
+    free(b->masks);
+    free(b->shifts);
+    free(b);
+}
+
+/* ------------------------------------------------------------ backward --- */
+
+static size_t dtype_size(int dtype) {
+    switch (dtype) {
+        case OR_U64: case OR_F64: case OR_1F64: return 8;
+        default: return 4;
+    }
+}
+
+/* zero_value_for_dtype / max_scale_value_for_dtype,
+ * native_core/include/FormationRuntime.h:257-312 (the "1-float" kinds store
+ * success-1, so 'zero' is -1 and 'max' is 0). */
+static double dtype_zero(int dtype) { return (dtype == OR_1F32 || dtype == OR_1F64) ? -1.0 : 0.0; }
+static double dtype_max(int dtype) {
+    switch (dtype) {
+        case OR_U32: return 4000000000.0;
+        case OR_U64: return 1600000000000000000.0;
+        case OR_F32: case OR_F64: return 1.0;
+        default: return 0.0;
+    }
+}
+
+/* exact search: the value stored for key, or the dtype's zero on a miss
+ * (search_arr, native_core/src/BookSolver.cpp:329-346) */
+#define DEFINE_LOOKUP(T, NAME)                                                       \
+    static T NAME(const uint64_t *k, const T *r, size_t n, uint64_t key, T zero) {  \
+        size_t lo = 0, hi = n;                                                       \
+        while (lo < hi) {                                                            \
+            size_t mid = lo + (hi - lo) / 2;                                         \
+            if (k[mid] < key) lo = mid + 1; else hi = mid;                           \
+        }                                                                            \
+        return (lo < n && k[lo] == key) ? r[lo] : zero;                              \
+    }
+DEFINE_LOOKUP(uint32_t, lookup_u32)
+DEFINE_LOOKUP(uint64_t, lookup_u64)
+DEFINE_LOOKUP(float, lookup_f32)
+DEFINE_LOOKUP(double, lookup_f64)
+
+/* recalculate_layer, native_core/src/BookSolver.cpp:413-470, per board:
+ *   success and do_check -> max scale;
+ *   else acc = 0.0 (double); for every empty nibble i ascending:
+ *     best2 = max over kept moves of rate_{t+1}(canonical(move(b | 1<<4i))), T-typed, from zero
+ *     acc   = fma(double(best2), 1 - p4, acc)
+ *     best4 = likewise from layer t+2 with b | 2<<4i
+ *     acc   = fma(double(best4), p4, acc)
+ *   rate = T(acc / double(#empty)), or zero when there is no empty nibble.
+ * The two fma() calls are the reference's `success_probability += ...`
+ * statements as its -Ofast -march=x86-64-v3 build compiles them (FMA
+ * contraction; native_core/CMakeLists.txt:80-87). */
+#define DEFINE_SOLVE(T, NAME, LOOKUP, CAST)                                                     \
+    static void NAME(const uint64_t *keys0, size_t n0, T *out, const uint64_t *k1, const T *r1,  \
+                     size_t n1, const uint64_t *k2, const T *r2, size_t n2, const or_spec *spec,  \
+                     int target, int do_check, int dtype, double p4) {                          \
+        const T zero = (T)dtype_zero(dtype), maxv = (T)dtype_max(dtype);                         \
+        const double w2 = 1.0 - p4;                                                              \
+        _Pragma("omp parallel for schedule(dynamic, 1024)")                                      \
+        for (size_t k = 0; k < n0; ++k) {                                                        \
+            uint64_t b = keys0[k], mv[4];                                                        \
+            if (do_check && or_is_success(b, target, spec)) {                                    \
+                out[k] = maxv;                                                                   \
+                continue;                                                                        \
+            }                                                                                    \
+            double acc = 0.0;                                                                    \
+            int empty = 0;                                                                       \
+            for (int i = 0; i < 16; ++i) {                                                       \
+                if ((b >> (4 * i)) & 0xF) continue;                                              \
+                ++empty;                                                                         \
+                for (uint64_t v = 1; v <= 2; ++v) {                                              \
+                    uint64_t s = b | (v << (4 * i));                                             \
+                    T best = zero;                                                               \
+                    or_move_all_dir(s, mv);                                                      \
+                    for (int d = 0; d < 4; ++d) {                                                \
+                        if (mv[d] == s || !or_is_pattern(mv[d], spec)) continue;                 \
+                        uint64_t key = or_canonical(mv[d], spec->symm_mode);                     \
+                        T got = (v == 1) ? LOOKUP(k1, r1, n1, key, zero)                         \
+                                         : LOOKUP(k2, r2, n2, key, zero);                        \
+                        if (best < got) best = got;                                              \
+                    }                                                                            \
+                    acc = fma((double)best, v == 1 ? w2 : p4, acc);                              \
+                }                                                                                \
+            }                                                                                    \
+            out[k] = empty > 0 ? CAST(acc / (double)empty) : zero;                               \
+        }                                                                                        \
+    }
+#define CAST_U32(x) ((uint32_t)(x))
+#define CAST_U64(x) ((uint64_t)(x))
+#define CAST_F32(x) ((float)(x))
+#define CAST_F64(x) ((double)(x))
+DEFINE_SOLVE(uint32_t, solve_u32, lookup_u32, CAST_U32)
+DEFINE_SOLVE(uint64_t, solve_u64, lookup_u64, CAST_U64)
+DEFINE_SOLVE(float, solve_f32, lookup_f32, CAST_F32)
+DEFINE_SOLVE(double, solve_f64, lookup_f64, CAST_F64)
+
+void or_solve_layer(const uint64_t *keys0, size_t n0, void *rates0,
+                    const uint64_t *k1, const void *r1, size_t n1,
+                    const uint64_t *k2, const void *r2, size_t n2,
+                    const or_spec *spec, int target, int do_check, int dtype, double p4) {
+    init_tables();
+    switch (dtype) {
+        case OR_U32:
+            solve_u32(keys0, n0, (uint32_t *)rates0, k1, (const uint32_t *)r1, n1, k2, (const uint32_t *)r2, n2,
+                      spec, target, do_check, dtype, p4);
+            break;
+        case OR_U64:
+            solve_u64(keys0, n0, (uint64_t *)rates0, k1, (const uint64_t *)r1, n1, k2, (const uint64_t *)r2, n2,
+                      spec, target, do_check, dtype, p4);
+            break;
+        case OR_F32: case OR_1F32:
+            solve_f32(keys0, n0, (float *)rates0, k1, (const float *)r1, n1, k2, (const float *)r2, n2,
+                      spec, target, do_check, dtype, p4);
+            break;
+        default:
+            solve_f64(keys0, n0, (double *)rates0, k1, (const double *)r1, n1, k2, (const double *)r2, n2,
+                      spec, target, do_check, dtype, p4);
+            break;
+    }
+}
+
+/* final_situation_process for layers steps-2 and steps-1
+ * (native_core/src/BookSolver.cpp:237-284): success -> max scale, else zero;
+ * then recalculate_process_impl (:513-605) for layers steps-3 .. 0 with
+ * do_check = i > docheck_step (:562). */
+int or_solve(or_build *b, int dtype, double spawn_rate4) {
+    init_tables();
+    const size_t es = dtype_size(dtype);
+    b->dtype = dtype;
+    const double zero = dtype_zero(dtype), maxv = dtype_max(dtype);
+    for (int t = b->steps - 2; t < b->steps; ++t) {
+        if (t < 0) continue;
+        free(b->rates[t]);
+        b->rates[t] = malloc(es * (b->len[t] + 1));
+        for (size_t k = 0; k < b->len[t]; ++k) {
+            int s = or_is_success(b->keys[t][k], b->target, &b->spec);
+            double v = s ? maxv : zero;
+            switch (dtype) {
+                case OR_U32: ((uint32_t *)b->rates[t])[k] = (uint32_t)v; break;
+                case OR_U64: ((uint64_t *)b->rates[t])[k] = (uint64_t)v; break;
+                case OR_F32: case OR_1F32: ((float *)b->rates[t])[k] = (float)v; break;
+                default: ((double *)b->rates[t])[k] = v; break;
+            }
+        }
+    }
+    for (int t = b->steps - 3; t >= 0; --t) {
+        free(b->rates[t]);
+        b->rates[t] = malloc(es * (b->len[t] + 1));
+        or_solve_layer(b->keys[t], b->len[t], b->rates[t], b->keys[t + 1], b->rates[t + 1], b->len[t + 1],
+                       b->keys[t + 2], b->rates[t + 2], b->len[t + 2], &b->spec, b->target,
+                       t > b->docheck, dtype, spawn_rate4);
+    }
+    return 0;
+}

@@ -1,0 +1,189 @@
+"""ctypes wrapper around the CPU oracle (egtb_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg as the checker. The product package never imports
+this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libegtb_oracle.so")
+
+DTYPES = {"uint32": 0, "uint64": 1, "float32": 2, "float64": 3, "1-float32": 4, "1-float64": 5}
+NP_DTYPES = {0: np.uint32, 1: np.uint64, 2: np.float32, 3: np.float64, 4: np.float32, 5: np.float64}
+
+
+class _Spec(ctypes.Structure):
+    _fields_ = [
+        ("masks", ctypes.POINTER(ctypes.c_uint64)),
+        ("n_masks", ctypes.c_int),
+        ("shifts", ctypes.POINTER(ctypes.c_uint8)),
+        ("n_shifts", ctypes.c_int),
+        ("symm_mode", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def build() -> str:
+    """Compile the oracle with make (gcc is part of the image)."""
+    subprocess.run(["make", "-s", "-C", HERE, "port"], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(
+            os.path.join(HERE, "egtb_oracle.c")
+        ):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+        L.or_generate.restype = ctypes.c_void_p
+        L.or_generate.argtypes = [u64p, ctypes.c_size_t, ctypes.POINTER(_Spec), ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.or_num_layers.argtypes = [ctypes.c_void_p]
+        L.or_layer_len.restype = ctypes.c_size_t
+        L.or_layer_len.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.or_layer_keys.restype = ctypes.c_void_p
+        L.or_layer_keys.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.or_layer_rates.restype = ctypes.c_void_p
+        L.or_layer_rates.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.or_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+        L.or_free.argtypes = [ctypes.c_void_p]
+        L.or_apply_sym.restype = ctypes.c_uint64
+        L.or_apply_sym.argtypes = [ctypes.c_uint64, ctypes.c_int]
+        L.or_canonical.restype = ctypes.c_uint64
+        L.or_canonical.argtypes = [ctypes.c_uint64, ctypes.c_int]
+        L.or_move_all_dir_batch.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        L.or_canonical_batch.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p]
+        L.or_row_tables.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.or_expand.restype = ctypes.c_size_t
+        L.or_expand.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(_Spec), ctypes.c_int, ctypes.c_int,
+                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+        L.or_solve_layer.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                     ctypes.POINTER(_Spec), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+        _lib = L
+    return _lib
+
+
+class Spec:
+    """Holds the C spec struct and keeps its arrays alive."""
+
+    def __init__(self, masks, shifts, symm_mode):
+        self.masks = np.ascontiguousarray(np.asarray(list(masks), dtype=np.uint64))
+        self.shifts = np.ascontiguousarray(np.asarray(list(shifts), dtype=np.uint8))
+        self.c = _Spec(
+            self.masks.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+            len(self.masks),
+            self.shifts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+            len(self.shifts),
+            int(symm_mode),
+        )
+
+
+def move_all_dir(boards: np.ndarray) -> np.ndarray:
+    b = np.ascontiguousarray(boards, dtype=np.uint64)
+    out = np.zeros((len(b), 4), dtype=np.uint64)
+    lib().or_move_all_dir_batch(b.ctypes.data, len(b), out.ctypes.data)
+    return out
+
+
+def canonical(boards: np.ndarray, mode: int) -> np.ndarray:
+    b = np.ascontiguousarray(boards, dtype=np.uint64)
+    out = np.zeros(len(b), dtype=np.uint64)
+    lib().or_canonical_batch(b.ctypes.data, len(b), int(mode), out.ctypes.data)
+    return out
+
+
+def apply_sym(board: int, idx: int) -> int:
+    return int(lib().or_apply_sym(int(board), int(idx)))
+
+
+def row_tables():
+    left = np.zeros(65536, dtype=np.uint16)
+    right = np.zeros(65536, dtype=np.uint16)
+    lib().or_row_tables(left.ctypes.data, right.ctypes.data)
+    return left, right
+
+
+def expand(parents: np.ndarray, spec: Spec, target: int, do_check: bool):
+    p = np.ascontiguousarray(parents, dtype=np.uint64)
+    cap = len(p) * 64 + 16
+    o1 = np.zeros(cap, dtype=np.uint64)
+    o2 = np.zeros(cap, dtype=np.uint64)
+    n2 = ctypes.c_size_t(0)
+    n1 = lib().or_expand(p.ctypes.data, len(p), ctypes.byref(spec.c), int(target), int(bool(do_check)),
+                         o1.ctypes.data, o2.ctypes.data, cap, ctypes.byref(n2))
+    return o1[:n1], o2[: n2.value]
+
+
+def solve_layer(keys0, k1, r1, k2, r2, spec: Spec, target: int, do_check: bool, dtype: str, p4: float):
+    d = DTYPES[dtype]
+    keys0 = np.ascontiguousarray(keys0, dtype=np.uint64)
+    k1 = np.ascontiguousarray(k1, dtype=np.uint64)
+    k2 = np.ascontiguousarray(k2, dtype=np.uint64)
+    r1 = np.ascontiguousarray(r1, dtype=NP_DTYPES[d])
+    r2 = np.ascontiguousarray(r2, dtype=NP_DTYPES[d])
+    out = np.zeros(len(keys0), dtype=NP_DTYPES[d])
+    lib().or_solve_layer(keys0.ctypes.data, len(keys0), out.ctypes.data, k1.ctypes.data, r1.ctypes.data, len(k1),
+                         k2.ctypes.data, r2.ctypes.data, len(k2), ctypes.byref(spec.c), int(target),
+                         int(bool(do_check)), d, float(p4))
+    return out
+
+
+class Build:
+    """A full forward + backward build held in host memory."""
+
+    def __init__(self, seeds, spec: Spec, target: int, steps: int, docheck: int):
+        s = np.ascontiguousarray(seeds, dtype=np.uint64)
+        self.spec = spec
+        self.h = lib().or_generate(s.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), len(s), ctypes.byref(spec.c),
+                                   int(target), int(steps), int(docheck))
+        self.steps = steps
+        self.dtype = None
+
+    def layer(self, t: int) -> np.ndarray:
+        n = lib().or_layer_len(self.h, t)
+        p = lib().or_layer_keys(self.h, t)
+        if n == 0:
+            return np.zeros(0, dtype=np.uint64)
+        return np.ctypeslib.as_array((ctypes.c_uint64 * n).from_address(p)).copy()
+
+    def solve(self, dtype: str = "float32", p4: float = 0.1) -> None:
+        self.dtype = DTYPES[dtype]
+        lib().or_solve(self.h, self.dtype, float(p4))
+
+    def rates(self, t: int) -> np.ndarray:
+        n = lib().or_layer_len(self.h, t)
+        dt = NP_DTYPES[self.dtype]
+        if n == 0:
+            return np.zeros(0, dtype=dt)
+        p = lib().or_layer_rates(self.h, t)
+        return np.frombuffer((ctypes.c_char * (n * np.dtype(dt).itemsize)).from_address(p), dtype=dt).copy()
+
+    def book(self, t: int, dtype: str) -> bytes:
+        """The .book bytes of layer t: packed {u64 board; T rate}, rate > zero only
+        (compact_live_entries + write_layer_file, native_core/src/BookSolver.cpp:380-394,206-231)."""
+        keys, rates = self.layer(t), self.rates(t)
+        zero = -1.0 if dtype.startswith("1-") else 0.0
+        live = rates > zero
+        rec = np.zeros(int(live.sum()), dtype=[("board", "<u8"), ("rate", rates.dtype)])
+        rec["board"] = keys[live]
+        rec["rate"] = rates[live]
+        return rec.tobytes()
+
+    def __del__(self):
+        try:
+            lib().or_free(self.h)
+        except Exception:
+            pass

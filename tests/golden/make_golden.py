@@ -1,0 +1,259 @@
+"""Generate the golden fixtures in tests/golden/ by running the REFERENCE's own
+classic-path code (compiled from its sources by `make -C oracle ref`).
+
+The reference ships no golden vectors, known-answer tests or fixtures, so the
+fixtures are outputs of the reference itself, run in this container:
+
+  cases.json   per build case: the PatternSpec/RunOptions inputs, every raw
+               layer's length and SHA-256 (run_pattern_generate writes them) and
+               every .book file's SHA-256 (run_pattern_build writes them)
+  prims.npz    board primitives on seeded random boards: move_all_dir,
+               canonical_by_mode for modes 0-3, apply_sym_like 0-7, row tables
+  reader.json  ClassicBookReader.move_on_dic answers on positions sampled from
+               the books of the small cases
+  free5_32.npz one complete small build (raw layers and books) as data
+
+Usage:  python tests/golden/make_golden.py            # small cases
+        python tests/golden/make_golden.py --full     # + full-size L3-256, 442-512
+Reads the reference's pattern catalog from /root/reference (this container
+only); the fixtures carry every input, so nothing reads /root/reference later.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import reference as R  # noqa: E402
+
+GOLDEN = os.path.dirname(os.path.abspath(__file__))
+REF_CATALOG = "/root/reference/docs_and_configs/patterns_config.json"
+WORK = os.environ.get("GOLDEN_WORK", "/dev/shm/egtb_golden")
+
+
+def _cellmask(free):
+    m = 0
+    for r in range(4):
+        for c in range(4):
+            if (r, c) not in free:
+                m |= 0xF << (4 * ((3 - r) * 4 + (3 - c)))
+    return m
+
+
+def _board(tiles, base):
+    b = base
+    for (r, c), v in tiles.items():
+        b |= v << (4 * ((3 - r) * 4 + (3 - c)))
+    return b
+
+
+def custom_patterns() -> dict:
+    """Small patterns, in the reference's catalog format, that cover the
+    symmetry modes the reference's small catalog entries do not reach quickly."""
+    pats = {}
+    d9 = [(r, c) for r in range(3) for c in range(3)]
+    m = _cellmask(d9)
+    pats["diag9"] = {"valid pattern": [hex(m)], "target pos": hex(0xFFFFFFFFFFFFFFFF & ~m),
+                     "canonical mode": "diagonal",
+                     "seed boards": [hex(_board({(0, 0): 1, (0, 1): 2}, m)), hex(_board({(0, 0): 2, (1, 1): 1}, m))],
+                     "extra steps": 24}
+    h8 = [(r, c) for r in range(2) for c in range(4)]
+    m = _cellmask(h8)
+    pats["horiz8"] = {"valid pattern": [hex(m)], "target pos": hex(0xFFFFFFFFFFFFFFFF & ~m),
+                      "canonical mode": "horizontal",
+                      "seed boards": [hex(_board({(1, 0): 1, (1, 1): 2}, m)), hex(_board({(1, 3): 2, (0, 3): 1}, m))],
+                      "extra steps": 48}
+    cells = [(r, c) for r in range(4) for c in range(4)]
+    for n_free in (5, 6):
+        fb = 0
+        for (r, c) in cells[n_free:]:
+            fb |= 0xF << (4 * ((3 - r) * 4 + (3 - c)))
+        pats[f"free{n_free}"] = {"valid pattern": [], "target pos": "0xffffffffffffffff", "canonical mode": "full",
+                                 "seed boards": [hex(fb | (1 << 60) | (2 << 56))], "extra steps": 16}
+    return pats
+
+
+SMALL_CASES = [
+    ("44", 6, "float32"), ("44", 7, "uint32"),
+    ("L3", 5, "float32"), ("L3", 5, "uint32"), ("L3", 5, "uint64"), ("L3", 5, "float64"),
+    ("L3", 5, "1-float32"), ("L3", 5, "1-float64"),
+    ("442", 6, "float32"), ("diag9", 6, "float32"), ("horiz8", 6, "float32"),
+    ("free5", 5, "float32"), ("free6", 5, "float32"), ("LL", 5, "float32"), ("t", 6, "uint32"),
+]
+FULL_CASES = [("L3", 8, "float32"), ("442", 9, "float32")]
+
+
+def sha(path: str) -> str:
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        for chunk in iter(lambda: f.read(1 << 24), b""):
+            h.update(chunk)
+    return h.hexdigest()
+
+
+def run_case(catalog, pat, target, dtype):
+    masks, shifts, symm, seeds, steps, docheck, s0 = R.pattern_params(catalog[pat], target)
+    T = 2 ** target
+    name = f"{pat}_{T}"
+    gdir = R.fresh_dir(os.path.join(WORK, f"{name}_{dtype}", "gen") + "/")
+    bdir = R.fresh_dir(os.path.join(WORK, f"{name}_{dtype}", "build") + "/")
+    spec, o = R.make_spec_options(masks, shifts, symm, target, steps, docheck, gdir + name + "_", dtype)
+    started, last0, last1 = R.run_generate(seeds, spec, o)
+    raw_len, raw_sha = [], []
+    for t in range(steps - 2):
+        p = gdir + f"{name}_{t}"
+        raw_len.append(os.path.getsize(p) // 8)
+        raw_sha.append(sha(p))
+    spec, o = R.make_spec_options(masks, shifts, symm, target, steps, docheck, bdir + name + "_", dtype)
+    R.run_build(seeds, spec, o)
+    book_len, book_sha = [], []
+    rec = 12 if dtype in ("uint32", "float32", "1-float32") else 16
+    for t in range(steps):
+        p = bdir + f"{name}_{t}.book"
+        book_len.append(os.path.getsize(p) // rec)
+        book_sha.append(sha(p))
+    case = {
+        "pattern": pat, "target": target, "dtype": dtype, "spawn_rate4": 0.1,
+        "masks": [hex(m) for m in masks], "shifts": shifts, "symm_mode": symm,
+        "seeds": [hex(int(s)) for s in seeds], "steps": steps, "docheck_step": docheck,
+        "tile_sum0": s0, "pattern_full": name,
+        "raw_len": raw_len, "raw_sha256": raw_sha,
+        "partial_len": [int(last0.size), int(last1.size)],
+        "book_len": book_len, "book_sha256": book_sha,
+    }
+    return case, bdir
+
+
+def prims_fixture():
+    L = ctypes.CDLL(os.path.join(R.REF_DIR, "libref_prims.so"))
+    rng = np.random.default_rng(2048)
+    n = 20000
+    # random boards with small tiles, a share of 0xF cells and empty cells
+    cells = rng.integers(0, 16, size=(n, 16))
+    cells = np.where(rng.random((n, 16)) < 0.35, 0, cells)
+    boards = np.zeros(n, dtype=np.uint64)
+    for k in range(16):
+        boards |= cells[:, k].astype(np.uint64) << np.uint64(4 * k)
+    out = {"boards": boards}
+    mv = np.zeros(n * 4, dtype=np.uint64)
+    L.ref_move_all_dir_batch(boards.ctypes.data, ctypes.c_size_t(n), mv.ctypes.data)
+    out["moves"] = mv.reshape(n, 4)
+    for mode in range(4):
+        c = np.zeros(n, dtype=np.uint64)
+        L.ref_canonical_batch(boards.ctypes.data, ctypes.c_size_t(n), mode, c.ctypes.data)
+        out[f"canonical_{mode}"] = c
+    for idx in range(8):
+        c = np.zeros(n, dtype=np.uint64)
+        L.ref_apply_sym_batch(boards.ctypes.data, ctypes.c_size_t(n), idx, c.ctypes.data)
+        out[f"sym_{idx}"] = c
+    left = np.zeros(65536, dtype=np.uint16)
+    right = np.zeros(65536, dtype=np.uint16)
+    L.ref_row_tables(left.ctypes.data, right.ctypes.data)
+    out["row_left"] = left
+    out["row_right"] = right
+    np.savez_compressed(os.path.join(GOLDEN, "prims.npz"), **out)
+
+
+def decode(board: int):
+    return [[(1 << v) if (v := (board >> (4 * ((3 - r) * 4 + (3 - c)))) & 0xF) else 0 for c in range(4)]
+            for r in range(4)]
+
+
+def reader_fixture(case, bdir, rng, n_pos=60):
+    """move_on_dic answers for positions sampled like sample_classic_book_state
+    (native_core/src/ReaderRuntime.cpp:945-993): a book key plus one spawn, then
+    a random orientation; one in eight gets a random free-cell nibble changed."""
+    fc = R.module()
+    spec = fc.PatternSpec()
+    spec.name = case["pattern"]
+    spec.pattern_masks = [int(m, 16) for m in case["masks"]]
+    spec.success_shifts = case["shifts"]
+    spec.symm_mode = case["symm_mode"]
+    reader = fc.ClassicBookReader(spec, False)
+    rec = 12 if case["dtype"] in ("uint32", "float32", "1-float32") else 16
+    path_list = [(bdir, case["dtype"])]
+    out = []
+    nonempty = [t for t, n in enumerate(case["book_len"]) if n > 0]
+    if not nonempty:
+        return out
+    for _ in range(n_pos):
+        t = int(rng.choice(nonempty))
+        data = np.fromfile(bdir + f"{case['pattern_full']}_{t}.book", dtype=np.uint8)
+        recs = data.reshape(-1, rec)
+        key = int(recs[int(rng.integers(len(recs)))][:8].view(np.uint64)[0])
+        empties = [i for i in range(16) if (key >> (4 * i)) & 0xF == 0]
+        if not empties:
+            continue
+        i = int(rng.choice(empties))
+        v = 2 if rng.random() < 0.1 else 1
+        pos = key | (v << (4 * i))
+        if rng.random() < 0.125:
+            j = int(rng.integers(16))
+            if (pos >> (4 * j)) & 0xF != 0xF:
+                pos = (pos & ~(0xF << (4 * j))) | (int(rng.integers(0, 6)) << (4 * j))
+        op = int(rng.integers(8))
+        board = decode(pos)
+        b = np.array(board)
+        if op in (1, 5):
+            b = np.rot90(b, 1)
+        elif op in (2, 6):
+            b = np.rot90(b, 2)
+        elif op in (3, 7):
+            b = np.rot90(b, 3)
+        if op >= 4:
+            b = b[:, ::-1]
+        board = b.tolist()
+        res, dt = reader.move_on_dic(board, path_list, case["pattern_full"], -case["tile_sum0"])
+        out.append({"board": board, "result": [[k, v] for k, v in res.items()], "dtype": dt})
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--full", action="store_true", help="also the full-size L3-256 and 442-512 builds")
+    ap.add_argument("--only", default="", help="comma-separated case keys to (re)generate")
+    args = ap.parse_args()
+    R.build()
+    catalog = json.load(open(REF_CATALOG))
+    catalog.update(custom_patterns())
+    prims_fixture()
+    cases_path = os.path.join(GOLDEN, "cases.json")
+    cases = json.load(open(cases_path)) if os.path.exists(cases_path) else {}
+    reader = {}
+    rng = np.random.default_rng(7)
+    todo = SMALL_CASES + (FULL_CASES if args.full else [])
+    only = set(filter(None, args.only.split(",")))
+    for pat, target, dtype in todo:
+        key = f"{pat}_{2 ** target}_{dtype}"
+        if only and key not in only:
+            continue
+        print("case", key, flush=True)
+        case, bdir = run_case(catalog, pat, target, dtype)
+        case["size_class"] = "full" if (pat, target, dtype) in FULL_CASES else "small"
+        cases[key] = case
+        if case["size_class"] == "small" and pat in ("44", "L3", "diag9", "horiz8", "free6", "442"):
+            reader[key] = reader_fixture(case, bdir, rng)
+        if key == "free5_32_float32":
+            data = {}
+            for t in range(case["steps"]):
+                raw = bdir + f"free5_32_{t}.book"
+                data[f"book_{t}"] = np.fromfile(raw, dtype=np.uint8)
+            np.savez_compressed(os.path.join(GOLDEN, "free5_32.npz"), **data)
+    json.dump(cases, open(cases_path, "w"), indent=0)
+    if reader:
+        rpath = os.path.join(GOLDEN, "reader.json")
+        old = json.load(open(rpath)) if os.path.exists(rpath) else {}
+        old.update(reader)
+        json.dump(old, open(rpath, "w"))
+    print("wrote", cases_path)
+
+
+if __name__ == "__main__":
+    main()
