@@ -1,0 +1,156 @@
+"""ctypes binding of libegtb_gpu.so (the C ABI declared in include/egtb_gpu.h).
+
+The shared library is built in-tree by build_lib.py into _lib/. Loading fails
+loudly when it is missing: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libegtb_gpu.so")
+
+EGTB_OK = 0
+ERR_NAMES = {
+    -1: "EGTB_ERR_ARG",
+    -2: "EGTB_ERR_CUDA",
+    -3: "EGTB_ERR_NOMEM",
+    -4: "EGTB_ERR_IO",
+    -5: "EGTB_ERR_CAPACITY",
+    -6: "EGTB_ERR_TIMEOUT",
+    -7: "EGTB_ERR_UNSUPPORTED",
+}
+MAX_MASKS = 32
+MAX_PATH = 4096
+
+DTYPE_CODES = {"uint32": 0, "uint64": 1, "float32": 2, "float64": 3, "1-float32": 4, "1-float64": 5}
+
+
+class NativeError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+class PatternSpecC(ctypes.Structure):
+    _fields_ = [
+        ("name", ctypes.c_char * 64),
+        ("pattern_masks", ctypes.c_uint64 * MAX_MASKS),
+        ("n_masks", ctypes.c_int32),
+        ("success_shifts", ctypes.c_uint8 * 16),
+        ("n_shifts", ctypes.c_int32),
+        ("symm_mode", ctypes.c_int32),
+    ]
+
+
+class RunOptionsC(ctypes.Structure):
+    _fields_ = [
+        ("target", ctypes.c_int32),
+        ("steps", ctypes.c_int32),
+        ("docheck_step", ctypes.c_int32),
+        ("pathname", ctypes.c_char * MAX_PATH),
+        ("is_free", ctypes.c_int32),
+        ("is_variant", ctypes.c_int32),
+        ("spawn_rate4", ctypes.c_double),
+        ("success_rate_dtype", ctypes.c_int32),
+        ("deletion_threshold", ctypes.c_double),
+        ("compress", ctypes.c_int32),
+        ("compress_temp_files", ctypes.c_int32),
+        ("optimal_branch_only", ctypes.c_int32),
+        ("chunked_solve", ctypes.c_int32),
+        ("num_threads", ctypes.c_int32),
+        ("direct_io", ctypes.c_int32),
+        ("direct_io_queue_depth", ctypes.c_int32),
+        ("direct_io_chunk_mib", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+        ("write_files", ctypes.c_int32),
+    ]
+
+
+class BuildStatsC(ctypes.Structure):
+    _fields_ = [
+        ("raw_boards", ctypes.c_uint64),
+        ("book_entries", ctypes.c_uint64),
+        ("max_layer", ctypes.c_uint64),
+        ("candidates", ctypes.c_uint64),
+        ("lookups", ctypes.c_uint64),
+        ("layers", ctypes.c_int32),
+        ("retries", ctypes.c_int32),
+        ("forward_ms", ctypes.c_double),
+        ("backward_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+# every entry point of include/egtb_gpu.h with its ctypes signature
+_P = ctypes.c_void_p
+_SIGS = {
+    "egtb_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
+    "egtb_version": (ctypes.c_char_p, []),
+    "egtb_device_count": (ctypes.c_int, []),
+    "egtb_get_build_progress": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
+    "egtb_reset_build_progress": (ctypes.c_int, [ctypes.c_uint32]),
+    "egtb_build": (ctypes.c_int, [_P, ctypes.c_size_t, ctypes.POINTER(PatternSpecC), ctypes.POINTER(RunOptionsC),
+                                  ctypes.POINTER(BuildStatsC)]),
+    "egtb_generate": (ctypes.c_int, [_P, ctypes.c_size_t, ctypes.POINTER(PatternSpecC), ctypes.POINTER(RunOptionsC),
+                                     ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(BuildStatsC)]),
+    "egtb_solve": (ctypes.c_int, [_P, ctypes.c_size_t, _P, ctypes.c_size_t, ctypes.POINTER(PatternSpecC),
+                                  ctypes.POINTER(RunOptionsC), ctypes.POINTER(BuildStatsC)]),
+    "egtb_move_all_dir": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, _P]),
+    "egtb_canonical": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, ctypes.c_int32, _P]),
+    "egtb_apply_sym": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, ctypes.c_int32, _P]),
+    "egtb_book_open": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(PatternSpecC),
+                                      ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(_P)]),
+    "egtb_book_close": (ctypes.c_int, [_P]),
+    "egtb_book_load_all": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
+    "egtb_book_lookup": (ctypes.c_int, [_P, _P, ctypes.c_size_t, ctypes.c_int32, _P, _P, _P]),
+    "egtb_book_lookup_device": (ctypes.c_int, [_P, _P, ctypes.c_size_t, ctypes.c_int32, _P, _P, _P]),
+    "egtb_find_classic_value": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int32,
+                                               ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
+                                               ctypes.POINTER(ctypes.c_int32)]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded library; raises when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"libegtb_gpu.so is not built ({LIB_PATH}); run __graft_entry__.build() or "
+                "python 2048endgametablebase_b200/build_lib.py"
+            )
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols() -> list[str]:
+    return sorted(_SIGS)
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(4096)
+    lib().egtb_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int) -> None:
+    if rc != EGTB_OK:
+        raise NativeError(rc, f"{ERR_NAMES.get(rc, rc)}: {last_error()}")
+
+
+def device_count() -> int:
+    return int(lib().egtb_device_count())

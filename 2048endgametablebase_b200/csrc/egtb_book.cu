@@ -1,0 +1,593 @@
+// Book lookup of libegtb_gpu: books of a table held in device memory as
+// sorted keys + rates (+ one splitter per 16 keys) and a batched kernel that
+// answers move_on_dic for many positions at once (the reader side of the
+// reference, native_core/src/ReaderRuntime.cpp:739-840 and 1050-1133).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "egtb_host.h"
+#include "egtb_device.cuh"
+
+namespace egtb {
+
+struct BookLayer {
+    uint64_t *keys = nullptr;
+    void *rates = nullptr;
+    uint64_t *split = nullptr;
+    unsigned long long n = 0;
+    int state = 0;  // 0 not looked at, 1 loaded, 2 file missing
+    int sorted = 1;
+};
+
+// Layer descriptor read by the lookup kernel.
+struct LayerDesc {
+    const uint64_t *keys;
+    const void *rates;
+    const uint64_t *split;
+    unsigned long long n;
+    int exists;
+    int sorted;
+};
+
+}  // namespace egtb
+
+struct egtb_book {
+    std::string dir, pattern_full;
+    int dtype = 0;
+    int device = 0;
+    long long nums_adjust = 0;
+    egtb::DevSpec spec;
+    std::vector<egtb::BookLayer> layers;
+    egtb::LayerDesc *d_desc = nullptr;
+    int d_desc_cap = 0;
+    bool desc_dirty = true;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    // scratch for host-buffer lookups
+    uint64_t *d_pos = nullptr;
+    double *d_val = nullptr;
+    uint8_t *d_valid = nullptr;
+    int8_t *d_op = nullptr;
+    size_t scratch_cap = 0;
+};
+
+namespace egtb {
+
+static std::string layer_path(const egtb_book &b, long long nums) {
+    return b.dir + "/" + b.pattern_full + "_" + std::to_string(nums) + ".book";
+}
+
+template <typename T>
+__global__ void split_records_kernel(const unsigned char *__restrict__ recs, unsigned long long n,
+                                     uint64_t *__restrict__ keys, T *__restrict__ rates, uint64_t *__restrict__ split,
+                                     int *__restrict__ unsorted) {
+    constexpr int rec = 8 + (int)sizeof(T);
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(recs + i * rec);
+        const uint64_t k = (uint64_t)w[0] | ((uint64_t)w[1] << 32);
+        keys[i] = k;
+        T r;
+        memcpy(&r, recs + i * rec + 8, sizeof(T));
+        rates[i] = r;
+        if ((i % kSplitStride) == 0) split[i / kSplitStride] = k;
+        if (i > 0) {
+            const uint32_t *q = reinterpret_cast<const uint32_t *>(recs + (i - 1) * rec);
+            const uint64_t kp = (uint64_t)q[0] | ((uint64_t)q[1] << 32);
+            if (kp >= k) *unsorted = 1;
+        }
+    }
+}
+
+// Load layer `nums` from its .book file (state 2 when the file is missing).
+static void load_layer(egtb_book &b, long long nums) {
+    if (nums < 0) return;
+    if ((long long)b.layers.size() <= nums) b.layers.resize(nums + 1);
+    BookLayer &L = b.layers[nums];
+    const std::string path = layer_path(b, nums);
+    if (L.state == 1) return;
+    if (!file_exists(path)) {
+        L.state = 2;
+        b.desc_dirty = true;
+        return;
+    }
+    const size_t rec = record_size(b.dtype);
+    std::vector<unsigned char> host = read_file(path);
+    const unsigned long long n = host.size() / rec;
+    L.n = n;
+    const size_t es = dtype_size(b.dtype);
+    EGTB_CUDA(cudaMalloc(&L.keys, std::max<size_t>(n, 1) * 8));
+    EGTB_CUDA(cudaMalloc(&L.rates, std::max<size_t>(n, 1) * es));
+    EGTB_CUDA(cudaMalloc(&L.split, (n / kSplitStride + 1) * 8));
+    if (n) {
+        unsigned char *d = nullptr;
+        int *d_flag = nullptr;
+        EGTB_CUDA(cudaMalloc(&d, n * rec));
+        EGTB_CUDA(cudaMalloc(&d_flag, sizeof(int)));
+        EGTB_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(int), b.stream));
+        EGTB_CUDA(cudaMemcpyAsync(d, host.data(), n * rec, cudaMemcpyHostToDevice, b.stream));
+        const int grid = 592;
+        if (es == 4) {
+            if (b.dtype == EGTB_DTYPE_UINT32)
+                split_records_kernel<uint32_t><<<grid, 256, 0, b.stream>>>(d, n, L.keys, (uint32_t *)L.rates, L.split, d_flag);
+            else
+                split_records_kernel<float><<<grid, 256, 0, b.stream>>>(d, n, L.keys, (float *)L.rates, L.split, d_flag);
+        } else {
+            if (b.dtype == EGTB_DTYPE_UINT64)
+                split_records_kernel<uint64_t><<<grid, 256, 0, b.stream>>>(d, n, L.keys, (uint64_t *)L.rates, L.split, d_flag);
+            else
+                split_records_kernel<double><<<grid, 256, 0, b.stream>>>(d, n, L.keys, (double *)L.rates, L.split, d_flag);
+        }
+        int unsorted = 0;
+        EGTB_CUDA(cudaMemcpyAsync(&unsorted, d_flag, sizeof(int), cudaMemcpyDeviceToHost, b.stream));
+        EGTB_CUDA(cudaStreamSynchronize(b.stream));
+        EGTB_CUDA(cudaGetLastError());
+        cudaFree(d);
+        cudaFree(d_flag);
+        L.sorted = unsorted ? 0 : 1;
+    }
+    L.state = 1;
+    b.desc_dirty = true;
+}
+
+static void upload_desc(egtb_book &b) {
+    if (!b.desc_dirty) return;
+    const int n = (int)b.layers.size();
+    if (n > b.d_desc_cap) {
+        if (b.d_desc) cudaFree(b.d_desc);
+        b.d_desc_cap = std::max(n, 64);
+        EGTB_CUDA(cudaMalloc(&b.d_desc, sizeof(LayerDesc) * b.d_desc_cap));
+    }
+    std::vector<LayerDesc> h(std::max(n, 1));
+    for (int i = 0; i < n; ++i) {
+        const BookLayer &L = b.layers[i];
+        h[i] = {L.keys, L.rates, L.split, L.n, L.state == 1 ? 1 : 0, L.sorted};
+    }
+    if (n) EGTB_CUDA(cudaMemcpyAsync(b.d_desc, h.data(), sizeof(LayerDesc) * n, cudaMemcpyHostToDevice, b.stream));
+    EGTB_CUDA(cudaStreamSynchronize(b.stream));
+    b.desc_dirty = false;
+}
+
+__device__ __forceinline__ long long tile_sum(uint64_t b) {
+    long long s = 0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const int v = (int)((b >> (4 * k)) & 0xF);
+        s += v ? (1ll << v) : 0ll;
+    }
+    return s;
+}
+
+// find_success_entry_in_file's probe sequence (ReaderRuntime.cpp:279-316),
+// used for layers whose file is not in ascending order (a table's layer 0
+// holds the seeds as given).
+template <typename T>
+__device__ __forceinline__ bool probe_unsorted(const uint64_t *keys, const T *rates, unsigned long long n, uint64_t key,
+                                               T &out) {
+    if (n == 0) return false;
+    unsigned long long left = 0, right = n - 1;
+    while (left <= right) {
+        const unsigned long long mid = (left + right) / 2;
+        const uint64_t k = keys[mid];
+        if (k == key) {
+            out = rates[mid];
+            return true;
+        }
+        if (k < key) {
+            left = mid + 1;
+        } else {
+            if (mid == 0) break;
+            right = mid - 1;
+        }
+    }
+    return false;
+}
+
+// normalize_raw_value + maybe_round_value (ReaderRuntime.cpp:208-214,271-277):
+// integer kinds divide by their scale; names containing "32" are rounded to
+// 9 decimals above 1e-7. The reference's -Ofast build turns the division by
+// 10^9 into a multiplication by its reciprocal, reproduced here.
+template <typename T>
+__device__ __forceinline__ double present(T raw, double scale, int round9) {
+    double v = (double)raw;
+    if (scale > 1.0) v = v / scale;
+    if (round9 && fabs(v) > 1e-7) v = round(v * 1e9) * 1e-9;
+    return v;
+}
+
+// Operation index -> symmetry applied to the board (apply_operation,
+// ReaderRuntime.cpp:127-147, as cell maps).
+__device__ __constant__ int kOpSym[8] = {0, 6, 5, 7, 1, 4, 2, 3};
+
+// adjust_direction (ReaderRuntime.cpp:149-169) for the move index m of the
+// transformed board (0 left, 1 right, 2 up, 3 down); returns the slot in the
+// order up, right, down, left.
+__device__ __forceinline__ int adjusted_slot(int op, int m) {
+    // name of move m: left=3, right=1, up=0, down=2 in {up,right,down,left}
+    int idx = (m == 0) ? 3 : (m == 1) ? 1 : (m == 2) ? 0 : 2;
+    if (op >= 4) {
+        if (idx == 3) idx = 1;
+        else if (idx == 1) idx = 3;
+    }
+    return (idx + (op & 3)) & 3;
+}
+
+template <typename T, typename OutT>
+__global__ void __launch_bounds__(256)
+lookup_kernel(const LayerDesc *__restrict__ desc, int n_desc, const uint64_t *__restrict__ pos, size_t n,
+              long long nums_adjust, DevSpec spec, const uint32_t *__restrict__ tab, int op_mode, double scale,
+              int round9, T zero, OutT *__restrict__ values4, uint8_t *__restrict__ valid, int8_t *__restrict__ op_used) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint64_t board = pos[i];
+        OutT out[4] = {0, 0, 0, 0};
+        uint8_t mask = 0;
+        int used = -1;
+        const long long nums = (tile_sum(board) + nums_adjust) / 2;  // C division, ReaderRuntime.cpp:749
+        if (nums < 0) {
+            used = -2;
+        } else if (nums >= n_desc || !desc[nums].exists) {
+            used = -3;
+        } else {
+            const LayerDesc L = desc[nums];
+            const T *rates = (const T *)L.rates;
+            // [last_op, 0..7] (operation_sequence, ReaderRuntime.cpp:171-182), or one op
+            const int single = op_mode >= 8 ? op_mode - 8 : -1;
+            const int count = single >= 0 ? 1 : 9;
+            for (int j = 0; j < count && used < 0; ++j) {
+                const int op = single >= 0 ? single : (j == 0 ? op_mode : j - 1);
+                const uint64_t tb = apply_sym(board, kOpSym[op]);
+                if (!is_pattern(tb, spec)) continue;
+                uint64_t mv[4];
+                move_all_dir(tab, tb, mv);
+                uint8_t m = 0;
+                OutT vals[4] = {0, 0, 0, 0};
+#pragma unroll
+                for (int d = 0; d < 4; ++d) {
+                    if (mv[d] == tb || !is_pattern(mv[d], spec)) continue;
+                    const uint64_t key = canonical(mv[d], spec.symm);
+                    T r = zero;
+                    if (L.sorted) {
+                        r = layer_lookup<T>(L.keys, rates, L.n, L.split, key, zero);
+                    } else {
+                        T got;
+                        if (probe_unsorted<T>(L.keys, rates, L.n, key, got)) r = got;
+                    }
+                    const int slot = adjusted_slot(op, d);
+                    vals[slot] = (OutT)present<T>(r, scale, round9);
+                    m |= (uint8_t)(1u << slot);
+                }
+                if (m) {
+                    used = op;
+                    mask = m;
+#pragma unroll
+                    for (int d = 0; d < 4; ++d) out[d] = vals[d];
+                }
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < 4; ++d) values4[4 * i + d] = out[d];
+        valid[i] = mask;
+        if (op_used) op_used[i] = (int8_t)used;
+    }
+}
+
+static bool round9_for(int dtype) {
+    // names containing "32": uint32, float32, 1-float32
+    return dtype == EGTB_DTYPE_UINT32 || dtype == EGTB_DTYPE_FLOAT32 || dtype == EGTB_DTYPE_1_FLOAT32;
+}
+
+static double scale_for(int dtype) {
+    // dtype_info_for_name max_scale (ReaderRuntime.cpp:186-206); only > 1 divides
+    if (dtype == EGTB_DTYPE_UINT32) return 4e9;
+    if (dtype == EGTB_DTYPE_UINT64) return 1.6e18;
+    return dtype_is_one_minus(dtype) ? 0.0 : 1.0;
+}
+
+template <typename OutT>
+static void launch_lookup(egtb_book &b, const uint64_t *d_pos, size_t n, int op_mode, OutT *d_vals, uint8_t *d_valid,
+                          int8_t *d_op, cudaStream_t s) {
+    const uint32_t *tab = device_row_table();
+    const int grid = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
+    if (n == 0) return;
+    const double scale = scale_for(b.dtype);
+    const int r9 = round9_for(b.dtype) ? 1 : 0;
+    const int nd = (int)b.layers.size();
+    switch (b.dtype) {
+        case EGTB_DTYPE_UINT32:
+            lookup_kernel<uint32_t, OutT><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
+                                                               scale, r9, 0u, d_vals, d_valid, d_op);
+            break;
+        case EGTB_DTYPE_UINT64:
+            lookup_kernel<uint64_t, OutT><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
+                                                               scale, r9, 0ull, d_vals, d_valid, d_op);
+            break;
+        case EGTB_DTYPE_FLOAT32: case EGTB_DTYPE_1_FLOAT32:
+            lookup_kernel<float, OutT><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
+                                                            scale, r9, (float)dtype_zero(b.dtype), d_vals, d_valid, d_op);
+            break;
+        default:
+            lookup_kernel<double, OutT><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
+                                                             scale, r9, dtype_zero(b.dtype), d_vals, d_valid, d_op);
+            break;
+    }
+    EGTB_CUDA(cudaGetLastError());
+}
+
+static long long host_tile_sum(uint64_t b) {
+    long long s = 0;
+    for (int k = 0; k < 16; ++k) {
+        const int v = (int)((b >> (4 * k)) & 0xF);
+        s += v ? (1ll << v) : 0ll;
+    }
+    return s;
+}
+
+// ----------------------------------------------- single-file value cache --
+
+struct FileBook {
+    std::string path;
+    uint64_t size = 0;
+    int dtype = 0;
+    BookLayer layer;
+};
+
+static std::mutex g_fb_mu;
+static std::vector<std::unique_ptr<FileBook>> g_fb;  // small LRU by path
+
+template <typename T>
+__global__ void find_one_kernel(const uint64_t *keys, const T *rates, unsigned long long n, int sorted, uint64_t key,
+                                double scale, T zero, double *out) {
+    // find_success_entry_in_file (ReaderRuntime.cpp:279-316): a hit gives the
+    // normalised value, a miss the dtype's zero value as it is
+    bool hit = false;
+    T r = zero;
+    if (sorted) {
+        unsigned long long lo = 0, len = n;
+        while (len > 0) {
+            const unsigned long long half = len >> 1;
+            if (keys[lo + half] < key) {
+                lo += half + 1;
+                len -= half + 1;
+            } else {
+                len = half;
+            }
+        }
+        hit = lo < n && keys[lo] == key;
+        if (hit) r = rates[lo];
+    } else {
+        hit = probe_unsorted<T>(keys, rates, n, key, r);
+    }
+    double v = (double)r;
+    if (hit && scale > 1.0) v = v / scale;
+    *out = hit ? v : (double)zero;
+}
+
+}  // namespace egtb
+
+using namespace egtb;
+
+extern "C" int egtb_book_open(const char *dir, const char *pattern_full, int32_t dtype, const egtb_pattern_spec *spec,
+                              int64_t nums_adjust, int32_t device, egtb_book **out) {
+    return guarded([&] {
+        if (!dir || !pattern_full || !spec || !out) throw Error(EGTB_ERR_ARG, "NULL argument");
+        dtype_size(dtype);
+        int n = 0;
+        EGTB_CUDA(cudaGetDeviceCount(&n));
+        if (device < 0 || device >= n) throw Error(EGTB_ERR_ARG, "device not present");
+        EGTB_CUDA(cudaSetDevice(device));
+        auto b = std::make_unique<egtb_book>();
+        b->dir = dir;
+        while (b->dir.size() > 1 && b->dir.back() == '/') b->dir.pop_back();
+        b->pattern_full = pattern_full;
+        b->dtype = dtype;
+        b->device = device;
+        b->nums_adjust = nums_adjust;
+        b->spec = make_dev_spec(*spec, 0);
+        EGTB_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        *out = b.release();
+    });
+}
+
+extern "C" int egtb_book_close(egtb_book *b) {
+    return guarded([&] {
+        if (!b) return;
+        cudaSetDevice(b->device);
+        cudaStreamSynchronize(b->stream);
+        for (auto &L : b->layers) {
+            if (L.keys) cudaFree(L.keys);
+            if (L.rates) cudaFree(L.rates);
+            if (L.split) cudaFree(L.split);
+        }
+        if (b->d_desc) cudaFree(b->d_desc);
+        if (b->d_pos) cudaFree(b->d_pos);
+        if (b->d_val) cudaFree(b->d_val);
+        if (b->d_valid) cudaFree(b->d_valid);
+        if (b->d_op) cudaFree(b->d_op);
+        cudaStreamDestroy(b->stream);
+        delete b;
+    });
+}
+
+extern "C" int egtb_book_load_all(egtb_book *b, int32_t *layers_loaded) {
+    return guarded([&] {
+        if (!b) throw Error(EGTB_ERR_ARG, "NULL book");
+        std::lock_guard<std::mutex> lk(b->mu);
+        EGTB_CUDA(cudaSetDevice(b->device));
+        // scan layer files until a long run of missing indices
+        int loaded = 0, misses = 0;
+        for (long long nums = 0; misses < 64; ++nums) {
+            load_layer(*b, nums);
+            if (b->layers[nums].state == 1) {
+                ++loaded;
+                misses = 0;
+            } else {
+                ++misses;
+            }
+        }
+        upload_desc(*b);
+        if (layers_loaded) *layers_loaded = loaded;
+    });
+}
+
+extern "C" int egtb_book_lookup(egtb_book *b, const uint64_t *positions, size_t n, int32_t last_op, double *values4,
+                                uint8_t *valid_mask, int8_t *op_used) {
+    return guarded([&] {
+        if (!b) throw Error(EGTB_ERR_ARG, "NULL book");
+        if (n && (!positions || !values4 || !valid_mask)) throw Error(EGTB_ERR_ARG, "NULL buffer");
+        if (last_op < 0 || last_op > 15) throw Error(EGTB_ERR_ARG, "last_op out of range");
+        std::lock_guard<std::mutex> lk(b->mu);
+        EGTB_CUDA(cudaSetDevice(b->device));
+        // make sure every layer these positions read is loaded (or known missing);
+        // a missing file is looked for again on every call, as the reference does
+        std::vector<char> seen;
+        for (size_t i = 0; i < n; ++i) {
+            const long long nums = (host_tile_sum(positions[i]) + b->nums_adjust) / 2;
+            if (nums < 0) continue;
+            if ((long long)seen.size() <= nums) seen.resize(nums + 1, 0);
+            if (seen[nums]) continue;
+            seen[nums] = 1;
+            if ((long long)b->layers.size() > nums && b->layers[nums].state == 2) {
+                b->layers[nums].state = 0;
+                b->desc_dirty = true;
+            }
+            load_layer(*b, nums);
+        }
+        upload_desc(*b);
+        if (n == 0) return;
+        if (n > b->scratch_cap) {
+            if (b->d_pos) cudaFree(b->d_pos);
+            if (b->d_val) cudaFree(b->d_val);
+            if (b->d_valid) cudaFree(b->d_valid);
+            if (b->d_op) cudaFree(b->d_op);
+            b->scratch_cap = std::max<size_t>(n, 4096);
+            EGTB_CUDA(cudaMalloc(&b->d_pos, b->scratch_cap * 8));
+            EGTB_CUDA(cudaMalloc(&b->d_val, b->scratch_cap * 32));
+            EGTB_CUDA(cudaMalloc(&b->d_valid, b->scratch_cap));
+            EGTB_CUDA(cudaMalloc(&b->d_op, b->scratch_cap));
+        }
+        EGTB_CUDA(cudaMemcpyAsync(b->d_pos, positions, n * 8, cudaMemcpyHostToDevice, b->stream));
+        launch_lookup<double>(*b, b->d_pos, n, last_op, b->d_val, b->d_valid, b->d_op, b->stream);
+        EGTB_CUDA(cudaMemcpyAsync(values4, b->d_val, n * 32, cudaMemcpyDeviceToHost, b->stream));
+        EGTB_CUDA(cudaMemcpyAsync(valid_mask, b->d_valid, n, cudaMemcpyDeviceToHost, b->stream));
+        if (op_used) EGTB_CUDA(cudaMemcpyAsync(op_used, b->d_op, n, cudaMemcpyDeviceToHost, b->stream));
+        EGTB_CUDA(cudaStreamSynchronize(b->stream));
+    });
+}
+
+extern "C" int egtb_book_lookup_device(egtb_book *b, const uint64_t *d_positions, size_t n, int32_t last_op,
+                                       float *d_values4, uint8_t *d_valid_mask, void *stream) {
+    return guarded([&] {
+        if (!b) throw Error(EGTB_ERR_ARG, "NULL book");
+        if (last_op < 0 || last_op > 15) throw Error(EGTB_ERR_ARG, "last_op out of range");
+        if (b->desc_dirty) {
+            std::lock_guard<std::mutex> lk(b->mu);
+            upload_desc(*b);
+        }
+        if (!b->d_desc && n) throw Error(EGTB_ERR_ARG, "no layers loaded (egtb_book_load_all)");
+        launch_lookup<float>(*b, d_positions, n, last_op, d_values4, d_valid_mask, nullptr, (cudaStream_t)stream);
+    });
+}
+
+extern "C" int egtb_find_classic_value(const char *pathname, const char *filename, uint64_t key, int32_t dtype,
+                                       int32_t device, double *value, int32_t *found) {
+    return guarded([&] {
+        if (!pathname || !filename || !value || !found) throw Error(EGTB_ERR_ARG, "NULL argument");
+        dtype_size(dtype);
+        std::string path = std::string(pathname);
+        if (!path.empty() && path.back() != '/') path += "/";
+        path += filename;
+        *value = 0.0;
+        *found = 0;
+        if (!file_exists(path)) return;  // the file could not be opened: not found
+        int n = 0;
+        EGTB_CUDA(cudaGetDeviceCount(&n));
+        if (device < 0 || device >= n) throw Error(EGTB_ERR_ARG, "device not present");
+        EGTB_CUDA(cudaSetDevice(device));
+        std::lock_guard<std::mutex> lk(g_fb_mu);
+        FileBook *fb = nullptr;
+        const uint64_t sz = file_size(path);
+        for (auto &e : g_fb)
+            if (e->path == path && e->size == sz && e->dtype == dtype) fb = e.get();
+        if (!fb) {
+            if (g_fb.size() >= 8) {
+                auto &old = g_fb.front();
+                cudaFree(old->layer.keys);
+                cudaFree(old->layer.rates);
+                cudaFree(old->layer.split);
+                g_fb.erase(g_fb.begin());
+            }
+            auto e = std::make_unique<FileBook>();
+            e->path = path;
+            e->size = sz;
+            e->dtype = dtype;
+            cudaStream_t st = nullptr;
+            EGTB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            std::unique_ptr<CUstream_st, void (*)(cudaStream_t)> st_guard(st, [](cudaStream_t q) { cudaStreamDestroy(q); });
+            const size_t rec = record_size(dtype);
+            std::vector<unsigned char> host = read_file(path);
+            BookLayer &L = e->layer;
+            L.n = host.size() / rec;
+            const size_t es = dtype_size(dtype);
+            EGTB_CUDA(cudaMalloc(&L.keys, std::max<size_t>(L.n, 1) * 8));
+            EGTB_CUDA(cudaMalloc(&L.rates, std::max<size_t>(L.n, 1) * es));
+            EGTB_CUDA(cudaMalloc(&L.split, (L.n / kSplitStride + 1) * 8));
+            if (L.n) {
+                unsigned char *d = nullptr;
+                int *flag = nullptr;
+                EGTB_CUDA(cudaMalloc(&d, L.n * rec));
+                EGTB_CUDA(cudaMalloc(&flag, sizeof(int)));
+                EGTB_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));
+                EGTB_CUDA(cudaMemcpyAsync(d, host.data(), L.n * rec, cudaMemcpyHostToDevice, st));
+                if (dtype == EGTB_DTYPE_UINT32)
+                    split_records_kernel<uint32_t><<<592, 256, 0, st>>>(d, L.n, L.keys, (uint32_t *)L.rates, L.split, flag);
+                else if (dtype == EGTB_DTYPE_UINT64)
+                    split_records_kernel<uint64_t><<<592, 256, 0, st>>>(d, L.n, L.keys, (uint64_t *)L.rates, L.split, flag);
+                else if (es == 4)
+                    split_records_kernel<float><<<592, 256, 0, st>>>(d, L.n, L.keys, (float *)L.rates, L.split, flag);
+                else
+                    split_records_kernel<double><<<592, 256, 0, st>>>(d, L.n, L.keys, (double *)L.rates, L.split, flag);
+                int unsorted = 0;
+                EGTB_CUDA(cudaMemcpyAsync(&unsorted, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+                EGTB_CUDA(cudaStreamSynchronize(st));
+                cudaFree(d);
+                cudaFree(flag);
+                L.sorted = unsorted ? 0 : 1;
+            }
+            L.state = 1;
+            g_fb.push_back(std::move(e));
+            fb = g_fb.back().get();
+        }
+        double *d_out = nullptr;
+        EGTB_CUDA(cudaMalloc(&d_out, sizeof(double)));
+        const BookLayer &L = fb->layer;
+        const double scale = scale_for(dtype);
+        switch (dtype) {
+            case EGTB_DTYPE_UINT32:
+                find_one_kernel<uint32_t><<<1, 1>>>(L.keys, (const uint32_t *)L.rates, L.n, L.sorted, key, scale, 0u, d_out);
+                break;
+            case EGTB_DTYPE_UINT64:
+                find_one_kernel<uint64_t><<<1, 1>>>(L.keys, (const uint64_t *)L.rates, L.n, L.sorted, key, scale, 0ull, d_out);
+                break;
+            case EGTB_DTYPE_FLOAT32: case EGTB_DTYPE_1_FLOAT32:
+                find_one_kernel<float><<<1, 1>>>(L.keys, (const float *)L.rates, L.n, L.sorted, key, scale,
+                                                 (float)dtype_zero(dtype), d_out);
+                break;
+            default:
+                find_one_kernel<double><<<1, 1>>>(L.keys, (const double *)L.rates, L.n, L.sorted, key, scale,
+                                                  dtype_zero(dtype), d_out);
+                break;
+        }
+        EGTB_CUDA(cudaGetLastError());
+        EGTB_CUDA(cudaMemcpy(value, d_out, sizeof(double), cudaMemcpyDeviceToHost));
+        cudaFree(d_out);
+        *found = 1;
+    });
+}

@@ -1,0 +1,1120 @@
+// Build engine of libegtb_gpu: the forward layer generation and backward solve
+// of the classic tablebase path on one B200, behind the C ABI of
+// include/egtb_gpu.h (egtb_build / egtb_generate / egtb_solve / progress /
+// board primitives).
+//
+// Fused build (egtb_build with no layer files on disk): every raw layer stays
+// in one device arena (16-aligned offsets, splitter every 16 keys) for the
+// whole build. Forward step i expands layer i-1 into two candidate buffers
+// (spawn-2 children for layer i, spawn-4 children for layer i+1; a layer's
+// candidates always live in buffer layer&1), then radix-sorts and uniques
+// buffer i&1 into the arena as layer i. All sizes stay on the device, so the
+// host enqueues the whole forward without waiting; capacity overflows are
+// flagged by the kernels and the forward is re-run with larger buffers.
+// Backward solve runs layer by layer on the same arena, then every layer is
+// packed into .book records on the device and written by a thread pool.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "egtb_host.h"
+#include "egtb_kernels.cuh"
+
+namespace egtb {
+
+// ------------------------------------------------------------- progress ---
+
+static std::atomic<uint32_t> g_progress_total{0};
+static std::atomic<uint32_t> g_progress_host{0};
+static unsigned *g_progress_mapped = nullptr;      // host view (device-written)
+static unsigned *g_progress_mapped_dev = nullptr;  // device view
+static std::mutex g_progress_mu;
+
+static unsigned *progress_device_ptr() {
+    std::lock_guard<std::mutex> lk(g_progress_mu);
+    if (!g_progress_mapped) {
+        unsigned *h = nullptr;
+        if (cudaHostAlloc(&h, sizeof(unsigned), cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        *h = 0;
+        unsigned *d = nullptr;
+        if (cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFreeHost(h);
+            return nullptr;
+        }
+        g_progress_mapped = h;
+        g_progress_mapped_dev = d;
+    }
+    return g_progress_mapped_dev;
+}
+
+// update_build_progress, native_core/include/FormationRuntime.h:62-66
+static void set_progress(uint32_t cur, uint32_t total) {
+    g_progress_total.store(total, std::memory_order_relaxed);
+    g_progress_host.store(cur, std::memory_order_relaxed);
+    if (g_progress_mapped) *(volatile unsigned *)g_progress_mapped = cur;
+}
+
+static uint32_t read_progress() {
+    uint32_t cur = g_progress_host.load(std::memory_order_relaxed);
+    if (g_progress_mapped) {
+        const uint32_t d = *(volatile unsigned *)g_progress_mapped;
+        if (d > cur) cur = d;
+    }
+    return cur;
+}
+
+__global__ void progress_kernel(unsigned *p, unsigned v) {
+    if (p) *(volatile unsigned *)p = v;
+}
+
+// ---------------------------------------------------------------- engine ---
+
+static unsigned long long align16(unsigned long long x) { return (x + 15ull) & ~15ull; }
+
+struct Engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    const uint32_t *tab = nullptr;
+    std::mutex mu;
+
+    // capacities (elements)
+    unsigned long long arena_cap = 0, cand_cap = 0;
+    int steps_cap = 0;
+    int filter_bits = 22;
+
+    uint64_t *arena = nullptr;
+    void *rates = nullptr;
+    uint64_t *split = nullptr;
+    uint64_t *cand[2] = {nullptr, nullptr};
+    uint64_t *tmp = nullptr;
+    unsigned *tile_hist = nullptr;  // 256 x sort_tiles
+    unsigned *digit_tot = nullptr;  // 256 x 8
+    unsigned *tile_cnt = nullptr;
+    unsigned long long *tile_off = nullptr;
+    unsigned long long sort_tiles = 0, comp_tiles = 0;
+    uint64_t *filter = nullptr;
+    unsigned long long *layer_off = nullptr, *layer_len = nullptr, *book_len = nullptr;
+    unsigned long long *layer_max = nullptr;  // ordered encoding of the largest rate per layer
+    unsigned char *book = nullptr;
+    unsigned long long book_cap_bytes = 0;
+    DevCtl *ctl = nullptr;
+    cudaEvent_t ev[4];
+
+    // pinned host staging
+    unsigned char *pinned = nullptr;
+    size_t pinned_cap = 0;
+
+    int sm_count = 148;
+
+    void init(int dev) {
+        device = dev;
+        EGTB_CUDA(cudaSetDevice(dev));
+        EGTB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        tab = device_row_table();
+        cudaDeviceProp prop;
+        EGTB_CUDA(cudaGetDeviceProperties(&prop, dev));
+        sm_count = prop.multiProcessorCount;
+        EGTB_CUDA(cudaMalloc(&ctl, sizeof(DevCtl)));
+        for (auto &e : ev) EGTB_CUDA(cudaEventCreate(&e));
+        const char *fb = getenv("EGTB_FILTER_BITS");
+        if (fb) filter_bits = std::max(10, std::min(30, atoi(fb)));
+        EGTB_CUDA(cudaMalloc(&filter, sizeof(uint64_t) << filter_bits));
+        progress_device_ptr();
+    }
+
+    template <typename P>
+    static void release(P *&p) {
+        if (p) cudaFree((void *)p);
+        p = nullptr;
+    }
+
+    void alloc_or_throw(void **p, size_t bytes, const char *what) {
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            *p = nullptr;
+            throw Error(EGTB_ERR_CAPACITY, std::string("device allocation of ") + std::to_string(bytes >> 20) +
+                                               " MiB for " + what + " failed");
+        }
+    }
+
+    void ensure_steps(int steps) {
+        if (steps + 3 <= steps_cap) return;
+        release(layer_off);
+        release(layer_len);
+        release(book_len);
+        release(layer_max);
+        steps_cap = std::max(steps + 3, 1024);
+        alloc_or_throw((void **)&layer_off, sizeof(unsigned long long) * steps_cap, "layer offsets");
+        alloc_or_throw((void **)&layer_len, sizeof(unsigned long long) * steps_cap, "layer lengths");
+        alloc_or_throw((void **)&book_len, sizeof(unsigned long long) * steps_cap, "book lengths");
+        alloc_or_throw((void **)&layer_max, sizeof(unsigned long long) * steps_cap, "layer maxima");
+    }
+
+    void ensure_arena(unsigned long long cap) {
+        if (cap <= arena_cap) return;
+        release(arena);
+        release(rates);
+        release(split);
+        release(book);
+        arena_cap = align16(cap);
+        alloc_or_throw((void **)&arena, sizeof(uint64_t) * arena_cap, "layer arena");
+        alloc_or_throw(&rates, sizeof(uint64_t) * arena_cap, "rates");
+        alloc_or_throw((void **)&split, sizeof(uint64_t) * (arena_cap / kSplitStride + 1), "splitters");
+        book_cap_bytes = arena_cap * 16ull;
+        alloc_or_throw((void **)&book, book_cap_bytes, "books");
+        ensure_comp_tiles();
+    }
+
+    void ensure_cand(unsigned long long cap) {
+        if (cap <= cand_cap) return;
+        if (cap >= (1ull << 32)) throw Error(EGTB_ERR_CAPACITY, "candidate buffer above 2^32 keys");
+        release(cand[0]);
+        release(cand[1]);
+        release(tmp);
+        release(tile_hist);
+        release(digit_tot);
+        cand_cap = cap;
+        alloc_or_throw((void **)&cand[0], sizeof(uint64_t) * cand_cap, "candidates");
+        alloc_or_throw((void **)&cand[1], sizeof(uint64_t) * cand_cap, "candidates");
+        alloc_or_throw((void **)&tmp, sizeof(uint64_t) * cand_cap, "sort buffer");
+        sort_tiles = cand_cap / kTileKeys + 2;
+        alloc_or_throw((void **)&tile_hist, sizeof(unsigned) * 256 * sort_tiles, "sort histograms");
+        alloc_or_throw((void **)&digit_tot, sizeof(unsigned) * 256 * 8, "digit totals");
+        ensure_comp_tiles();
+    }
+
+    void ensure_comp_tiles() {
+        const unsigned long long need = std::max(arena_cap, cand_cap) / kTileKeys + 2;
+        if (need <= comp_tiles) return;
+        release(tile_cnt);
+        release(tile_off);
+        comp_tiles = need;
+        alloc_or_throw((void **)&tile_cnt, sizeof(unsigned) * comp_tiles, "tile counts");
+        alloc_or_throw((void **)&tile_off, sizeof(unsigned long long) * comp_tiles, "tile offsets");
+    }
+
+    unsigned char *ensure_pinned(size_t bytes) {
+        if (bytes <= pinned_cap) return pinned;
+        if (pinned) cudaFreeHost(pinned);
+        pinned = nullptr;
+        pinned_cap = 0;
+        size_t want = std::max<size_t>(bytes, 64ull << 20);
+        if (cudaHostAlloc((void **)&pinned, want, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            pinned = nullptr;
+            throw Error(EGTB_ERR_NOMEM, "pinned host allocation of " + std::to_string(want >> 20) + " MiB failed");
+        }
+        pinned_cap = want;
+        return pinned;
+    }
+
+    int grid_for(int threads_per_block, int blocks_per_sm) const { return sm_count * blocks_per_sm; }
+};
+
+static std::mutex g_engines_mu;
+static std::vector<std::unique_ptr<Engine>> g_engines;
+
+static Engine &engine_for(int device) {
+    int n = 0;
+    EGTB_CUDA(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) throw Error(EGTB_ERR_ARG, "device " + std::to_string(device) + " not present");
+    std::lock_guard<std::mutex> lk(g_engines_mu);
+    if ((int)g_engines.size() < n) g_engines.resize(n);
+    if (!g_engines[device]) {
+        EGTB_CUDA(cudaSetDevice(device));
+        auto e = std::make_unique<Engine>();
+        e->init(device);
+        g_engines[device] = std::move(e);
+    }
+    EGTB_CUDA(cudaSetDevice(device));
+    return *g_engines[device];
+}
+
+// Bytes of the sort key that can differ between candidates: a nibble pinned
+// to 0xF by every mask, and by every symmetry image of that intersection, is
+// 0xF in every canonical key.
+static std::vector<int> varying_byte_shifts(const egtb_pattern_spec &s) {
+    uint64_t pinned = 0;
+    if (s.n_masks > 0) {
+        pinned = ~0ull;
+        for (int i = 0; i < s.n_masks; ++i) pinned &= s.pattern_masks[i];
+        // keep only nibbles that are fully 0xF
+        uint64_t nib = 0;
+        for (int k = 0; k < 16; ++k)
+            if (((pinned >> (4 * k)) & 0xF) == 0xF) nib |= 0xFull << (4 * k);
+        pinned = nib;
+        auto sym = [](uint64_t b, int idx) {
+            uint64_t o = 0;
+            for (int r = 0; r < 4; ++r)
+                for (int c = 0; c < 4; ++c) {
+                    uint64_t v = (b >> (4 * ((3 - r) * 4 + (3 - c)))) & 0xF;
+                    int R = r, C = c;
+                    switch (idx) {
+                        case 1: C = 3 - c; break;
+                        case 2: R = 3 - r; break;
+                        case 3: R = c; C = r; break;
+                        case 4: R = 3 - c; C = 3 - r; break;
+                        case 5: R = 3 - r; C = 3 - c; break;
+                        case 6: R = 3 - c; C = r; break;
+                        case 7: R = c; C = 3 - r; break;
+                        default: break;
+                    }
+                    o |= v << (4 * ((3 - R) * 4 + (3 - C)));
+                }
+            return o;
+        };
+        uint64_t inter = pinned;
+        if (s.symm_mode == EGTB_SYMM_DIAGONAL) inter &= sym(pinned, 3);
+        if (s.symm_mode == EGTB_SYMM_HORIZONTAL) inter &= sym(pinned, 1);
+        if (s.symm_mode == EGTB_SYMM_FULL)
+            for (int g = 1; g < 8; ++g) inter &= sym(pinned, g);
+        pinned = inter;
+    }
+    std::vector<int> shifts;
+    for (int byte = 0; byte < 8; ++byte)
+        if (((pinned >> (8 * byte)) & 0xFF) != 0xFF) shifts.push_back(8 * byte);
+    return shifts;
+}
+
+// ------------------------------------------------------------ forward -----
+
+struct ForwardPlan {
+    int steps, docheck, first_step;  // first_step: generation starts at step i = first_step
+    DevSpec spec;
+    std::vector<int> shifts;
+};
+
+// Sort the candidates of buffer x and unique them into the arena as layer L.
+static void enqueue_sort_unique(Engine &E, const ForwardPlan &P, int x, int L) {
+    cudaStream_t s = E.stream;
+    unsigned long long *n_ptr = &E.ctl->cand_count[x];
+    const int g_sort = E.sm_count * 4;
+    EGTB_CUDA(cudaMemsetAsync(E.digit_tot, 0, sizeof(unsigned) * 256 * 8, s));
+    uint64_t *src = E.cand[x], *dst = E.tmp;
+    int p = 0;
+    for (int sh : P.shifts) {
+        unsigned *dt = E.digit_tot + 256 * p;
+        radix_count_kernel<<<g_sort, kSortThreads, 0, s>>>(src, n_ptr, E.cand_cap, sh, E.tile_hist, E.sort_tiles, dt);
+        radix_scan_kernel<<<256, 1024, 0, s>>>(n_ptr, E.cand_cap, E.tile_hist, E.sort_tiles, dt);
+        radix_scatter_kernel<<<g_sort, kSortThreads, 0, s>>>(src, dst, n_ptr, E.cand_cap, sh, E.tile_hist,
+                                                             E.sort_tiles, dt);
+        std::swap(src, dst);
+        ++p;
+    }
+    unique_count_kernel<<<g_sort, kSortThreads, 0, s>>>(src, n_ptr, E.cand_cap, E.tile_cnt);
+    tile_scan_kernel<<<1, 1024, 0, s>>>(n_ptr, E.cand_cap, E.tile_off, E.tile_cnt, &E.ctl->n_unique);
+    close_layer_kernel<<<1, 1, 0, s>>>(L, &E.ctl->n_unique, E.layer_off, E.layer_len, E.arena_cap, E.ctl);
+    unique_write_kernel<<<g_sort, kSortThreads, 0, s>>>(src, n_ptr, E.cand_cap, E.tile_off, E.arena, E.split,
+                                                         E.layer_off, L, E.arena_cap);
+}
+
+__global__ void add_candidates_kernel(DevCtl *ctl, int x) { ctl->candidates += ctl->cand_count[x]; }
+
+// Enqueue forward steps first_step .. steps-2 and the final partial layer.
+// Preconditions on the device: layer first_step-1 in the arena at
+// layer_off[first_step-1] (16-aligned) with layer_off[first_step] set after
+// it, cand_count[first_step&1] holding the partial of layer first_step.
+static void enqueue_forward(Engine &E, const ForwardPlan &P, unsigned *progress) {
+    cudaStream_t s = E.stream;
+    const int g_exp = E.sm_count * 8;
+    for (int i = P.first_step; i < P.steps - 1; ++i) {
+        const int t = i - 1;
+        const int x1 = i & 1, x2 = (i + 1) & 1;
+        EGTB_CUDA(cudaMemsetAsync(&E.ctl->cand_count[x2], 0, sizeof(unsigned long long), s));
+        expand_kernel<<<g_exp, kExpandThreads, 0, s>>>(E.arena, E.layer_off, E.layer_len, t, P.spec,
+                                                       i > P.docheck ? 1 : 0, E.tab, E.cand[x1], E.cand[x2], E.ctl,
+                                                       x1, x2, E.cand_cap, E.filter, E.filter_bits);
+        add_candidates_kernel<<<1, 1, 0, s>>>(E.ctl, x1);
+        enqueue_sort_unique(E, P, x1, i);
+        progress_kernel<<<1, 1, 0, s>>>(progress, (unsigned)i);
+    }
+    const int L = P.steps - 1;
+    add_candidates_kernel<<<1, 1, 0, s>>>(E.ctl, L & 1);
+    enqueue_sort_unique(E, P, L & 1, L);
+}
+
+static DevCtl read_ctl(Engine &E) {
+    DevCtl c;
+    EGTB_CUDA(cudaMemcpyAsync(&c, E.ctl, sizeof c, cudaMemcpyDeviceToHost, E.stream));
+    EGTB_CUDA(cudaStreamSynchronize(E.stream));
+    return c;
+}
+
+// Reset control state and place the starting layers.
+// start_layer = first_step-1 holds `base` keys; partial (layer first_step) holds `partial` keys.
+static void stage_start(Engine &E, const ForwardPlan &P, const uint64_t *base, size_t n_base, const uint64_t *partial,
+                        size_t n_partial) {
+    cudaStream_t s = E.stream;
+    EGTB_CUDA(cudaMemsetAsync(E.ctl, 0, sizeof(DevCtl), s));
+    EGTB_CUDA(cudaMemsetAsync(E.filter, 0, sizeof(uint64_t) << E.filter_bits, s));
+    EGTB_CUDA(cudaMemsetAsync(E.layer_off, 0, sizeof(unsigned long long) * E.steps_cap, s));
+    EGTB_CUDA(cudaMemsetAsync(E.layer_len, 0, sizeof(unsigned long long) * E.steps_cap, s));
+    const int t0 = P.first_step - 1;
+    if (n_base > E.arena_cap) throw Error(EGTB_ERR_CAPACITY, "start layer larger than the arena");
+    if (n_partial > E.cand_cap) throw Error(EGTB_ERR_CAPACITY, "partial layer larger than the candidate buffer");
+    std::vector<unsigned long long> off(P.steps + 2, 0), len(P.steps + 2, 0);
+    len[t0] = n_base;
+    off[t0 + 1] = align16(n_base);
+    // layers before t0 are empty and sit at offset 0
+    EGTB_CUDA(cudaMemcpyAsync(E.layer_off, off.data(), sizeof(unsigned long long) * (P.steps + 2),
+                              cudaMemcpyHostToDevice, s));
+    EGTB_CUDA(cudaMemcpyAsync(E.layer_len, len.data(), sizeof(unsigned long long) * (P.steps + 2),
+                              cudaMemcpyHostToDevice, s));
+    if (n_base)
+        EGTB_CUDA(cudaMemcpyAsync(E.arena, base, sizeof(uint64_t) * n_base, cudaMemcpyHostToDevice, s));
+    if (n_partial) {
+        EGTB_CUDA(cudaMemcpyAsync(E.cand[P.first_step & 1], partial, sizeof(uint64_t) * n_partial,
+                                  cudaMemcpyHostToDevice, s));
+        unsigned long long np = n_partial;
+        EGTB_CUDA(cudaMemcpyAsync(&E.ctl->cand_count[P.first_step & 1], &np, sizeof np, cudaMemcpyHostToDevice, s));
+    }
+    // the host buffers above may be pageable: finish the copies before returning
+    EGTB_CUDA(cudaStreamSynchronize(s));
+}
+
+// Run the forward with capacity regrowth. Returns the number of retries.
+static int run_forward(Engine &E, const ForwardPlan &P, const uint64_t *base, size_t n_base, const uint64_t *partial,
+                       size_t n_partial, float *ms) {
+    int retries = 0;
+    E.ensure_steps(P.steps);
+    E.ensure_cand(std::max<unsigned long long>(E.cand_cap, std::max<size_t>(1ull << 22, n_partial * 2)));
+    E.ensure_arena(std::max<unsigned long long>(E.arena_cap, std::max<size_t>(1ull << 26, n_base * 4)));
+    unsigned *progress = progress_device_ptr();
+    for (;;) {
+        stage_start(E, P, base, n_base, partial, n_partial);
+        EGTB_CUDA(cudaEventRecord(E.ev[0], E.stream));
+        enqueue_forward(E, P, progress);
+        EGTB_CUDA(cudaEventRecord(E.ev[1], E.stream));
+        DevCtl c = read_ctl(E);
+        EGTB_CUDA(cudaGetLastError());
+        if (c.err == 0) {
+            EGTB_CUDA(cudaEventElapsedTime(ms, E.ev[0], E.ev[1]));
+            return retries;
+        }
+        ++retries;
+        if (retries > 24) throw Error(EGTB_ERR_CAPACITY, "forward pass did not fit after repeated regrowth");
+        if (c.err & kErrCandOverflow) E.ensure_cand(E.cand_cap * 2);
+        if (c.err & kErrArenaOverflow) E.ensure_arena(E.arena_cap * 2);
+    }
+}
+
+// ----------------------------------------------------------- backward -----
+
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+static double ordered_to_double(unsigned long long o) {
+    unsigned long long b = (o >> 63) ? (o & 0x7FFFFFFFFFFFFFFFull) : ~o;
+    double d;
+    std::memcpy(&d, &b, sizeof d);
+    return d;
+}
+
+template <typename T>
+__global__ void layer_max_kernel(const T *__restrict__ rates, const unsigned long long *__restrict__ layer_off,
+                                 const unsigned long long *__restrict__ layer_len, int t, T zero,
+                                 unsigned long long *__restrict__ out) {
+    const unsigned long long n = layer_len[t], o = layer_off[t];
+    double m = -INFINITY;
+    bool any = false;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const T r = rates[o + i];
+        if (r > zero) {
+            any = true;
+            const double d = (double)r;
+            m = d > m ? d : m;
+        }
+    }
+    unsigned long long b = any ? ordered_bits(m) : 0ull;
+    for (int s = 16; s > 0; s >>= 1) {
+        unsigned long long y = __shfl_xor_sync(0xFFFFFFFFu, b, s);
+        b = y > b ? y : b;
+    }
+    if ((threadIdx.x & 31) == 0 && b) atomicMax(out + t, b);
+}
+
+__global__ void book_len_kernel(const unsigned long long *total, unsigned long long *book_len, int t) {
+    book_len[t] = *total;
+}
+
+template <typename T>
+static void enqueue_pack(Engine &E, int t, T zero) {
+    cudaStream_t s = E.stream;
+    const int g = E.sm_count * 4;
+    book_count_kernel<T><<<g, kSortThreads, 0, s>>>((const T *)E.rates, E.layer_off, E.layer_len, t, zero, E.tile_cnt);
+    tile_scan_kernel<<<1, 1024, 0, s>>>(E.layer_len + t, E.arena_cap, E.tile_off, E.tile_cnt, &E.ctl->n_unique);
+    book_len_kernel<<<1, 1, 0, s>>>(&E.ctl->n_unique, E.book_len, t);
+}
+
+template <typename T>
+static void enqueue_pack_write(Engine &E, int t, T zero, unsigned long long book_off_bytes) {
+    const int g = E.sm_count * 4;
+    book_write_kernel<T><<<g, kSortThreads, 0, E.stream>>>(E.arena, (const T *)E.rates, E.layer_off, E.layer_len, t,
+                                                           zero, E.tile_off, E.book, book_off_bytes,
+                                                           E.book_cap_bytes, E.ctl);
+}
+
+struct BackwardPlan {
+    int steps, docheck, dtype;
+    double p4;
+    DevSpec spec;
+};
+
+// Solve every layer on the device-resident arena (layers 0..steps-1 present)
+// and pack all books; book bytes of layer t start at layer_off[t] * rec.
+template <typename T>
+static void enqueue_backward(Engine &E, const BackwardPlan &B, const std::vector<unsigned long long> &off,
+                             unsigned *progress) {
+    cudaStream_t s = E.stream;
+    const T zero = (T)dtype_zero(B.dtype), maxv = (T)dtype_max(B.dtype);
+    const int g = E.sm_count * 8;
+    T *rates = (T *)E.rates;
+    const uint32_t total = (uint32_t)(B.steps * 2);
+    for (int t = B.steps - 2; t < B.steps; ++t)
+        if (t >= 0) final_layer_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec, zero, maxv);
+    for (int t = B.steps - 3; t >= 0; --t) {
+        progress_kernel<<<1, 1, 0, s>>>(progress, total - (unsigned)t - 2u);
+        solve_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.split, E.layer_off, E.layer_len, t, B.spec,
+                                          t > B.docheck ? 1 : 0, E.tab, B.p4, zero, maxv, E.ctl);
+    }
+    EGTB_CUDA(cudaMemsetAsync(E.layer_max, 0, sizeof(unsigned long long) * E.steps_cap, s));
+    const size_t rec = 8 + sizeof(T);
+    for (int t = 0; t < B.steps; ++t) {
+        enqueue_pack<T>(E, t, zero);
+        enqueue_pack_write<T>(E, t, zero, off[t] * rec);
+        layer_max_kernel<T><<<E.sm_count, 256, 0, s>>>(rates, E.layer_off, E.layer_len, t, zero, E.layer_max);
+    }
+}
+
+// ---------------------------------------------------------------- output --
+
+static std::vector<unsigned long long> d2h_u64(Engine &E, const unsigned long long *d, int n) {
+    std::vector<unsigned long long> h(n);
+    EGTB_CUDA(cudaMemcpyAsync(h.data(), d, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost, E.stream));
+    EGTB_CUDA(cudaStreamSynchronize(E.stream));
+    return h;
+}
+
+// stats.txt lines, ensure_stats_header + recalculate_process_impl,
+// native_core/src/BookSolver.cpp:286-293,569-581 (layers in solve order).
+static void write_stats(const egtb_run_options &o, int dtype, const std::vector<int> &layers,
+                        const std::vector<unsigned long long> &raw_len, const std::vector<unsigned long long> &book_len,
+                        const std::vector<unsigned long long> &maxbits, double seconds_per_layer) {
+    const std::string path = std::string(o.pathname) + "stats.txt";
+    const bool exists = file_exists(path);
+    std::ofstream f(path, std::ios::app);
+    if (!f) throw Error(EGTB_ERR_IO, "cannot open " + path);
+    if (!exists) f << "layer,length,max success rate,speed,deletion_threshold,time\n";
+    const double zero = dtype_zero(dtype), maxs = dtype_max(dtype);
+    for (int t : layers) {
+        if (book_len[t] == 0) continue;
+        const double m = maxbits[t] ? ordered_to_double(maxbits[t]) : zero;
+        const double max_success = (m - zero) / (maxs - zero);
+        f << t << "," << raw_len[t] << "," << max_success << ","
+          << round_to_2((double)raw_len[t] / std::max(seconds_per_layer, 0.01) / 1e6) << " mbps,"
+          << o.deletion_threshold << "," << now_string() << "\n";
+    }
+}
+
+static int writer_threads(const egtb_run_options &o) {
+    if (o.num_threads > 0) return std::min(o.num_threads, 32);
+    return 8;
+}
+
+// Copy byte ranges [dev_off[i], +bytes[i]) of a device buffer to pinned host
+// memory and write them to files with a thread pool.
+static void write_ranges(Engine &E, const unsigned char *dev, const std::vector<std::string> &paths,
+                         const std::vector<unsigned long long> &dev_off, const std::vector<unsigned long long> &bytes,
+                         int threads) {
+    unsigned long long total = 0;
+    for (auto b : bytes) total += b;
+    unsigned char *h = E.ensure_pinned(std::max<unsigned long long>(total, 1));
+    unsigned long long pos = 0;
+    std::vector<unsigned long long> hoff(paths.size());
+    for (size_t i = 0; i < paths.size(); ++i) {
+        hoff[i] = pos;
+        if (bytes[i])
+            EGTB_CUDA(cudaMemcpyAsync(h + pos, dev + dev_off[i], bytes[i], cudaMemcpyDeviceToHost, E.stream));
+        pos += bytes[i];
+    }
+    EGTB_CUDA(cudaStreamSynchronize(E.stream));
+    WriterPool pool(threads);
+    for (size_t i = 0; i < paths.size(); ++i) pool.submit(paths[i], h + hoff[i], bytes[i]);
+    pool.wait();
+}
+
+// ------------------------------------------------------------- restart ----
+
+static bool any_layer_file(const egtb_run_options &o) {
+    const std::string p = o.pathname;
+    for (int i = 0; i < o.steps + 1; ++i) {
+        const std::string b = p + std::to_string(i);
+        if (file_exists(b) || file_exists(b + ".book") || file_exists(b + ".z") || file_exists(b + ".book.7z") ||
+            file_exists(b + ".7z"))
+            return true;
+    }
+    return false;
+}
+
+// handle_restart, native_core/src/BookGenerator.cpp:384-430: the first step
+// that is not already on disk. Invalid files (empty or misaligned) are removed
+// on the way, as the reference does.
+static int first_step_to_run(const egtb_run_options &o, int rec) {
+    const std::string p = o.pathname;
+    for (int i = 1; i < o.steps - 1; ++i) {
+        const std::string pi = p + std::to_string(i), pi1 = p + std::to_string(i + 1);
+        remove_invalid(pi, 8);
+        remove_invalid(pi1, 8);
+        remove_invalid(pi + ".book", rec);
+        remove_invalid(pi1 + ".book", rec);
+        remove_invalid(pi + ".z", 0);
+        remove_invalid(pi + ".book.7z", 0);
+        remove_invalid(pi + ".7z", 0);
+        remove_invalid(pi1 + ".z", 0);
+        const bool skip = (file_valid(pi1, 8) && file_valid(pi, 8)) || (file_valid(pi1 + ".book", rec) && file_valid(pi, 8)) ||
+                          (file_valid(pi1 + ".z", 0) && file_valid(pi, 8)) || file_valid(pi + ".book", rec) ||
+                          file_valid(pi + ".z", 0) || file_valid(pi + ".book.7z", 0) || file_valid(pi + ".7z", 0);
+        if (!skip) return i;
+    }
+    return o.steps - 1;  // every step on disk
+}
+
+static std::vector<uint64_t> read_u64_file(const std::string &path) {
+    const uint64_t sz = file_size(path);
+    std::vector<uint64_t> v(sz / 8);
+    if (!v.empty()) read_file_into(path, v.data(), v.size() * 8);
+    return v;
+}
+
+static void check_common(const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec *spec,
+                         const egtb_run_options *o) {
+    if (!spec || !o) throw Error(EGTB_ERR_ARG, "spec and options are required");
+    if (n_seeds && !seeds) throw Error(EGTB_ERR_ARG, "seeds pointer is NULL");
+    if (o->is_variant) throw Error(EGTB_ERR_UNSUPPORTED, "variant boards (wall-merge mover) are not built");
+    if (o->compress || o->optimal_branch_only)
+        throw Error(EGTB_ERR_UNSUPPORTED, "compress / optimal_branch_only post-passes are not built");
+    dtype_size(o->success_rate_dtype);
+    if (o->steps > (1 << 20)) throw Error(EGTB_ERR_ARG, "steps out of range");
+}
+
+static ForwardPlan make_forward_plan(const egtb_pattern_spec &spec, const egtb_run_options &o, int first_step) {
+    ForwardPlan P;
+    P.steps = o.steps;
+    P.docheck = o.docheck_step;
+    P.first_step = first_step;
+    P.spec = make_dev_spec(spec, o.target);
+    P.shifts = varying_byte_shifts(spec);
+    return P;
+}
+
+static double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// --------------------------------------------------------- fused build ----
+
+template <typename T>
+static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec &spec,
+                        const egtb_run_options &o, egtb_build_stats *st) {
+    const auto t_start = std::chrono::steady_clock::now();
+    const int steps = o.steps;
+    const uint32_t total = (uint32_t)(steps * 2);
+    set_progress(0, total);
+    ForwardPlan P = make_forward_plan(spec, o, 1);
+    float fwd_ms = 0.f, bwd_ms = 0.f;
+    const int retries = run_forward(E, P, seeds, n_seeds, nullptr, 0, &fwd_ms);
+    std::vector<unsigned long long> off = d2h_u64(E, E.layer_off, steps + 1);
+    std::vector<unsigned long long> len = d2h_u64(E, E.layer_len, steps + 1);
+    BackwardPlan B{steps, o.docheck_step, o.success_rate_dtype, o.spawn_rate4, P.spec};
+    EGTB_CUDA(cudaEventRecord(E.ev[2], E.stream));
+    enqueue_backward<T>(E, B, off, progress_device_ptr());
+    EGTB_CUDA(cudaEventRecord(E.ev[3], E.stream));
+    EGTB_CUDA(cudaStreamSynchronize(E.stream));
+    EGTB_CUDA(cudaGetLastError());
+    EGTB_CUDA(cudaEventElapsedTime(&bwd_ms, E.ev[2], E.ev[3]));
+    DevCtl c = read_ctl(E);
+    if (c.err) throw Error(EGTB_ERR_CAPACITY, "book buffer overflow");
+    std::vector<unsigned long long> blen = d2h_u64(E, E.book_len, steps);
+    std::vector<unsigned long long> maxb = d2h_u64(E, E.layer_max, steps);
+    const size_t rec = 8 + sizeof(T);
+    if (o.write_files) {
+        std::vector<std::string> paths;
+        std::vector<unsigned long long> doff, bytes;
+        for (int t = 0; t < steps; ++t) {
+            paths.push_back(std::string(o.pathname) + std::to_string(t) + ".book");
+            doff.push_back(off[t] * rec);
+            bytes.push_back(blen[t] * rec);
+        }
+        write_ranges(E, E.book, paths, doff, bytes, writer_threads(o));
+        std::vector<int> order;
+        for (int t = steps - 3; t >= 0; --t) order.push_back(t);
+        write_stats(o, o.success_rate_dtype, order, len, blen, maxb,
+                    (fwd_ms + bwd_ms) * 1e-3 / std::max(1, steps));
+    }
+    set_progress(total, total);
+    if (st) {
+        std::memset(st, 0, sizeof *st);
+        for (int t = 0; t < steps; ++t) {
+            st->raw_boards += len[t];
+            st->book_entries += blen[t];
+            st->max_layer = std::max<uint64_t>(st->max_layer, len[t]);
+        }
+        st->candidates = c.candidates;
+        st->lookups = c.lookups;
+        st->layers = steps;
+        st->retries = retries;
+        st->forward_ms = fwd_ms;
+        st->backward_ms = bwd_ms;
+        st->total_ms = ms_since(t_start);
+    }
+}
+
+// ------------------------------------------------- generate (files) -------
+
+template <typename T>
+static void generate_files(Engine &E, const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec &spec,
+                           const egtb_run_options &o, int *started, egtb_build_stats *st) {
+    const auto t_start = std::chrono::steady_clock::now();
+    const int steps = o.steps;
+    const size_t rec = 8 + sizeof(T);
+    const std::string p = o.pathname;
+    *started = 0;
+    const uint32_t total = (uint32_t)(steps * 2);
+    set_progress(0, total);
+    if (steps < 3) {
+        remove_file(p + std::to_string(steps - 2));
+        return;
+    }
+    const int i0 = first_step_to_run(o, (int)rec);
+    float fwd_ms = 0.f;
+    int retries = 0;
+    std::vector<unsigned long long> off, len;
+    if (i0 <= steps - 2) {
+        *started = 1;
+        std::vector<uint64_t> base, partial;
+        if (i0 == 1) {
+            write_file(p + "0", seeds, n_seeds * 8);  // BookGenerator.cpp:417-419
+            base.assign(seeds, seeds + n_seeds);
+        } else {
+            base = read_u64_file(p + std::to_string(i0 - 1));
+            partial = read_u64_file(p + std::to_string(i0));
+        }
+        ForwardPlan P = make_forward_plan(spec, o, i0);
+        retries = run_forward(E, P, base.data(), base.size(), partial.data(), partial.size(), &fwd_ms);
+        off = d2h_u64(E, E.layer_off, steps + 1);
+        len = d2h_u64(E, E.layer_len, steps + 1);
+        // raw layers i0 .. steps-3
+        std::vector<std::string> paths;
+        std::vector<unsigned long long> doff, bytes;
+        for (int t = i0; t <= steps - 3; ++t) {
+            paths.push_back(p + std::to_string(t));
+            doff.push_back(off[t] * 8);
+            bytes.push_back(len[t] * 8);
+        }
+        // final_steps: success-only books of layers steps-2 and steps-1
+        const T zero = (T)dtype_zero(o.success_rate_dtype), maxv = (T)dtype_max(o.success_rate_dtype);
+        DevSpec ds = make_dev_spec(spec, o.target);
+        EGTB_CUDA(cudaMemsetAsync(E.ctl, 0, sizeof(DevCtl), E.stream));
+        for (int t = steps - 2; t < steps; ++t) {
+            final_layer_kernel<T><<<E.sm_count * 4, 256, 0, E.stream>>>(E.arena, (T *)E.rates, E.layer_off,
+                                                                          E.layer_len, t, ds, zero, maxv);
+            enqueue_pack<T>(E, t, zero);
+            enqueue_pack_write<T>(E, t, zero, off[t] * rec);
+        }
+        std::vector<unsigned long long> blen = d2h_u64(E, E.book_len, steps);
+        write_ranges(E, (const unsigned char *)E.arena, paths, doff, bytes, writer_threads(o));
+        std::vector<std::string> bpaths = {p + std::to_string(steps - 2) + ".book", p + std::to_string(steps - 1) + ".book"};
+        std::vector<unsigned long long> boff = {off[steps - 2] * rec, off[steps - 1] * rec};
+        std::vector<unsigned long long> bbytes = {blen[steps - 2] * rec, blen[steps - 1] * rec};
+        write_ranges(E, E.book, bpaths, boff, bbytes, writer_threads(o));
+        if (st) {
+            std::memset(st, 0, sizeof *st);
+            for (int t = i0; t < steps; ++t) {
+                st->raw_boards += len[t];
+                st->max_layer = std::max<uint64_t>(st->max_layer, len[t]);
+            }
+            st->book_entries = blen[steps - 2] + blen[steps - 1];
+            DevCtl c = read_ctl(E);
+            st->candidates = c.candidates;
+        }
+    }
+    remove_file(p + std::to_string(steps - 2));  // final_steps, BookSolver.cpp:279-282
+    if (st) {
+        st->layers = steps;
+        st->retries = retries;
+        st->forward_ms = fwd_ms;
+        st->total_ms = ms_since(t_start);
+    }
+}
+
+// ---------------------------------------------------- solve (files) -------
+
+// Split packed records into the arena slot (keys) and rates.
+template <typename T>
+__global__ void unpack_records_kernel(const unsigned char *__restrict__ recs, unsigned long long n,
+                                      uint64_t *__restrict__ keys, T *__restrict__ rates) {
+    constexpr int rec = 8 + (int)sizeof(T);
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(recs + i * rec);
+        keys[i] = (uint64_t)w[0] | ((uint64_t)w[1] << 32);
+        T r;
+        std::memcpy(&r, recs + i * rec + 8, sizeof(T));
+        rates[i] = r;
+    }
+}
+
+__global__ void splitters_kernel(const uint64_t *__restrict__ keys, unsigned long long n, uint64_t *__restrict__ split) {
+    const unsigned long long ns = (n + kSplitStride - 1) / kSplitStride;
+    for (unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; j < ns;
+         j += (unsigned long long)gridDim.x * blockDim.x)
+        split[j] = keys[j * kSplitStride];
+}
+
+// recalculate_process_impl, native_core/src/BookSolver.cpp:513-605, with the
+// three live layers (i, i+1, i+2) in rotating arena slots.
+template <typename T>
+static void solve_files(Engine &E, const void *d1_recs, size_t n1, const void *d2_recs, size_t n2,
+                        const egtb_pattern_spec &spec, const egtb_run_options &o, egtb_build_stats *st) {
+    const auto t_start = std::chrono::steady_clock::now();
+    const int steps = o.steps;
+    const size_t rec = 8 + sizeof(T);
+    const std::string p = o.pathname;
+    const T zero = (T)dtype_zero(o.success_rate_dtype), maxv = (T)dtype_max(o.success_rate_dtype);
+    const uint32_t total = (uint32_t)(steps * 2);
+    DevSpec ds = make_dev_spec(spec, o.target);
+    cudaStream_t s = E.stream;
+    E.ensure_steps(4);
+
+    // the largest layer decides the slot size
+    unsigned long long slot = 16;
+    for (int i = 0; i < steps; ++i) {
+        slot = std::max<unsigned long long>(slot, file_size(p + std::to_string(i)) / 8);
+        slot = std::max<unsigned long long>(slot, file_size(p + std::to_string(i) + ".book") / rec);
+    }
+    slot = std::max<unsigned long long>(slot, std::max(n1, n2));
+    slot = align16(slot);
+    E.ensure_arena(slot * 3);
+    E.ensure_cand(std::max<unsigned long long>(E.cand_cap, 1ull << 22));
+
+    // host copies of the two successor layers (packed records)
+    std::vector<unsigned char> h1((const unsigned char *)d1_recs, (const unsigned char *)d1_recs + n1 * rec);
+    std::vector<unsigned char> h2((const unsigned char *)d2_recs, (const unsigned char *)d2_recs + n2 * rec);
+    bool started = false;
+    int slot_of[3] = {0, 1, 2};  // slot of layer i, i+1, i+2
+    bool resident = false;       // layers i+1, i+2 already on the device
+    bool skipped_since_start = false;
+    write_stats(o, o.success_rate_dtype, {}, {}, {}, {}, 0.0);  // header first (ensure_stats_header)
+    unsigned long long dlen1 = 0, dlen2 = 0;
+    unsigned char *d_stage = nullptr;
+    EGTB_CUDA(cudaMalloc(&d_stage, std::max<size_t>(slot * rec, 16)));
+    std::unique_ptr<unsigned char, void (*)(unsigned char *)> stage_guard(d_stage, [](unsigned char *q) { cudaFree(q); });
+    T *rates = (T *)E.rates;
+
+    auto upload_layer = [&](const std::vector<unsigned char> &recs, int sl) -> unsigned long long {
+        const unsigned long long n = recs.size() / rec;
+        if (n > slot) throw Error(EGTB_ERR_CAPACITY, "layer larger than its slot");
+        if (n) {
+            EGTB_CUDA(cudaMemcpyAsync(d_stage, recs.data(), n * rec, cudaMemcpyHostToDevice, s));
+            unpack_records_kernel<T><<<E.sm_count * 4, 256, 0, s>>>(d_stage, n, E.arena + sl * slot, rates + sl * slot);
+            splitters_kernel<<<E.sm_count, 256, 0, s>>>(E.arena + sl * slot, n, E.split + sl * slot / kSplitStride);
+            EGTB_CUDA(cudaStreamSynchronize(s));
+        }
+        return n;
+    };
+
+    for (int i = steps - 3; i >= 0; --i) {
+        set_progress(total - (uint32_t)i - 2u, total);
+        const std::string pi = p + std::to_string(i);
+        remove_invalid(pi + ".book", rec);
+        remove_invalid(pi + ".z", 0);
+        remove_invalid(pi + ".book.7z", 0);
+        if (file_valid(pi + ".book", rec) || file_valid(pi + ".z", 0) || file_valid(pi + ".book.7z", 0)) {
+            resident = false;
+            if (started) skipped_since_start = true;
+            continue;
+        }
+        if (!started) {
+            started = true;
+            if (i != steps - 3 || h1.empty() || h2.empty()) {
+                h1 = read_file(p + std::to_string(i + 1) + ".book");
+                h2 = read_file(p + std::to_string(i + 2) + ".book");
+            }
+        }
+        if (!resident) {
+            if (skipped_since_start) {
+                // resuming after a layer that was already on disk
+                h1 = read_file(p + std::to_string(i + 1) + ".book");
+                h2 = read_file(p + std::to_string(i + 2) + ".book");
+                skipped_since_start = false;
+            }
+            dlen1 = upload_layer(h1, slot_of[1]);
+            dlen2 = upload_layer(h2, slot_of[2]);
+            resident = true;
+        }
+        std::vector<uint64_t> raw = read_u64_file(pi);
+        const unsigned long long n0 = raw.size();
+        if (n0 > slot) throw Error(EGTB_ERR_CAPACITY, "raw layer larger than its slot");
+        uint64_t *k0 = E.arena + slot_of[0] * slot;
+        if (n0) EGTB_CUDA(cudaMemcpyAsync(k0, raw.data(), n0 * 8, cudaMemcpyHostToDevice, s));
+        unsigned long long off_h[3] = {slot_of[0] * slot, slot_of[1] * slot, slot_of[2] * slot};
+        unsigned long long len_h[3] = {n0, dlen1, dlen2};
+        EGTB_CUDA(cudaMemcpyAsync(E.layer_off, off_h, sizeof off_h, cudaMemcpyHostToDevice, s));
+        EGTB_CUDA(cudaMemcpyAsync(E.layer_len, len_h, sizeof len_h, cudaMemcpyHostToDevice, s));
+        EGTB_CUDA(cudaMemsetAsync(E.ctl, 0, sizeof(DevCtl), s));
+        EGTB_CUDA(cudaMemsetAsync(E.layer_max, 0, sizeof(unsigned long long) * 4, s));
+        const auto t0 = std::chrono::steady_clock::now();
+        solve_kernel<T><<<E.sm_count * 8, 256, 0, s>>>(E.arena, rates, E.split, E.layer_off, E.layer_len, 0, ds,
+                                                        i > o.docheck_step ? 1 : 0, E.tab, o.spawn_rate4, zero, maxv, E.ctl);
+        splitters_kernel<<<E.sm_count, 256, 0, s>>>(k0, n0, E.split + slot_of[0] * slot / kSplitStride);
+        enqueue_pack<T>(E, 0, zero);
+        enqueue_pack_write<T>(E, 0, zero, 0);
+        layer_max_kernel<T><<<E.sm_count, 256, 0, s>>>(rates, E.layer_off, E.layer_len, 0, zero, E.layer_max);
+        unsigned long long nb = 0, mb = 0;
+        EGTB_CUDA(cudaMemcpyAsync(&nb, E.book_len, 8, cudaMemcpyDeviceToHost, s));
+        EGTB_CUDA(cudaMemcpyAsync(&mb, E.layer_max, 8, cudaMemcpyDeviceToHost, s));
+        EGTB_CUDA(cudaStreamSynchronize(s));
+        EGTB_CUDA(cudaGetLastError());
+        std::vector<unsigned char> book(nb * rec);
+        if (nb) EGTB_CUDA(cudaMemcpy(book.data(), E.book, nb * rec, cudaMemcpyDeviceToHost));
+        const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (nb) {
+            std::vector<int> lay = {i};
+            std::vector<unsigned long long> rl(i + 1, 0), bl(i + 1, 0), mx(i + 1, 0);
+            rl[i] = n0;
+            bl[i] = nb;
+            mx[i] = mb;
+            write_stats(o, o.success_rate_dtype, lay, rl, bl, mx, secs);
+        }
+        write_file(pi + ".book", book.data(), book.size());
+        remove_file(pi);
+        if (o.deletion_threshold > 0.0) {
+            // compact layer i+2 with the threshold and rewrite its book
+            // (BookSolver.cpp:589-593); computation is unaffected.
+            const double thr_d = o.deletion_threshold * (dtype_max(o.success_rate_dtype) - dtype_zero(o.success_rate_dtype)) +
+                                 dtype_zero(o.success_rate_dtype);
+            const T thr = (T)thr_d;
+            std::vector<unsigned char> kept;
+            for (size_t r = 0; r < h2.size() / rec; ++r) {
+                T v;
+                std::memcpy(&v, h2.data() + r * rec + 8, sizeof(T));
+                if (v > thr) kept.insert(kept.end(), h2.begin() + r * rec, h2.begin() + (r + 1) * rec);
+            }
+            write_file(p + std::to_string(i + 2) + ".book", kept.data(), kept.size());
+        }
+        if (i > 0) {
+            // rotate: layer i becomes i+1, i+1 becomes i+2
+            const int old2 = slot_of[2];
+            slot_of[2] = slot_of[1];
+            slot_of[1] = slot_of[0];
+            slot_of[0] = old2;
+            dlen2 = dlen1;
+            dlen1 = n0;
+            h2.swap(h1);
+            h1.swap(book);
+            resident = true;
+        }
+        if (st) {
+            st->raw_boards += n0;
+            st->book_entries += nb;
+            st->max_layer = std::max<uint64_t>(st->max_layer, n0);
+        }
+    }
+    if (st) {
+        st->layers = steps;
+        st->total_ms = ms_since(t_start);
+    }
+}
+
+// ------------------------------------------------------ primitives -------
+
+__global__ void prim_moves_kernel(const uint32_t *tab, const uint64_t *in, size_t n, uint64_t *out4) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        uint64_t m[4];
+        move_all_dir(tab, in[i], m);
+        for (int d = 0; d < 4; ++d) out4[4 * i + d] = m[d];
+    }
+}
+
+__global__ void prim_canonical_kernel(const uint64_t *in, size_t n, int mode, uint64_t *out) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = canonical(in[i], mode);
+}
+
+__global__ void prim_sym_kernel(const uint64_t *in, size_t n, int idx, uint64_t *out) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = apply_sym(in[i], idx);
+}
+
+template <typename Launch>
+static void run_prim(int device, const uint64_t *boards, size_t n, size_t out_per, uint64_t *out, Launch launch) {
+    if (n == 0) return;
+    if (!boards || !out) throw Error(EGTB_ERR_ARG, "NULL buffer");
+    Engine &E = engine_for(device);
+    std::lock_guard<std::mutex> lk(E.mu);
+    uint64_t *din = nullptr, *dout = nullptr;
+    EGTB_CUDA(cudaMalloc(&din, n * 8));
+    std::unique_ptr<uint64_t, void (*)(uint64_t *)> g1(din, [](uint64_t *q) { cudaFree(q); });
+    EGTB_CUDA(cudaMalloc(&dout, n * 8 * out_per));
+    std::unique_ptr<uint64_t, void (*)(uint64_t *)> g2(dout, [](uint64_t *q) { cudaFree(q); });
+    EGTB_CUDA(cudaMemcpyAsync(din, boards, n * 8, cudaMemcpyHostToDevice, E.stream));
+    launch(E, din, dout);
+    EGTB_CUDA(cudaGetLastError());
+    EGTB_CUDA(cudaMemcpyAsync(out, dout, n * 8 * out_per, cudaMemcpyDeviceToHost, E.stream));
+    EGTB_CUDA(cudaStreamSynchronize(E.stream));
+}
+
+}  // namespace egtb
+
+// =================================================================== C ABI ===
+
+using namespace egtb;
+
+extern "C" const char *egtb_version(void) { return "egtb_gpu 0.1 sm_100a"; }
+
+extern "C" int egtb_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+extern "C" int egtb_get_build_progress(uint32_t *current, uint32_t *total) {
+    if (!current || !total) return EGTB_ERR_ARG;
+    // get_build_progress, native_core/include/FormationRuntime.h:73-82
+    uint32_t t = g_progress_total.load(std::memory_order_relaxed);
+    uint32_t c = read_progress();
+    if (c > t) t = c;
+    *current = c;
+    *total = t;
+    return EGTB_OK;
+}
+
+extern "C" int egtb_reset_build_progress(uint32_t total) {
+    g_progress_total.store(total, std::memory_order_relaxed);
+    g_progress_host.store(0, std::memory_order_relaxed);
+    if (g_progress_mapped) *(volatile unsigned *)g_progress_mapped = 0;
+    return EGTB_OK;
+}
+
+template <typename F>
+static int dispatch_dtype(int dtype, F &&f) {
+    switch (dtype) {
+        case EGTB_DTYPE_UINT32: f((uint32_t)0); break;
+        case EGTB_DTYPE_UINT64: f((uint64_t)0); break;
+        case EGTB_DTYPE_FLOAT32: case EGTB_DTYPE_1_FLOAT32: f(0.0f); break;
+        case EGTB_DTYPE_FLOAT64: case EGTB_DTYPE_1_FLOAT64: f(0.0); break;
+        default: throw Error(EGTB_ERR_ARG, "unknown success_rate_dtype");
+    }
+    return 0;
+}
+
+extern "C" int egtb_generate(const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec *spec,
+                             const egtb_run_options *options, int32_t *started, egtb_build_stats *stats) {
+    return guarded([&] {
+        check_common(seeds, n_seeds, spec, options);
+        Engine &E = engine_for(options->device);
+        std::lock_guard<std::mutex> lk(E.mu);
+        int st = 0;
+        if (stats) std::memset(stats, 0, sizeof *stats);
+        dispatch_dtype(options->success_rate_dtype, [&](auto z) {
+            using T = decltype(z);
+            generate_files<T>(E, seeds, n_seeds, *spec, *options, &st, stats);
+        });
+        if (started) *started = st;
+    });
+}
+
+extern "C" int egtb_solve(const void *d1_records, size_t n1, const void *d2_records, size_t n2,
+                          const egtb_pattern_spec *spec, const egtb_run_options *options, egtb_build_stats *stats) {
+    return guarded([&] {
+        check_common(nullptr, 0, spec, options);
+        if ((n1 && !d1_records) || (n2 && !d2_records)) throw Error(EGTB_ERR_ARG, "NULL record buffer");
+        Engine &E = engine_for(options->device);
+        std::lock_guard<std::mutex> lk(E.mu);
+        if (stats) std::memset(stats, 0, sizeof *stats);
+        dispatch_dtype(options->success_rate_dtype, [&](auto z) {
+            using T = decltype(z);
+            solve_files<T>(E, d1_records, n1, d2_records, n2, *spec, *options, stats);
+        });
+    });
+}
+
+extern "C" int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec *spec,
+                          const egtb_run_options *options, egtb_build_stats *stats) {
+    return guarded([&] {
+        check_common(seeds, n_seeds, spec, options);
+        // run_pattern_build_cpp resets the progress first (BookSolver.cpp:828)
+        egtb_reset_build_progress((uint32_t)(options->steps > 0 ? options->steps * 2 : 0));
+        Engine &E = engine_for(options->device);
+        std::lock_guard<std::mutex> lk(E.mu);
+        if (stats) std::memset(stats, 0, sizeof *stats);
+        const bool resume = options->write_files && any_layer_file(*options);
+        dispatch_dtype(options->success_rate_dtype, [&](auto z) {
+            using T = decltype(z);
+            if (options->steps < 3) {
+                int st = 0;
+                generate_files<T>(E, seeds, n_seeds, *spec, *options, &st, stats);
+                return;
+            }
+            if (!resume) {
+                fused_build<T>(E, seeds, n_seeds, *spec, *options, stats);
+            } else {
+                int st = 0;
+                egtb_build_stats g;
+                std::memset(&g, 0, sizeof g);
+                generate_files<T>(E, seeds, n_seeds, *spec, *options, &st, &g);
+                solve_files<T>(E, nullptr, 0, nullptr, 0, *spec, *options, stats);
+                if (stats) {
+                    stats->forward_ms = g.forward_ms;
+                    stats->candidates = g.candidates;
+                }
+            }
+        });
+    });
+}
+
+extern "C" int egtb_move_all_dir(int device, const uint64_t *boards, size_t n, uint64_t *out4) {
+    return guarded([&] {
+        run_prim(device, boards, n, 4, out4, [&](Engine &E, uint64_t *din, uint64_t *dout) {
+            prim_moves_kernel<<<E.sm_count * 4, 256, 0, E.stream>>>(E.tab, din, n, dout);
+        });
+    });
+}
+
+extern "C" int egtb_canonical(int device, const uint64_t *boards, size_t n, int32_t symm_mode, uint64_t *out) {
+    return guarded([&] {
+        if (symm_mode < 0 || symm_mode > 3) throw Error(EGTB_ERR_UNSUPPORTED, "symmetry mode not built");
+        run_prim(device, boards, n, 1, out, [&](Engine &E, uint64_t *din, uint64_t *dout) {
+            prim_canonical_kernel<<<E.sm_count * 4, 256, 0, E.stream>>>(din, n, symm_mode, dout);
+        });
+    });
+}
+
+extern "C" int egtb_apply_sym(int device, const uint64_t *boards, size_t n, int32_t symm_index, uint64_t *out) {
+    return guarded([&] {
+        run_prim(device, boards, n, 1, out, [&](Engine &E, uint64_t *din, uint64_t *dout) {
+            prim_sym_kernel<<<E.sm_count * 4, 256, 0, E.stream>>>(din, n, symm_index, dout);
+        });
+    });
+}

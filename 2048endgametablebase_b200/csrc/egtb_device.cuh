@@ -188,4 +188,32 @@ __device__ __forceinline__ uint64_t filter_slot(uint64_t key, int bits) {
     return (key * 0x9E3779B97F4A7C15ull) >> (64 - bits);
 }
 
+constexpr int kSplitStride = 16;  // one splitter per 16 keys (one 128-byte line)
+
+// Exact search of key in layer keys[0..n) with splitters split[j] =
+// keys[16j]: branchless search over the splitters, then over one 16-key line.
+template <typename T>
+__device__ __forceinline__ T layer_lookup(const uint64_t *__restrict__ keys, const T *__restrict__ rates,
+                                          unsigned long long n, const uint64_t *__restrict__ split, uint64_t key,
+                                          T zero) {
+    if (n == 0) return zero;
+    const unsigned long long ns = (n + kSplitStride - 1) / kSplitStride;
+    if (key < __ldg(split)) return zero;
+    unsigned long long lo = 0, len = ns;
+    while (len > 1) {
+        const unsigned long long half = len >> 1;
+        lo = (__ldg(split + lo + half) <= key) ? lo + half : lo;
+        len -= half;
+    }
+    unsigned long long b = lo * kSplitStride;
+    unsigned long long m = n - b < (unsigned long long)kSplitStride ? n - b : (unsigned long long)kSplitStride;
+    // lower bound inside the line
+    while (m > 1) {
+        const unsigned long long half = m >> 1;
+        b = (__ldg(keys + b + half) <= key) ? b + half : b;
+        m -= half;
+    }
+    return __ldg(keys + b) == key ? rates[b] : zero;
+}
+
 }  // namespace egtb

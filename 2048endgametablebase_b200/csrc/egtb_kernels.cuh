@@ -19,7 +19,6 @@ constexpr unsigned kErrBookOverflow = 4u;
 constexpr int kTileKeys = 4096;     // keys per sort / compaction tile
 constexpr int kSortThreads = 256;   // 8 warps x 16 keys x 32 lanes
 constexpr int kKeysPerThread = kTileKeys / kSortThreads;
-constexpr int kSplitStride = 16;    // one splitter per 16 keys (one 128-byte line)
 
 // Control block in device memory.
 struct DevCtl {
@@ -216,19 +215,17 @@ radix_scan_kernel(const unsigned long long *n_ptr, unsigned long long cap, unsig
     const unsigned long long n = clamp_n(*n_ptr, cap);
     const unsigned long long ntiles = (n + kTileKeys - 1) / kTileKeys;
     const int d = blockIdx.x;
-    unsigned long long base = 0, tot = 0;
-    unsigned long long v = (threadIdx.x < 256 && (int)threadIdx.x < d) ? digit_tot[threadIdx.x] : 0;
-    block_excl_scan<unsigned long long>(v, sm, &tot);
-    base = tot;
+    unsigned long long tot = 0;
     unsigned *row = tile_hist + (unsigned long long)d * max_tiles;
+    unsigned long long run = 0;
     for (unsigned long long c0 = 0; c0 < ntiles; c0 += blockDim.x) {
         const unsigned long long i = c0 + threadIdx.x;
         unsigned long long x = i < ntiles ? row[i] : 0;
         unsigned long long ex = block_excl_scan<unsigned long long>(x, sm, &tot);
-        // offsets fit 32 bits only for small sorts; store as (base + ex) relative
-        // to nothing: the scatter adds the 64-bit digit base it recomputes.
-        if (i < ntiles) row[i] = (unsigned)(ex);
-        base += tot;
+        // offset inside the digit (candidate buffers hold < 2^32 keys); the
+        // scatter adds the 64-bit start of the digit
+        if (i < ntiles) row[i] = (unsigned)(run + ex);
+        run += tot;
     }
 }
 
@@ -407,32 +404,6 @@ unique_write_kernel(const uint64_t *__restrict__ keys, const unsigned long long 
 }
 
 // ------------------------------------------------------ backward ---------
-
-// Exact search of key in layer keys[0..n) with splitters split[j] =
-// keys[16j]: branchless search over the splitters, then over one 16-key line.
-template <typename T>
-__device__ __forceinline__ T layer_lookup(const uint64_t *__restrict__ keys, const T *__restrict__ rates,
-                                          unsigned long long n, const uint64_t *__restrict__ split, uint64_t key,
-                                          T zero) {
-    if (n == 0) return zero;
-    const unsigned long long ns = (n + kSplitStride - 1) / kSplitStride;
-    if (key < __ldg(split)) return zero;
-    unsigned long long lo = 0, len = ns;
-    while (len > 1) {
-        const unsigned long long half = len >> 1;
-        lo = (__ldg(split + lo + half) <= key) ? lo + half : lo;
-        len -= half;
-    }
-    unsigned long long b = lo * kSplitStride;
-    unsigned long long m = n - b < (unsigned long long)kSplitStride ? n - b : (unsigned long long)kSplitStride;
-    // lower bound inside the line
-    while (m > 1) {
-        const unsigned long long half = m >> 1;
-        b = (__ldg(keys + b + half) <= key) ? b + half : b;
-        m -= half;
-    }
-    return __ldg(keys + b) == key ? rates[b] : zero;
-}
 
 template <typename T> __device__ __forceinline__ T cast_rate(double x);
 template <> __device__ __forceinline__ uint32_t cast_rate<uint32_t>(double x) { return (uint32_t)__double2uint_rz(x); }

@@ -24,6 +24,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define EGTB_API __attribute__((visibility("default")))
+#else
+#define EGTB_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -116,20 +122,20 @@ typedef struct egtb_build_stats {
 /* ------------------------------------------------------------ errors ---- */
 
 /* Message of the calling thread's last failure (empty when none). */
-int egtb_last_error(char *buf, size_t len);
+EGTB_API int egtb_last_error(char *buf, size_t len);
 
 /* Library version string, e.g. "egtb_gpu 0.1 sm_100a". */
-const char *egtb_version(void);
+EGTB_API const char *egtb_version(void);
 
 /* Number of visible CUDA devices (0 when none). */
-int egtb_device_count(void);
+EGTB_API int egtb_device_count(void);
 
 /* ---------------------------------------------------------- progress ---- */
 
 /* get_build_progress / reset_build_progress,
  * native_core/src/bindings_formation.cpp:140-155, FormationRuntime.h:57-84 */
-int egtb_get_build_progress(uint32_t *current, uint32_t *total);
-int egtb_reset_build_progress(uint32_t total);
+EGTB_API int egtb_get_build_progress(uint32_t *current, uint32_t *total);
+EGTB_API int egtb_reset_build_progress(uint32_t total);
 
 /* ------------------------------------------------------------ build ----- */
 
@@ -139,7 +145,7 @@ int egtb_reset_build_progress(uint32_t total);
  * With no layer files present the whole build stays in device memory and
  * only books are written; with layer files present it resumes through
  * egtb_generate + egtb_solve like the reference. stats may be NULL. */
-int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec *spec,
+EGTB_API int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec *spec,
                const egtb_run_options *options, egtb_build_stats *stats);
 
 /* run_pattern_generate, native_core/src/BookSolver.cpp:766-782 (bound at
@@ -147,14 +153,14 @@ int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec *s
  * <pathname><steps-3> and the success-only books of layers steps-2 and
  * steps-1 (final_steps, BookSolver.cpp:263-284). *started is 0 when every
  * step was already on disk. */
-int egtb_generate(const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec *spec,
+EGTB_API int egtb_generate(const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec *spec,
                   const egtb_run_options *options, int32_t *started, egtb_build_stats *stats);
 
 /* run_pattern_solve, native_core/src/BookSolver.cpp:784-821 (bound at
  * bindings_formation.cpp:210-218): backward pass from the raw layer files.
  * d1/d2 are the packed book records of layers steps-2 and steps-1 (n1/n2
  * records; may be empty, then they are read from their .book files). */
-int egtb_solve(const void *d1_records, size_t n1, const void *d2_records, size_t n2,
+EGTB_API int egtb_solve(const void *d1_records, size_t n1, const void *d2_records, size_t n2,
                const egtb_pattern_spec *spec, const egtb_run_options *options, egtb_build_stats *stats);
 
 /* ------------------------------------------------------- primitives ----- */
@@ -162,9 +168,9 @@ int egtb_solve(const void *d1_records, size_t n1, const void *d2_records, size_t
 /* Batched board primitives on the device, host buffers in and out
  * (move_all_dir native_core/include/CommonMover.h:136-139; canonical_by_mode
  * SymmetryUtils.h:31-49; apply_sym_like SymmetryUtils.h:9-29). */
-int egtb_move_all_dir(int device, const uint64_t *boards, size_t n, uint64_t *out4);
-int egtb_canonical(int device, const uint64_t *boards, size_t n, int32_t symm_mode, uint64_t *out);
-int egtb_apply_sym(int device, const uint64_t *boards, size_t n, int32_t symm_index, uint64_t *out);
+EGTB_API int egtb_move_all_dir(int device, const uint64_t *boards, size_t n, uint64_t *out4);
+EGTB_API int egtb_canonical(int device, const uint64_t *boards, size_t n, int32_t symm_mode, uint64_t *out);
+EGTB_API int egtb_apply_sym(int device, const uint64_t *boards, size_t n, int32_t symm_index, uint64_t *out);
 
 /* ------------------------------------------------------------ books ----- */
 
@@ -175,12 +181,12 @@ typedef struct egtb_book egtb_book;
  * ClassicBookReader, native_core/src/ReaderRuntime.cpp:1050-1067).
  * nums_adjust is the pattern's -(seed tile sum) (Config.py:265). Layers
  * are loaded on first use; max_layers bounds the layer index scanned. */
-int egtb_book_open(const char *dir, const char *pattern_full, int32_t dtype, const egtb_pattern_spec *spec,
+EGTB_API int egtb_book_open(const char *dir, const char *pattern_full, int32_t dtype, const egtb_pattern_spec *spec,
                    int64_t nums_adjust, int32_t device, egtb_book **out);
-int egtb_book_close(egtb_book *book);
+EGTB_API int egtb_book_close(egtb_book *book);
 
 /* Load every book layer of the table now (otherwise loaded on first lookup). */
-int egtb_book_load_all(egtb_book *book, int32_t *layers_loaded);
+EGTB_API int egtb_book_load_all(egtb_book *book, int32_t *layers_loaded);
 
 /* Batched move_on_dic on encoded positions (encode_board_matrix,
  * native_core/include/BoardCodec.h:20-30), host buffers, op order
@@ -191,18 +197,18 @@ int egtb_book_load_all(egtb_book *book, int32_t *layers_loaded);
  * (bit d set when direction d has a numeric value) and the operation index
  * that matched (-1 when none; -2 when the layer index is negative; -3 when
  * the layer's book file does not exist). */
-int egtb_book_lookup(egtb_book *book, const uint64_t *positions, size_t n, int32_t last_op,
+EGTB_API int egtb_book_lookup(egtb_book *book, const uint64_t *positions, size_t n, int32_t last_op,
                      double *values4, uint8_t *valid_mask, int8_t *op_used);
 
 /* Same on device memory and a caller stream (cudaStream_t passed as void*),
  * float32 values; used by the serving loop. Layers must be loaded. */
-int egtb_book_lookup_device(egtb_book *book, const uint64_t *d_positions, size_t n, int32_t last_op,
+EGTB_API int egtb_book_lookup_device(egtb_book *book, const uint64_t *d_positions, size_t n, int32_t last_op,
                             float *d_values4, uint8_t *d_valid_mask, void *stream);
 
 /* find_classic_value, native_core/src/ReaderRuntime.cpp:1107-1133 (bound at
  * bindings_formation.cpp:180-194): the normalised value of one key in one
  * book file; *found = 0 when the file does not exist (value 0 then). */
-int egtb_find_classic_value(const char *pathname, const char *filename, uint64_t key, int32_t dtype,
+EGTB_API int egtb_find_classic_value(const char *pathname, const char *filename, uint64_t key, int32_t dtype,
                             int32_t device, double *value, int32_t *found);
 
 #ifdef __cplusplus

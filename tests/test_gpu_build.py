@@ -1,0 +1,153 @@
+"""GPU builds through the drop-in formation_core (C ABI) against the
+reference's own layer files and books (SHA-256 per file, tests/golden)."""
+import os
+
+import numpy as np
+import pytest
+
+import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def _generate(case, d):
+    F = H.fc()
+    spec, o = H.spec_options(case, d + case["pattern_full"] + "_")
+    started, l0, l1 = F.run_pattern_generate(H.seeds(case), spec, o)
+    return started, l0, l1
+
+
+@pytest.mark.parametrize("key", H.SMALL_CASES)
+def test_generate_raw_layers_bit_exact(key, tmp_root):
+    case = H.cases()[key]
+    d = H.fresh(os.path.join(tmp_root, "gen_" + key) + "/")
+    started, l0, l1 = _generate(case, d)
+    assert started
+    steps = case["steps"]
+    name = case["pattern_full"]
+    for t in range(steps - 2):
+        p = d + f"{name}_{t}"
+        if t == steps - 2:
+            continue
+        assert os.path.exists(p), p
+        assert os.path.getsize(p) // 8 == case["raw_len"][t], (key, t)
+        assert H.sha(p) == case["raw_sha256"][t], (key, t)
+    # the last two layers are written as success-only books
+    for t in (steps - 2, steps - 1):
+        assert H.sha(d + f"{name}_{t}.book") == case["book_sha256"][t], (key, t)
+    assert l0.size == case["book_len"][steps - 2] and l1.size == case["book_len"][steps - 1]
+
+
+@pytest.mark.parametrize("key", H.SMALL_CASES)
+def test_build_books_bit_exact(key, tmp_root):
+    case = H.cases()[key]
+    F = H.fc()
+    d = H.fresh(os.path.join(tmp_root, "build_" + key) + "/")
+    spec, o = H.spec_options(case, d + case["pattern_full"] + "_")
+    F.run_pattern_build(H.seeds(case), spec, o)
+    name = case["pattern_full"]
+    for t in range(case["steps"]):
+        p = d + f"{name}_{t}.book"
+        assert H.sha(p) == case["book_sha256"][t], (key, t)
+    # no raw layer is left behind, as after the reference's solve
+    assert not any(os.path.exists(d + f"{name}_{t}") for t in range(case["steps"]))
+    st = F.last_build_stats()
+    assert st["raw_boards"] >= sum(case["raw_len"])
+    assert st["book_entries"] == sum(case["book_len"])
+    lines = open(d + f"{name}_stats.txt").read().splitlines()
+    assert lines[0] == "layer,length,max success rate,speed,deletion_threshold,time"
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("key", H.FULL_CASES)
+def test_full_size_build_bit_exact(key, tmp_root):
+    """The benchmark tables at full size (L3-256, 442-512)."""
+    case = H.cases()[key]
+    F = H.fc()
+    d = H.fresh(os.path.join(tmp_root, "full_" + key) + "/")
+    spec, o = H.spec_options(case, d + case["pattern_full"] + "_")
+    F.run_pattern_build(H.seeds(case), spec, o)
+    name = case["pattern_full"]
+    bad = [t for t in range(case["steps"]) if H.sha(d + f"{name}_{t}.book") != case["book_sha256"][t]]
+    assert not bad, bad[:10]
+    st = F.last_build_stats()
+    assert st["raw_boards"] >= sum(case["raw_len"])
+    assert st["book_entries"] == sum(case["book_len"])
+    H.fresh(d)
+
+
+@pytest.mark.parametrize("key", ["L3_32_float32", "diag9_64_float32", "L3_32_uint32"])
+def test_generate_then_solve_matches_build(key, tmp_root):
+    """run_pattern_generate + run_pattern_solve (the file-based path) give the reference's books."""
+    case = H.cases()[key]
+    F = H.fc()
+    d = H.fresh(os.path.join(tmp_root, "gs_" + key) + "/")
+    spec, o = H.spec_options(case, d + case["pattern_full"] + "_")
+    started, l0, l1 = F.run_pattern_generate(H.seeds(case), spec, o)
+    F.run_pattern_solve(l0, l1, spec, o)
+    name = case["pattern_full"]
+    for t in range(case["steps"]):
+        assert H.sha(d + f"{name}_{t}.book") == case["book_sha256"][t], (key, t)
+
+
+def test_resume_after_interrupted_forward(tmp_root):
+    """Raw layers from an interrupted run: the forward restarts at the first missing step."""
+    case = H.cases()["L3_32_float32"]
+    F = H.fc()
+    d = H.fresh(os.path.join(tmp_root, "resume") + "/")
+    name = case["pattern_full"]
+    spec, o = H.spec_options(case, d + name + "_")
+    F.run_pattern_generate(H.seeds(case), spec, o)
+    # keep raw layers 0..20 only, as if the run stopped after step 20
+    for f in os.listdir(d):
+        stem = f.split("_")[-1]
+        if stem.endswith(".book") or (stem.isdigit() and int(stem) > 20):
+            os.remove(d + f)
+    F.run_pattern_build(H.seeds(case), spec, o)
+    for t in range(case["steps"]):
+        assert H.sha(d + f"{name}_{t}.book") == case["book_sha256"][t], t
+
+
+def test_resume_after_interrupted_solve(tmp_root):
+    """Books of the top layers present: the solve restarts below them."""
+    case = H.cases()["44_64_float32"]
+    F = H.fc()
+    d = H.fresh(os.path.join(tmp_root, "resume2") + "/")
+    name = case["pattern_full"]
+    spec, o = H.spec_options(case, d + name + "_")
+    started, l0, l1 = F.run_pattern_generate(H.seeds(case), spec, o)
+    F.run_pattern_solve(l0, l1, spec, o)
+    # drop the books of layers 0..30 and put their raw layers back
+    F2 = H.fresh(os.path.join(tmp_root, "resume2_raw") + "/")
+    spec2, o2 = H.spec_options(case, F2 + name + "_")
+    F.run_pattern_generate(H.seeds(case), spec2, o2)
+    for t in range(31):
+        os.remove(d + f"{name}_{t}.book")
+        os.replace(F2 + f"{name}_{t}", d + f"{name}_{t}")
+    F.run_pattern_solve(F.PatternLayer(), F.PatternLayer(), spec, o)
+    for t in range(case["steps"]):
+        assert H.sha(d + f"{name}_{t}.book") == case["book_sha256"][t], t
+
+
+def test_progress_reaches_total(tmp_root):
+    case = H.cases()["44_64_float32"]
+    F = H.fc()
+    d = H.fresh(os.path.join(tmp_root, "progress") + "/")
+    spec, o = H.spec_options(case, d + case["pattern_full"] + "_")
+    F.reset_build_progress(0)
+    F.run_pattern_build(H.seeds(case), spec, o)
+    cur, tot = F.get_build_progress()
+    assert tot == 2 * case["steps"] and cur == tot
+
+
+def test_invalid_options_raise(tmp_root):
+    F = H.fc()
+    case = H.cases()["44_64_float32"]
+    spec, o = H.spec_options(case, os.path.join(tmp_root, "bad_"))
+    o.is_variant = True
+    with pytest.raises(RuntimeError, match="variant"):
+        F.run_pattern_build(H.seeds(case), spec, o)
+    o.is_variant = False
+    spec.symm_mode = 4
+    with pytest.raises(RuntimeError, match="symmetry"):
+        F.run_pattern_build(H.seeds(case), spec, o)

@@ -1,0 +1,65 @@
+"""The CPU oracle (oracle/egtb_oracle.c) against the reference's own outputs
+(tests/golden, produced by tests/golden/make_golden.py from the reference
+compiled out of its sources). This pins the oracle the GPU tests check against."""
+import numpy as np
+import pytest
+
+import helpers as H
+import oracle as O
+
+
+def test_row_tables_match_reference():
+    p = H.prims()
+    left, right = O.row_tables()
+    assert np.array_equal(left, p["row_left"])
+    assert np.array_equal(right, p["row_right"])
+
+
+def test_moves_match_reference():
+    p = H.prims()
+    assert np.array_equal(O.move_all_dir(p["boards"]), p["moves"])
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_canonical_match_reference(mode):
+    p = H.prims()
+    assert np.array_equal(O.canonical(p["boards"], mode), p[f"canonical_{mode}"])
+
+
+@pytest.mark.parametrize("idx", range(8))
+def test_symmetries_match_reference(idx):
+    p = H.prims()
+    b = p["boards"][:2000]
+    got = np.array([O.apply_sym(int(x), idx) for x in b], dtype=np.uint64)
+    assert np.array_equal(got, p[f"sym_{idx}"][:2000])
+
+
+def _build(case):
+    spec = O.Spec([int(m, 16) for m in case["masks"]], case["shifts"], case["symm_mode"])
+    return O.Build(H.seeds(case), spec, case["target"], case["steps"], case["docheck_step"])
+
+
+@pytest.mark.parametrize("key", H.SMALL_CPU_CASES)
+def test_oracle_raw_layers_and_books(key):
+    case = H.cases()[key]
+    b = _build(case)
+    steps = case["steps"]
+    for t in range(steps - 2):
+        layer = b.layer(t)
+        assert len(layer) == case["raw_len"][t], (key, t)
+        assert H.sha_bytes(layer.astype("<u8").tobytes()) == case["raw_sha256"][t], (key, t)
+    assert [len(b.layer(steps - 2)), len(b.layer(steps - 1))] >= [0, 0]
+    b.solve(case["dtype"], case["spawn_rate4"])
+    for t in range(steps):
+        book = b.book(t, case["dtype"])
+        assert H.sha_bytes(book) == case["book_sha256"][t], (key, t)
+
+
+def test_free5_book_data_fixture():
+    """One complete build kept as data: the oracle's books byte for byte."""
+    case = H.cases()["free5_32_float32"]
+    data = np.load(H.os.path.join(H.GOLDEN, "free5_32.npz"))
+    b = _build(case)
+    b.solve("float32", 0.1)
+    for t in range(case["steps"]):
+        assert b.book(t, "float32") == data[f"book_{t}"].tobytes(), t
