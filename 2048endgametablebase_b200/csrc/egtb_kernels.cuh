@@ -118,6 +118,7 @@ expand_kernel(const uint64_t *__restrict__ arena, const unsigned long long *__re
               DevCtl *ctl, int which1, int which2, unsigned long long cap, uint64_t *filter, int filter_bits) {
     __shared__ uint64_t stage[kExpandThreads / 32][2][kStage];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (ctl->err & kErrArenaOverflow) return;
     const unsigned long long n = layer_len[t];
     const uint64_t *par = arena + layer_off[t];
     int cnt[2] = {0, 0};
@@ -356,10 +357,19 @@ tile_scan_kernel(const unsigned long long *n_ptr, unsigned long long cap, unsign
 __global__ void close_layer_kernel(int t, const unsigned long long *total, unsigned long long *layer_off,
                                    unsigned long long *layer_len, unsigned long long arena_cap, DevCtl *ctl) {
     const unsigned long long n = *total;
-    layer_len[t] = n;
     const unsigned long long end = layer_off[t] + n;
-    layer_off[t + 1] = (end + kSplitStride - 1) & ~(unsigned long long)(kSplitStride - 1);
-    if (layer_off[t + 1] > arena_cap) atomicOr(&ctl->err, kErrArenaOverflow);
+    const unsigned long long next = (end + kSplitStride - 1) & ~(unsigned long long)(kSplitStride - 1);
+    if (next > arena_cap || (ctl->err & kErrArenaOverflow)) {
+        // does not fit: flag it and leave the layer empty, so every later
+        // kernel of this pass stays inside the arena; the host re-runs the
+        // pass with a larger arena
+        atomicOr(&ctl->err, kErrArenaOverflow);
+        layer_len[t] = 0;
+        layer_off[t + 1] = layer_off[t];
+        return;
+    }
+    layer_len[t] = n;
+    layer_off[t + 1] = next;
 }
 
 // Write the unique keys of a sorted run as layer t of the arena, with the
