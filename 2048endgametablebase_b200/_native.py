@@ -80,10 +80,15 @@ class BuildStatsC(ctypes.Structure):
         ("forward_ms", ctypes.c_double),
         ("backward_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
+        ("kernel_launches", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class KernelTimeC(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_uint64), ("total_ms", ctypes.c_double)]
 
 
 # every entry point of include/egtb_gpu.h with its ctypes signature
@@ -92,6 +97,10 @@ _SIGS = {
     "egtb_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
     "egtb_version": (ctypes.c_char_p, []),
     "egtb_device_count": (ctypes.c_int, []),
+    "egtb_set_stream": (ctypes.c_int, [ctypes.c_int, _P]),
+    "egtb_profile": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    "egtb_profile_read": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(KernelTimeC), ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_int)]),
     "egtb_get_build_progress": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
     "egtb_reset_build_progress": (ctypes.c_int, [ctypes.c_uint32]),
     "egtb_build": (ctypes.c_int, [_P, ctypes.c_size_t, ctypes.POINTER(PatternSpecC), ctypes.POINTER(RunOptionsC),
@@ -150,6 +159,21 @@ def last_error() -> str:
 def check(rc: int) -> None:
     if rc != EGTB_OK:
         raise NativeError(rc, f"{ERR_NAMES.get(rc, rc)}: {last_error()}")
+
+
+def profile(device: int, enable: bool) -> None:
+    check(lib().egtb_profile(int(device), int(bool(enable))))
+
+
+def profile_read(device: int) -> dict[str, tuple[int, float]]:
+    arr = (KernelTimeC * 16)()
+    n = ctypes.c_int(0)
+    check(lib().egtb_profile_read(int(device), arr, 16, ctypes.byref(n)))
+    return {arr[i].name.decode(): (int(arr[i].launches), float(arr[i].total_ms)) for i in range(n.value)}
+
+
+def set_stream(device: int, stream_ptr: int | None) -> None:
+    check(lib().egtb_set_stream(int(device), ctypes.c_void_p(stream_ptr or None)))
 
 
 def device_count() -> int:

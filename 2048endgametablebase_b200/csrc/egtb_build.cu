@@ -85,9 +85,67 @@ __global__ void progress_kernel(unsigned *p, unsigned v) {
 
 static unsigned long long align16(unsigned long long x) { return (x + 15ull) & ~15ull; }
 
+// Launch a kernel on the engine's stream and count it.
+#define EGTB_LAUNCH(E, ...)  \
+    do {                     \
+        __VA_ARGS__;         \
+        ++(E).launches;      \
+    } while (0)
+
+static const char *kKindNames[] = {"expand", "sort_pass", "unique", "solve", "book_pack", "final_layers"};
+enum { K_EXPAND = 0, K_SORT_PASS, K_UNIQUE, K_SOLVE, K_PACK, K_FINAL, K_NKINDS };
+
 struct Engine {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // stream in use
+    cudaStream_t own_stream = nullptr;  // the library's stream
+    unsigned long long launches = 0;
+    // per-kind device timing
+    bool prof = false;
+    struct ProfPair {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    std::vector<ProfPair> prof_pending;
+    std::vector<cudaEvent_t> prof_pool;
+    unsigned long long prof_launches[K_NKINDS] = {};
+    double prof_ms[K_NKINDS] = {};
+
+    int prof_begin(int kind) {
+        if (!prof) return -1;
+        cudaEvent_t a, b;
+        if (prof_pool.size() >= 2) {
+            a = prof_pool.back();
+            prof_pool.pop_back();
+            b = prof_pool.back();
+            prof_pool.pop_back();
+        } else {
+            EGTB_CUDA(cudaEventCreate(&a));
+            EGTB_CUDA(cudaEventCreate(&b));
+        }
+        EGTB_CUDA(cudaEventRecord(a, stream));
+        prof_pending.push_back({kind, a, b});
+        return (int)prof_pending.size() - 1;
+    }
+    void prof_end(int idx) {
+        if (idx < 0) return;
+        EGTB_CUDA(cudaEventRecord(prof_pending[idx].b, stream));
+    }
+    // after a stream synchronisation: fold the recorded pairs into the totals
+    void prof_resolve() {
+        for (auto &p : prof_pending) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+                prof_ms[p.kind] += ms;
+                prof_launches[p.kind] += 1;
+            } else {
+                cudaGetLastError();
+            }
+            prof_pool.push_back(p.a);
+            prof_pool.push_back(p.b);
+        }
+        prof_pending.clear();
+    }
     const uint32_t *tab = nullptr;
     std::mutex mu;
 
@@ -123,7 +181,8 @@ struct Engine {
     void init(int dev) {
         device = dev;
         EGTB_CUDA(cudaSetDevice(dev));
-        EGTB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        EGTB_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+        stream = own_stream;
         tab = device_row_table();
         cudaDeviceProp prop;
         EGTB_CUDA(cudaGetDeviceProperties(&prop, dev));
@@ -309,18 +368,20 @@ static void enqueue_sort_unique(Engine &E, const ForwardPlan &P, int x, int L) {
     int p = 0;
     for (int sh : P.shifts) {
         unsigned *dt = E.digit_tot + 256 * p;
-        radix_count_kernel<<<g_sort, kSortThreads, 0, s>>>(src, n_ptr, E.cand_cap, sh, E.tile_hist, E.sort_tiles, dt);
-        radix_scan_kernel<<<256, 1024, 0, s>>>(n_ptr, E.cand_cap, E.tile_hist, E.sort_tiles, dt);
-        radix_scatter_kernel<<<g_sort, kSortThreads, 0, s>>>(src, dst, n_ptr, E.cand_cap, sh, E.tile_hist,
-                                                             E.sort_tiles, dt);
+        const int pi = E.prof_begin(K_SORT_PASS);
+        EGTB_LAUNCH(E, radix_count_kernel<<<g_sort, kSortThreads, 0, s>>>(src, n_ptr, E.cand_cap, sh, E.tile_hist, E.sort_tiles, dt));
+        EGTB_LAUNCH(E, radix_scan_kernel<<<256, 1024, 0, s>>>(n_ptr, E.cand_cap, E.tile_hist, E.sort_tiles, dt));
+        EGTB_LAUNCH(E, radix_scatter_kernel<<<g_sort, kSortThreads, 0, s>>>(src, dst, n_ptr, E.cand_cap, sh, E.tile_hist, E.sort_tiles, dt));
+        E.prof_end(pi);
         std::swap(src, dst);
         ++p;
     }
-    unique_count_kernel<<<g_sort, kSortThreads, 0, s>>>(src, n_ptr, E.cand_cap, E.tile_cnt);
-    tile_scan_kernel<<<1, 1024, 0, s>>>(n_ptr, E.cand_cap, E.tile_off, E.tile_cnt, &E.ctl->n_unique);
-    close_layer_kernel<<<1, 1, 0, s>>>(L, &E.ctl->n_unique, E.layer_off, E.layer_len, E.arena_cap, E.ctl);
-    unique_write_kernel<<<g_sort, kSortThreads, 0, s>>>(src, n_ptr, E.cand_cap, E.tile_off, E.arena, E.split,
-                                                         E.layer_off, L, E.arena_cap);
+    const int pu = E.prof_begin(K_UNIQUE);
+    EGTB_LAUNCH(E, unique_count_kernel<<<g_sort, kSortThreads, 0, s>>>(src, n_ptr, E.cand_cap, E.tile_cnt));
+    EGTB_LAUNCH(E, tile_scan_kernel<<<1, 1024, 0, s>>>(n_ptr, E.cand_cap, E.tile_off, E.tile_cnt, &E.ctl->n_unique));
+    EGTB_LAUNCH(E, close_layer_kernel<<<1, 1, 0, s>>>(L, &E.ctl->n_unique, E.layer_off, E.layer_len, E.arena_cap, E.ctl));
+    EGTB_LAUNCH(E, unique_write_kernel<<<g_sort, kSortThreads, 0, s>>>(src, n_ptr, E.cand_cap, E.tile_off, E.arena, E.split, E.layer_off, L, E.arena_cap));
+    E.prof_end(pu);
 }
 
 __global__ void add_candidates_kernel(DevCtl *ctl, int x) { ctl->candidates += ctl->cand_count[x]; }
@@ -336,15 +397,15 @@ static void enqueue_forward(Engine &E, const ForwardPlan &P, unsigned *progress)
         const int t = i - 1;
         const int x1 = i & 1, x2 = (i + 1) & 1;
         EGTB_CUDA(cudaMemsetAsync(&E.ctl->cand_count[x2], 0, sizeof(unsigned long long), s));
-        expand_kernel<<<g_exp, kExpandThreads, 0, s>>>(E.arena, E.layer_off, E.layer_len, t, P.spec,
-                                                       i > P.docheck ? 1 : 0, E.tab, E.cand[x1], E.cand[x2], E.ctl,
-                                                       x1, x2, E.cand_cap, E.filter, E.filter_bits);
-        add_candidates_kernel<<<1, 1, 0, s>>>(E.ctl, x1);
+        const int pe = E.prof_begin(K_EXPAND);
+        EGTB_LAUNCH(E, expand_kernel<<<g_exp, kExpandThreads, 0, s>>>(E.arena, E.layer_off, E.layer_len, t, P.spec, i > P.docheck ? 1 : 0, E.tab, E.cand[x1], E.cand[x2], E.ctl, x1, x2, E.cand_cap, E.filter, E.filter_bits));
+        E.prof_end(pe);
+        EGTB_LAUNCH(E, add_candidates_kernel<<<1, 1, 0, s>>>(E.ctl, x1));
         enqueue_sort_unique(E, P, x1, i);
-        progress_kernel<<<1, 1, 0, s>>>(progress, (unsigned)i);
+        EGTB_LAUNCH(E, progress_kernel<<<1, 1, 0, s>>>(progress, (unsigned)i));
     }
     const int L = P.steps - 1;
-    add_candidates_kernel<<<1, 1, 0, s>>>(E.ctl, L & 1);
+    EGTB_LAUNCH(E, add_candidates_kernel<<<1, 1, 0, s>>>(E.ctl, L & 1));
     enqueue_sort_unique(E, P, L & 1, L);
 }
 
@@ -402,6 +463,7 @@ static int run_forward(Engine &E, const ForwardPlan &P, const uint64_t *base, si
         EGTB_CUDA(cudaEventRecord(E.ev[1], E.stream));
         DevCtl c = read_ctl(E);
         EGTB_CUDA(cudaGetLastError());
+        E.prof_resolve();
         if (c.err == 0) {
             EGTB_CUDA(cudaEventElapsedTime(ms, E.ev[0], E.ev[1]));
             return retries;
@@ -459,17 +521,15 @@ template <typename T>
 static void enqueue_pack(Engine &E, int t, T zero) {
     cudaStream_t s = E.stream;
     const int g = E.sm_count * 4;
-    book_count_kernel<T><<<g, kSortThreads, 0, s>>>((const T *)E.rates, E.layer_off, E.layer_len, t, zero, E.tile_cnt);
-    tile_scan_kernel<<<1, 1024, 0, s>>>(E.layer_len + t, E.arena_cap, E.tile_off, E.tile_cnt, &E.ctl->n_unique);
-    book_len_kernel<<<1, 1, 0, s>>>(&E.ctl->n_unique, E.book_len, t);
+    EGTB_LAUNCH(E, book_count_kernel<T><<<g, kSortThreads, 0, s>>>((const T *)E.rates, E.layer_off, E.layer_len, t, zero, E.tile_cnt));
+    EGTB_LAUNCH(E, tile_scan_kernel<<<1, 1024, 0, s>>>(E.layer_len + t, E.arena_cap, E.tile_off, E.tile_cnt, &E.ctl->n_unique));
+    EGTB_LAUNCH(E, book_len_kernel<<<1, 1, 0, s>>>(&E.ctl->n_unique, E.book_len, t));
 }
 
 template <typename T>
 static void enqueue_pack_write(Engine &E, int t, T zero, unsigned long long book_off_bytes) {
     const int g = E.sm_count * 4;
-    book_write_kernel<T><<<g, kSortThreads, 0, E.stream>>>(E.arena, (const T *)E.rates, E.layer_off, E.layer_len, t,
-                                                           zero, E.tile_off, E.book, book_off_bytes,
-                                                           E.book_cap_bytes, E.ctl);
+    EGTB_LAUNCH(E, book_write_kernel<T><<<g, kSortThreads, 0, E.stream>>>(E.arena, (const T *)E.rates, E.layer_off, E.layer_len, t, zero, E.tile_off, E.book, book_off_bytes, E.book_cap_bytes, E.ctl));
 }
 
 struct BackwardPlan {
@@ -488,19 +548,24 @@ static void enqueue_backward(Engine &E, const BackwardPlan &B, const std::vector
     const int g = E.sm_count * 8;
     T *rates = (T *)E.rates;
     const uint32_t total = (uint32_t)(B.steps * 2);
+    const int pf = E.prof_begin(K_FINAL);
     for (int t = B.steps - 2; t < B.steps; ++t)
-        if (t >= 0) final_layer_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec, zero, maxv);
+        if (t >= 0) EGTB_LAUNCH(E, final_layer_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec, zero, maxv));
+    E.prof_end(pf);
     for (int t = B.steps - 3; t >= 0; --t) {
-        progress_kernel<<<1, 1, 0, s>>>(progress, total - (unsigned)t - 2u);
-        solve_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.split, E.layer_off, E.layer_len, t, B.spec,
-                                          t > B.docheck ? 1 : 0, E.tab, B.p4, zero, maxv, E.ctl);
+        EGTB_LAUNCH(E, progress_kernel<<<1, 1, 0, s>>>(progress, total - (unsigned)t - 2u));
+        const int ps = E.prof_begin(K_SOLVE);
+        EGTB_LAUNCH(E, solve_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.split, E.layer_off, E.layer_len, t, B.spec, t > B.docheck ? 1 : 0, E.tab, B.p4, zero, maxv, E.ctl));
+        E.prof_end(ps);
     }
     EGTB_CUDA(cudaMemsetAsync(E.layer_max, 0, sizeof(unsigned long long) * E.steps_cap, s));
     const size_t rec = 8 + sizeof(T);
     for (int t = 0; t < B.steps; ++t) {
+        const int pp = E.prof_begin(K_PACK);
         enqueue_pack<T>(E, t, zero);
         enqueue_pack_write<T>(E, t, zero, off[t] * rec);
-        layer_max_kernel<T><<<E.sm_count, 256, 0, s>>>(rates, E.layer_off, E.layer_len, t, zero, E.layer_max);
+        E.prof_end(pp);
+        EGTB_LAUNCH(E, layer_max_kernel<T><<<E.sm_count, 256, 0, s>>>(rates, E.layer_off, E.layer_len, t, zero, E.layer_max));
     }
 }
 
@@ -635,6 +700,7 @@ template <typename T>
 static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec &spec,
                         const egtb_run_options &o, egtb_build_stats *st) {
     const auto t_start = std::chrono::steady_clock::now();
+    const unsigned long long launches0 = E.launches;
     const int steps = o.steps;
     const uint32_t total = (uint32_t)(steps * 2);
     set_progress(0, total);
@@ -650,6 +716,7 @@ static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const 
     EGTB_CUDA(cudaStreamSynchronize(E.stream));
     EGTB_CUDA(cudaGetLastError());
     EGTB_CUDA(cudaEventElapsedTime(&bwd_ms, E.ev[2], E.ev[3]));
+    E.prof_resolve();
     DevCtl c = read_ctl(E);
     if (c.err) throw Error(EGTB_ERR_CAPACITY, "book buffer overflow");
     std::vector<unsigned long long> blen = d2h_u64(E, E.book_len, steps);
@@ -672,8 +739,10 @@ static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const 
     set_progress(total, total);
     if (st) {
         std::memset(st, 0, sizeof *st);
+        // raw boards of layers 0..steps-3: the layers the solve computes and
+        // stats.txt lists (the last two layers keep only their successes)
         for (int t = 0; t < steps; ++t) {
-            st->raw_boards += len[t];
+            if (t <= steps - 3) st->raw_boards += len[t];
             st->book_entries += blen[t];
             st->max_layer = std::max<uint64_t>(st->max_layer, len[t]);
         }
@@ -684,6 +753,7 @@ static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const 
         st->forward_ms = fwd_ms;
         st->backward_ms = bwd_ms;
         st->total_ms = ms_since(t_start);
+        st->kernel_launches = E.launches - launches0;
     }
 }
 
@@ -734,8 +804,7 @@ static void generate_files(Engine &E, const uint64_t *seeds, size_t n_seeds, con
         DevSpec ds = make_dev_spec(spec, o.target);
         EGTB_CUDA(cudaMemsetAsync(E.ctl, 0, sizeof(DevCtl), E.stream));
         for (int t = steps - 2; t < steps; ++t) {
-            final_layer_kernel<T><<<E.sm_count * 4, 256, 0, E.stream>>>(E.arena, (T *)E.rates, E.layer_off,
-                                                                          E.layer_len, t, ds, zero, maxv);
+            EGTB_LAUNCH(E, final_layer_kernel<T><<<E.sm_count * 4, 256, 0, E.stream>>>(E.arena, (T *)E.rates, E.layer_off, E.layer_len, t, ds, zero, maxv));
             enqueue_pack<T>(E, t, zero);
             enqueue_pack_write<T>(E, t, zero, off[t] * rec);
         }
@@ -747,7 +816,7 @@ static void generate_files(Engine &E, const uint64_t *seeds, size_t n_seeds, con
         write_ranges(E, E.book, bpaths, boff, bbytes, writer_threads(o));
         if (st) {
             std::memset(st, 0, sizeof *st);
-            for (int t = i0; t < steps; ++t) {
+            for (int t = i0; t <= steps - 3; ++t) {
                 st->raw_boards += len[t];
                 st->max_layer = std::max<uint64_t>(st->max_layer, len[t]);
             }
@@ -834,8 +903,8 @@ static void solve_files(Engine &E, const void *d1_recs, size_t n1, const void *d
         if (n > slot) throw Error(EGTB_ERR_CAPACITY, "layer larger than its slot");
         if (n) {
             EGTB_CUDA(cudaMemcpyAsync(d_stage, recs.data(), n * rec, cudaMemcpyHostToDevice, s));
-            unpack_records_kernel<T><<<E.sm_count * 4, 256, 0, s>>>(d_stage, n, E.arena + sl * slot, rates + sl * slot);
-            splitters_kernel<<<E.sm_count, 256, 0, s>>>(E.arena + sl * slot, n, E.split + sl * slot / kSplitStride);
+            EGTB_LAUNCH(E, unpack_records_kernel<T><<<E.sm_count * 4, 256, 0, s>>>(d_stage, n, E.arena + sl * slot, rates + sl * slot));
+            EGTB_LAUNCH(E, splitters_kernel<<<E.sm_count, 256, 0, s>>>(E.arena + sl * slot, n, E.split + sl * slot / kSplitStride));
             EGTB_CUDA(cudaStreamSynchronize(s));
         }
         return n;
@@ -882,12 +951,11 @@ static void solve_files(Engine &E, const void *d1_recs, size_t n1, const void *d
         EGTB_CUDA(cudaMemsetAsync(E.ctl, 0, sizeof(DevCtl), s));
         EGTB_CUDA(cudaMemsetAsync(E.layer_max, 0, sizeof(unsigned long long) * 4, s));
         const auto t0 = std::chrono::steady_clock::now();
-        solve_kernel<T><<<E.sm_count * 8, 256, 0, s>>>(E.arena, rates, E.split, E.layer_off, E.layer_len, 0, ds,
-                                                        i > o.docheck_step ? 1 : 0, E.tab, o.spawn_rate4, zero, maxv, E.ctl);
-        splitters_kernel<<<E.sm_count, 256, 0, s>>>(k0, n0, E.split + slot_of[0] * slot / kSplitStride);
+        EGTB_LAUNCH(E, solve_kernel<T><<<E.sm_count * 8, 256, 0, s>>>(E.arena, rates, E.split, E.layer_off, E.layer_len, 0, ds, i > o.docheck_step ? 1 : 0, E.tab, o.spawn_rate4, zero, maxv, E.ctl));
+        EGTB_LAUNCH(E, splitters_kernel<<<E.sm_count, 256, 0, s>>>(k0, n0, E.split + slot_of[0] * slot / kSplitStride));
         enqueue_pack<T>(E, 0, zero);
         enqueue_pack_write<T>(E, 0, zero, 0);
-        layer_max_kernel<T><<<E.sm_count, 256, 0, s>>>(rates, E.layer_off, E.layer_len, 0, zero, E.layer_max);
+        EGTB_LAUNCH(E, layer_max_kernel<T><<<E.sm_count, 256, 0, s>>>(rates, E.layer_off, E.layer_len, 0, zero, E.layer_max));
         unsigned long long nb = 0, mb = 0;
         EGTB_CUDA(cudaMemcpyAsync(&nb, E.book_len, 8, cudaMemcpyDeviceToHost, s));
         EGTB_CUDA(cudaMemcpyAsync(&mb, E.layer_max, 8, cudaMemcpyDeviceToHost, s));
@@ -999,6 +1067,46 @@ extern "C" int egtb_device_count(void) {
     return n;
 }
 
+extern "C" int egtb_set_stream(int device, void *stream) {
+    return guarded([&] {
+        Engine &E = engine_for(device);
+        std::lock_guard<std::mutex> lk(E.mu);
+        EGTB_CUDA(cudaStreamSynchronize(E.stream));
+        E.stream = stream ? (cudaStream_t)stream : E.own_stream;
+    });
+}
+
+extern "C" int egtb_profile(int device, int enable) {
+    return guarded([&] {
+        Engine &E = engine_for(device);
+        std::lock_guard<std::mutex> lk(E.mu);
+        E.prof_resolve();
+        E.prof = enable != 0;
+        for (int k = 0; k < K_NKINDS; ++k) {
+            E.prof_launches[k] = 0;
+            E.prof_ms[k] = 0.0;
+        }
+    });
+}
+
+extern "C" int egtb_profile_read(int device, egtb_kernel_time *out, int max_kinds, int *n_kinds) {
+    return guarded([&] {
+        if (!out || !n_kinds) throw Error(EGTB_ERR_ARG, "NULL argument");
+        Engine &E = engine_for(device);
+        std::lock_guard<std::mutex> lk(E.mu);
+        E.prof_resolve();
+        int n = 0;
+        for (int k = 0; k < K_NKINDS && n < max_kinds; ++k) {
+            std::memset(&out[n], 0, sizeof out[n]);
+            std::strncpy(out[n].name, kKindNames[k], sizeof out[n].name - 1);
+            out[n].launches = E.prof_launches[k];
+            out[n].total_ms = E.prof_ms[k];
+            ++n;
+        }
+        *n_kinds = n;
+    });
+}
+
 extern "C" int egtb_get_build_progress(uint32_t *current, uint32_t *total) {
     if (!current || !total) return EGTB_ERR_ARG;
     // get_build_progress, native_core/include/FormationRuntime.h:73-82
@@ -1097,7 +1205,7 @@ extern "C" int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_patt
 extern "C" int egtb_move_all_dir(int device, const uint64_t *boards, size_t n, uint64_t *out4) {
     return guarded([&] {
         run_prim(device, boards, n, 4, out4, [&](Engine &E, uint64_t *din, uint64_t *dout) {
-            prim_moves_kernel<<<E.sm_count * 4, 256, 0, E.stream>>>(E.tab, din, n, dout);
+            EGTB_LAUNCH(E, prim_moves_kernel<<<E.sm_count * 4, 256, 0, E.stream>>>(E.tab, din, n, dout));
         });
     });
 }
@@ -1106,7 +1214,7 @@ extern "C" int egtb_canonical(int device, const uint64_t *boards, size_t n, int3
     return guarded([&] {
         if (symm_mode < 0 || symm_mode > 3) throw Error(EGTB_ERR_UNSUPPORTED, "symmetry mode not built");
         run_prim(device, boards, n, 1, out, [&](Engine &E, uint64_t *din, uint64_t *dout) {
-            prim_canonical_kernel<<<E.sm_count * 4, 256, 0, E.stream>>>(din, n, symm_mode, dout);
+            EGTB_LAUNCH(E, prim_canonical_kernel<<<E.sm_count * 4, 256, 0, E.stream>>>(din, n, symm_mode, dout));
         });
     });
 }
@@ -1114,7 +1222,7 @@ extern "C" int egtb_canonical(int device, const uint64_t *boards, size_t n, int3
 extern "C" int egtb_apply_sym(int device, const uint64_t *boards, size_t n, int32_t symm_index, uint64_t *out) {
     return guarded([&] {
         run_prim(device, boards, n, 1, out, [&](Engine &E, uint64_t *din, uint64_t *dout) {
-            prim_sym_kernel<<<E.sm_count * 4, 256, 0, E.stream>>>(din, n, symm_index, dout);
+            EGTB_LAUNCH(E, prim_sym_kernel<<<E.sm_count * 4, 256, 0, E.stream>>>(din, n, symm_index, dout));
         });
     });
 }

@@ -1,0 +1,378 @@
+"""Benchmark of the classic table build on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload 442-512|L3-256]
+
+One step = one complete table build (forward layer generation + backward
+solve + .book packing) of the named table: by default the 442 pattern at
+target 512 (304 layers, 67.7 M raw boards), the configuration the table-build
+metric is quoted on. Metric: raw boards per second (the sum of the raw layer
+sizes 0..steps-3, which is what the reference's stats.txt lists, over the
+build time).
+
+  value : K device-resident builds on one stream (seeds already in HBM's
+          reach, books left in HBM), timed with CUDA events on that stream.
+  e2e   : K builds through the drop-in formation_core.run_pattern_build (the
+          C ABI egtb_build) from host seeds to .book files on local disk
+          (/dev/shm when writable), wall clock around each call.
+  roofline : the dominant kernel's algorithmic bytes over its device time,
+          measured with CUDA events on the launching stream during the timed
+          steps, against MEASURED_PEAKS.json's HBM copy bandwidth.
+  cpu_baseline : the reference's own classic-path code (oracle/_ref, compiled
+          from its sources) building the same table on this host's cores.
+
+Under torchrun each rank builds its own copy of the table (replicas: one
+table does not shard across GPUs without an exchange per layer step);
+time = max over ranks. --impl reference runs the reference's CPU build on
+rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "442-512": ("442", 9),
+    "L3-256": ("L3", 8),
+}
+
+
+def load_peaks() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return 6650.0, "fallback"
+
+
+def workload_params(name: str):
+    pats = importlib.import_module("2048endgametablebase_b200.patterns")
+    pattern, target = WORKLOADS[name]
+    meta = pats.pattern_catalog[pattern]
+    s0 = -int(meta["nums_adjust"])
+    steps, docheck = pats.steps_and_docheck(s0, target, int(meta["extra_steps"]))
+    return pattern, target, meta, steps, docheck
+
+
+def make_spec_options(fc, pattern, target, meta, steps, docheck, pathname, device):
+    spec = fc.PatternSpec()
+    spec.name = pattern
+    spec.pattern_masks = list(meta["pattern_masks"])
+    spec.success_shifts = list(meta["success_shifts"])
+    spec.symm_mode = importlib.import_module("2048endgametablebase_b200.patterns").SYMM_MODES[meta["canonical_mode"]]
+    o = fc.RunOptions()
+    o.target, o.steps, o.docheck_step = target, steps, docheck
+    o.pathname = pathname
+    o.success_rate_dtype = "float32"
+    o.spawn_rate4 = 0.1
+    o.device = device
+    o.num_threads = min(32, os.cpu_count() or 8)
+    return spec, o
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:  # noqa: BLE001
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                rows.append(parts)
+        os.remove(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(r[1]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def reference_build_seconds(pattern, target, meta, steps, docheck, threads) -> tuple[float, int]:
+    """One build of the table by the reference's compiled classic path
+    (oracle/_ref/formation_core, checker/baseline only)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reference as R  # noqa: E402
+
+    base = "/dev/shm" if os.access("/dev/shm", os.W_OK) else None
+    d = tempfile.mkdtemp(prefix="egtb_ref_", dir=base) + "/"
+    try:
+        spec, o = R.make_spec_options(meta["pattern_masks"], meta["success_shifts"],
+                                      R.SYMM[meta["canonical_mode"]], target, steps, docheck,
+                                      d + f"{pattern}_{2 ** target}_", "float32", 0.1, threads)
+        t0 = time.perf_counter()
+        R.run_build(np.asarray(meta["seed_boards"], dtype=np.uint64), spec, o)
+        dt = time.perf_counter() - t0
+        lines = open(d + f"{pattern}_{2 ** target}_stats.txt").read().splitlines()[1:]
+        boards = sum(int(line.split(",")[1]) for line in lines if line)
+        return dt, boards
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+        lf = os.path.join(os.path.dirname(d.rstrip("/")), "length_factors_list.txt")
+        if os.path.exists(lf):
+            os.remove(lf)
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def run_reference_arm(args, world, rank, pg):
+    pattern, target, meta, steps, docheck = workload_params(args.workload)
+    threads = os.cpu_count() or 1
+    if rank == 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import reference as R  # noqa: E402
+
+        if not R.available():
+            print(json.dumps({"impl": "reference", "unavailable": "reference classic path not built (make -C oracle ref)"}))
+            return
+        for _ in range(args.warmup):
+            reference_build_seconds(pattern, target, meta, steps, docheck, threads)
+        total, boards = 0.0, 0
+        for _ in range(args.steps):
+            dt, boards = reference_build_seconds(pattern, target, meta, steps, docheck, threads)
+            total += dt
+        v = boards * args.steps / total
+        line = {
+            "metric": "table-build boards/s", "value": v, "unit": "boards/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 accumulate, float32 rates", "data": "synthetic (seeded table build, no input data)",
+            "config": {"workload": f"{pattern}-{2 ** target} classic table build", "pattern": pattern, "target": 2 ** target,
+                       "steps": steps, "boards_per_build": boards, "success_rate_dtype": "float32"},
+            "cpu_baseline": {"value": v, "unit": "boards/s", "cores": threads, "kind": "reference",
+                             "sample": f"{args.steps} full builds of {pattern}-{2 ** target}"},
+            "e2e": {"value": v, "unit": "boards/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="442-512", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (default: --steps)")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="one device-resident build and nothing else (for an ncu launch list)")
+    args = ap.parse_args()
+    world, rank, local, pg = dist_setup()
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    P = importlib.import_module("2048endgametablebase_b200")
+    N = P._native
+    fc = importlib.import_module("2048endgametablebase_b200.native_core.formation_core")
+    pattern, target, meta, steps, docheck = workload_params(args.workload)
+    base = "/dev/shm" if os.access("/dev/shm", os.W_OK) else None
+    work = tempfile.mkdtemp(prefix=f"egtb_bench_r{rank}_", dir=base)
+    spec, o = make_spec_options(fc, pattern, target, meta, steps, docheck, os.path.join(work, "x_"), local)
+    seeds = np.ascontiguousarray(np.asarray(meta["seed_boards"], dtype=np.uint64))
+    c_spec = spec.to_c()
+    c_dev = o.to_c(write_files=False)
+    stream = torch.cuda.current_stream(local)
+    N.set_stream(local, stream.cuda_stream)
+
+    def device_build():
+        st = N.BuildStatsC()
+        N.check(N.lib().egtb_build(seeds.ctypes.data, len(seeds), ctypes.byref(c_spec), ctypes.byref(c_dev),
+                                   ctypes.byref(st)))
+        return st
+
+    if args.profile_run:
+        st = device_build()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_run": args.workload, "stats": st.as_dict()}))
+        shutil.rmtree(work, ignore_errors=True)
+        return
+    for _ in range(max(3, args.warmup)):
+        st = device_build()
+    # ---- value: device-resident builds, CUDA events on the build stream
+    N.profile(local, True)
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            stats.append(device_build())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    ms = ev0.elapsed_time(ev1)
+    prof = N.profile_read(local)
+    N.profile(local, False)
+    clocks = clk.summary()
+    if pg is not None:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    launches = int(sum(s.kernel_launches for s in stats))
+
+    # ---- e2e: the drop-in API from host seeds to .book files
+    e2e_steps = args.e2e_steps or args.steps
+    dirs = []
+    for i in range(e2e_steps):
+        d = os.path.join(work, f"e2e{i}")
+        os.makedirs(d, exist_ok=True)
+        dirs.append(d)
+    N.set_stream(local, None)
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    wall = 0.0
+    book_bytes = 0
+    for i in range(e2e_steps):
+        spec_i, o_i = make_spec_options(fc, pattern, target, meta, steps, docheck, os.path.join(dirs[i], "x_"), local)
+        t0 = time.perf_counter()
+        fc.run_pattern_build(seeds, spec_i, o_i)
+        wall += time.perf_counter() - t0
+        book_bytes = sum(os.path.getsize(os.path.join(dirs[i], f)) for f in os.listdir(dirs[i]) if f.endswith(".book"))
+        shutil.rmtree(dirs[i], ignore_errors=True)
+    if pg is not None:
+        t = torch.tensor([wall], device=f"cuda:{local}", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        wall = float(t.item())
+
+    if rank == 0:
+        layer_boards = int(stats[-1].raw_boards)
+        value = layer_boards * args.steps * world / (ms / 1e3)
+        e2e = layer_boards * e2e_steps * world / wall
+        peak, peak_kind = load_peaks()
+        roof = roofline(prof, stats[-1], args.steps, layer_boards, peak, peak_kind, pattern)
+        line = {
+            "metric": "table-build boards/s",
+            "value": value,
+            "unit": "boards/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "u64 keys, f64 fma accumulate, float32 rates",
+            "data": "synthetic (seeded table build from the pattern's seed boards; no input data)",
+            "config": {"workload": f"{pattern}-{2 ** target} classic table build", "pattern": pattern,
+                       "target": 2 ** target, "steps": steps, "boards_per_build": layer_boards,
+                       "success_rate_dtype": "float32", "parallelism": f"replicas x{world}",
+                       "l2": "working set per build 0.5-1.2 GB > 126 MB L2 (no flush needed)"},
+            "e2e": {"value": e2e, "unit": "boards/s", "h2d_bytes_per_step": int(seeds.nbytes),
+                    "d2h_bytes_per_step": int(book_bytes), "ms_per_step": wall / e2e_steps * 1e3,
+                    "path": "formation_core.run_pattern_build -> egtb_build, books written to " + (base or "tmp")},
+            "roofline": roof,
+            "kernel_times_ms": {k: round(v[1], 3) for k, v in prof.items()},
+            "clocks": clocks,
+            "gpu_launches": launches,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import reference as R  # noqa: E402
+
+            if R.available():
+                threads = os.cpu_count() or 1
+                dt, rb = reference_build_seconds(pattern, target, meta, steps, docheck, threads)
+                line["cpu_baseline"] = {"value": rb / dt, "unit": "boards/s", "cores": threads, "kind": "reference",
+                                        "sample": f"1 full build of {pattern}-{2 ** target} ({rb} boards, {dt:.2f} s)"}
+        print(json.dumps(line), flush=True)
+    shutil.rmtree(work, ignore_errors=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def roofline(prof, st, k, layer_boards, peak, peak_kind, pattern):
+    """Dominant kernel's algorithmic bytes / its measured device time."""
+    if not prof:
+        return None
+    name, (count, total) = max(prof.items(), key=lambda kv: kv[1][1])
+    if total <= 0:
+        return None
+    per_build = {
+        # expand: read parents, write candidates
+        "expand": 8 * int(st.raw_boards) + 8 * int(st.candidates),
+        # every radix pass reads and writes each candidate key once
+        "sort_pass": 16 * int(st.candidates) * max(1, round(prof["sort_pass"][0] / max(1, k) / max(1, st.layers - 1))),
+        "unique": 8 * int(st.candidates) + 8 * int(st.raw_boards),
+        # solve: one board key + one rate per board, one 32-byte key sector and one 32-byte rate sector per probe
+        "solve": 12 * layer_boards + 64 * int(st.lookups),
+        "book_pack": 12 * int(st.raw_boards) + 12 * int(st.book_entries),
+        "final_layers": 12 * 1,
+    }
+    bytes_total = per_build.get(name, 0) * k
+    achieved = bytes_total / (total / 1e3) / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+            "launches_per_step": count / k, "avg_launch_us": total / count * 1e3}
+
+
+if __name__ == "__main__":
+    main()

@@ -117,7 +117,15 @@ typedef struct egtb_build_stats {
     double forward_ms;         /* device time */
     double backward_ms;        /* device time */
     double total_ms;           /* host wall time of the call */
+    uint64_t kernel_launches;  /* kernels this call launched */
 } egtb_build_stats;
+
+/* Accumulated device time of one kind of kernel (egtb_profile_read). */
+typedef struct egtb_kernel_time {
+    char name[32];
+    uint64_t launches;   /* timed units (one unit may be a short chain of kernels) */
+    double total_ms;
+} egtb_kernel_time;
 
 /* ------------------------------------------------------------ errors ---- */
 
@@ -129,6 +137,19 @@ EGTB_API const char *egtb_version(void);
 
 /* Number of visible CUDA devices (0 when none). */
 EGTB_API int egtb_device_count(void);
+
+/* Use the caller's CUDA stream (a cudaStream_t passed as void*) for all
+ * device work of this device; NULL returns to the library's own stream.
+ * No reference counterpart: lets a host framework order builds on its own
+ * stream and time them with its own events. */
+EGTB_API int egtb_set_stream(int device, void *stream);
+
+/* Per-kernel-kind device timing with CUDA events on the launching stream
+ * (no reference counterpart; the reference logs phase fractions through
+ * Config.logger, BookGenerator.cpp:129-146). egtb_profile(device, 1) clears
+ * and enables it; egtb_profile_read fills up to max_kinds entries. */
+EGTB_API int egtb_profile(int device, int enable);
+EGTB_API int egtb_profile_read(int device, egtb_kernel_time *out, int max_kinds, int *n_kinds);
 
 /* ---------------------------------------------------------- progress ---- */
 
