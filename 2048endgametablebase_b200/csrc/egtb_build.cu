@@ -29,6 +29,7 @@
 
 #include "egtb_host.h"
 #include "egtb_kernels.cuh"
+#include "egtb_sort.cuh"
 
 namespace egtb {
 
@@ -92,8 +93,8 @@ static unsigned long long align16(unsigned long long x) { return (x + 15ull) & ~
         ++(E).launches;      \
     } while (0)
 
-static const char *kKindNames[] = {"expand", "sort_pass", "unique", "solve", "book_pack", "final_layers"};
-enum { K_EXPAND = 0, K_SORT_PASS, K_UNIQUE, K_SOLVE, K_PACK, K_FINAL, K_NKINDS };
+static const char *kKindNames[] = {"expand", "sort_pass", "unique", "solve", "book_pack", "final_layers", "rate_index"};
+enum { K_EXPAND = 0, K_SORT_PASS, K_UNIQUE, K_SOLVE, K_PACK, K_FINAL, K_INDEX, K_NKINDS };
 
 struct Engine {
     int device = 0;
@@ -159,8 +160,12 @@ struct Engine {
     uint64_t *split = nullptr;
     uint64_t *cand[2] = {nullptr, nullptr};
     uint64_t *tmp = nullptr;
-    unsigned *tile_hist = nullptr;  // 256 x sort_tiles
-    unsigned *digit_tot = nullptr;  // 256 x 8
+    unsigned *hist = nullptr;               // digit histograms, kMaxPasses x 256
+    unsigned *counters = nullptr;           // tile counters of the sort passes and the unique kernel
+    unsigned long long *status = nullptr;   // look-back words, sort_tiles x 256
+    unsigned long long *ustatus = nullptr;  // look-back words of the unique kernel, sort_tiles
+    unsigned epoch = 1;                     // tags the look-back words of one kernel launch
+    int sweep_grid = 0;                     // resident blocks of the onesweep kernel
     unsigned *tile_cnt = nullptr;
     unsigned long long *tile_off = nullptr;
     unsigned long long sort_tiles = 0, comp_tiles = 0;
@@ -169,6 +174,9 @@ struct Engine {
     unsigned long long *layer_max = nullptr;  // ordered encoding of the largest rate per layer
     unsigned char *book = nullptr;
     unsigned long long book_cap_bytes = 0;
+    ulonglong2 *index[3] = {nullptr, nullptr, nullptr};  // rate index of layers L % 3
+    unsigned long long index_cap = 0;                    // slots per index
+    unsigned long long *first_tile = nullptr;            // all-layer packing: first tile of every layer
     DevCtl *ctl = nullptr;
     cudaEvent_t ev[4];
 
@@ -192,6 +200,12 @@ struct Engine {
         const char *fb = getenv("EGTB_FILTER_BITS");
         if (fb) filter_bits = std::max(10, std::min(30, atoi(fb)));
         EGTB_CUDA(cudaMalloc(&filter, sizeof(uint64_t) << filter_bits));
+        EGTB_CUDA(cudaMalloc(&hist, sizeof(unsigned) * kMaxPasses * 256));
+        EGTB_CUDA(cudaMemset(hist, 0, sizeof(unsigned) * kMaxPasses * 256));
+        EGTB_CUDA(cudaMalloc(&counters, sizeof(unsigned) * 16));
+        int per_sm = 0;
+        EGTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel, kSortThreads, 0));
+        sweep_grid = sm_count * std::max(1, per_sm);
         progress_device_ptr();
     }
 
@@ -222,6 +236,15 @@ struct Engine {
         alloc_or_throw((void **)&layer_len, sizeof(unsigned long long) * steps_cap, "layer lengths");
         alloc_or_throw((void **)&book_len, sizeof(unsigned long long) * steps_cap, "book lengths");
         alloc_or_throw((void **)&layer_max, sizeof(unsigned long long) * steps_cap, "layer maxima");
+        release(first_tile);
+        alloc_or_throw((void **)&first_tile, sizeof(unsigned long long) * steps_cap, "tile map");
+    }
+
+    void ensure_index(unsigned long long slots) {
+        if (slots <= index_cap) return;
+        for (auto &p : index) release(p);
+        index_cap = slots;
+        for (auto &p : index) alloc_or_throw((void **)&p, sizeof(ulonglong2) * index_cap, "rate index");
     }
 
     void ensure_arena(unsigned long long cap) {
@@ -245,15 +268,17 @@ struct Engine {
         release(cand[0]);
         release(cand[1]);
         release(tmp);
-        release(tile_hist);
-        release(digit_tot);
+        release(status);
+        release(ustatus);
         cand_cap = cap;
         alloc_or_throw((void **)&cand[0], sizeof(uint64_t) * cand_cap, "candidates");
         alloc_or_throw((void **)&cand[1], sizeof(uint64_t) * cand_cap, "candidates");
         alloc_or_throw((void **)&tmp, sizeof(uint64_t) * cand_cap, "sort buffer");
         sort_tiles = cand_cap / kTileKeys + 2;
-        alloc_or_throw((void **)&tile_hist, sizeof(unsigned) * 256 * sort_tiles, "sort histograms");
-        alloc_or_throw((void **)&digit_tot, sizeof(unsigned) * 256 * 8, "digit totals");
+        alloc_or_throw((void **)&status, sizeof(unsigned long long) * 256 * sort_tiles, "sort look-back");
+        alloc_or_throw((void **)&ustatus, sizeof(unsigned long long) * sort_tiles, "unique look-back");
+        EGTB_CUDA(cudaMemset(status, 0, sizeof(unsigned long long) * 256 * sort_tiles));
+        EGTB_CUDA(cudaMemset(ustatus, 0, sizeof(unsigned long long) * sort_tiles));
         ensure_comp_tiles();
     }
 
@@ -304,10 +329,10 @@ static Engine &engine_for(int device) {
     return *g_engines[device];
 }
 
-// Bytes of the sort key that can differ between candidates: a nibble pinned
-// to 0xF by every mask, and by every symmetry image of that intersection, is
-// 0xF in every canonical key.
-static std::vector<int> varying_byte_shifts(const egtb_pattern_spec &s) {
+// Nibbles that can differ between canonical keys: a nibble pinned to 0xF by
+// every mask, and by every symmetry image of that intersection, is 0xF in
+// every canonical key, so the sort skips it.
+static uint64_t pinned_nibbles(const egtb_pattern_spec &s) {
     uint64_t pinned = 0;
     if (s.n_masks > 0) {
         pinned = ~0ull;
@@ -344,10 +369,23 @@ static std::vector<int> varying_byte_shifts(const egtb_pattern_spec &s) {
             for (int g = 1; g < 8; ++g) inter &= sym(pinned, g);
         pinned = inter;
     }
-    std::vector<int> shifts;
-    for (int byte = 0; byte < 8; ++byte)
-        if (((pinned >> (8 * byte)) & 0xFF) != 0xFF) shifts.push_back(8 * byte);
-    return shifts;
+    return pinned;
+}
+
+// Digits of the LSD passes: the free nibbles from least significant up, two per pass.
+static SortPlan sort_plan(const egtb_pattern_spec &s) {
+    const uint64_t pinned = pinned_nibbles(s);
+    std::vector<int> free_nib;
+    for (int k = 0; k < 16; ++k)
+        if (((pinned >> (4 * k)) & 0xF) != 0xF) free_nib.push_back(k);
+    SortPlan sp;
+    std::memset(&sp, 0, sizeof sp);
+    sp.passes = (int)(free_nib.size() + 1) / 2;
+    for (int p = 0; p < sp.passes; ++p) {
+        sp.lo[p] = free_nib[2 * p];
+        sp.hi[p] = 2 * p + 1 < (int)free_nib.size() ? free_nib[2 * p + 1] : -1;
+    }
+    return sp;
 }
 
 // ------------------------------------------------------------ forward -----
@@ -355,36 +393,32 @@ static std::vector<int> varying_byte_shifts(const egtb_pattern_spec &s) {
 struct ForwardPlan {
     int steps, docheck, first_step;  // first_step: generation starts at step i = first_step
     DevSpec spec;
-    std::vector<int> shifts;
+    SortPlan sort;
 };
 
-// Sort the candidates of buffer x and unique them into the arena as layer L.
-static void enqueue_sort_unique(Engine &E, const ForwardPlan &P, int x, int L) {
+// Sort the candidates of buffer x and unique them into the arena as layer L:
+// one histogram kernel, one onesweep kernel per pass, one unique kernel.
+static void enqueue_sort_unique(Engine &E, const ForwardPlan &P, int x, int L, unsigned *progress) {
     cudaStream_t s = E.stream;
     unsigned long long *n_ptr = &E.ctl->cand_count[x];
-    const int g_sort = E.sm_count * 4;
-    EGTB_CUDA(cudaMemsetAsync(E.digit_tot, 0, sizeof(unsigned) * 256 * 8, s));
+    EGTB_LAUNCH(E, sort_hist_kernel<<<E.sm_count * 2, 256, 0, s>>>(E.cand[x], n_ptr, E.cand_cap, P.sort, E.hist,
+                                                                   E.counters, E.ctl));
     uint64_t *src = E.cand[x], *dst = E.tmp;
-    int p = 0;
-    for (int sh : P.shifts) {
-        unsigned *dt = E.digit_tot + 256 * p;
+    for (int p = 0; p < P.sort.passes; ++p) {
         const int pi = E.prof_begin(K_SORT_PASS);
-        EGTB_LAUNCH(E, radix_count_kernel<<<g_sort, kSortThreads, 0, s>>>(src, n_ptr, E.cand_cap, sh, E.tile_hist, E.sort_tiles, dt));
-        EGTB_LAUNCH(E, radix_scan_kernel<<<256, 1024, 0, s>>>(n_ptr, E.cand_cap, E.tile_hist, E.sort_tiles, dt));
-        EGTB_LAUNCH(E, radix_scatter_kernel<<<g_sort, kSortThreads, 0, s>>>(src, dst, n_ptr, E.cand_cap, sh, E.tile_hist, E.sort_tiles, dt));
+        EGTB_LAUNCH(E, onesweep_kernel<<<E.sweep_grid, kSortThreads, 0, s>>>(src, dst, n_ptr, E.cand_cap, P.sort, p,
+                                                                             E.hist, E.counters, E.status, E.epoch++,
+                                                                             E.ctl));
         E.prof_end(pi);
         std::swap(src, dst);
-        ++p;
     }
     const int pu = E.prof_begin(K_UNIQUE);
-    EGTB_LAUNCH(E, unique_count_kernel<<<g_sort, kSortThreads, 0, s>>>(src, n_ptr, E.cand_cap, E.tile_cnt));
-    EGTB_LAUNCH(E, tile_scan_kernel<<<1, 1024, 0, s>>>(n_ptr, E.cand_cap, E.tile_off, E.tile_cnt, &E.ctl->n_unique));
-    EGTB_LAUNCH(E, close_layer_kernel<<<1, 1, 0, s>>>(L, &E.ctl->n_unique, E.layer_off, E.layer_len, E.arena_cap, E.ctl));
-    EGTB_LAUNCH(E, unique_write_kernel<<<g_sort, kSortThreads, 0, s>>>(src, n_ptr, E.cand_cap, E.tile_off, E.arena, E.split, E.layer_off, L, E.arena_cap));
+    EGTB_LAUNCH(E, unique_layer_kernel<<<E.sweep_grid, kSortThreads, 0, s>>>(src, x, E.cand_cap, E.arena, E.layer_off,
+                                                                             E.layer_len, L, E.arena_cap, E.counters,
+                                                                             E.ustatus, E.epoch++, E.hist, E.ctl,
+                                                                             progress));
     E.prof_end(pu);
 }
-
-__global__ void add_candidates_kernel(DevCtl *ctl, int x) { ctl->candidates += ctl->cand_count[x]; }
 
 // Enqueue forward steps first_step .. steps-2 and the final partial layer.
 // Preconditions on the device: layer first_step-1 in the arena at
@@ -396,17 +430,14 @@ static void enqueue_forward(Engine &E, const ForwardPlan &P, unsigned *progress)
     for (int i = P.first_step; i < P.steps - 1; ++i) {
         const int t = i - 1;
         const int x1 = i & 1, x2 = (i + 1) & 1;
-        EGTB_CUDA(cudaMemsetAsync(&E.ctl->cand_count[x2], 0, sizeof(unsigned long long), s));
+        // buffer x2's count was reset by the unique kernel that consumed it
         const int pe = E.prof_begin(K_EXPAND);
         EGTB_LAUNCH(E, expand_kernel<<<g_exp, kExpandThreads, 0, s>>>(E.arena, E.layer_off, E.layer_len, t, P.spec, i > P.docheck ? 1 : 0, E.tab, E.cand[x1], E.cand[x2], E.ctl, x1, x2, E.cand_cap, E.filter, E.filter_bits));
         E.prof_end(pe);
-        EGTB_LAUNCH(E, add_candidates_kernel<<<1, 1, 0, s>>>(E.ctl, x1));
-        enqueue_sort_unique(E, P, x1, i);
-        EGTB_LAUNCH(E, progress_kernel<<<1, 1, 0, s>>>(progress, (unsigned)i));
+        enqueue_sort_unique(E, P, x1, i, progress);
     }
     const int L = P.steps - 1;
-    EGTB_LAUNCH(E, add_candidates_kernel<<<1, 1, 0, s>>>(E.ctl, L & 1));
-    enqueue_sort_unique(E, P, L & 1, L);
+    enqueue_sort_unique(E, P, L & 1, L, progress);
 }
 
 static DevCtl read_ctl(Engine &E) {
@@ -422,6 +453,7 @@ static void stage_start(Engine &E, const ForwardPlan &P, const uint64_t *base, s
                         size_t n_partial) {
     cudaStream_t s = E.stream;
     EGTB_CUDA(cudaMemsetAsync(E.ctl, 0, sizeof(DevCtl), s));
+    EGTB_CUDA(cudaMemsetAsync(E.hist, 0, sizeof(unsigned) * kMaxPasses * 256, s));
     EGTB_CUDA(cudaMemsetAsync(E.filter, 0, sizeof(uint64_t) << E.filter_bits, s));
     EGTB_CUDA(cudaMemsetAsync(E.layer_off, 0, sizeof(unsigned long long) * E.steps_cap, s));
     EGTB_CUDA(cudaMemsetAsync(E.layer_len, 0, sizeof(unsigned long long) * E.steps_cap, s));
@@ -448,13 +480,24 @@ static void stage_start(Engine &E, const ForwardPlan &P, const uint64_t *base, s
     EGTB_CUDA(cudaStreamSynchronize(s));
 }
 
+static unsigned long long env_keys(const char *name, unsigned long long dflt) {
+    const char *v = getenv(name);
+    if (!v || !*v) return dflt;
+    const unsigned long long x = strtoull(v, nullptr, 10);
+    return x ? x : dflt;
+}
+
 // Run the forward with capacity regrowth. Returns the number of retries.
 static int run_forward(Engine &E, const ForwardPlan &P, const uint64_t *base, size_t n_base, const uint64_t *partial,
                        size_t n_partial, float *ms) {
     int retries = 0;
     E.ensure_steps(P.steps);
-    E.ensure_cand(std::max<unsigned long long>(E.cand_cap, std::max<size_t>(1ull << 22, n_partial * 2)));
-    E.ensure_arena(std::max<unsigned long long>(E.arena_cap, std::max<size_t>(1ull << 26, n_base * 4)));
+    // first capacities: 4 Mi candidate keys, 128 Mi layer keys (EGTB_INIT_CAND_KEYS /
+    // EGTB_INIT_ARENA_KEYS override); a pass that outgrows them is re-run larger
+    static const unsigned long long init_cand = env_keys("EGTB_INIT_CAND_KEYS", 1ull << 22);
+    static const unsigned long long init_arena = env_keys("EGTB_INIT_ARENA_KEYS", 1ull << 27);
+    E.ensure_cand(std::max<unsigned long long>(E.cand_cap, std::max<unsigned long long>(init_cand, n_partial * 2)));
+    E.ensure_arena(std::max<unsigned long long>(E.arena_cap, std::max<unsigned long long>(init_arena, n_base * 4)));
     unsigned *progress = progress_device_ptr();
     for (;;) {
         stage_start(E, P, base, n_base, partial, n_partial);
@@ -468,6 +511,7 @@ static int run_forward(Engine &E, const ForwardPlan &P, const uint64_t *base, si
             EGTB_CUDA(cudaEventElapsedTime(ms, E.ev[0], E.ev[1]));
             return retries;
         }
+        if (c.err & kErrTimeout) throw Error(EGTB_ERR_TIMEOUT, "a bounded device wait gave up in the forward pass");
         ++retries;
         if (retries > 24) throw Error(EGTB_ERR_CAPACITY, "forward pass did not fit after repeated regrowth");
         if (c.err & kErrCandOverflow) E.ensure_cand(E.cand_cap * 2);
@@ -476,11 +520,6 @@ static int run_forward(Engine &E, const ForwardPlan &P, const uint64_t *base, si
 }
 
 // ----------------------------------------------------------- backward -----
-
-__device__ __forceinline__ unsigned long long ordered_bits(double v) {
-    unsigned long long b = (unsigned long long)__double_as_longlong(v);
-    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
-}
 
 static double ordered_to_double(unsigned long long o) {
     unsigned long long b = (o >> 63) ? (o & 0x7FFFFFFFFFFFFFFFull) : ~o;
@@ -538,35 +577,86 @@ struct BackwardPlan {
     DevSpec spec;
 };
 
-// Solve every layer on the device-resident arena (layers 0..steps-1 present)
-// and pack all books; book bytes of layer t start at layer_off[t] * rec.
+// Slots of the rate index of a layer of n entries: a power of two >= 2n.
+static unsigned long long index_slots(unsigned long long n) {
+    unsigned long long c = 64;
+    while (c < 2 * n) c <<= 1;
+    return c;
+}
+
+// Build the rate index of layer L (live entries only) into idx.
 template <typename T>
-static void enqueue_backward(Engine &E, const BackwardPlan &B, const std::vector<unsigned long long> &off,
+static void enqueue_index_at(Engine &E, int L, unsigned long long n, T zero, ulonglong2 *idx) {
+    const unsigned long long slots = index_slots(n);
+    EGTB_CUDA(cudaMemsetAsync(idx, 0, sizeof(ulonglong2) * slots, E.stream));
+    EGTB_LAUNCH(E, index_insert_kernel<T><<<E.sm_count * 8, 256, 0, E.stream>>>(E.arena, (const T *)E.rates, E.layer_off,
+                                                                             E.layer_len, L, zero, idx, slots - 1));
+}
+
+// ... in index slot L % 3 (fused build: layers t, t+1, t+2 use distinct slots).
+template <typename T>
+static void enqueue_index(Engine &E, int L, unsigned long long n, T zero) {
+    enqueue_index_at<T>(E, L, n, zero, E.index[L % 3]);
+}
+
+// Pack every layer's live entries as .book records in one pass; the book of
+// layer t starts at byte layer_off[t] * rec of E.book.
+template <typename T>
+static void enqueue_pack_all(Engine &E, int steps, const std::vector<unsigned long long> &len, T zero) {
+    cudaStream_t s = E.stream;
+    std::vector<unsigned long long> ft(steps + 1, 0);
+    for (int L = 0; L < steps; ++L) ft[L + 1] = ft[L] + (len[L] + kTileKeys - 1) / kTileKeys;
+    const unsigned long long n_tiles = ft[steps];
+    if (n_tiles > E.comp_tiles) throw Error(EGTB_ERR_CAPACITY, "tile buffers too small for packing");
+    EGTB_CUDA(cudaMemcpyAsync(E.first_tile, ft.data(), sizeof(unsigned long long) * (steps + 1), cudaMemcpyHostToDevice, s));
+    EGTB_CUDA(cudaMemsetAsync(E.layer_max, 0, sizeof(unsigned long long) * steps, s));
+    const int g = E.sm_count * 4;
+    EGTB_LAUNCH(E, book_count_all_kernel<T><<<g, kSortThreads, 0, s>>>((const T *)E.rates, E.layer_off, E.layer_len,
+                                                                   E.first_tile, steps, n_tiles, zero, E.tile_cnt,
+                                                                   E.layer_max));
+    EGTB_LAUNCH(E, scan_tiles_kernel<<<1, 1024, 0, s>>>(E.tile_cnt, n_tiles, E.tile_off, &E.ctl->n_unique));
+    EGTB_LAUNCH(E, book_lens_kernel<<<(steps + 255) / 256, 256, 0, s>>>(E.first_tile, steps, n_tiles, E.tile_off,
+                                                                       &E.ctl->n_unique, E.book_len));
+    EGTB_LAUNCH(E, book_write_all_kernel<T><<<g, kSortThreads, 0, s>>>(E.arena, (const T *)E.rates, E.layer_off,
+                                                                   E.layer_len, E.first_tile, steps, n_tiles, zero,
+                                                                   E.tile_off, E.book, E.book_cap_bytes, E.ctl));
+}
+
+// Solve every layer on the device-resident arena (layers 0..steps-1 present)
+// and pack all books.
+template <typename T>
+static void enqueue_backward(Engine &E, const BackwardPlan &B, const std::vector<unsigned long long> &len,
                              unsigned *progress) {
     cudaStream_t s = E.stream;
     const T zero = (T)dtype_zero(B.dtype), maxv = (T)dtype_max(B.dtype);
     const int g = E.sm_count * 8;
     T *rates = (T *)E.rates;
     const uint32_t total = (uint32_t)(B.steps * 2);
+    unsigned long long biggest = 0;
+    for (int L = 0; L < B.steps; ++L) biggest = std::max(biggest, len[L]);
+    E.ensure_index(index_slots(biggest));
     const int pf = E.prof_begin(K_FINAL);
     for (int t = B.steps - 2; t < B.steps; ++t)
         if (t >= 0) EGTB_LAUNCH(E, final_layer_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec, zero, maxv));
+    for (int t = B.steps - 1; t >= B.steps - 2 && t >= 1; --t) enqueue_index<T>(E, t, len[t], zero);
     E.prof_end(pf);
     for (int t = B.steps - 3; t >= 0; --t) {
         EGTB_LAUNCH(E, progress_kernel<<<1, 1, 0, s>>>(progress, total - (unsigned)t - 2u));
         const int ps = E.prof_begin(K_SOLVE);
-        EGTB_LAUNCH(E, solve_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.split, E.layer_off, E.layer_len, t, B.spec, t > B.docheck ? 1 : 0, E.tab, B.p4, zero, maxv, E.ctl));
+        EGTB_LAUNCH(E, solve_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec,
+                                                         t > B.docheck ? 1 : 0, E.tab, B.p4, zero, maxv,
+                                                         E.index[(t + 1) % 3], index_slots(len[t + 1]) - 1,
+                                                         E.index[(t + 2) % 3], index_slots(len[t + 2]) - 1, E.ctl));
         E.prof_end(ps);
+        if (t > 0) {
+            const int pi = E.prof_begin(K_INDEX);
+            enqueue_index<T>(E, t, len[t], zero);
+            E.prof_end(pi);
+        }
     }
-    EGTB_CUDA(cudaMemsetAsync(E.layer_max, 0, sizeof(unsigned long long) * E.steps_cap, s));
-    const size_t rec = 8 + sizeof(T);
-    for (int t = 0; t < B.steps; ++t) {
-        const int pp = E.prof_begin(K_PACK);
-        enqueue_pack<T>(E, t, zero);
-        enqueue_pack_write<T>(E, t, zero, off[t] * rec);
-        E.prof_end(pp);
-        EGTB_LAUNCH(E, layer_max_kernel<T><<<E.sm_count, 256, 0, s>>>(rates, E.layer_off, E.layer_len, t, zero, E.layer_max));
-    }
+    const int pp = E.prof_begin(K_PACK);
+    enqueue_pack_all<T>(E, B.steps, len, zero);
+    E.prof_end(pp);
 }
 
 // ---------------------------------------------------------------- output --
@@ -686,7 +776,7 @@ static ForwardPlan make_forward_plan(const egtb_pattern_spec &spec, const egtb_r
     P.docheck = o.docheck_step;
     P.first_step = first_step;
     P.spec = make_dev_spec(spec, o.target);
-    P.shifts = varying_byte_shifts(spec);
+    P.sort = sort_plan(spec);
     return P;
 }
 
@@ -711,7 +801,7 @@ static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const 
     std::vector<unsigned long long> len = d2h_u64(E, E.layer_len, steps + 1);
     BackwardPlan B{steps, o.docheck_step, o.success_rate_dtype, o.spawn_rate4, P.spec};
     EGTB_CUDA(cudaEventRecord(E.ev[2], E.stream));
-    enqueue_backward<T>(E, B, off, progress_device_ptr());
+    enqueue_backward<T>(E, B, len, progress_device_ptr());
     EGTB_CUDA(cudaEventRecord(E.ev[3], E.stream));
     EGTB_CUDA(cudaStreamSynchronize(E.stream));
     EGTB_CUDA(cudaGetLastError());
@@ -883,6 +973,9 @@ static void solve_files(Engine &E, const void *d1_recs, size_t n1, const void *d
     slot = align16(slot);
     E.ensure_arena(slot * 3);
     E.ensure_cand(std::max<unsigned long long>(E.cand_cap, 1ull << 22));
+    E.ensure_index(index_slots(slot));
+    int idx_of[3] = {0, 1, 2};  // rate index of layer i, i+1, i+2
+    bool index_fresh = false;   // indexes of i+1, i+2 match the resident layers
 
     // host copies of the two successor layers (packed records)
     std::vector<unsigned char> h1((const unsigned char *)d1_recs, (const unsigned char *)d1_recs + n1 * rec);
@@ -938,6 +1031,7 @@ static void solve_files(Engine &E, const void *d1_recs, size_t n1, const void *d
             dlen1 = upload_layer(h1, slot_of[1]);
             dlen2 = upload_layer(h2, slot_of[2]);
             resident = true;
+            index_fresh = false;
         }
         std::vector<uint64_t> raw = read_u64_file(pi);
         const unsigned long long n0 = raw.size();
@@ -951,7 +1045,16 @@ static void solve_files(Engine &E, const void *d1_recs, size_t n1, const void *d
         EGTB_CUDA(cudaMemsetAsync(E.ctl, 0, sizeof(DevCtl), s));
         EGTB_CUDA(cudaMemsetAsync(E.layer_max, 0, sizeof(unsigned long long) * 4, s));
         const auto t0 = std::chrono::steady_clock::now();
-        EGTB_LAUNCH(E, solve_kernel<T><<<E.sm_count * 8, 256, 0, s>>>(E.arena, rates, E.split, E.layer_off, E.layer_len, 0, ds, i > o.docheck_step ? 1 : 0, E.tab, o.spawn_rate4, zero, maxv, E.ctl));
+        if (!index_fresh) {
+            enqueue_index_at<T>(E, 1, dlen1, zero, E.index[idx_of[1]]);
+            enqueue_index_at<T>(E, 2, dlen2, zero, E.index[idx_of[2]]);
+            index_fresh = true;
+        }
+        EGTB_LAUNCH(E, solve_kernel<T><<<E.sm_count * 8, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, 0, ds,
+                                                                    i > o.docheck_step ? 1 : 0, E.tab, o.spawn_rate4, zero, maxv,
+                                                                    E.index[idx_of[1]], index_slots(dlen1) - 1,
+                                                                    E.index[idx_of[2]], index_slots(dlen2) - 1, E.ctl));
+        if (i > 0) enqueue_index_at<T>(E, 0, n0, zero, E.index[idx_of[0]]);
         EGTB_LAUNCH(E, splitters_kernel<<<E.sm_count, 256, 0, s>>>(k0, n0, E.split + slot_of[0] * slot / kSplitStride));
         enqueue_pack<T>(E, 0, zero);
         enqueue_pack_write<T>(E, 0, zero, 0);
@@ -994,6 +1097,10 @@ static void solve_files(Engine &E, const void *d1_recs, size_t n1, const void *d
             slot_of[2] = slot_of[1];
             slot_of[1] = slot_of[0];
             slot_of[0] = old2;
+            const int oldi = idx_of[2];
+            idx_of[2] = idx_of[1];
+            idx_of[1] = idx_of[0];
+            idx_of[0] = oldi;
             dlen2 = dlen1;
             dlen1 = n0;
             h2.swap(h1);

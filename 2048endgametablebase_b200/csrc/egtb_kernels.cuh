@@ -111,7 +111,7 @@ __device__ __forceinline__ void stage_flush(uint64_t *stage, int &count, uint64_
 // sort (its role is the reference's lossy prefilter, BookGenerator.cpp:
 // 101-127; results never depend on it). Each warp stages its survivors in
 // shared memory and appends them with one atomic per 32+ keys.
-__global__ void __launch_bounds__(kExpandThreads)
+static __global__ void __launch_bounds__(kExpandThreads)
 expand_kernel(const uint64_t *__restrict__ arena, const unsigned long long *__restrict__ layer_off,
               const unsigned long long *__restrict__ layer_len, int t, DevSpec spec, int do_check,
               const uint32_t *__restrict__ tab, uint64_t *__restrict__ out1, uint64_t *__restrict__ out2,
@@ -175,168 +175,8 @@ expand_kernel(const uint64_t *__restrict__ arena, const unsigned long long *__re
     stage_flush(stage[warp][1], cnt[1], out2, counters[1], cap, &ctl->err);
 }
 
-// -------------------------------------------------- LSD radix sort -------
-//
-// One 8-bit digit per pass; only the bytes that can differ between keys are
-// sorted (bytes made of pinned nibbles are constant). Each pass is three
-// kernels: per-tile digit counts, a digit-major scan of those counts, and a
-// stable scatter (warp-striped ranking with __match_any_sync, tile staged in
-// shared memory so the global writes run along digit runs).
-
-__global__ void __launch_bounds__(kSortThreads)
-radix_count_kernel(const uint64_t *__restrict__ keys, const unsigned long long *n_ptr, unsigned long long cap,
-                   int shift, unsigned *__restrict__ tile_hist, unsigned long long max_tiles,
-                   unsigned *__restrict__ digit_tot) {
-    __shared__ unsigned hist[256];
-    const unsigned long long n = clamp_n(*n_ptr, cap);
-    const unsigned long long ntiles = (n + kTileKeys - 1) / kTileKeys;
-    for (unsigned long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        hist[threadIdx.x] = 0;
-        __syncthreads();
-        const unsigned long long base = tile * kTileKeys;
-#pragma unroll 4
-        for (int i = 0; i < kKeysPerThread; ++i) {
-            const unsigned long long idx = base + (unsigned long long)i * kSortThreads + threadIdx.x;
-            if (idx < n) atomicAdd(&hist[(unsigned)(keys[idx] >> shift) & 0xFFu], 1u);
-        }
-        __syncthreads();
-        const unsigned c = hist[threadIdx.x];
-        tile_hist[(unsigned long long)threadIdx.x * max_tiles + tile] = c;
-        if (c) atomicAdd(&digit_tot[threadIdx.x], c);
-        __syncthreads();
-    }
-}
-
-// One block per digit: offset of (digit, tile) = keys of smaller digits +
-// keys of this digit in earlier tiles.
-__global__ void __launch_bounds__(1024)
-radix_scan_kernel(const unsigned long long *n_ptr, unsigned long long cap, unsigned *__restrict__ tile_hist,
-                  unsigned long long max_tiles, const unsigned *__restrict__ digit_tot) {
-    __shared__ unsigned long long sm[33];
-    const unsigned long long n = clamp_n(*n_ptr, cap);
-    const unsigned long long ntiles = (n + kTileKeys - 1) / kTileKeys;
-    const int d = blockIdx.x;
-    unsigned long long tot = 0;
-    unsigned *row = tile_hist + (unsigned long long)d * max_tiles;
-    unsigned long long run = 0;
-    for (unsigned long long c0 = 0; c0 < ntiles; c0 += blockDim.x) {
-        const unsigned long long i = c0 + threadIdx.x;
-        unsigned long long x = i < ntiles ? row[i] : 0;
-        unsigned long long ex = block_excl_scan<unsigned long long>(x, sm, &tot);
-        // offset inside the digit (candidate buffers hold < 2^32 keys); the
-        // scatter adds the 64-bit start of the digit
-        if (i < ntiles) row[i] = (unsigned)(run + ex);
-        run += tot;
-    }
-}
-
-__global__ void __launch_bounds__(kSortThreads)
-radix_scatter_kernel(const uint64_t *__restrict__ in, uint64_t *__restrict__ out, const unsigned long long *n_ptr,
-                     unsigned long long cap, int shift, const unsigned *__restrict__ tile_off,
-                     unsigned long long max_tiles, const unsigned *__restrict__ digit_tot) {
-    __shared__ uint64_t tkeys[kTileKeys];
-    __shared__ unsigned short wcnt[kSortThreads / 32][256];
-    __shared__ unsigned loff[256];
-    __shared__ unsigned long long dbase[256];
-    __shared__ unsigned long long sm[33];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned long long n = clamp_n(*n_ptr, cap);
-    const unsigned long long ntiles = (n + kTileKeys - 1) / kTileKeys;
-    {
-        // 64-bit start of every digit in the output
-        unsigned long long tot;
-        unsigned long long v = digit_tot[threadIdx.x];
-        unsigned long long ex = block_excl_scan<unsigned long long>(v, sm, &tot);
-        dbase[threadIdx.x] = ex;
-    }
-    for (unsigned long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        for (int i = threadIdx.x; i < (kSortThreads / 32) * 256; i += kSortThreads) (&wcnt[0][0])[i] = 0;
-        __syncthreads();
-        const unsigned long long base = tile * kTileKeys + (unsigned long long)warp * (kTileKeys / 8);
-        uint64_t k[kKeysPerThread];
-        unsigned short rank[kKeysPerThread];
-        unsigned short dig[kKeysPerThread];
-#pragma unroll
-        for (int r = 0; r < kKeysPerThread; ++r) {
-            const unsigned long long idx = base + (unsigned long long)r * 32 + lane;
-            const bool valid = idx < n;
-            k[r] = valid ? in[idx] : 0;
-            const unsigned d = valid ? (unsigned)(k[r] >> shift) & 0xFFu : 256u;
-            dig[r] = (unsigned short)d;
-            const unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
-            const unsigned before = __popc(peers & ((1u << lane) - 1u));
-            unsigned short c = 0;
-            if (valid) c = wcnt[warp][d];
-            rank[r] = (unsigned short)(c + before);
-            __syncwarp();
-            if (valid && before == 0) wcnt[warp][d] = (unsigned short)(c + __popc(peers));
-            __syncwarp();
-        }
-        __syncthreads();
-        // per digit: warp offsets and tile total
-        {
-            const int d = threadIdx.x;
-            unsigned s = 0;
-#pragma unroll
-            for (int w = 0; w < kSortThreads / 32; ++w) {
-                unsigned c = wcnt[w][d];
-                wcnt[w][d] = (unsigned short)s;
-                s += c;
-            }
-            unsigned long long tot;
-            unsigned long long ex = block_excl_scan<unsigned long long>((unsigned long long)s, sm, &tot);
-            loff[d] = (unsigned)ex;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < kKeysPerThread; ++r) {
-            const unsigned d = dig[r];
-            if (d < 256u) tkeys[loff[d] + wcnt[warp][d] + rank[r]] = k[r];
-        }
-        __syncthreads();
-        const unsigned long long tile_n = (n - tile * kTileKeys) < (unsigned long long)kTileKeys
-                                              ? (n - tile * kTileKeys) : (unsigned long long)kTileKeys;
-        for (unsigned i = threadIdx.x; i < tile_n; i += kSortThreads) {
-            const uint64_t key = tkeys[i];
-            const unsigned d = (unsigned)(key >> shift) & 0xFFu;
-            const unsigned long long dst =
-                dbase[d] + (unsigned long long)tile_off[(unsigned long long)d * max_tiles + tile] + (i - loff[d]);
-            out[dst] = key;
-        }
-        __syncthreads();
-    }
-}
-
-// ------------------------------------------- unique / compaction ---------
-
-// Per tile: number of positions i with keys[i] != keys[i-1] (i = 0 counts).
-__global__ void __launch_bounds__(kSortThreads)
-unique_count_kernel(const uint64_t *__restrict__ keys, const unsigned long long *n_ptr, unsigned long long cap,
-                    unsigned *__restrict__ tile_cnt) {
-    __shared__ unsigned long long sm[33];
-    const unsigned long long n = clamp_n(*n_ptr, cap);
-    const unsigned long long ntiles = (n + kTileKeys - 1) / kTileKeys;
-    for (unsigned long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        unsigned long long c = 0;
-        const unsigned long long base = tile * kTileKeys + (unsigned long long)threadIdx.x * kKeysPerThread;
-        uint64_t prev = (base > 0 && base < n) ? keys[base - 1] : ~keys[0];
-#pragma unroll
-        for (int i = 0; i < kKeysPerThread; ++i) {
-            const unsigned long long idx = base + i;
-            if (idx < n) {
-                const uint64_t k = keys[idx];
-                c += (idx == 0 || k != prev);
-                prev = k;
-            }
-        }
-        unsigned long long tot;
-        block_excl_scan<unsigned long long>(c, sm, &tot);
-        if (threadIdx.x == 0) tile_cnt[tile] = (unsigned)tot;
-    }
-}
-
 // Single block: exclusive scan of the tile counts; total -> *total_out.
-__global__ void __launch_bounds__(1024)
+static __global__ void __launch_bounds__(1024)
 tile_scan_kernel(const unsigned long long *n_ptr, unsigned long long cap, unsigned long long *__restrict__ tile_io,
                  const unsigned *__restrict__ tile_cnt, unsigned long long *total_out) {
     __shared__ unsigned long long sm[33];
@@ -353,66 +193,6 @@ tile_scan_kernel(const unsigned long long *n_ptr, unsigned long long cap, unsign
     if (threadIdx.x == 0) *total_out = run;
 }
 
-// Close a new layer: record its length and the next layer's 16-aligned offset.
-__global__ void close_layer_kernel(int t, const unsigned long long *total, unsigned long long *layer_off,
-                                   unsigned long long *layer_len, unsigned long long arena_cap, DevCtl *ctl) {
-    const unsigned long long n = *total;
-    const unsigned long long end = layer_off[t] + n;
-    const unsigned long long next = (end + kSplitStride - 1) & ~(unsigned long long)(kSplitStride - 1);
-    if (next > arena_cap || (ctl->err & kErrArenaOverflow)) {
-        // does not fit: flag it and leave the layer empty, so every later
-        // kernel of this pass stays inside the arena; the host re-runs the
-        // pass with a larger arena
-        atomicOr(&ctl->err, kErrArenaOverflow);
-        layer_len[t] = 0;
-        layer_off[t + 1] = layer_off[t];
-        return;
-    }
-    layer_len[t] = n;
-    layer_off[t + 1] = next;
-}
-
-// Write the unique keys of a sorted run as layer t of the arena, with the
-// layer's splitters (every 16th key).
-__global__ void __launch_bounds__(kSortThreads)
-unique_write_kernel(const uint64_t *__restrict__ keys, const unsigned long long *n_ptr, unsigned long long cap,
-                    const unsigned long long *__restrict__ tile_off, uint64_t *__restrict__ arena,
-                    uint64_t *__restrict__ split, const unsigned long long *__restrict__ layer_off, int t,
-                    unsigned long long arena_cap) {
-    __shared__ unsigned long long sm[33];
-    const unsigned long long n = clamp_n(*n_ptr, cap);
-    const unsigned long long ntiles = (n + kTileKeys - 1) / kTileKeys;
-    const unsigned long long off = layer_off[t];
-    for (unsigned long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const unsigned long long base = tile * kTileKeys + (unsigned long long)threadIdx.x * kKeysPerThread;
-        uint64_t k[kKeysPerThread];
-        unsigned head = 0, c = 0;
-        uint64_t prev = (base > 0 && base < n) ? keys[base - 1] : 0;
-#pragma unroll
-        for (int i = 0; i < kKeysPerThread; ++i) {
-            const unsigned long long idx = base + i;
-            k[i] = idx < n ? keys[idx] : 0;
-            const bool h = idx < n && (idx == 0 || k[i] != prev);
-            prev = k[i];
-            head |= (unsigned)h << i;
-            c += h;
-        }
-        unsigned long long tot;
-        unsigned long long pos = tile_off[tile] + block_excl_scan<unsigned long long>(c, sm, &tot);
-#pragma unroll
-        for (int i = 0; i < kKeysPerThread; ++i) {
-            if (head >> i & 1u) {
-                const unsigned long long g = off + pos;
-                if (g < arena_cap) {
-                    arena[g] = k[i];
-                    if ((pos & (kSplitStride - 1)) == 0) split[g / kSplitStride] = k[i];
-                }
-                ++pos;
-            }
-        }
-    }
-}
-
 // ------------------------------------------------------ backward ---------
 
 template <typename T> __device__ __forceinline__ T cast_rate(double x);
@@ -420,6 +200,63 @@ template <> __device__ __forceinline__ uint32_t cast_rate<uint32_t>(double x) { 
 template <> __device__ __forceinline__ uint64_t cast_rate<uint64_t>(double x) { return (uint64_t)__double2ull_rz(x); }
 template <> __device__ __forceinline__ float cast_rate<float>(double x) { return __double2float_rn(x); }
 template <> __device__ __forceinline__ double cast_rate<double>(double x) { return x; }
+
+// ------------------------------------------------- layer rate index ------
+//
+// The backward pass looks up every child position in the rates of layers
+// t+1 and t+2. Each of those layers gets an open-addressing hash index of its
+// live entries (rate > zero; a missing key reads as zero, exactly like a
+// zero-rate entry): 16-byte slots {key, rate bits}, key 0 = empty (no board
+// is 0), capacity a power of two of at least twice the layer, linear probing.
+// A lookup costs ~1.3 dependent 16-byte loads instead of the ~18 of a binary
+// search, and the eight lookups of one empty cell are issued together.
+
+__device__ __forceinline__ uint64_t mix64(uint64_t k) {
+    k ^= k >> 33;
+    k *= 0xFF51AFD7ED558CCDull;
+    k ^= k >> 33;
+    k *= 0xC4CEB9FE1A85EC53ull;
+    k ^= k >> 33;
+    return k;
+}
+
+template <typename T> __device__ __forceinline__ unsigned long long rate_bits(T r) {
+    if constexpr (sizeof(T) == 4) return (unsigned long long)__float_as_uint(*reinterpret_cast<const float *>(&r));
+    else return (unsigned long long)__double_as_longlong(*reinterpret_cast<const double *>(&r));
+}
+template <typename T> __device__ __forceinline__ T rate_from_bits(unsigned long long b) {
+    T r;
+    if constexpr (sizeof(T) == 4) {
+        const unsigned u = (unsigned)b;
+        memcpy(&r, &u, 4);
+    } else {
+        memcpy(&r, &b, 8);
+    }
+    return r;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+index_insert_kernel(const uint64_t *__restrict__ arena, const T *__restrict__ rates,
+                    const unsigned long long *__restrict__ layer_off, const unsigned long long *__restrict__ layer_len,
+                    int t, T zero, ulonglong2 *__restrict__ slots, unsigned long long mask) {
+    const unsigned long long n = layer_len[t], o = layer_off[t];
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const T r = rates[o + i];
+        if (!(r > zero)) continue;
+        const uint64_t key = arena[o + i];
+        unsigned long long h = mix64(key) & mask;
+        for (unsigned long long probe = 0; probe <= mask; ++probe) {
+            const unsigned long long prev = atomicCAS(&slots[h].x, 0ull, (unsigned long long)key);
+            if (prev == 0ull || prev == key) {
+                slots[h].y = rate_bits<T>(r);
+                break;
+            }
+            h = (h + 1) & mask;
+        }
+    }
+}
 
 // Backward solve of layer t (recalculate_layer, native_core/src/BookSolver.cpp:
 // 413-470). Per board: success with do_check -> max; else for every empty
@@ -429,16 +266,12 @@ template <> __device__ __forceinline__ double cast_rate<double>(double x) { retu
 // reference's `+=` statements as its -Ofast x86-64-v3 build contracts them.
 template <typename T>
 __global__ void __launch_bounds__(256)
-solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates, const uint64_t *__restrict__ split,
+solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
              const unsigned long long *__restrict__ layer_off, const unsigned long long *__restrict__ layer_len,
              int t, DevSpec spec, int do_check, const uint32_t *__restrict__ tab, double p4, T zero, T maxv,
-             DevCtl *ctl) {
-    const unsigned long long n0 = layer_len[t];
-    const unsigned long long o0 = layer_off[t], o1 = layer_off[t + 1], o2 = layer_off[t + 2];
-    const unsigned long long n1 = layer_len[t + 1], n2 = layer_len[t + 2];
-    const uint64_t *k1 = arena + o1, *k2 = arena + o2;
-    const T *r1 = rates + o1, *r2 = rates + o2;
-    const uint64_t *s1 = split + o1 / kSplitStride, *s2 = split + o2 / kSplitStride;
+             const ulonglong2 *__restrict__ idx1, unsigned long long m1, const ulonglong2 *__restrict__ idx2,
+             unsigned long long m2, DevCtl *ctl) {
+    const unsigned long long n0 = layer_len[t], o0 = layer_off[t];
     const double w2 = 1.0 - p4;
     unsigned long long looks = 0;
     for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n0;
@@ -457,23 +290,52 @@ solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates, const ui
             const int k = (__ffsll((long long)empt) - 1) >> 2;
             empt &= empt - 1;
             ++nempty;
+            // the eight children of this cell: j = 0..3 spawn 2, j = 4..7 spawn 4
+            uint64_t key[8];
+            unsigned pend = 0;
 #pragma unroll
             for (int v = 1; v <= 2; ++v) {
                 uint64_t mv[4], s;
                 spawn_moves(tab, mc, k, (uint64_t)v, s, mv);
-                T best = zero;
 #pragma unroll
                 for (int d = 0; d < 4; ++d) {
-                    if (mv[d] != s && is_pattern(mv[d], spec)) {
-                        const uint64_t key = canonical(mv[d], spec.symm);
-                        const T got = v == 1 ? layer_lookup<T>(k1, r1, n1, s1, key, zero)
-                                             : layer_lookup<T>(k2, r2, n2, s2, key, zero);
-                        ++looks;
-                        if (best < got) best = got;
+                    const int j = (v - 1) * 4 + d;
+                    key[j] = canonical(mv[d], spec.symm);
+                    if (mv[d] != s && is_pattern(mv[d], spec)) pend |= 1u << j;
+                }
+            }
+            looks += __popc(pend);
+            unsigned long long h[8];
+            T got[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                got[j] = zero;
+                h[j] = mix64(key[j]) & (j < 4 ? m1 : m2);
+            }
+            while (pend) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    if (pend >> j & 1u) {
+                        const ulonglong2 sl = __ldg((j < 4 ? idx1 : idx2) + h[j]);
+                        if (sl.x == key[j]) {
+                            got[j] = rate_from_bits<T>(sl.y);
+                            pend &= ~(1u << j);
+                        } else if (sl.x == 0ull) {
+                            pend &= ~(1u << j);
+                        } else {
+                            h[j] = (h[j] + 1) & (j < 4 ? m1 : m2);
+                        }
                     }
                 }
-                acc = fma((double)best, v == 1 ? w2 : p4, acc);
             }
+            T best2 = zero, best4 = zero;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (best2 < got[j]) best2 = got[j];
+                if (best4 < got[j + 4]) best4 = got[j + 4];
+            }
+            acc = fma((double)best2, w2, acc);
+            acc = fma((double)best4, p4, acc);
         }
         rates[o0 + i] = nempty > 0 ? cast_rate<T>(acc / (double)nempty) : zero;
     }
@@ -554,6 +416,140 @@ book_write_kernel(const uint64_t *__restrict__ arena, const T *__restrict__ rate
                         *reinterpret_cast<T *>(book + byte + 8) = r;
                     } else {
                         // 12-byte records are only 4-byte aligned
+                        uint32_t *w = reinterpret_cast<uint32_t *>(book + byte);
+                        w[0] = (uint32_t)key;
+                        w[1] = (uint32_t)(key >> 32);
+                        w[2] = *reinterpret_cast<const uint32_t *>(&r);
+                    }
+                } else {
+                    atomicOr(&ctl->err, kErrBookOverflow);
+                }
+                ++pos;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------- all-layer book packing ----
+//
+// After the backward pass every layer is packed at once: the tiles of all
+// layers form one sequence (layer L owns tiles first_tile[L] ..
+// first_tile[L+1]-1), one count kernel, one scan, one write kernel.
+
+__device__ __forceinline__ int layer_of_tile(const unsigned long long *first_tile, int n_layers,
+                                             unsigned long long g) {
+    int lo = 0, hi = n_layers;  // largest L with first_tile[L] <= g
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (first_tile[mid] <= g) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSortThreads)
+book_count_all_kernel(const T *__restrict__ rates, const unsigned long long *__restrict__ layer_off,
+                      const unsigned long long *__restrict__ layer_len, const unsigned long long *__restrict__ first_tile,
+                      int n_layers, unsigned long long n_tiles, T zero, unsigned *__restrict__ tile_cnt,
+                      unsigned long long *__restrict__ layer_max) {
+    __shared__ unsigned long long sm[33];
+    __shared__ unsigned long long smax;
+    for (unsigned long long g = blockIdx.x; g < n_tiles; g += gridDim.x) {
+        const int L = layer_of_tile(first_tile, n_layers, g);
+        const unsigned long long n = layer_len[L], o = layer_off[L];
+        const unsigned long long base = (g - first_tile[L]) * kTileKeys + threadIdx.x;
+        if (threadIdx.x == 0) smax = 0;
+        unsigned long long c = 0, mx = 0;
+#pragma unroll 4
+        for (int i = 0; i < kKeysPerThread; ++i) {
+            const unsigned long long idx = base + (unsigned long long)i * kSortThreads;
+            if (idx < n) {
+                const T r = rates[o + idx];
+                if (r > zero) {
+                    ++c;
+                    const unsigned long long ob = ordered_bits((double)r);
+                    mx = ob > mx ? ob : mx;
+                }
+            }
+        }
+        unsigned long long tot;
+        block_excl_scan<unsigned long long>(c, sm, &tot);
+        if (mx) atomicMax(&smax, mx);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tile_cnt[g] = (unsigned)tot;
+            if (smax) atomicMax(layer_max + L, smax);
+        }
+        __syncthreads();
+    }
+}
+
+// Single block: exclusive scan of `count` tile counts.
+static __global__ void __launch_bounds__(1024)
+scan_tiles_kernel(const unsigned *__restrict__ cnt, unsigned long long count, unsigned long long *__restrict__ off,
+                  unsigned long long *total_out) {
+    __shared__ unsigned long long sm[33];
+    unsigned long long run = 0, tot;
+    for (unsigned long long c0 = 0; c0 < count; c0 += blockDim.x) {
+        const unsigned long long i = c0 + threadIdx.x;
+        const unsigned long long x = i < count ? cnt[i] : 0;
+        const unsigned long long ex = block_excl_scan<unsigned long long>(x, sm, &tot);
+        if (i < count) off[i] = run + ex;
+        run += tot;
+    }
+    if (threadIdx.x == 0) *total_out = run;
+}
+
+static __global__ void book_lens_kernel(const unsigned long long *__restrict__ first_tile, int n_layers,
+                                 unsigned long long n_tiles, const unsigned long long *__restrict__ tile_off,
+                                 const unsigned long long *__restrict__ total, unsigned long long *__restrict__ book_len) {
+    for (int L = blockIdx.x * blockDim.x + threadIdx.x; L < n_layers; L += gridDim.x * blockDim.x) {
+        const unsigned long long a = first_tile[L] < n_tiles ? tile_off[first_tile[L]] : *total;
+        const unsigned long long b = first_tile[L + 1] < n_tiles ? tile_off[first_tile[L + 1]] : *total;
+        book_len[L] = b - a;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSortThreads)
+book_write_all_kernel(const uint64_t *__restrict__ arena, const T *__restrict__ rates,
+                      const unsigned long long *__restrict__ layer_off, const unsigned long long *__restrict__ layer_len,
+                      const unsigned long long *__restrict__ first_tile, int n_layers, unsigned long long n_tiles, T zero,
+                      const unsigned long long *__restrict__ tile_off, unsigned char *__restrict__ book,
+                      unsigned long long book_cap_bytes, DevCtl *ctl) {
+    __shared__ unsigned long long sm[33];
+    constexpr int rec = 8 + (int)sizeof(T);
+    for (unsigned long long g = blockIdx.x; g < n_tiles; g += gridDim.x) {
+        const int L = layer_of_tile(first_tile, n_layers, g);
+        const unsigned long long n = layer_len[L], o = layer_off[L];
+        const unsigned long long base = (g - first_tile[L]) * kTileKeys + (unsigned long long)threadIdx.x * kKeysPerThread;
+        unsigned live = 0, c = 0;
+#pragma unroll
+        for (int i = 0; i < kKeysPerThread; ++i) {
+            const unsigned long long idx = base + i;
+            const bool l = idx < n && rates[o + idx] > zero;
+            live |= (unsigned)l << i;
+            c += l;
+        }
+        unsigned long long tot;
+        unsigned long long pos = tile_off[g] - tile_off[first_tile[L]] +
+                                 block_excl_scan<unsigned long long>(c, sm, &tot);
+        const unsigned long long book0 = o * rec;
+        for (int i = 0; i < kKeysPerThread; ++i) {
+            if (live >> i & 1u) {
+                const unsigned long long byte = book0 + pos * rec;
+                if (byte + rec <= book_cap_bytes) {
+                    const uint64_t key = arena[o + base + i];
+                    const T r = rates[o + base + i];
+                    if constexpr (rec == 16) {
+                        *reinterpret_cast<uint64_t *>(book + byte) = key;
+                        *reinterpret_cast<T *>(book + byte + 8) = r;
+                    } else {
                         uint32_t *w = reinterpret_cast<uint32_t *>(book + byte);
                         w[0] = (uint32_t)key;
                         w[1] = (uint32_t)(key >> 32);

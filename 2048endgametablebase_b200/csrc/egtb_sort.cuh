@@ -1,0 +1,300 @@
+// Onesweep LSD radix sort + single-pass unique of a layer's candidates.
+//
+// Digits are 8 bits made of two free nibbles (nibbles pinned to 0xF in every
+// canonical key never vary, so they are not sorted). One kernel computes the
+// digit histograms of every pass; each pass is then ONE kernel: a block claims
+// the next tile (4096 keys) with an atomic, ranks its keys per digit
+// (warp-striped, __match_any_sync), publishes its per-digit counts, looks back
+// over the previous tiles' counts (decoupled look-back) for its global digit
+// offsets, and scatters through shared memory so global writes run along digit
+// runs. The unique kernel keeps the first of every run of equal keys, writes
+// them as layer L of the arena (same look-back scheme for the output offset)
+// and closes the layer (length, next offset, capacity check).
+//
+// Every wait on another block is bounded: after kSpinLimit polls the kernel
+// flags kErrTimeout and carries on (the host reports EGTB_ERR_TIMEOUT). A tile
+// id is only ever held by a running block, which publishes its own counts
+// before it waits, so the waits always end.
+#pragma once
+
+#include <cstdint>
+
+#include "egtb_kernels.cuh"
+
+namespace egtb {
+
+constexpr unsigned kErrTimeout = 8u;
+constexpr unsigned long long kFlagAgg = 1ull << 32;
+constexpr unsigned long long kFlagPrefix = 2ull << 32;
+constexpr unsigned long long kFlagMask = 3ull << 32;
+constexpr unsigned kSpinLimit = 1u << 22;
+constexpr int kMaxPasses = 8;
+constexpr int kCounterUnique = 15;  // tile counter slot of the unique kernel
+
+// Digit layout of every pass: digit = nibble lo | nibble hi << 4 (hi < 0: none).
+struct SortPlan {
+    int passes;
+    int lo[kMaxPasses];
+    int hi[kMaxPasses];
+};
+
+// status word: [63:34] epoch, [33:32] flag, [31:0] count
+__device__ __forceinline__ unsigned long long status_word(unsigned epoch, unsigned long long flag, unsigned count) {
+    return ((unsigned long long)(epoch & 0x3FFFFFFFu) << 34) | flag | (unsigned long long)count;
+}
+
+__device__ __forceinline__ unsigned sort_digit(uint64_t key, const SortPlan &sp, int p) {
+    unsigned d = (unsigned)(key >> (4 * sp.lo[p])) & 0xFu;
+    if (sp.hi[p] >= 0) d |= ((unsigned)(key >> (4 * sp.hi[p])) & 0xFu) << 4;
+    return d;
+}
+
+__device__ __forceinline__ void publish_status(unsigned long long *p, unsigned long long w) {
+    *(volatile unsigned long long *)p = w;
+}
+
+constexpr int kLookWindow = 16;
+
+// Sum of the counts of tiles tile-1, tile-2, ... back to (and including) the
+// nearest one that published its inclusive prefix. Words are at
+// base[j * stride]; kLookWindow predecessors are read at once, so a chain of
+// tiles that all started together is walked kLookWindow tiles per round trip.
+__device__ __forceinline__ unsigned long long look_back(const unsigned long long *base, unsigned long long stride,
+                                                        long long tile, unsigned epoch, DevCtl *ctl) {
+    const unsigned long long want = (unsigned long long)(epoch & 0x3FFFFFFFu);
+    unsigned long long excl = 0;
+    long long j = tile - 1;
+    unsigned spins = 0;
+    while (j >= 0) {
+        unsigned long long w[kLookWindow];
+#pragma unroll
+        for (int q = 0; q < kLookWindow; ++q)
+            w[q] = (j - q >= 0) ? *(const volatile unsigned long long *)(base + (unsigned long long)(j - q) * stride) : 0ull;
+        int used = 0;
+        bool done = false;
+#pragma unroll
+        for (int q = 0; q < kLookWindow; ++q) {
+            if (done || used < q || j - q < 0) continue;
+            if ((w[q] >> 34) != want || !(w[q] & kFlagMask)) continue;  // not published yet
+            excl += (unsigned)(w[q] & 0xFFFFFFFFull);
+            used = q + 1;
+            if ((w[q] & kFlagMask) == kFlagPrefix) done = true;
+        }
+        if (done) return excl;
+        j -= used;
+        if (used == 0) {
+            if (++spins > kSpinLimit) {
+                atomicOr(&ctl->err, kErrTimeout);
+                return excl;
+            }
+            if (spins > 64) __nanosleep(128);
+        }
+    }
+    return excl;
+}
+
+// Digit histograms of every pass; also resets the tile counters of the coming
+// passes and counts the candidates.
+static __global__ void __launch_bounds__(256)
+sort_hist_kernel(const uint64_t *__restrict__ keys, const unsigned long long *n_ptr, unsigned long long cap, SortPlan sp,
+                 unsigned *__restrict__ hist, unsigned *__restrict__ counters, DevCtl *ctl) {
+    __shared__ unsigned h[kMaxPasses][256];
+    const unsigned long long n = clamp_n(*n_ptr, cap);
+    for (int i = threadIdx.x; i < kMaxPasses * 256; i += blockDim.x) (&h[0][0])[i] = 0;
+    if (blockIdx.x == 0 && threadIdx.x < 16) counters[threadIdx.x] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->candidates += n;
+        ctl->n_sort = n;  // stable copy for the unique kernel, which resets the buffer count
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const unsigned long long step = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < n; base += step) {
+        const unsigned long long i = base + threadIdx.x;
+        const bool valid = i < n;
+        const uint64_t k = valid ? keys[i] : 0;
+        for (int p = 0; p < sp.passes; ++p) {
+            const unsigned d = valid ? sort_digit(k, sp, p) : 256u;
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
+            if (valid && (__ffs(peers) - 1) == lane) atomicAdd(&h[p][d], (unsigned)__popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < sp.passes * 256; i += blockDim.x) {
+        const unsigned c = (&h[0][0])[i];
+        if (c) atomicAdd(hist + i, c);
+    }
+}
+
+// One pass: src -> dst ordered by digit p, stable.
+static __global__ void __launch_bounds__(kSortThreads)
+onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, const unsigned long long *n_ptr,
+                unsigned long long cap, SortPlan sp, int p, const unsigned *__restrict__ hist,
+                unsigned *__restrict__ counters, unsigned long long *__restrict__ status, unsigned epoch, DevCtl *ctl) {
+    __shared__ uint64_t tkeys[kTileKeys];
+    __shared__ unsigned short wcnt[kSortThreads / 32][256];
+    __shared__ unsigned loff[256];
+    __shared__ unsigned long long gbase[256];
+    __shared__ unsigned ghist[256];
+    __shared__ unsigned long long sm[33];
+    __shared__ unsigned tile_sh;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned long long n = clamp_n(*n_ptr, cap);
+    const unsigned long long ntiles = (n + kTileKeys - 1) / kTileKeys;
+    {
+        // start of every digit in the output (same in every block)
+        unsigned long long tot;
+        const unsigned long long ex = block_excl_scan<unsigned long long>(hist[p * 256 + threadIdx.x], sm, &tot);
+        ghist[threadIdx.x] = (unsigned)ex;
+    }
+    for (;;) {
+        if (threadIdx.x == 0) tile_sh = atomicAdd(&counters[p], 1u);
+        for (int i = threadIdx.x; i < (kSortThreads / 32) * 256; i += kSortThreads) (&wcnt[0][0])[i] = 0;
+        __syncthreads();
+        const unsigned long long tile = tile_sh;
+        if (tile >= ntiles) break;
+        const unsigned long long base = tile * kTileKeys + (unsigned long long)warp * (kTileKeys / 8);
+        uint64_t k[kKeysPerThread];
+        unsigned short rank[kKeysPerThread];
+        unsigned short dig[kKeysPerThread];
+#pragma unroll
+        for (int r = 0; r < kKeysPerThread; ++r) {
+            const unsigned long long idx = base + (unsigned long long)r * 32 + lane;
+            const bool valid = idx < n;
+            k[r] = valid ? src[idx] : 0;
+            const unsigned d = valid ? sort_digit(k[r], sp, p) : 256u;
+            dig[r] = (unsigned short)d;
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
+            const unsigned before = __popc(peers & ((1u << lane) - 1u));
+            unsigned short c = 0;
+            if (valid) c = wcnt[warp][d];
+            rank[r] = (unsigned short)(c + before);
+            __syncwarp();
+            if (valid && before == 0) wcnt[warp][d] = (unsigned short)(c + __popc(peers));
+            __syncwarp();
+        }
+        __syncthreads();
+        {
+            const int d = threadIdx.x;
+            unsigned cnt = 0;
+#pragma unroll
+            for (int w = 0; w < kSortThreads / 32; ++w) {
+                const unsigned c = wcnt[w][d];
+                wcnt[w][d] = (unsigned short)cnt;
+                cnt += c;
+            }
+            // publish this tile's count, then look back for the counts before it
+            unsigned long long *my = status + tile * 256 + d;
+            unsigned long long excl = 0;
+            if (tile == 0) {
+                publish_status(my, status_word(epoch, kFlagPrefix, cnt));
+            } else {
+                publish_status(my, status_word(epoch, kFlagAgg, cnt));
+                excl = look_back(status + d, 256, (long long)tile, epoch, ctl);
+                publish_status(my, status_word(epoch, kFlagPrefix, (unsigned)(excl + cnt)));
+            }
+            gbase[d] = (unsigned long long)ghist[d] + excl;
+            unsigned long long tot;
+            loff[d] = (unsigned)block_excl_scan<unsigned long long>((unsigned long long)cnt, sm, &tot);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kKeysPerThread; ++r) {
+            const unsigned d = dig[r];
+            if (d < 256u) tkeys[loff[d] + wcnt[warp][d] + rank[r]] = k[r];
+        }
+        __syncthreads();
+        const unsigned long long rem = n - tile * kTileKeys;
+        const unsigned tile_n = rem < (unsigned long long)kTileKeys ? (unsigned)rem : (unsigned)kTileKeys;
+        for (unsigned i = threadIdx.x; i < tile_n; i += kSortThreads) {
+            const uint64_t key = tkeys[i];
+            const unsigned d = sort_digit(key, sp, p);
+            dst[gbase[d] + (i - loff[d])] = key;
+        }
+        __syncthreads();
+    }
+}
+
+// Unique + layer write + layer close, single pass. keys: sorted candidates
+// of buffer x; layer L goes to arena[layer_off[L] ..]. The last tile records
+// layer_len[L] and the next 16-aligned offset, resets the buffer's count and
+// the histograms for the next sort, and reports progress.
+static __global__ void __launch_bounds__(kSortThreads)
+unique_layer_kernel(const uint64_t *__restrict__ keys, int x, unsigned long long cap, uint64_t *__restrict__ arena,
+                    unsigned long long *__restrict__ layer_off, unsigned long long *__restrict__ layer_len, int L,
+                    unsigned long long arena_cap, unsigned *__restrict__ counters,
+                    unsigned long long *__restrict__ ustatus, unsigned epoch, unsigned *__restrict__ hist,
+                    DevCtl *ctl, unsigned *progress) {
+    __shared__ unsigned long long sm[33];
+    __shared__ unsigned tile_sh;
+    __shared__ unsigned long long excl_sh;
+    const unsigned long long n = clamp_n(ctl->n_sort, cap);
+    const unsigned long long ntiles = (n + kTileKeys - 1) / kTileKeys;
+    const unsigned long long off = layer_off[L];
+    auto close = [&](unsigned long long total) {
+        const unsigned long long end = off + total;
+        const unsigned long long next = (end + kSplitStride - 1) & ~(unsigned long long)(kSplitStride - 1);
+        if (next > arena_cap || (ctl->err & kErrArenaOverflow)) {
+            atomicOr(&ctl->err, kErrArenaOverflow);
+            layer_len[L] = 0;
+            layer_off[L + 1] = off;
+        } else {
+            layer_len[L] = total;
+            layer_off[L + 1] = next;
+        }
+        ctl->cand_count[x] = 0;
+        for (int i = 0; i < kMaxPasses * 256; ++i) hist[i] = 0;
+        if (progress) *(volatile unsigned *)progress = (unsigned)L;
+    };
+    if (ntiles == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) close(0);
+        return;
+    }
+    for (;;) {
+        if (threadIdx.x == 0) tile_sh = atomicAdd(&counters[kCounterUnique], 1u);
+        __syncthreads();
+        const unsigned long long tile = tile_sh;
+        if (tile >= ntiles) break;
+        const unsigned long long base = tile * kTileKeys + (unsigned long long)threadIdx.x * kKeysPerThread;
+        uint64_t k[kKeysPerThread];
+        unsigned head = 0, c = 0;
+        uint64_t prev = (base > 0 && base < n) ? keys[base - 1] : 0;
+#pragma unroll
+        for (int i = 0; i < kKeysPerThread; ++i) {
+            const unsigned long long idx = base + i;
+            k[i] = idx < n ? keys[idx] : 0;
+            const bool hd = idx < n && (idx == 0 || k[i] != prev);
+            prev = k[i];
+            head |= (unsigned)hd << i;
+            c += hd;
+        }
+        unsigned long long tile_total;
+        const unsigned long long local = block_excl_scan<unsigned long long>((unsigned long long)c, sm, &tile_total);
+        if (threadIdx.x == 0) {
+            unsigned long long *my = ustatus + tile;
+            unsigned long long excl = 0;
+            if (tile == 0) {
+                publish_status(my, status_word(epoch, kFlagPrefix, (unsigned)tile_total));
+            } else {
+                publish_status(my, status_word(epoch, kFlagAgg, (unsigned)tile_total));
+                excl = look_back(ustatus, 1, (long long)tile, epoch, ctl);
+                publish_status(my, status_word(epoch, kFlagPrefix, (unsigned)(excl + tile_total)));
+            }
+            excl_sh = excl;
+            if (tile == ntiles - 1) close(excl + tile_total);
+        }
+        __syncthreads();
+        unsigned long long pos = excl_sh + local;
+#pragma unroll
+        for (int i = 0; i < kKeysPerThread; ++i) {
+            if (head >> i & 1u) {
+                const unsigned long long g = off + pos;
+                if (g < arena_cap) arena[g] = k[i];
+                ++pos;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace egtb

@@ -193,6 +193,16 @@ EGTB_API int egtb_move_all_dir(int device, const uint64_t *boards, size_t n, uin
 EGTB_API int egtb_canonical(int device, const uint64_t *boards, size_t n, int32_t symm_mode, uint64_t *out);
 EGTB_API int egtb_apply_sym(int device, const uint64_t *boards, size_t n, int32_t symm_index, uint64_t *out);
 
+/* Sort the n keys at d_keys (device memory) ascending, drop repeats, write
+ * the unique keys to d_out (device, room for n keys, must not alias d_keys)
+ * and their count to *d_n_out (device). Enqueued on `stream`
+ * (cudaStream_t as void*, NULL = legacy default stream); scratch is taken
+ * and returned stream-ordered. The device counterpart of the reference's
+ * sort/unique plug-in seam (sort_uint64, native_core/xss_wrapper.cpp:14-31;
+ * unique_sorted_u64_inplace, native_core/src/unique_wrapper.cpp:12-14). */
+EGTB_API int egtb_sort_unique_u64(int device, const uint64_t *d_keys, size_t n, uint64_t *d_out,
+                                  uint64_t *d_n_out, void *stream);
+
 /* ------------------------------------------------------------ books ----- */
 
 typedef struct egtb_book egtb_book;

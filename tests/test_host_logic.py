@@ -1,0 +1,84 @@
+"""Host-side logic that mirrors the reference's Python layer: pattern catalog
+parsing, steps/docheck, option defaults, reader result ordering."""
+import numpy as np
+import pytest
+
+import helpers as H
+
+
+def patterns():
+    import importlib
+    return importlib.import_module("2048endgametablebase_b200.patterns")
+
+
+def test_builtin_catalog_matches_golden_cases():
+    P = patterns()
+    for key in ("L3_32_float32", "442_64_float32", "L3_256_float32", "442_512_float32"):
+        case = H.cases()[key]
+        meta = P.pattern_catalog[case["pattern"]]
+        assert [hex(int(m)) for m in meta["pattern_masks"]] == case["masks"]
+        assert list(meta["success_shifts"]) == case["shifts"]
+        assert [hex(int(s)) for s in meta["seed_boards"]] == case["seeds"]
+        assert -meta["nums_adjust"] == case["tile_sum0"]
+        steps, docheck = P.steps_and_docheck(case["tile_sum0"], case["target"], meta["extra_steps"])
+        assert (steps, docheck) == (case["steps"], case["docheck_step"])
+
+
+def test_4432_is_diagonal_with_13_free_cells():
+    P = patterns()
+    meta = P.pattern_catalog["4432"]
+    assert meta["canonical_mode"] == "diagonal"
+    assert bin(int(meta["pattern_masks"][0])).count("1") == 12  # three pinned cells
+
+
+def test_seed_filter_keeps_the_first_tile_sum():
+    P = patterns()
+    e = P.parse_entry("x", {"valid pattern": ["0xf"], "seed boards": ["0x12f", "0x11f", "0x21f"]})
+    assert [hex(int(b)) for b in e["seed_boards"]] == ["0x12f", "0x21f"]
+
+
+def test_success_shifts_from_target_pos():
+    P = patterns()
+    assert P.find_f_nibble_positions(0xF000000) == [24]
+    assert P.find_f_nibble_positions(0xFFFFFFFFFFFFFFFF) == list(range(0, 64, 4))
+
+
+def test_run_options_defaults_match_reference():
+    F = H.fc()
+    o = F.RunOptions()
+    assert (o.spawn_rate4, o.success_rate_dtype, o.direct_io_queue_depth, o.direct_io_chunk_mib) == (
+        0.1, "uint32", 16, 8)
+    assert F.dtype_code("nonsense") == 0 and F.dtype_code("1-float64") == 5
+
+
+def test_adjust_direction_is_a_bijection_per_op():
+    F = H.fc()
+    for op in range(8):
+        names = {F._adjust_direction(op, d) for d in ("up", "right", "down", "left")}
+        assert names == {"up", "right", "down", "left"}
+
+
+def test_sorted_entries_are_stable_and_descending():
+    F = H.fc()
+    vals = np.array([0.5, 0.9, 0.5, 0.1])  # up, right, down, left
+    entries = F.ClassicBookReader._sorted_entries(0, vals, 0b0111)
+    # kOrderedResultKeys order is down, right, left, up; left has no value
+    assert entries == [("right", 0.9), ("down", 0.5), ("up", 0.5), ("left", None)]
+
+
+def test_encode_matrix_and_c_division():
+    F = H.fc()
+    enc, total = F._encode_matrix([[2, 0, 0, 0], [0, 4, 0, 0], [0, 0, 0, 0], [0, 0, 0, 32768]])
+    assert enc == (1 << 60) | (2 << 40) | (15 << 0)
+    assert total == 2 + 4 + 32768
+
+
+@pytest.mark.parametrize("key", ["L3_32_float32", "diag9_64_float32"])
+def test_reader_fixture_ordering_rules(key):
+    """Every golden answer is in the reference's order: numeric values
+    descending, then the unmoved directions."""
+    for entry in H.reader_cases()[key]:
+        vals = [v for _, v in entry["result"] if isinstance(v, float)]
+        assert vals == sorted(vals, reverse=True)
+        kinds = [isinstance(v, float) for _, v in entry["result"]]
+        assert kinds == sorted(kinds, reverse=True)
