@@ -88,6 +88,9 @@ SMALL_CASES = [
     ("free5", 5, "float32"), ("free6", 5, "float32"), ("LL", 5, "float32"), ("t", 6, "uint32"),
 ]
 FULL_CASES = [("L3", 8, "float32"), ("442", 9, "float32")]
+# the 13-cell diagonal table (config-2 family) at the largest target the
+# reference can build here (2.25e9 boards, ~45 GB of files, ~10 min)
+HUGE_CASES = [("4432", 7, "float32")]
 
 
 def sha(path: str) -> str:
@@ -128,6 +131,9 @@ def run_case(catalog, pat, target, dtype):
         "partial_len": [int(last0.size), int(last1.size)],
         "book_len": book_len, "book_sha256": book_sha,
     }
+    if (pat, target, dtype) in HUGE_CASES:
+        import shutil
+        shutil.rmtree(gdir, ignore_errors=True)
     return case, bdir
 
 
@@ -218,6 +224,7 @@ def reader_fixture(case, bdir, rng, n_pos=60):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--full", action="store_true", help="also the full-size L3-256 and 442-512 builds")
+    ap.add_argument("--huge", action="store_true", help="also the 4432-128 build (needs ~45 GB of disk in GOLDEN_WORK)")
     ap.add_argument("--only", default="", help="comma-separated case keys to (re)generate")
     args = ap.parse_args()
     R.build()
@@ -228,7 +235,7 @@ def main():
     cases = json.load(open(cases_path)) if os.path.exists(cases_path) else {}
     reader = {}
     rng = np.random.default_rng(7)
-    todo = SMALL_CASES + (FULL_CASES if args.full else [])
+    todo = SMALL_CASES + (FULL_CASES if args.full else []) + (HUGE_CASES if args.huge else [])
     only = set(filter(None, args.only.split(",")))
     for pat, target, dtype in todo:
         key = f"{pat}_{2 ** target}_{dtype}"
@@ -236,10 +243,14 @@ def main():
             continue
         print("case", key, flush=True)
         case, bdir = run_case(catalog, pat, target, dtype)
-        case["size_class"] = "full" if (pat, target, dtype) in FULL_CASES else "small"
+        case["size_class"] = ("full" if (pat, target, dtype) in FULL_CASES else
+                              "huge" if (pat, target, dtype) in HUGE_CASES else "small")
         cases[key] = case
         if case["size_class"] == "small" and pat in ("44", "L3", "diag9", "horiz8", "free6", "442"):
             reader[key] = reader_fixture(case, bdir, rng)
+        if case["size_class"] == "huge":
+            import shutil
+            shutil.rmtree(os.path.dirname(bdir.rstrip("/")), ignore_errors=True)
         if key == "free5_32_float32":
             data = {}
             for t in range(case["steps"]):
