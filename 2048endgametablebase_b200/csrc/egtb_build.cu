@@ -93,7 +93,8 @@ static unsigned long long align16(unsigned long long x) { return (x + 15ull) & ~
         ++(E).launches;      \
     } while (0)
 
-static const char *kKindNames[] = {"expand", "sort_pass", "unique", "solve", "book_pack", "final_layers", "rate_index"};
+static const char *kKindNames[] = {"expand", "sort_pass", "layer_sort", "solve", "book_pack", "final_layers",
+                                   "rate_index"};
 enum { K_EXPAND = 0, K_SORT_PASS, K_UNIQUE, K_SOLVE, K_PACK, K_FINAL, K_INDEX, K_NKINDS };
 
 struct Engine {
@@ -153,7 +154,6 @@ struct Engine {
     // capacities (elements)
     unsigned long long arena_cap = 0, cand_cap = 0;
     int steps_cap = 0;
-    int filter_bits = 22;
 
     uint64_t *arena = nullptr;
     void *rates = nullptr;
@@ -169,7 +169,10 @@ struct Engine {
     unsigned *tile_cnt = nullptr;
     unsigned long long *tile_off = nullptr;
     unsigned long long sort_tiles = 0, comp_tiles = 0;
-    uint64_t *filter = nullptr;
+    uint64_t *dset[2] = {nullptr, nullptr};  // exact dedup sets of the layers under construction (by parity)
+    unsigned long long dset_cap = 0;          // slots per set
+    unsigned long long *dense_off = nullptr;  // layer sort: dense offsets of the layers
+    unsigned long long candidates = 0;        // children probed by the last forward pass
     unsigned long long *layer_off = nullptr, *layer_len = nullptr, *book_len = nullptr;
     unsigned long long *layer_max = nullptr;  // ordered encoding of the largest rate per layer
     unsigned char *book = nullptr;
@@ -197,9 +200,6 @@ struct Engine {
         sm_count = prop.multiProcessorCount;
         EGTB_CUDA(cudaMalloc(&ctl, sizeof(DevCtl)));
         for (auto &e : ev) EGTB_CUDA(cudaEventCreate(&e));
-        const char *fb = getenv("EGTB_FILTER_BITS");
-        if (fb) filter_bits = std::max(10, std::min(30, atoi(fb)));
-        EGTB_CUDA(cudaMalloc(&filter, sizeof(uint64_t) << filter_bits));
         EGTB_CUDA(cudaMalloc(&hist, sizeof(unsigned) * kMaxPasses * 256));
         EGTB_CUDA(cudaMemset(hist, 0, sizeof(unsigned) * kMaxPasses * 256));
         EGTB_CUDA(cudaMalloc(&counters, sizeof(unsigned) * 16));
@@ -238,6 +238,28 @@ struct Engine {
         alloc_or_throw((void **)&layer_max, sizeof(unsigned long long) * steps_cap, "layer maxima");
         release(first_tile);
         alloc_or_throw((void **)&first_tile, sizeof(unsigned long long) * steps_cap, "tile map");
+        release(dense_off);
+        alloc_or_throw((void **)&dense_off, sizeof(unsigned long long) * steps_cap, "dense offsets");
+    }
+
+    void ensure_dedup(unsigned long long slots) {
+        if (slots <= dset_cap) return;
+        for (auto &p : dset) release(p);
+        dset_cap = slots;
+        for (auto &p : dset) alloc_or_throw((void **)&p, sizeof(uint64_t) * dset_cap, "dedup set");
+    }
+
+    // look-back words for sorts of up to max(cand_cap, arena_cap) keys
+    void ensure_status() {
+        const unsigned long long need = std::max(cand_cap, arena_cap) / kTileKeys + 2;
+        if (need <= sort_tiles) return;
+        release(status);
+        release(ustatus);
+        sort_tiles = need;
+        alloc_or_throw((void **)&status, sizeof(unsigned long long) * 256 * sort_tiles, "sort look-back");
+        alloc_or_throw((void **)&ustatus, sizeof(unsigned long long) * sort_tiles, "unique look-back");
+        EGTB_CUDA(cudaMemset(status, 0, sizeof(unsigned long long) * 256 * sort_tiles));
+        EGTB_CUDA(cudaMemset(ustatus, 0, sizeof(unsigned long long) * sort_tiles));
     }
 
     void ensure_index(unsigned long long slots) {
@@ -260,6 +282,7 @@ struct Engine {
         book_cap_bytes = arena_cap * 16ull;
         alloc_or_throw((void **)&book, book_cap_bytes, "books");
         ensure_comp_tiles();
+        ensure_status();
     }
 
     void ensure_cand(unsigned long long cap) {
@@ -268,17 +291,11 @@ struct Engine {
         release(cand[0]);
         release(cand[1]);
         release(tmp);
-        release(status);
-        release(ustatus);
         cand_cap = cap;
         alloc_or_throw((void **)&cand[0], sizeof(uint64_t) * cand_cap, "candidates");
         alloc_or_throw((void **)&cand[1], sizeof(uint64_t) * cand_cap, "candidates");
         alloc_or_throw((void **)&tmp, sizeof(uint64_t) * cand_cap, "sort buffer");
-        sort_tiles = cand_cap / kTileKeys + 2;
-        alloc_or_throw((void **)&status, sizeof(unsigned long long) * 256 * sort_tiles, "sort look-back");
-        alloc_or_throw((void **)&ustatus, sizeof(unsigned long long) * sort_tiles, "unique look-back");
-        EGTB_CUDA(cudaMemset(status, 0, sizeof(unsigned long long) * 256 * sort_tiles));
-        EGTB_CUDA(cudaMemset(ustatus, 0, sizeof(unsigned long long) * sort_tiles));
+        ensure_status();
         ensure_comp_tiles();
     }
 
@@ -394,6 +411,8 @@ struct ForwardPlan {
     int steps, docheck, first_step;  // first_step: generation starts at step i = first_step
     DevSpec spec;
     SortPlan sort;
+    long long s0;      // tile sum of layer 0; layer t has tile sum s0 + 2t
+    FreeNibbles free;  // nibbles that vary between keys
 };
 
 // Sort the candidates of buffer x and unique them into the arena as layer L:
@@ -420,24 +439,27 @@ static void enqueue_sort_unique(Engine &E, const ForwardPlan &P, int x, int L, u
     E.prof_end(pu);
 }
 
-// Enqueue forward steps first_step .. steps-2 and the final partial layer.
-// Preconditions on the device: layer first_step-1 in the arena at
-// layer_off[first_step-1] (16-aligned) with layer_off[first_step] set after
-// it, cand_count[first_step&1] holding the partial of layer first_step.
+// Enqueue forward steps first_step .. steps-2 (one fused expand + dedup
+// kernel each) and close the last two layers. Preconditions on the device:
+// layer first_step-1 in its staging buffer, layer first_step's keys so far in
+// its staging buffer and set, layer_off[first_step-1] set.
 static void enqueue_forward(Engine &E, const ForwardPlan &P, unsigned *progress) {
     cudaStream_t s = E.stream;
     const int g_exp = E.sm_count * 8;
+    uint64_t *stage[3] = {E.cand[0], E.cand[1], E.tmp};
     for (int i = P.first_step; i < P.steps - 1; ++i) {
         const int t = i - 1;
-        const int x1 = i & 1, x2 = (i + 1) & 1;
-        // buffer x2's count was reset by the unique kernel that consumed it
         const int pe = E.prof_begin(K_EXPAND);
-        EGTB_LAUNCH(E, expand_kernel<<<g_exp, kExpandThreads, 0, s>>>(E.arena, E.layer_off, E.layer_len, t, P.spec, i > P.docheck ? 1 : 0, E.tab, E.cand[x1], E.cand[x2], E.ctl, x1, x2, E.cand_cap, E.filter, E.filter_bits));
+        EGTB_LAUNCH(E, expand_dedup_kernel<<<g_exp, kExpandThreads, 0, s>>>(
+                           stage[t % 3], stage[(t + 1) % 3], stage[(t + 2) % 3], t % 3, (t + 1) % 3, (t + 2) % 3,
+                           E.arena, E.layer_off, E.layer_len, E.arena_cap, t, P.spec, i > P.docheck ? 1 : 0, E.tab,
+                           E.dset[(t + 1) & 1], E.dset[(t + 2) & 1], E.dset_cap - 1, P.s0 + 2ll * (t + 1),
+                           P.s0 + 2ll * (t + 2), E.cand_cap, E.ctl, progress, (unsigned)i));
         E.prof_end(pe);
-        enqueue_sort_unique(E, P, x1, i, progress);
     }
-    const int L = P.steps - 1;
-    enqueue_sort_unique(E, P, L & 1, L, progress);
+    for (int L = std::max(P.first_step, P.steps - 2); L < P.steps; ++L)
+        EGTB_LAUNCH(E, flush_layer_kernel<<<E.sm_count * 2, 256, 0, s>>>(stage[L % 3], L % 3, E.arena, E.layer_off,
+                                                                          E.layer_len, E.arena_cap, L, E.ctl));
 }
 
 static DevCtl read_ctl(Engine &E) {
@@ -447,34 +469,30 @@ static DevCtl read_ctl(Engine &E) {
     return c;
 }
 
-// Reset control state and place the starting layers.
-// start_layer = first_step-1 holds `base` keys; partial (layer first_step) holds `partial` keys.
+__global__ void set_u64_kernel(unsigned long long *p, unsigned long long v) { *p = v; }
+
+// Reset control state and place the starting layers: layer first_step-1
+// (`base`) and what is known of layer first_step (`partial`, also entered in
+// that layer's set).
 static void stage_start(Engine &E, const ForwardPlan &P, const uint64_t *base, size_t n_base, const uint64_t *partial,
                         size_t n_partial) {
     cudaStream_t s = E.stream;
     EGTB_CUDA(cudaMemsetAsync(E.ctl, 0, sizeof(DevCtl), s));
     EGTB_CUDA(cudaMemsetAsync(E.hist, 0, sizeof(unsigned) * kMaxPasses * 256, s));
-    EGTB_CUDA(cudaMemsetAsync(E.filter, 0, sizeof(uint64_t) << E.filter_bits, s));
+    for (auto *d : E.dset) EGTB_CUDA(cudaMemsetAsync(d, 0, sizeof(uint64_t) * E.dset_cap, s));
     EGTB_CUDA(cudaMemsetAsync(E.layer_off, 0, sizeof(unsigned long long) * E.steps_cap, s));
     EGTB_CUDA(cudaMemsetAsync(E.layer_len, 0, sizeof(unsigned long long) * E.steps_cap, s));
-    const int t0 = P.first_step - 1;
-    if (n_base > E.arena_cap) throw Error(EGTB_ERR_CAPACITY, "start layer larger than the arena");
-    if (n_partial > E.cand_cap) throw Error(EGTB_ERR_CAPACITY, "partial layer larger than the candidate buffer");
-    std::vector<unsigned long long> off(P.steps + 2, 0), len(P.steps + 2, 0);
-    len[t0] = n_base;
-    off[t0 + 1] = align16(n_base);
-    // layers before t0 are empty and sit at offset 0
-    EGTB_CUDA(cudaMemcpyAsync(E.layer_off, off.data(), sizeof(unsigned long long) * (P.steps + 2),
-                              cudaMemcpyHostToDevice, s));
-    EGTB_CUDA(cudaMemcpyAsync(E.layer_len, len.data(), sizeof(unsigned long long) * (P.steps + 2),
-                              cudaMemcpyHostToDevice, s));
-    if (n_base)
-        EGTB_CUDA(cudaMemcpyAsync(E.arena, base, sizeof(uint64_t) * n_base, cudaMemcpyHostToDevice, s));
+    if (n_base > E.cand_cap || n_partial > E.cand_cap)
+        throw Error(EGTB_ERR_CAPACITY, "start layer larger than the staging buffers");
+    uint64_t *stage[3] = {E.cand[0], E.cand[1], E.tmp};
+    const int t0 = P.first_step - 1, t1 = P.first_step;
+    if (n_base) EGTB_CUDA(cudaMemcpyAsync(stage[t0 % 3], base, sizeof(uint64_t) * n_base, cudaMemcpyHostToDevice, s));
+    EGTB_LAUNCH(E, set_u64_kernel<<<1, 1, 0, s>>>(&E.ctl->stage_count[t0 % 3], (unsigned long long)n_base));
     if (n_partial) {
-        EGTB_CUDA(cudaMemcpyAsync(E.cand[P.first_step & 1], partial, sizeof(uint64_t) * n_partial,
-                                  cudaMemcpyHostToDevice, s));
-        unsigned long long np = n_partial;
-        EGTB_CUDA(cudaMemcpyAsync(&E.ctl->cand_count[P.first_step & 1], &np, sizeof np, cudaMemcpyHostToDevice, s));
+        EGTB_CUDA(cudaMemcpyAsync(stage[t1 % 3], partial, sizeof(uint64_t) * n_partial, cudaMemcpyHostToDevice, s));
+        EGTB_LAUNCH(E, set_u64_kernel<<<1, 1, 0, s>>>(&E.ctl->stage_count[t1 % 3], (unsigned long long)n_partial));
+        EGTB_LAUNCH(E, dedup_seed_kernel<<<E.sm_count * 4, 256, 0, s>>>(stage[t1 % 3], n_partial, E.dset[t1 & 1],
+                                                                          E.dset_cap - 1, P.s0 + 2ll * t1, E.ctl));
     }
     // the host buffers above may be pageable: finish the copies before returning
     EGTB_CUDA(cudaStreamSynchronize(s));
@@ -487,27 +505,95 @@ static unsigned long long env_keys(const char *name, unsigned long long dflt) {
     return x ? x : dflt;
 }
 
-// Run the forward with capacity regrowth. Returns the number of retries.
+// Sort layers 1 .. steps-1 in place (layer 0 keeps the seeds' order): one
+// radix sort over composite keys when layer index and free nibbles fit 64
+// bits, else one sort per layer. len: host copy of the layer lengths.
+static void enqueue_sort_layers(Engine &E, const ForwardPlan &P, const std::vector<unsigned long long> &len) {
+    cudaStream_t s = E.stream;
+    const int steps = P.steps;
+    if (steps < 2) return;
+    std::vector<unsigned long long> doff(steps + 1, 0);
+    for (int L = 0; L < steps; ++L) doff[L + 1] = doff[L] + len[L];
+    EGTB_CUDA(cudaMemcpyAsync(E.dense_off, doff.data(), sizeof(unsigned long long) * (steps + 1),
+                              cudaMemcpyHostToDevice, s));
+    int lb = 0;
+    while ((1ull << lb) < (unsigned long long)(steps - 1)) ++lb;
+    const int F = P.free.count;
+    uint64_t *comp = (uint64_t *)E.book, *other = comp + E.arena_cap;
+    auto sort_range = [&](int l0, int l1, int nibbles) {
+        const unsigned long long total = doff[l1] - doff[l0];
+        if (total < 2) return;
+        SortPlan sp;
+        std::memset(&sp, 0, sizeof sp);
+        sp.passes = (nibbles + 1) / 2;
+        for (int q = 0; q < sp.passes; ++q) {
+            sp.lo[q] = 2 * q;
+            sp.hi[q] = 2 * q + 1 < nibbles ? 2 * q + 1 : -1;
+        }
+        EGTB_LAUNCH(E, compose_kernel<<<E.sm_count * 8, 256, 0, s>>>(E.arena, E.layer_off, E.dense_off, l0, l1, P.free,
+                                                                      comp));
+        EGTB_CUDA(cudaMemsetAsync(E.hist, 0, sizeof(unsigned) * kMaxPasses * 256, s));
+        EGTB_LAUNCH(E, set_u64_kernel<<<1, 1, 0, s>>>(&E.ctl->cand_count[0], total));
+        EGTB_LAUNCH(E, sort_hist_kernel<<<E.sm_count * 2, 256, 0, s>>>(comp, &E.ctl->cand_count[0], E.arena_cap, sp,
+                                                                       E.hist, E.counters, E.ctl));
+        uint64_t *src = comp, *dst = other;
+        for (int q = 0; q < sp.passes; ++q) {
+            const int pi = E.prof_begin(K_SORT_PASS);
+            EGTB_LAUNCH(E, onesweep_kernel<<<E.sweep_grid, kSortThreads, 0, s>>>(src, dst, &E.ctl->cand_count[0],
+                                                                                 E.arena_cap, sp, q, E.hist, E.counters,
+                                                                                 E.status, E.epoch++, E.ctl));
+            E.prof_end(pi);
+            std::swap(src, dst);
+        }
+        EGTB_LAUNCH(E, decompose_kernel<<<E.sm_count * 8, 256, 0, s>>>(src, E.layer_off, E.dense_off, l0, l1, P.free,
+                                                                        E.arena));
+    };
+    const int pu = E.prof_begin(K_UNIQUE);
+    if (4 * F + lb <= 64 && F < 16) {
+        sort_range(1, steps, F + (lb + 3) / 4);
+    } else {
+        for (int L = 1; L < steps; ++L) sort_range(L, L + 1, F);
+    }
+    E.prof_end(pu);
+}
+
+// Run the forward with capacity regrowth, then sort the layers. Returns the
+// number of retries.
 static int run_forward(Engine &E, const ForwardPlan &P, const uint64_t *base, size_t n_base, const uint64_t *partial,
                        size_t n_partial, float *ms) {
     int retries = 0;
     E.ensure_steps(P.steps);
-    // first capacities: 4 Mi candidate keys, 128 Mi layer keys (EGTB_INIT_CAND_KEYS /
-    // EGTB_INIT_ARENA_KEYS override); a pass that outgrows them is re-run larger
+    // first capacities: 4 Mi keys per staging buffer, 128 Mi layer keys, 4 Mi
+    // slots per dedup set (EGTB_INIT_CAND_KEYS / EGTB_INIT_ARENA_KEYS /
+    // EGTB_INIT_SET_SLOTS override); a pass that outgrows them is re-run larger
     static const unsigned long long init_cand = env_keys("EGTB_INIT_CAND_KEYS", 1ull << 22);
     static const unsigned long long init_arena = env_keys("EGTB_INIT_ARENA_KEYS", 1ull << 27);
-    E.ensure_cand(std::max<unsigned long long>(E.cand_cap, std::max<unsigned long long>(init_cand, n_partial * 2)));
+    static const unsigned long long init_set = env_keys("EGTB_INIT_SET_SLOTS", 1ull << 22);
+    E.ensure_cand(std::max<unsigned long long>(E.cand_cap, std::max<unsigned long long>(init_cand,
+                                                                                         2 * std::max(n_partial, n_base))));
     E.ensure_arena(std::max<unsigned long long>(E.arena_cap, std::max<unsigned long long>(init_arena, n_base * 4)));
+    unsigned long long set_need = init_set;
+    while (set_need < 4 * std::max<unsigned long long>(n_partial, 1)) set_need <<= 1;
+    E.ensure_dedup(std::max(E.dset_cap, set_need));
     unsigned *progress = progress_device_ptr();
     for (;;) {
         stage_start(E, P, base, n_base, partial, n_partial);
         EGTB_CUDA(cudaEventRecord(E.ev[0], E.stream));
         enqueue_forward(E, P, progress);
-        EGTB_CUDA(cudaEventRecord(E.ev[1], E.stream));
         DevCtl c = read_ctl(E);
         EGTB_CUDA(cudaGetLastError());
         E.prof_resolve();
         if (c.err == 0) {
+            std::vector<unsigned long long> len(P.steps + 1);
+            EGTB_CUDA(cudaMemcpy(len.data(), E.layer_len, sizeof(unsigned long long) * (P.steps + 1),
+                                 cudaMemcpyDeviceToHost));
+            E.candidates = c.candidates;
+            enqueue_sort_layers(E, P, len);
+            EGTB_CUDA(cudaEventRecord(E.ev[1], E.stream));
+            DevCtl c2 = read_ctl(E);
+            EGTB_CUDA(cudaGetLastError());
+            E.prof_resolve();
+            if (c2.err & kErrTimeout) throw Error(EGTB_ERR_TIMEOUT, "a bounded device wait gave up in the layer sort");
             EGTB_CUDA(cudaEventElapsedTime(ms, E.ev[0], E.ev[1]));
             return retries;
         }
@@ -516,6 +602,7 @@ static int run_forward(Engine &E, const ForwardPlan &P, const uint64_t *base, si
         if (retries > 24) throw Error(EGTB_ERR_CAPACITY, "forward pass did not fit after repeated regrowth");
         if (c.err & kErrCandOverflow) E.ensure_cand(E.cand_cap * 2);
         if (c.err & kErrArenaOverflow) E.ensure_arena(E.arena_cap * 2);
+        if (c.err & kErrDedupOverflow) E.ensure_dedup(E.dset_cap * 4);
     }
 }
 
@@ -770,6 +857,27 @@ static void check_common(const uint64_t *seeds, size_t n_seeds, const egtb_patte
     if (o->steps > (1 << 20)) throw Error(EGTB_ERR_ARG, "steps out of range");
 }
 
+static long long seed_tile_sum(uint64_t b) {
+    long long s = 0;
+    for (int k = 0; k < 16; ++k) {
+        const int v = (int)((b >> (4 * k)) & 0xF);
+        s += v ? (1ll << v) : 0ll;
+    }
+    return s;
+}
+
+// Tile sum of layer 0. The layer sets rely on every layer having one tile
+// sum, which the reference's pattern catalog guarantees by keeping only the
+// seeds of the first seed's sum (Config.py:241-248).
+static long long layer0_tile_sum(const uint64_t *seeds, size_t n) {
+    if (n == 0) return 0;
+    const long long s0 = seed_tile_sum(seeds[0]);
+    for (size_t i = 1; i < n; ++i)
+        if (seed_tile_sum(seeds[i]) != s0)
+            throw Error(EGTB_ERR_ARG, "seed boards must share one tile sum (as the pattern catalog keeps them)");
+    return s0;
+}
+
 static ForwardPlan make_forward_plan(const egtb_pattern_spec &spec, const egtb_run_options &o, int first_step) {
     ForwardPlan P;
     P.steps = o.steps;
@@ -777,6 +885,12 @@ static ForwardPlan make_forward_plan(const egtb_pattern_spec &spec, const egtb_r
     P.first_step = first_step;
     P.spec = make_dev_spec(spec, o.target);
     P.sort = sort_plan(spec);
+    P.s0 = 0;
+    const uint64_t pinned = pinned_nibbles(spec);
+    std::memset(&P.free, 0, sizeof P.free);
+    P.free.pinned = pinned;
+    for (int k = 0; k < 16; ++k)
+        if (((pinned >> (4 * k)) & 0xF) != 0xF) P.free.idx[P.free.count++] = k;
     return P;
 }
 
@@ -795,6 +909,7 @@ static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const 
     const uint32_t total = (uint32_t)(steps * 2);
     set_progress(0, total);
     ForwardPlan P = make_forward_plan(spec, o, 1);
+    P.s0 = layer0_tile_sum(seeds, n_seeds);
     float fwd_ms = 0.f, bwd_ms = 0.f;
     const int retries = run_forward(E, P, seeds, n_seeds, nullptr, 0, &fwd_ms);
     std::vector<unsigned long long> off = d2h_u64(E, E.layer_off, steps + 1);
@@ -836,7 +951,7 @@ static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const 
             st->book_entries += blen[t];
             st->max_layer = std::max<uint64_t>(st->max_layer, len[t]);
         }
-        st->candidates = c.candidates;
+        st->candidates = E.candidates;
         st->lookups = c.lookups;
         st->layers = steps;
         st->retries = retries;
@@ -878,6 +993,8 @@ static void generate_files(Engine &E, const uint64_t *seeds, size_t n_seeds, con
             partial = read_u64_file(p + std::to_string(i0));
         }
         ForwardPlan P = make_forward_plan(spec, o, i0);
+        P.s0 = n_seeds ? layer0_tile_sum(seeds, n_seeds)
+                       : (base.empty() ? 0 : seed_tile_sum(base[0]) - 2ll * (i0 - 1));
         retries = run_forward(E, P, base.data(), base.size(), partial.data(), partial.size(), &fwd_ms);
         off = d2h_u64(E, E.layer_off, steps + 1);
         len = d2h_u64(E, E.layer_len, steps + 1);
@@ -911,8 +1028,7 @@ static void generate_files(Engine &E, const uint64_t *seeds, size_t n_seeds, con
                 st->max_layer = std::max<uint64_t>(st->max_layer, len[t]);
             }
             st->book_entries = blen[steps - 2] + blen[steps - 1];
-            DevCtl c = read_ctl(E);
-            st->candidates = c.candidates;
+            st->candidates = E.candidates;
         }
     }
     remove_file(p + std::to_string(steps - 2));  // final_steps, BookSolver.cpp:279-282

@@ -188,6 +188,16 @@ __device__ __forceinline__ uint64_t filter_slot(uint64_t key, int bits) {
     return (key * 0x9E3779B97F4A7C15ull) >> (64 - bits);
 }
 
+// 64-bit mix (the finaliser of MurmurHash3) for the device hash sets.
+__device__ __forceinline__ uint64_t mix64(uint64_t k) {
+    k ^= k >> 33;
+    k *= 0xFF51AFD7ED558CCDull;
+    k ^= k >> 33;
+    k *= 0xC4CEB9FE1A85EC53ull;
+    k ^= k >> 33;
+    return k;
+}
+
 constexpr int kSplitStride = 16;  // one splitter per 16 keys (one 128-byte line)
 
 // Exact search of key in layer keys[0..n) with splitters split[j] =

@@ -15,6 +15,7 @@ namespace egtb {
 constexpr unsigned kErrCandOverflow = 1u;
 constexpr unsigned kErrArenaOverflow = 2u;
 constexpr unsigned kErrBookOverflow = 4u;
+constexpr unsigned kErrDedupOverflow = 16u;
 
 constexpr int kTileKeys = 4096;     // keys per sort / compaction tile
 constexpr int kSortThreads = 256;   // 8 warps x 16 keys x 32 lanes
@@ -22,7 +23,9 @@ constexpr int kKeysPerThread = kTileKeys / kSortThreads;
 
 // Control block in device memory.
 struct DevCtl {
-    unsigned long long cand_count[2];   // keys in the two candidate buffers
+    unsigned long long stage_count[3];  // keys in the three layer staging buffers (layer L in buffer L % 3)
+    unsigned long long blocks_done;     // last-block detection of the expand kernel
+    unsigned long long cand_count[2];   // keys handed to a sort (sort API, per-layer fallback sorts)
     unsigned long long n_sort;          // keys handed to the sort
     unsigned long long n_unique;        // result of the last unique / compaction
     unsigned long long candidates;      // statistics: keys that reached a sort
@@ -102,34 +105,124 @@ __device__ __forceinline__ void stage_flush(uint64_t *stage, int &count, uint64_
     count = 0;
 }
 
-// Forward expand of layer t (gen_boards_*, native_core/src/BookGenerator.cpp:
-// 472-760): every parent, unless do_check and it is a success, every empty
-// nibble k ascending, spawn 2 (v=1) and 4 (v=2), the four moves; a child is
-// kept when it moved and matches the pattern, and is emitted canonicalised:
-// v=1 children to the stream of layer t+1, v=2 children to the stream of
-// layer t+2. A direct-mapped table drops most repeats before they reach the
-// sort (its role is the reference's lossy prefilter, BookGenerator.cpp:
-// 101-127; results never depend on it). Each warp stages its survivors in
-// shared memory and appends them with one atomic per 32+ keys.
+// ------------------------------------------------- exact dedup sets ------
+//
+// Every layer under construction has a hash set of its keys (open addressing,
+// u64 slots, linear probing). Keys of one layer share one tile sum, so a slot
+// whose key has another tile sum - a key of an older layer, or 0 - is free:
+// the two sets (by layer parity) are never cleared. A key placed at slot p
+// only ever passed slots holding keys of its own layer, which stay until the
+// layer is done, so a later probe for it always reaches p.
+
+// Tile-value sums of every byte of a board (two nibbles; 0xF counts 32768).
+__device__ __forceinline__ void init_byte_sums(unsigned *bsum) {
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+        const unsigned lo = i & 15, hi = i >> 4;
+        bsum[i] = (lo ? 1u << lo : 0u) + (hi ? 1u << hi : 0u);
+    }
+}
+
+__device__ __forceinline__ long long board_tile_sum(uint64_t b, const unsigned *bsum) {
+    long long s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += bsum[(b >> (8 * i)) & 0xFFu];
+    return s;
+}
+
+// 1 when key is new in the set of the layer whose tile sum is want_sum.
+__device__ __forceinline__ int dedup_insert(uint64_t *tab, unsigned long long mask, uint64_t key, long long want_sum,
+                                           const unsigned *bsum, unsigned *err) {
+    unsigned long long h = mix64(key) & mask;
+    for (unsigned long long probe = 0; probe <= mask; ++probe) {
+        unsigned long long cur = __ldcg((const unsigned long long *)tab + h);
+        for (;;) {
+            if (cur == key) return 0;
+            if (board_tile_sum(cur, bsum) != want_sum) {
+                const unsigned long long prev =
+                    atomicCAS((unsigned long long *)tab + h, cur, (unsigned long long)key);
+                if (prev == cur) return 1;
+                cur = prev;
+                continue;
+            }
+            break;
+        }
+        h = (h + 1) & mask;
+    }
+    atomicOr(err, kErrDedupOverflow);
+    return 0;
+}
+
+// Flush a warp's staged new keys to a layer's staging buffer; flags
+// kErrDedupOverflow when the layer passes half its set's capacity.
+__device__ __forceinline__ void stage_flush_layer(uint64_t *stage, int &count, uint64_t *__restrict__ out,
+                                                  unsigned long long *cnt, unsigned long long cap,
+                                                  unsigned long long dedup_half, unsigned *err) {
+    const int lane = threadIdx.x & 31;
+    if (count == 0) return;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(cnt, (unsigned long long)count);
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (base + (unsigned long long)count > cap) {
+        if (lane == 0) atomicOr(err, kErrCandOverflow);
+    } else {
+        for (int i = lane; i < count; i += 32) out[base + i] = stage[i];
+    }
+    if (lane == 0 && base + (unsigned long long)count > dedup_half) atomicOr(err, kErrDedupOverflow);
+    __syncwarp();
+    count = 0;
+}
+
+// One forward step (gen_boards_*, native_core/src/BookGenerator.cpp:472-760,
+// with sort + unique + merge, :1059-1078, done by the sets): expand layer t.
+// Every parent, unless do_check and it is a success; every empty nibble k
+// ascending; spawn 2 (v=1) and 4 (v=2); the four moves; a child is kept when
+// it moved and matches the pattern, is canonicalised, and is appended to
+// layer t+v's staging buffer iff it is new in layer t+v's set. The same
+// kernel copies layer t into the arena at layer_off[t] and closes it (length,
+// next 16-aligned offset, capacity check); its last block empties layer t's
+// staging buffer for layer t+3.
 static __global__ void __launch_bounds__(kExpandThreads)
-expand_kernel(const uint64_t *__restrict__ arena, const unsigned long long *__restrict__ layer_off,
-              const unsigned long long *__restrict__ layer_len, int t, DevSpec spec, int do_check,
-              const uint32_t *__restrict__ tab, uint64_t *__restrict__ out1, uint64_t *__restrict__ out2,
-              DevCtl *ctl, int which1, int which2, unsigned long long cap, uint64_t *filter, int filter_bits) {
+expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ stage1, uint64_t *__restrict__ stage2,
+                    int si_par, int si1, int si2, uint64_t *__restrict__ arena,
+                    unsigned long long *__restrict__ layer_off, unsigned long long *__restrict__ layer_len,
+                    unsigned long long arena_cap, int t, DevSpec spec, int do_check, const uint32_t *__restrict__ tab,
+                    uint64_t *__restrict__ set1, uint64_t *__restrict__ set2, unsigned long long set_mask,
+                    long long sum1, long long sum2, unsigned long long stage_cap, DevCtl *ctl,
+                    unsigned *progress, unsigned progress_value) {
     __shared__ uint64_t stage[kExpandThreads / 32][2][kStage];
+    __shared__ unsigned bsum[256];
+    __shared__ int last_block;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (ctl->err & kErrArenaOverflow) return;
-    const unsigned long long n = layer_len[t];
-    const uint64_t *par = arena + layer_off[t];
+    init_byte_sums(bsum);
+    const unsigned long long n = ctl->stage_count[si_par];
+    const unsigned long long off = layer_off[t];
+    const bool fits = !(ctl->err & kErrArenaOverflow) && off + n <= arena_cap;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const unsigned long long next = (off + n + kSplitStride - 1) & ~(unsigned long long)(kSplitStride - 1);
+        if (!fits || next > arena_cap) {
+            atomicOr(&ctl->err, kErrArenaOverflow);
+            layer_len[t] = 0;
+            layer_off[t + 1] = off;
+        } else {
+            layer_len[t] = n;
+            layer_off[t + 1] = next;
+        }
+    }
+    __syncthreads();
     int cnt[2] = {0, 0};
-    uint64_t *outs[2] = {out1, out2};
-    unsigned long long *counters[2] = {&ctl->cand_count[which1], &ctl->cand_count[which2]};
+    uint64_t *outs[2] = {stage1, stage2};
+    unsigned long long *counters[2] = {&ctl->stage_count[si1], &ctl->stage_count[si2]};
+    uint64_t *sets[2] = {set1, set2};
+    const long long sums[2] = {sum1, sum2};
+    const unsigned long long half = (set_mask + 1) / 2;
+    unsigned long long probes = 0;
     const unsigned long long nwarps = (unsigned long long)gridDim.x * (kExpandThreads / 32);
     for (unsigned long long base = ((unsigned long long)blockIdx.x * (kExpandThreads / 32) + warp) * 32; base < n;
          base += nwarps * 32) {
         const unsigned long long p = base + lane;
         bool active = p < n;
-        uint64_t b = active ? par[p] : 0;
+        uint64_t b = active ? stage_par[p] : 0;
+        if (active && fits) arena[off + p] = b;
         if (active && do_check && is_success(b, spec)) active = false;
         uint64_t empt = active ? empty_nibbles(b) : 0;
         MoveCtx mc;
@@ -153,9 +246,8 @@ expand_kernel(const uint64_t *__restrict__ arena, const unsigned long long *__re
                     uint64_t key = 0;
                     if (keep) {
                         key = canonical(mv[d], spec.symm);
-                        const uint64_t slot = filter_slot(key, filter_bits);
-                        if (filter[slot] == key) keep = false;
-                        else filter[slot] = key;
+                        ++probes;
+                        keep = dedup_insert(sets[v - 1], set_mask, key, sums[v - 1], bsum, &ctl->err) != 0;
                     }
                     const unsigned m = __ballot_sync(0xFFFFFFFFu, keep);
                     if (m) {
@@ -164,15 +256,132 @@ expand_kernel(const uint64_t *__restrict__ arena, const unsigned long long *__re
                         cnt[v - 1] += __popc(m);
                         __syncwarp();
                         if (cnt[v - 1] > kStage - 32)
-                            stage_flush(stage[warp][v - 1], cnt[v - 1], outs[v - 1], counters[v - 1], cap, &ctl->err);
+                            stage_flush_layer(stage[warp][v - 1], cnt[v - 1], outs[v - 1], counters[v - 1],
+                                              stage_cap, half, &ctl->err);
                     }
                 }
             }
             any = __ballot_sync(0xFFFFFFFFu, empt != 0);
         }
     }
-    stage_flush(stage[warp][0], cnt[0], out1, counters[0], cap, &ctl->err);
-    stage_flush(stage[warp][1], cnt[1], out2, counters[1], cap, &ctl->err);
+    stage_flush_layer(stage[warp][0], cnt[0], stage1, counters[0], stage_cap, half, &ctl->err);
+    stage_flush_layer(stage[warp][1], cnt[1], stage2, counters[1], stage_cap, half, &ctl->err);
+    for (int o = 16; o > 0; o >>= 1) probes += __shfl_xor_sync(0xFFFFFFFFu, probes, o);
+    if (lane == 0 && probes) atomicAdd(&ctl->candidates, probes);
+    // the last block to finish empties layer t's staging buffer
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+        last_block = atomicAdd(&ctl->blocks_done, 1ull) == (unsigned long long)gridDim.x - 1;
+    __syncthreads();
+    if (last_block && threadIdx.x == 0) {
+        ctl->stage_count[si_par] = 0;
+        ctl->blocks_done = 0;
+        if (progress) *(volatile unsigned *)progress = progress_value;
+    }
+}
+
+// Copy a finished layer from its staging buffer into the arena and close it
+// (the last two layers, which no expand step reads).
+static __global__ void __launch_bounds__(256)
+flush_layer_kernel(const uint64_t *__restrict__ stage_l, int si, uint64_t *__restrict__ arena,
+                   unsigned long long *__restrict__ layer_off, unsigned long long *__restrict__ layer_len,
+                   unsigned long long arena_cap, int L, DevCtl *ctl) {
+    const unsigned long long n = ctl->stage_count[si];
+    const unsigned long long off = layer_off[L];
+    const bool fits = !(ctl->err & kErrArenaOverflow) && off + n <= arena_cap;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const unsigned long long next = (off + n + kSplitStride - 1) & ~(unsigned long long)(kSplitStride - 1);
+        if (!fits || next > arena_cap) {
+            atomicOr(&ctl->err, kErrArenaOverflow);
+            layer_len[L] = 0;
+            layer_off[L + 1] = off;
+        } else {
+            layer_len[L] = n;
+            layer_off[L + 1] = next;
+        }
+    }
+    if (!fits) return;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        arena[off + i] = stage_l[i];
+}
+
+// Insert keys already known to be in layer L (a resumed partial layer).
+static __global__ void __launch_bounds__(256)
+dedup_seed_kernel(const uint64_t *__restrict__ keys, unsigned long long n, uint64_t *set, unsigned long long mask,
+                  long long want_sum, DevCtl *ctl) {
+    __shared__ unsigned bsum[256];
+    init_byte_sums(bsum);
+    __syncthreads();
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        dedup_insert(set, mask, keys[i], want_sum, bsum, &ctl->err);
+}
+
+// ------------------------------------------ sorting every layer at once ----
+//
+// After the forward pass each layer holds its unique keys in arrival order.
+// All layers but layer 0 (the seeds, kept as given) are sorted together by
+// composite keys (layer << 4F) | (the layer key's F free nibbles): one radix
+// sort, then every key goes back to its layer's region in ascending order.
+
+struct FreeNibbles {
+    int count;
+    int idx[16];       // free nibble positions, least significant first
+    uint64_t pinned;   // every other nibble is 0xF
+};
+
+__device__ __forceinline__ uint64_t compact_key(uint64_t key, const FreeNibbles &fn) {
+    uint64_t c = 0;
+#pragma unroll 16
+    for (int k = 0; k < fn.count; ++k) c |= ((key >> (4 * fn.idx[k])) & 0xFull) << (4 * k);
+    return c;
+}
+
+__device__ __forceinline__ uint64_t expand_key(uint64_t c, const FreeNibbles &fn) {
+    uint64_t key = fn.pinned;
+#pragma unroll 16
+    for (int k = 0; k < fn.count; ++k) key |= ((c >> (4 * k)) & 0xFull) << (4 * fn.idx[k]);
+    return key;
+}
+
+// dense index j -> layer L with doff[L] <= j < doff[L+1]
+__device__ __forceinline__ int layer_of_dense(const unsigned long long *doff, int lo, int hi, unsigned long long j) {
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (doff[mid] <= j) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+static __global__ void __launch_bounds__(256)
+compose_kernel(const uint64_t *__restrict__ arena, const unsigned long long *__restrict__ layer_off,
+               const unsigned long long *__restrict__ doff, int l0, int l1, FreeNibbles fn,
+               uint64_t *__restrict__ comp) {
+    const unsigned long long total = doff[l1] - doff[l0];
+    for (unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; j < total;
+         j += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long g = doff[l0] + j;
+        const int L = layer_of_dense(doff, l0, l1, g);
+        const uint64_t key = arena[layer_off[L] + (g - doff[L])];
+        const uint64_t layer_part = fn.count < 16 ? ((uint64_t)(L - l0) << (4 * fn.count)) : 0ull;
+        comp[j] = layer_part | compact_key(key, fn);
+    }
+}
+
+static __global__ void __launch_bounds__(256)
+decompose_kernel(const uint64_t *__restrict__ comp, const unsigned long long *__restrict__ layer_off,
+                 const unsigned long long *__restrict__ doff, int l0, int l1, FreeNibbles fn,
+                 uint64_t *__restrict__ arena) {
+    const unsigned long long total = doff[l1] - doff[l0];
+    for (unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; j < total;
+         j += (unsigned long long)gridDim.x * blockDim.x) {
+        const uint64_t c = comp[j];
+        const int L = l0 + (fn.count < 16 ? (int)(c >> (4 * fn.count)) : 0);
+        const unsigned long long g = doff[l0] + j;
+        arena[layer_off[L] + (g - doff[L])] = expand_key(fn.count < 16 ? c & ((1ull << (4 * fn.count)) - 1) : c, fn);
+    }
 }
 
 // Single block: exclusive scan of the tile counts; total -> *total_out.
@@ -211,14 +420,6 @@ template <> __device__ __forceinline__ double cast_rate<double>(double x) { retu
 // A lookup costs ~1.3 dependent 16-byte loads instead of the ~18 of a binary
 // search, and the eight lookups of one empty cell are issued together.
 
-__device__ __forceinline__ uint64_t mix64(uint64_t k) {
-    k ^= k >> 33;
-    k *= 0xFF51AFD7ED558CCDull;
-    k ^= k >> 33;
-    k *= 0xC4CEB9FE1A85EC53ull;
-    k ^= k >> 33;
-    return k;
-}
 
 template <typename T> __device__ __forceinline__ unsigned long long rate_bits(T r) {
     if constexpr (sizeof(T) == 4) return (unsigned long long)__float_as_uint(*reinterpret_cast<const float *>(&r));

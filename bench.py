@@ -356,16 +356,20 @@ def roofline(prof, st, k, layer_boards, peak, peak_kind, pattern):
     name, (count, total) = max(prof.items(), key=lambda kv: kv[1][1])
     if total <= 0:
         return None
+    passes = max(1, round(prof.get("sort_pass", (0, 0))[0] / max(1, k)))
     per_build = {
-        # expand: read parents, write candidates
-        "expand": 8 * int(st.raw_boards) + 8 * int(st.candidates),
-        # every radix pass reads and writes each candidate key once
-        "sort_pass": 16 * int(st.candidates) * max(1, round(prof["sort_pass"][0] / max(1, k) / max(1, st.layers - 1))),
-        "unique": 8 * int(st.candidates) + 8 * int(st.raw_boards),
+        # expand + dedup: read each parent, copy it to the arena, probe one set
+        # slot per kept child, write each new key
+        "expand": 16 * layer_boards + 8 * int(st.candidates) + 8 * layer_boards,
+        # the layer sort: every radix pass reads and writes each key once
+        "sort_pass": 16 * layer_boards * passes,
+        # compose (read key, write composite) + decompose (read, write)
+        "layer_sort": 32 * layer_boards,
         # solve: one board key + one rate per board, one 32-byte key sector and one 32-byte rate sector per probe
         "solve": 12 * layer_boards + 64 * int(st.lookups),
         "book_pack": 12 * int(st.raw_boards) + 12 * int(st.book_entries),
-        "final_layers": 12 * 1,
+        "rate_index": 28 * layer_boards,
+        "final_layers": 12,
     }
     bytes_total = per_build.get(name, 0) * k
     achieved = bytes_total / (total / 1e3) / 1e9
