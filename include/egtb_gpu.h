@@ -203,6 +203,17 @@ EGTB_API int egtb_apply_sym(int device, const uint64_t *boards, size_t n, int32_
 EGTB_API int egtb_sort_unique_u64(int device, const uint64_t *d_keys, size_t n, uint64_t *d_out,
                                   uint64_t *d_n_out, void *stream);
 
+/* egtb_sort_unique_u64 for callers that cannot have the library allocate
+ * device memory (their pool holds all of it, or cudaMalloc/cudaFree would
+ * stall a latency-critical path). No counterpart in the reference. Same
+ * arguments and result; n <= 1048576 keys (larger n: EGTB_ERR_ARG). Its
+ * scratch is a static device array of about 8.6 MB that every GPU loading
+ * the library holds until exit; the first call on a device looks up that
+ * array's address, so make the first call before any stream capture. All
+ * calls share the array: calls that overlap on the GPU race. */
+EGTB_API int egtb_sort_unique_u64_noalloc(int device, const uint64_t *d_keys, size_t n, uint64_t *d_out,
+                                          uint64_t *d_n_out, void *stream);
+
 /* ------------------------------------------------------------ books ----- */
 
 typedef struct egtb_book egtb_book;
