@@ -171,6 +171,8 @@ struct Engine {
     unsigned long long sort_tiles = 0, comp_tiles = 0;
     uint64_t *dset[2] = {nullptr, nullptr};  // exact dedup sets of the layers under construction (by parity)
     unsigned long long dset_cap = 0;          // slots per set
+    uint64_t *filter = nullptr;               // direct-mapped repeat filter in front of the sets
+    int filter_bits = 20;
     unsigned long long *dense_off = nullptr;  // layer sort: dense offsets of the layers
     unsigned long long candidates = 0;        // children probed by the last forward pass
     unsigned long long *layer_off = nullptr, *layer_len = nullptr, *book_len = nullptr;
@@ -200,11 +202,14 @@ struct Engine {
         sm_count = prop.multiProcessorCount;
         EGTB_CUDA(cudaMalloc(&ctl, sizeof(DevCtl)));
         for (auto &e : ev) EGTB_CUDA(cudaEventCreate(&e));
+        const char *fb = getenv("EGTB_FILTER_BITS");
+        if (fb) filter_bits = std::max(10, std::min(30, atoi(fb)));
+        EGTB_CUDA(cudaMalloc(&filter, sizeof(uint64_t) << filter_bits));
         EGTB_CUDA(cudaMalloc(&hist, sizeof(unsigned) * kMaxPasses * 256));
         EGTB_CUDA(cudaMemset(hist, 0, sizeof(unsigned) * kMaxPasses * 256));
         EGTB_CUDA(cudaMalloc(&counters, sizeof(unsigned) * 16));
         int per_sm = 0;
-        EGTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel, kSortThreads, 0));
+        EGTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel, kSweepThreads, 0));
         sweep_grid = sm_count * std::max(1, per_sm);
         progress_device_ptr();
     }
@@ -425,7 +430,7 @@ static void enqueue_sort_unique(Engine &E, const ForwardPlan &P, int x, int L, u
     uint64_t *src = E.cand[x], *dst = E.tmp;
     for (int p = 0; p < P.sort.passes; ++p) {
         const int pi = E.prof_begin(K_SORT_PASS);
-        EGTB_LAUNCH(E, onesweep_kernel<<<E.sweep_grid, kSortThreads, 0, s>>>(src, dst, n_ptr, E.cand_cap, P.sort, p,
+        EGTB_LAUNCH(E, onesweep_kernel<<<E.sweep_grid, kSweepThreads, 0, s>>>(src, dst, n_ptr, E.cand_cap, P.sort, p,
                                                                              E.hist, E.counters, E.status, E.epoch++,
                                                                              E.ctl));
         E.prof_end(pi);
@@ -454,7 +459,8 @@ static void enqueue_forward(Engine &E, const ForwardPlan &P, unsigned *progress)
                            stage[t % 3], stage[(t + 1) % 3], stage[(t + 2) % 3], t % 3, (t + 1) % 3, (t + 2) % 3,
                            E.arena, E.layer_off, E.layer_len, E.arena_cap, t, P.spec, i > P.docheck ? 1 : 0, E.tab,
                            E.dset[(t + 1) & 1], E.dset[(t + 2) & 1], E.dset_cap - 1, P.s0 + 2ll * (t + 1),
-                           P.s0 + 2ll * (t + 2), E.cand_cap, E.ctl, progress, (unsigned)i));
+                           P.s0 + 2ll * (t + 2), E.cand_cap, E.filter, E.filter_bits, E.ctl, progress,
+                           (unsigned)i));
         E.prof_end(pe);
     }
     for (int L = std::max(P.first_step, P.steps - 2); L < P.steps; ++L)
@@ -480,6 +486,7 @@ static void stage_start(Engine &E, const ForwardPlan &P, const uint64_t *base, s
     EGTB_CUDA(cudaMemsetAsync(E.ctl, 0, sizeof(DevCtl), s));
     EGTB_CUDA(cudaMemsetAsync(E.hist, 0, sizeof(unsigned) * kMaxPasses * 256, s));
     for (auto *d : E.dset) EGTB_CUDA(cudaMemsetAsync(d, 0, sizeof(uint64_t) * E.dset_cap, s));
+    EGTB_CUDA(cudaMemsetAsync(E.filter, 0, sizeof(uint64_t) << E.filter_bits, s));
     EGTB_CUDA(cudaMemsetAsync(E.layer_off, 0, sizeof(unsigned long long) * E.steps_cap, s));
     EGTB_CUDA(cudaMemsetAsync(E.layer_len, 0, sizeof(unsigned long long) * E.steps_cap, s));
     if (n_base > E.cand_cap || n_partial > E.cand_cap)
@@ -539,7 +546,7 @@ static void enqueue_sort_layers(Engine &E, const ForwardPlan &P, const std::vect
         uint64_t *src = comp, *dst = other;
         for (int q = 0; q < sp.passes; ++q) {
             const int pi = E.prof_begin(K_SORT_PASS);
-            EGTB_LAUNCH(E, onesweep_kernel<<<E.sweep_grid, kSortThreads, 0, s>>>(src, dst, &E.ctl->cand_count[0],
+            EGTB_LAUNCH(E, onesweep_kernel<<<E.sweep_grid, kSweepThreads, 0, s>>>(src, dst, &E.ctl->cand_count[0],
                                                                                  E.arena_cap, sp, q, E.hist, E.counters,
                                                                                  E.status, E.epoch++, E.ctl));
             E.prof_end(pi);
@@ -563,12 +570,12 @@ static int run_forward(Engine &E, const ForwardPlan &P, const uint64_t *base, si
                        size_t n_partial, float *ms) {
     int retries = 0;
     E.ensure_steps(P.steps);
-    // first capacities: 4 Mi keys per staging buffer, 128 Mi layer keys, 4 Mi
-    // slots per dedup set (EGTB_INIT_CAND_KEYS / EGTB_INIT_ARENA_KEYS /
+    // first capacities: 4 Mi keys per staging buffer, 128 Mi layer keys, 1 Mi
+    // slots per dedup set (small sets stay in L2) (EGTB_INIT_CAND_KEYS / EGTB_INIT_ARENA_KEYS /
     // EGTB_INIT_SET_SLOTS override); a pass that outgrows them is re-run larger
     static const unsigned long long init_cand = env_keys("EGTB_INIT_CAND_KEYS", 1ull << 22);
     static const unsigned long long init_arena = env_keys("EGTB_INIT_ARENA_KEYS", 1ull << 27);
-    static const unsigned long long init_set = env_keys("EGTB_INIT_SET_SLOTS", 1ull << 22);
+    static const unsigned long long init_set = env_keys("EGTB_INIT_SET_SLOTS", 1ull << 20);
     E.ensure_cand(std::max<unsigned long long>(E.cand_cap, std::max<unsigned long long>(init_cand,
                                                                                          2 * std::max(n_partial, n_base))));
     E.ensure_arena(std::max<unsigned long long>(E.arena_cap, std::max<unsigned long long>(init_arena, n_base * 4)));
@@ -602,7 +609,7 @@ static int run_forward(Engine &E, const ForwardPlan &P, const uint64_t *base, si
         if (retries > 24) throw Error(EGTB_ERR_CAPACITY, "forward pass did not fit after repeated regrowth");
         if (c.err & kErrCandOverflow) E.ensure_cand(E.cand_cap * 2);
         if (c.err & kErrArenaOverflow) E.ensure_arena(E.arena_cap * 2);
-        if (c.err & kErrDedupOverflow) E.ensure_dedup(E.dset_cap * 4);
+        if (c.err & kErrDedupOverflow) E.ensure_dedup(E.dset_cap * 2);
     }
 }
 
@@ -677,7 +684,7 @@ static void enqueue_index_at(Engine &E, int L, unsigned long long n, T zero, ulo
     const unsigned long long slots = index_slots(n);
     EGTB_CUDA(cudaMemsetAsync(idx, 0, sizeof(ulonglong2) * slots, E.stream));
     EGTB_LAUNCH(E, index_insert_kernel<T><<<E.sm_count * 8, 256, 0, E.stream>>>(E.arena, (const T *)E.rates, E.layer_off,
-                                                                             E.layer_len, L, zero, idx, slots - 1));
+                                                                             E.layer_len, L, zero, idx, slots - 1, E.ctl));
 }
 
 // ... in index slot L % 3 (fused build: layers t, t+1, t+2 use distinct slots).
@@ -923,6 +930,7 @@ static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const 
     EGTB_CUDA(cudaEventElapsedTime(&bwd_ms, E.ev[2], E.ev[3]));
     E.prof_resolve();
     DevCtl c = read_ctl(E);
+    if (c.err & kErrIndexOverflow) throw Error(EGTB_ERR_CAPACITY, "rate index probe chain too long");
     if (c.err) throw Error(EGTB_ERR_CAPACITY, "book buffer overflow");
     std::vector<unsigned long long> blen = d2h_u64(E, E.book_len, steps);
     std::vector<unsigned long long> maxb = d2h_u64(E, E.layer_max, steps);
@@ -1180,6 +1188,7 @@ static void solve_files(Engine &E, const void *d1_recs, size_t n1, const void *d
         EGTB_CUDA(cudaMemcpyAsync(&mb, E.layer_max, 8, cudaMemcpyDeviceToHost, s));
         EGTB_CUDA(cudaStreamSynchronize(s));
         EGTB_CUDA(cudaGetLastError());
+        if (read_ctl(E).err) throw Error(EGTB_ERR_CAPACITY, "rate index or book buffer overflow in the solve");
         std::vector<unsigned char> book(nb * rec);
         if (nb) EGTB_CUDA(cudaMemcpy(book.data(), E.book, nb * rec, cudaMemcpyDeviceToHost));
         const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -16,6 +16,7 @@ constexpr unsigned kErrCandOverflow = 1u;
 constexpr unsigned kErrArenaOverflow = 2u;
 constexpr unsigned kErrBookOverflow = 4u;
 constexpr unsigned kErrDedupOverflow = 16u;
+constexpr unsigned kErrIndexOverflow = 32u;
 
 constexpr int kTileKeys = 4096;     // keys per sort / compaction tile
 constexpr int kSortThreads = 256;   // 8 warps x 16 keys x 32 lanes
@@ -129,11 +130,17 @@ __device__ __forceinline__ long long board_tile_sum(uint64_t b, const unsigned *
     return s;
 }
 
+// Longest probe chain a set insert walks. The host keeps every set at most
+// half full, where chains stay far shorter; a longer chain means the set
+// overflowed: the insert flags it (the host regrows the set and re-runs the
+// pass) instead of walking an ever fuller table.
+constexpr int kMaxProbe = 128;
+
 // 1 when key is new in the set of the layer whose tile sum is want_sum.
 __device__ __forceinline__ int dedup_insert(uint64_t *tab, unsigned long long mask, uint64_t key, long long want_sum,
                                            const unsigned *bsum, unsigned *err) {
     unsigned long long h = mix64(key) & mask;
-    for (unsigned long long probe = 0; probe <= mask; ++probe) {
+    for (int probe = 0; probe < kMaxProbe; ++probe) {
         unsigned long long cur = __ldcg((const unsigned long long *)tab + h);
         for (;;) {
             if (cur == key) return 0;
@@ -152,22 +159,34 @@ __device__ __forceinline__ int dedup_insert(uint64_t *tab, unsigned long long ma
     return 0;
 }
 
-// Flush a warp's staged new keys to a layer's staging buffer; flags
+// Flush a warp's staged keys (children that passed the repeat filter): the
+// warp enters them in the layer's set 32 at a time, every lane busy, and
+// appends the ones that are new to the layer's staging buffer. Flags
 // kErrDedupOverflow when the layer passes half its set's capacity.
-__device__ __forceinline__ void stage_flush_layer(uint64_t *stage, int &count, uint64_t *__restrict__ out,
-                                                  unsigned long long *cnt, unsigned long long cap,
-                                                  unsigned long long dedup_half, unsigned *err) {
+__device__ __forceinline__ void stage_flush_dedup(uint64_t *stage, int &count, uint64_t *__restrict__ out,
+                                                  unsigned long long *cnt, unsigned long long cap, uint64_t *set,
+                                                  unsigned long long set_mask, long long want, const unsigned *bsum,
+                                                  unsigned *err) {
     const int lane = threadIdx.x & 31;
-    if (count == 0) return;
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(cnt, (unsigned long long)count);
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base + (unsigned long long)count > cap) {
-        if (lane == 0) atomicOr(err, kErrCandOverflow);
-    } else {
-        for (int i = lane; i < count; i += 32) out[base + i] = stage[i];
+    const unsigned long long half = (set_mask + 1) / 2;
+    for (int b = 0; b < count; b += 32) {
+        const int i = b + lane;
+        const uint64_t key = i < count ? stage[i] : 0;
+        const bool fresh = i < count && dedup_insert(set, set_mask, key, want, bsum, err) != 0;
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, fresh);
+        if (m) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(cnt, (unsigned long long)__popc(m));
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            const unsigned long long pos = base + __popc(m & ((1u << lane) - 1u));
+            if (base + __popc(m) > cap) {
+                if (lane == 0) atomicOr(err, kErrCandOverflow);
+            } else if (fresh) {
+                out[pos] = key;
+            }
+            if (lane == 0 && base + __popc(m) > half) atomicOr(err, kErrDedupOverflow);
+        }
     }
-    if (lane == 0 && base + (unsigned long long)count > dedup_half) atomicOr(err, kErrDedupOverflow);
     __syncwarp();
     count = 0;
 }
@@ -181,20 +200,21 @@ __device__ __forceinline__ void stage_flush_layer(uint64_t *stage, int &count, u
 // kernel copies layer t into the arena at layer_off[t] and closes it (length,
 // next 16-aligned offset, capacity check); its last block empties layer t's
 // staging buffer for layer t+3.
-static __global__ void __launch_bounds__(kExpandThreads)
+static __global__ void __launch_bounds__(kExpandThreads, 4)
 expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ stage1, uint64_t *__restrict__ stage2,
                     int si_par, int si1, int si2, uint64_t *__restrict__ arena,
                     unsigned long long *__restrict__ layer_off, unsigned long long *__restrict__ layer_len,
                     unsigned long long arena_cap, int t, DevSpec spec, int do_check, const uint32_t *__restrict__ tab,
                     uint64_t *__restrict__ set1, uint64_t *__restrict__ set2, unsigned long long set_mask,
-                    long long sum1, long long sum2, unsigned long long stage_cap, DevCtl *ctl,
-                    unsigned *progress, unsigned progress_value) {
+                    long long sum1, long long sum2, unsigned long long stage_cap, uint64_t *filter,
+                    int filter_bits, DevCtl *ctl, unsigned *progress, unsigned progress_value) {
     __shared__ uint64_t stage[kExpandThreads / 32][2][kStage];
     __shared__ unsigned bsum[256];
     __shared__ int last_block;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     init_byte_sums(bsum);
-    const unsigned long long n = ctl->stage_count[si_par];
+    // once this pass has overflowed a buffer it will be re-run: skip the work
+    const unsigned long long n = (ctl->err & (kErrCandOverflow | kErrDedupOverflow)) ? 0 : ctl->stage_count[si_par];
     const unsigned long long off = layer_off[t];
     const bool fits = !(ctl->err & kErrArenaOverflow) && off + n <= arena_cap;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -209,12 +229,7 @@ expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ sta
         }
     }
     __syncthreads();
-    int cnt[2] = {0, 0};
-    uint64_t *outs[2] = {stage1, stage2};
-    unsigned long long *counters[2] = {&ctl->stage_count[si1], &ctl->stage_count[si2]};
-    uint64_t *sets[2] = {set1, set2};
-    const long long sums[2] = {sum1, sum2};
-    const unsigned long long half = (set_mask + 1) / 2;
+    int cnt1 = 0, cnt2 = 0;  // keys staged in this warp for layers t+1 and t+2
     unsigned long long probes = 0;
     const unsigned long long nwarps = (unsigned long long)gridDim.x * (kExpandThreads / 32);
     for (unsigned long long base = ((unsigned long long)blockIdx.x * (kExpandThreads / 32) + warp) * 32; base < n;
@@ -236,8 +251,12 @@ expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ sta
                 k = (__ffsll((long long)empt) - 1) >> 2;
                 empt &= empt - 1;
             }
-#pragma unroll
+#pragma unroll 1
             for (int v = 1; v <= 2; ++v) {
+                uint64_t *const set = v == 1 ? set1 : set2;
+                const long long want = v == 1 ? sum1 : sum2;
+                uint64_t *const sbuf = stage[warp][v - 1];
+                int c = v == 1 ? cnt1 : cnt2;
                 uint64_t mv[4], s = 0;
                 if (k >= 0) spawn_moves(tab, mc, k, (uint64_t)v, s, mv);
 #pragma unroll
@@ -247,25 +266,32 @@ expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ sta
                     if (keep) {
                         key = canonical(mv[d], spec.symm);
                         ++probes;
-                        keep = dedup_insert(sets[v - 1], set_mask, key, sums[v - 1], bsum, &ctl->err) != 0;
+                        // a direct-mapped filter drops most repeats with one load;
+                        // a key it holds has already been staged for its set
+                        const uint64_t slot = filter_slot(key, filter_bits);
+                        if (filter[slot] == key) keep = false;
+                        else filter[slot] = key;
                     }
                     const unsigned m = __ballot_sync(0xFFFFFFFFu, keep);
                     if (m) {
-                        const int pos = cnt[v - 1] + __popc(m & ((1u << lane) - 1u));
-                        if (keep) stage[warp][v - 1][pos] = key;
-                        cnt[v - 1] += __popc(m);
+                        const int pos = c + __popc(m & ((1u << lane) - 1u));
+                        if (keep) sbuf[pos] = key;
+                        c += __popc(m);
                         __syncwarp();
-                        if (cnt[v - 1] > kStage - 32)
-                            stage_flush_layer(stage[warp][v - 1], cnt[v - 1], outs[v - 1], counters[v - 1],
-                                              stage_cap, half, &ctl->err);
+                        if (c > kStage - 32)
+                            stage_flush_dedup(sbuf, c, v == 1 ? stage1 : stage2, &ctl->stage_count[v == 1 ? si1 : si2],
+                                              stage_cap, set, set_mask, want, bsum, &ctl->err);
                     }
                 }
+                if (v == 1) cnt1 = c; else cnt2 = c;
             }
             any = __ballot_sync(0xFFFFFFFFu, empt != 0);
         }
     }
-    stage_flush_layer(stage[warp][0], cnt[0], stage1, counters[0], stage_cap, half, &ctl->err);
-    stage_flush_layer(stage[warp][1], cnt[1], stage2, counters[1], stage_cap, half, &ctl->err);
+    stage_flush_dedup(stage[warp][0], cnt1, stage1, &ctl->stage_count[si1], stage_cap, set1, set_mask, sum1, bsum,
+                      &ctl->err);
+    stage_flush_dedup(stage[warp][1], cnt2, stage2, &ctl->stage_count[si2], stage_cap, set2, set_mask, sum2, bsum,
+                      &ctl->err);
     for (int o = 16; o > 0; o >>= 1) probes += __shfl_xor_sync(0xFFFFFFFFu, probes, o);
     if (lane == 0 && probes) atomicAdd(&ctl->candidates, probes);
     // the last block to finish empties layer t's staging buffer
@@ -440,7 +466,7 @@ template <typename T>
 __global__ void __launch_bounds__(256)
 index_insert_kernel(const uint64_t *__restrict__ arena, const T *__restrict__ rates,
                     const unsigned long long *__restrict__ layer_off, const unsigned long long *__restrict__ layer_len,
-                    int t, T zero, ulonglong2 *__restrict__ slots, unsigned long long mask) {
+                    int t, T zero, ulonglong2 *__restrict__ slots, unsigned long long mask, DevCtl *ctl) {
     const unsigned long long n = layer_len[t], o = layer_off[t];
     for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (unsigned long long)gridDim.x * blockDim.x) {
@@ -448,14 +474,17 @@ index_insert_kernel(const uint64_t *__restrict__ arena, const T *__restrict__ ra
         if (!(r > zero)) continue;
         const uint64_t key = arena[o + i];
         unsigned long long h = mix64(key) & mask;
-        for (unsigned long long probe = 0; probe <= mask; ++probe) {
+        bool placed = false;
+        for (int probe = 0; probe < kMaxProbe * 32; ++probe) {
             const unsigned long long prev = atomicCAS(&slots[h].x, 0ull, (unsigned long long)key);
             if (prev == 0ull || prev == key) {
                 slots[h].y = rate_bits<T>(r);
+                placed = true;
                 break;
             }
             h = (h + 1) & mask;
         }
+        if (!placed) atomicOr(&ctl->err, kErrIndexOverflow);
     }
 }
 

@@ -53,7 +53,7 @@ __device__ __forceinline__ void publish_status(unsigned long long *p, unsigned l
     *(volatile unsigned long long *)p = w;
 }
 
-constexpr int kLookWindow = 16;
+constexpr int kLookWindow = 4;
 
 // Sum of the counts of tiles tile-1, tile-2, ... back to (and including) the
 // nearest one that published its inclusive prefix. Words are at
@@ -126,66 +126,76 @@ sort_hist_kernel(const uint64_t *__restrict__ keys, const unsigned long long *n_
     }
 }
 
-// One pass: src -> dst ordered by digit p, stable.
-static __global__ void __launch_bounds__(kSortThreads)
+// One pass: src -> dst ordered by digit p, stable. 512 threads per 4096-key
+// tile (16 warps x 8 rounds of 32 keys); threads 0..255 own one digit each
+// for the look-back.
+constexpr int kSweepThreads = 512;
+constexpr int kSweepWarps = kSweepThreads / 32;
+constexpr int kSweepKeys = kTileKeys / kSweepThreads;  // keys per thread
+
+static __global__ void __launch_bounds__(kSweepThreads, 2)
 onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, const unsigned long long *n_ptr,
                 unsigned long long cap, SortPlan sp, int p, const unsigned *__restrict__ hist,
                 unsigned *__restrict__ counters, unsigned long long *__restrict__ status, unsigned epoch, DevCtl *ctl) {
     __shared__ uint64_t tkeys[kTileKeys];
-    __shared__ unsigned short wcnt[kSortThreads / 32][256];
+    __shared__ unsigned short wcnt[kSweepWarps][256];
     __shared__ unsigned loff[256];
     __shared__ unsigned long long gbase[256];
     __shared__ unsigned ghist[256];
     __shared__ unsigned long long sm[33];
     __shared__ unsigned tile_sh;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int d = threadIdx.x;  // digit owned by this thread when d < 256
     const unsigned long long n = clamp_n(*n_ptr, cap);
     const unsigned long long ntiles = (n + kTileKeys - 1) / kTileKeys;
     {
         // start of every digit in the output (same in every block)
         unsigned long long tot;
-        const unsigned long long ex = block_excl_scan<unsigned long long>(hist[p * 256 + threadIdx.x], sm, &tot);
-        ghist[threadIdx.x] = (unsigned)ex;
+        const unsigned long long h = d < 256 ? hist[p * 256 + d] : 0ull;
+        const unsigned long long ex = block_excl_scan<unsigned long long>(h, sm, &tot);
+        if (d < 256) ghist[d] = (unsigned)ex;
     }
     for (;;) {
         if (threadIdx.x == 0) tile_sh = atomicAdd(&counters[p], 1u);
-        for (int i = threadIdx.x; i < (kSortThreads / 32) * 256; i += kSortThreads) (&wcnt[0][0])[i] = 0;
+        for (int i = threadIdx.x; i < kSweepWarps * 256; i += kSweepThreads) (&wcnt[0][0])[i] = 0;
         __syncthreads();
         const unsigned long long tile = tile_sh;
         if (tile >= ntiles) break;
-        const unsigned long long base = tile * kTileKeys + (unsigned long long)warp * (kTileKeys / 8);
-        uint64_t k[kKeysPerThread];
-        unsigned short rank[kKeysPerThread];
-        unsigned short dig[kKeysPerThread];
+        const unsigned long long base = tile * kTileKeys + (unsigned long long)warp * (kTileKeys / kSweepWarps);
+        uint64_t k[kSweepKeys];
+        unsigned rd[kSweepKeys];  // rank in the warp (low 16 bits) | digit << 16 (256 = no key)
+        // all loads first, so a thread has its reads in flight together
 #pragma unroll
-        for (int r = 0; r < kKeysPerThread; ++r) {
+        for (int r = 0; r < kSweepKeys; ++r) {
+            const unsigned long long idx = base + (unsigned long long)r * 32 + lane;
+            k[r] = idx < n ? src[idx] : 0;
+        }
+#pragma unroll
+        for (int r = 0; r < kSweepKeys; ++r) {
             const unsigned long long idx = base + (unsigned long long)r * 32 + lane;
             const bool valid = idx < n;
-            k[r] = valid ? src[idx] : 0;
-            const unsigned d = valid ? sort_digit(k[r], sp, p) : 256u;
-            dig[r] = (unsigned short)d;
-            const unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
+            const unsigned dg = valid ? sort_digit(k[r], sp, p) : 256u;
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, dg);
             const unsigned before = __popc(peers & ((1u << lane) - 1u));
-            unsigned short c = 0;
-            if (valid) c = wcnt[warp][d];
-            rank[r] = (unsigned short)(c + before);
+            unsigned c = 0;
+            if (valid) c = wcnt[warp][dg];
+            rd[r] = (c + before) | (dg << 16);
             __syncwarp();
-            if (valid && before == 0) wcnt[warp][d] = (unsigned short)(c + __popc(peers));
+            if (valid && before == 0) wcnt[warp][dg] = (unsigned short)(c + __popc(peers));
             __syncwarp();
         }
         __syncthreads();
-        {
-            const int d = threadIdx.x;
-            unsigned cnt = 0;
+        unsigned cnt = 0;
+        unsigned long long excl = 0;
+        if (d < 256) {
 #pragma unroll
-            for (int w = 0; w < kSortThreads / 32; ++w) {
+            for (int w = 0; w < kSweepWarps; ++w) {
                 const unsigned c = wcnt[w][d];
                 wcnt[w][d] = (unsigned short)cnt;
                 cnt += c;
             }
             // publish this tile's count, then look back for the counts before it
             unsigned long long *my = status + tile * 256 + d;
-            unsigned long long excl = 0;
             if (tile == 0) {
                 publish_status(my, status_word(epoch, kFlagPrefix, cnt));
             } else {
@@ -194,22 +204,25 @@ onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, co
                 publish_status(my, status_word(epoch, kFlagPrefix, (unsigned)(excl + cnt)));
             }
             gbase[d] = (unsigned long long)ghist[d] + excl;
+        }
+        {
             unsigned long long tot;
-            loff[d] = (unsigned)block_excl_scan<unsigned long long>((unsigned long long)cnt, sm, &tot);
+            const unsigned long long lo = block_excl_scan<unsigned long long>((unsigned long long)cnt, sm, &tot);
+            if (d < 256) loff[d] = (unsigned)lo;
         }
         __syncthreads();
 #pragma unroll
-        for (int r = 0; r < kKeysPerThread; ++r) {
-            const unsigned d = dig[r];
-            if (d < 256u) tkeys[loff[d] + wcnt[warp][d] + rank[r]] = k[r];
+        for (int r = 0; r < kSweepKeys; ++r) {
+            const unsigned dg = rd[r] >> 16;
+            if (dg < 256u) tkeys[loff[dg] + wcnt[warp][dg] + (rd[r] & 0xFFFFu)] = k[r];
         }
         __syncthreads();
         const unsigned long long rem = n - tile * kTileKeys;
         const unsigned tile_n = rem < (unsigned long long)kTileKeys ? (unsigned)rem : (unsigned)kTileKeys;
-        for (unsigned i = threadIdx.x; i < tile_n; i += kSortThreads) {
+        for (unsigned i = threadIdx.x; i < tile_n; i += kSweepThreads) {
             const uint64_t key = tkeys[i];
-            const unsigned d = sort_digit(key, sp, p);
-            dst[gbase[d] + (i - loff[d])] = key;
+            const unsigned dg = sort_digit(key, sp, p);
+            dst[gbase[dg] + (i - loff[dg])] = key;
         }
         __syncthreads();
     }

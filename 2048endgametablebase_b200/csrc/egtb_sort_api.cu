@@ -94,7 +94,7 @@ static void enqueue_sort_unique_u64(const uint64_t *d_in, size_t n, uint64_t *d_
     const uint64_t *src = d_in;
     for (int p = 0; p < sp.passes; ++p) {
         uint64_t *dst = (p % 2 == 0) ? d_out : s.tmp;
-        onesweep_kernel<<<grid, kSortThreads, 0, st>>>(src, dst, &s.ctl->cand_count[0], n, sp, p, s.hist, s.counters,
+        onesweep_kernel<<<grid, kSweepThreads, 0, st>>>(src, dst, &s.ctl->cand_count[0], n, sp, p, s.hist, s.counters,
                                                        s.status, (unsigned)(p + 1), s.ctl);
         src = dst;
     }
@@ -109,7 +109,7 @@ static int sweep_grid_for_device() {
     int dev = 0, sms = 0, per_sm = 0;
     EGTB_CUDA(cudaGetDevice(&dev));
     EGTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    EGTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel, kSortThreads, 0));
+    EGTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel, kSweepThreads, 0));
     return sms * std::max(1, per_sm);
 }
 

@@ -214,6 +214,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (default: --steps)")
     ap.add_argument("--profile-run", action="store_true",
                     help="one device-resident build and nothing else (for an ncu launch list)")
+    ap.add_argument("--profile-sort", type=int, default=0,
+                    help="one egtb_sort_unique_u64 of this many seeded random keys and nothing else (for ncu)")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     if args.impl == "reference":
@@ -244,6 +246,17 @@ def main():
                                    ctypes.byref(st)))
         return st
 
+    if args.profile_sort:
+        rng = np.random.default_rng(1)
+        keys = torch.from_numpy(rng.integers(0, 2 ** 62, size=args.profile_sort, dtype=np.int64)).cuda()
+        out = torch.empty_like(keys)
+        cnt = torch.zeros(1, dtype=torch.int64, device=keys.device)
+        N.check(N.lib().egtb_sort_unique_u64(local, keys.data_ptr(), args.profile_sort, out.data_ptr(), cnt.data_ptr(),
+                                             stream.cuda_stream))
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_sort": args.profile_sort, "unique": int(cnt.item())}))
+        shutil.rmtree(work, ignore_errors=True)
+        return
     if args.profile_run:
         st = device_build()
         torch.cuda.synchronize()
