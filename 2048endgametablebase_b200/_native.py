@@ -111,6 +111,8 @@ _SIGS = {
                                   ctypes.POINTER(RunOptionsC), ctypes.POINTER(BuildStatsC)]),
     "egtb_sort_unique_u64": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, _P, _P, _P]),
     "egtb_sort_unique_u64_noalloc": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, _P, _P, _P]),
+    "egtb_book_layer_copy": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32, _P, ctypes.c_size_t,
+                                            ctypes.POINTER(ctypes.c_uint64)]),
     "egtb_move_all_dir": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, _P]),
     "egtb_canonical": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, ctypes.c_int32, _P]),
     "egtb_apply_sym": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, ctypes.c_int32, _P]),

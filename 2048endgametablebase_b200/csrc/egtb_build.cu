@@ -157,6 +157,11 @@ struct Engine {
 
     uint64_t *arena = nullptr;
     void *rates = nullptr;
+    unsigned long long rates_bytes = 0;
+    // the last fused build, for egtb_book_layer_copy
+    int last_steps = 0;
+    size_t last_rec = 0;
+    std::vector<unsigned long long> last_off, last_blen;
     uint64_t *split = nullptr;
     uint64_t *cand[2] = {nullptr, nullptr};
     uint64_t *tmp = nullptr;
@@ -278,16 +283,25 @@ struct Engine {
         if (cap <= arena_cap) return;
         release(arena);
         release(rates);
+        rates_bytes = 0;
         release(split);
         release(book);
         arena_cap = align16(cap);
         alloc_or_throw((void **)&arena, sizeof(uint64_t) * arena_cap, "layer arena");
-        alloc_or_throw(&rates, sizeof(uint64_t) * arena_cap, "rates");
         alloc_or_throw((void **)&split, sizeof(uint64_t) * (arena_cap / kSplitStride + 1), "splitters");
         book_cap_bytes = arena_cap * 16ull;
         alloc_or_throw((void **)&book, book_cap_bytes, "books");
         ensure_comp_tiles();
         ensure_status();
+    }
+
+    // rates of every arena slot, in the build's dtype
+    void ensure_rates(size_t elem_bytes) {
+        const unsigned long long need = arena_cap * elem_bytes;
+        if (need <= rates_bytes) return;
+        release(rates);
+        rates_bytes = need;
+        alloc_or_throw(&rates, need, "rates");
     }
 
     void ensure_cand(unsigned long long cap) {
@@ -608,7 +622,7 @@ static int run_forward(Engine &E, const ForwardPlan &P, const uint64_t *base, si
         ++retries;
         if (retries > 24) throw Error(EGTB_ERR_CAPACITY, "forward pass did not fit after repeated regrowth");
         if (c.err & kErrCandOverflow) E.ensure_cand(E.cand_cap * 2);
-        if (c.err & kErrArenaOverflow) E.ensure_arena(E.arena_cap * 2);
+        if (c.err & kErrArenaOverflow) E.ensure_arena(E.arena_cap + E.arena_cap / 2);
         if (c.err & kErrDedupOverflow) E.ensure_dedup(E.dset_cap * 2);
     }
 }
@@ -922,6 +936,7 @@ static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const 
     std::vector<unsigned long long> off = d2h_u64(E, E.layer_off, steps + 1);
     std::vector<unsigned long long> len = d2h_u64(E, E.layer_len, steps + 1);
     BackwardPlan B{steps, o.docheck_step, o.success_rate_dtype, o.spawn_rate4, P.spec};
+    E.ensure_rates(sizeof(T));
     EGTB_CUDA(cudaEventRecord(E.ev[2], E.stream));
     enqueue_backward<T>(E, B, len, progress_device_ptr());
     EGTB_CUDA(cudaEventRecord(E.ev[3], E.stream));
@@ -935,6 +950,10 @@ static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const 
     std::vector<unsigned long long> blen = d2h_u64(E, E.book_len, steps);
     std::vector<unsigned long long> maxb = d2h_u64(E, E.layer_max, steps);
     const size_t rec = 8 + sizeof(T);
+    E.last_steps = steps;
+    E.last_rec = rec;
+    E.last_off = off;
+    E.last_blen = blen;
     if (o.write_files) {
         std::vector<std::string> paths;
         std::vector<unsigned long long> doff, bytes;
@@ -1017,6 +1036,7 @@ static void generate_files(Engine &E, const uint64_t *seeds, size_t n_seeds, con
         // final_steps: success-only books of layers steps-2 and steps-1
         const T zero = (T)dtype_zero(o.success_rate_dtype), maxv = (T)dtype_max(o.success_rate_dtype);
         DevSpec ds = make_dev_spec(spec, o.target);
+        E.ensure_rates(sizeof(T));
         EGTB_CUDA(cudaMemsetAsync(E.ctl, 0, sizeof(DevCtl), E.stream));
         for (int t = steps - 2; t < steps; ++t) {
             EGTB_LAUNCH(E, final_layer_kernel<T><<<E.sm_count * 4, 256, 0, E.stream>>>(E.arena, (T *)E.rates, E.layer_off, E.layer_len, t, ds, zero, maxv));
@@ -1096,6 +1116,7 @@ static void solve_files(Engine &E, const void *d1_recs, size_t n1, const void *d
     slot = std::max<unsigned long long>(slot, std::max(n1, n2));
     slot = align16(slot);
     E.ensure_arena(slot * 3);
+    E.ensure_rates(sizeof(T));
     E.ensure_cand(std::max<unsigned long long>(E.cand_cap, 1ull << 22));
     E.ensure_index(index_slots(slot));
     int idx_of[3] = {0, 1, 2};  // rate index of layer i, i+1, i+2
@@ -1431,6 +1452,21 @@ extern "C" int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_patt
                 }
             }
         });
+    });
+}
+
+extern "C" int egtb_book_layer_copy(int device, int32_t layer, void *dst, size_t dst_bytes, uint64_t *bytes) {
+    return guarded([&] {
+        if (!bytes) throw Error(EGTB_ERR_ARG, "NULL size pointer");
+        Engine &E = engine_for(device);
+        std::lock_guard<std::mutex> lk(E.mu);
+        if (layer < 0 || layer >= E.last_steps) throw Error(EGTB_ERR_ARG, "no such layer in the last in-memory build");
+        const unsigned long long nb = E.last_blen[layer] * E.last_rec;
+        *bytes = nb;
+        if (!dst) return;  // size query
+        if (dst_bytes < nb) throw Error(EGTB_ERR_ARG, "destination buffer too small");
+        if (nb)
+            EGTB_CUDA(cudaMemcpy(dst, E.book + E.last_off[layer] * E.last_rec, nb, cudaMemcpyDeviceToHost));
     });
 }
 

@@ -184,6 +184,13 @@ EGTB_API int egtb_generate(const uint64_t *seeds, size_t n_seeds, const egtb_pat
 EGTB_API int egtb_solve(const void *d1_records, size_t n1, const void *d2_records, size_t n2,
                const egtb_pattern_spec *spec, const egtb_run_options *options, egtb_build_stats *stats);
 
+/* Copy the .book records of one layer of the last egtb_build on this device
+ * (write_files = 0 keeps them in device memory) into dst; *bytes receives
+ * their size (dst = NULL: size only). No reference counterpart: the
+ * reference only writes books to files (write_layer_file,
+ * native_core/src/BookSolver.cpp:206-231); the bytes are the same. */
+EGTB_API int egtb_book_layer_copy(int device, int32_t layer, void *dst, size_t dst_bytes, uint64_t *bytes);
+
 /* ------------------------------------------------------- primitives ----- */
 
 /* Batched board primitives on the device, host buffers in and out

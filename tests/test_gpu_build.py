@@ -151,3 +151,26 @@ def test_invalid_options_raise(tmp_root):
     spec.symm_mode = 4
     with pytest.raises(RuntimeError, match="symmetry"):
         F.run_pattern_build(H.seeds(case), spec, o)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("key", [k for k, v in H.cases().items() if v.get("size_class") == "huge"])
+def test_huge_build_in_memory_bit_exact(key):
+    """The 13-cell diagonal table at target 128 (2.25e9 boards, 17.9 GB of books),
+    built in device memory and read back layer by layer."""
+    import ctypes
+    import hashlib
+    case = H.cases()[key]
+    N = H.pkg()._native
+    spec, o = H.spec_options(case, "/nonexistent/unused_")
+    c_spec, c_opt = spec.to_c(), o.to_c(write_files=False)
+    st = N.BuildStatsC()
+    s = H.seeds(case)
+    N.check(N.lib().egtb_build(s.ctypes.data, len(s), ctypes.byref(c_spec), ctypes.byref(c_opt), ctypes.byref(st)))
+    assert st.raw_boards == sum(case["raw_len"])
+    assert st.book_entries == sum(case["book_len"])
+    buf = np.empty(max(case["book_len"]) * 12 + 16, dtype=np.uint8)
+    size = ctypes.c_uint64(0)
+    for t in range(case["steps"]):
+        N.check(N.lib().egtb_book_layer_copy(0, t, buf.ctypes.data, buf.nbytes, ctypes.byref(size)))
+        assert hashlib.sha256(buf[: size.value].tobytes()).hexdigest() == case["book_sha256"][t], t
