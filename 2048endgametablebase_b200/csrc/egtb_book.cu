@@ -496,6 +496,10 @@ extern "C" int egtb_book_lookup_device(egtb_book *b, const uint64_t *d_positions
     });
 }
 
+namespace egtb {
+int book_device(const egtb_book *b) { return b->device; }
+}  // namespace egtb
+
 extern "C" int egtb_find_classic_value(const char *pathname, const char *filename, uint64_t key, int32_t dtype,
                                        int32_t device, double *value, int32_t *found) {
     return guarded([&] {

@@ -1,0 +1,333 @@
+// Serving loop of libegtb_gpu: books resident in device memory, a scheduler
+// thread that batches incoming position queries of any size into in-flight
+// slots (continuous batching), and a replay harness for latency measurement.
+//
+// A slot is one batch on its own CUDA stream with pinned input/output
+// buffers and a completion event. The scheduler retires finished slots,
+// copies their answers to the requests' buffers, and fills every free slot
+// with queued requests in arrival order while they fit in the slot's
+// position capacity (memory-based admission). Requests that arrive while
+// slots are on the GPU wait in the queue and join the next free slot, so up
+// to `slots` batches overlap on the device (copies and kernels of different
+// slots run concurrently).
+//
+// The reference answers one position per call from files
+// (ClassicBookReader.move_on_dic, native_core/src/ReaderRuntime.cpp:1050-1067);
+// every answer here is that call's answer with last_op = 0, as float32.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "egtb_host.h"
+
+// from egtb_book.cu
+namespace egtb {
+int book_device(const egtb_book *b);
+}  // namespace egtb
+
+namespace egtb {
+
+using Clock = std::chrono::steady_clock;
+
+struct ServeRequest {
+    uint64_t ticket = 0;
+    int book = 0;
+    const uint64_t *pos = nullptr;
+    size_t n = 0;
+    float *out = nullptr;
+    uint8_t *valid = nullptr;
+    Clock::time_point t_submit;
+    double latency_us = 0.0;
+    bool done = false;
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t event = nullptr;
+    uint64_t *h_pos = nullptr, *d_pos = nullptr;
+    float *h_out = nullptr, *d_out = nullptr;
+    uint8_t *h_valid = nullptr, *d_valid = nullptr;
+    size_t cap = 0;
+    bool busy = false;
+    std::vector<ServeRequest *> reqs;
+    std::vector<size_t> at;  // position offset of each request in the slot
+};
+
+}  // namespace egtb
+
+struct egtb_server {
+    int device = 0;
+    std::vector<egtb_book *> books;
+    std::vector<egtb::Slot> slots;
+    size_t max_per_batch = 0;  // 0: no limit; 1: one request per launch (the unbatched baseline)
+    std::mutex mu;
+    std::condition_variable cv_done;
+    std::deque<egtb::ServeRequest *> queue;
+    std::unordered_map<uint64_t, std::unique_ptr<egtb::ServeRequest>> live;
+    uint64_t next_ticket = 1;
+    std::atomic<bool> stop{false};
+    std::thread worker;
+    std::string error;
+    // statistics
+    uint64_t n_requests = 0, n_positions = 0, n_batches = 0, n_launches = 0;
+};
+
+namespace egtb {
+
+static void serve_loop(egtb_server *S) {
+    try {
+        EGTB_CUDA(cudaSetDevice(S->device));
+        std::vector<ServeRequest *> finished;
+        while (!S->stop.load(std::memory_order_relaxed)) {
+            bool worked = false;
+            // 1. retire finished slots
+            for (auto &sl : S->slots) {
+                if (!sl.busy) continue;
+                const cudaError_t q = cudaEventQuery(sl.event);
+                if (q == cudaErrorNotReady) continue;
+                EGTB_CUDA(q);
+                const auto now = Clock::now();
+                for (size_t r = 0; r < sl.reqs.size(); ++r) {
+                    ServeRequest *rq = sl.reqs[r];
+                    std::memcpy(rq->out, sl.h_out + 4 * sl.at[r], rq->n * 4 * sizeof(float));
+                    if (rq->valid) std::memcpy(rq->valid, sl.h_valid + sl.at[r], rq->n);
+                    rq->latency_us = std::chrono::duration<double, std::micro>(now - rq->t_submit).count();
+                    finished.push_back(rq);
+                }
+                sl.reqs.clear();
+                sl.at.clear();
+                sl.busy = false;
+                worked = true;
+            }
+            if (!finished.empty()) {
+                {
+                    std::lock_guard<std::mutex> lk(S->mu);
+                    for (auto *rq : finished) rq->done = true;
+                }
+                S->cv_done.notify_all();
+                finished.clear();
+            }
+            // 2. admit queued requests into every free slot
+            for (auto &sl : S->slots) {
+                if (sl.busy) continue;
+                std::vector<ServeRequest *> take;
+                {
+                    std::lock_guard<std::mutex> lk(S->mu);
+                    size_t used = 0;
+                    while (!S->queue.empty()) {
+                        ServeRequest *rq = S->queue.front();
+                        if (used + rq->n > sl.cap) break;  // does not fit: it opens the next slot
+                        if (S->max_per_batch && take.size() >= S->max_per_batch) break;
+                        take.push_back(rq);
+                        used += rq->n;
+                        S->queue.pop_front();
+                    }
+                }
+                if (take.empty()) break;
+                // group by book so every book gets one contiguous launch
+                std::stable_sort(take.begin(), take.end(),
+                                 [](const ServeRequest *a, const ServeRequest *b) { return a->book < b->book; });
+                size_t used = 0;
+                for (auto *rq : take) {
+                    sl.reqs.push_back(rq);
+                    sl.at.push_back(used);
+                    std::memcpy(sl.h_pos + used, rq->pos, rq->n * sizeof(uint64_t));
+                    used += rq->n;
+                }
+                EGTB_CUDA(cudaMemcpyAsync(sl.d_pos, sl.h_pos, used * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                                          sl.stream));
+                size_t i = 0;
+                while (i < take.size()) {
+                    size_t j = i;
+                    size_t cnt = 0;
+                    while (j < take.size() && take[j]->book == take[i]->book) cnt += take[j++]->n;
+                    const size_t a = sl.at[i];
+                    if (egtb_book_lookup_device(S->books[take[i]->book], sl.d_pos + a, cnt, 0, sl.d_out + 4 * a,
+                                                sl.d_valid + a, sl.stream) != EGTB_OK)
+                        throw Error(EGTB_ERR_CUDA, "book lookup launch failed");
+                    ++S->n_launches;
+                    i = j;
+                }
+                EGTB_CUDA(cudaMemcpyAsync(sl.h_out, sl.d_out, used * 4 * sizeof(float), cudaMemcpyDeviceToHost,
+                                          sl.stream));
+                EGTB_CUDA(cudaMemcpyAsync(sl.h_valid, sl.d_valid, used, cudaMemcpyDeviceToHost, sl.stream));
+                EGTB_CUDA(cudaEventRecord(sl.event, sl.stream));
+                sl.busy = true;
+                ++S->n_batches;
+                S->n_positions += used;
+                S->n_requests += take.size();
+                worked = true;
+            }
+            if (!worked) std::this_thread::yield();
+        }
+    } catch (const std::exception &e) {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->error = e.what();
+        S->stop = true;
+    }
+    S->cv_done.notify_all();
+}
+
+}  // namespace egtb
+
+using namespace egtb;
+
+extern "C" int egtb_serve_start(egtb_book *const *books, int32_t n_books, int32_t slots, uint64_t slot_positions,
+                                int32_t max_requests_per_batch, egtb_server **out) {
+    return guarded([&] {
+        if (!books || n_books <= 0 || !out) throw Error(EGTB_ERR_ARG, "books and out are required");
+        if (slots <= 0 || slots > 64) throw Error(EGTB_ERR_ARG, "slots must be 1..64");
+        if (slot_positions < 4096) throw Error(EGTB_ERR_ARG, "slot_positions must hold one full request (4096)");
+        for (int i = 0; i < n_books; ++i)
+            if (!books[i]) throw Error(EGTB_ERR_ARG, "NULL book");
+        auto S = std::make_unique<egtb_server>();
+        S->device = book_device(books[0]);
+        for (int i = 0; i < n_books; ++i) {
+            if (book_device(books[i]) != S->device) throw Error(EGTB_ERR_ARG, "all books must live on one device");
+            S->books.push_back(books[i]);
+        }
+        S->max_per_batch = max_requests_per_batch > 0 ? (size_t)max_requests_per_batch : 0;
+        EGTB_CUDA(cudaSetDevice(S->device));
+        S->slots.resize(slots);
+        for (auto &sl : S->slots) {
+            sl.cap = slot_positions;
+            EGTB_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+            EGTB_CUDA(cudaEventCreateWithFlags(&sl.event, cudaEventDisableTiming));
+            EGTB_CUDA(cudaHostAlloc((void **)&sl.h_pos, slot_positions * 8, cudaHostAllocDefault));
+            EGTB_CUDA(cudaHostAlloc((void **)&sl.h_out, slot_positions * 16, cudaHostAllocDefault));
+            EGTB_CUDA(cudaHostAlloc((void **)&sl.h_valid, slot_positions, cudaHostAllocDefault));
+            EGTB_CUDA(cudaMalloc(&sl.d_pos, slot_positions * 8));
+            EGTB_CUDA(cudaMalloc(&sl.d_out, slot_positions * 16));
+            EGTB_CUDA(cudaMalloc(&sl.d_valid, slot_positions));
+        }
+        egtb_server *raw = S.release();
+        raw->worker = std::thread(serve_loop, raw);
+        *out = raw;
+    });
+}
+
+extern "C" int egtb_serve_submit(egtb_server *S, int32_t book, const uint64_t *positions, uint64_t n, float *values4,
+                                 uint8_t *valid_mask, uint64_t *ticket) {
+    return guarded([&] {
+        if (!S || !ticket) throw Error(EGTB_ERR_ARG, "NULL argument");
+        if (book < 0 || book >= (int)S->books.size()) throw Error(EGTB_ERR_ARG, "book index out of range");
+        if (n == 0 || n > S->slots[0].cap) throw Error(EGTB_ERR_ARG, "request size must be 1..slot_positions");
+        if (!positions || !values4) throw Error(EGTB_ERR_ARG, "NULL buffer");
+        auto rq = std::make_unique<ServeRequest>();
+        rq->book = book;
+        rq->pos = positions;
+        rq->n = n;
+        rq->out = values4;
+        rq->valid = valid_mask;
+        rq->t_submit = Clock::now();
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (!S->error.empty()) throw Error(EGTB_ERR_CUDA, "server stopped: " + S->error);
+        rq->ticket = S->next_ticket++;
+        *ticket = rq->ticket;
+        S->queue.push_back(rq.get());
+        S->live.emplace(rq->ticket, std::move(rq));
+    });
+}
+
+extern "C" int egtb_serve_wait(egtb_server *S, uint64_t ticket, int32_t timeout_ms, double *latency_us) {
+    return guarded([&] {
+        if (!S) throw Error(EGTB_ERR_ARG, "NULL server");
+        std::unique_lock<std::mutex> lk(S->mu);
+        auto it = S->live.find(ticket);
+        if (it == S->live.end()) throw Error(EGTB_ERR_ARG, "unknown ticket");
+        ServeRequest *rq = it->second.get();
+        const bool ok = S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms < 0 ? 3600000 : timeout_ms),
+                                            [&] { return rq->done || !S->error.empty(); });
+        if (!S->error.empty()) throw Error(EGTB_ERR_CUDA, "server stopped: " + S->error);
+        if (!ok) throw Error(EGTB_ERR_TIMEOUT, "request not answered in time");
+        if (latency_us) *latency_us = rq->latency_us;
+        S->live.erase(it);
+    });
+}
+
+extern "C" int egtb_serve_stats(egtb_server *S, uint64_t *requests, uint64_t *positions, uint64_t *batches,
+                                uint64_t *launches) {
+    return guarded([&] {
+        if (!S) throw Error(EGTB_ERR_ARG, "NULL server");
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (requests) *requests = S->n_requests;
+        if (positions) *positions = S->n_positions;
+        if (batches) *batches = S->n_batches;
+        if (launches) *launches = S->n_launches;
+    });
+}
+
+extern "C" int egtb_serve_replay(egtb_server *S, const uint64_t *pool, const double *arrival_us, const uint32_t *sizes,
+                                 const uint64_t *offsets, const int32_t *books, uint64_t n_req, float *values4,
+                                 uint8_t *valid, double *latency_us, double *wall_us) {
+    return guarded([&] {
+        if (!S || !pool || !arrival_us || !sizes || !offsets || !books || !values4 || !latency_us)
+            throw Error(EGTB_ERR_ARG, "NULL argument");
+        std::vector<uint64_t> tickets(n_req, 0);
+        const auto t0 = Clock::now();
+        std::atomic<uint64_t> submitted{0};
+        std::atomic<bool> failed{false};
+        // the driver thread submits every request at its arrival time
+        std::thread driver([&] {
+            for (uint64_t i = 0; i < n_req; ++i) {
+                const auto due = t0 + std::chrono::nanoseconds((long long)(arrival_us[i] * 1000.0));
+                while (Clock::now() < due) {
+                }
+                if (egtb_serve_submit(S, books[i], pool + offsets[i], sizes[i], values4 + 4 * offsets[i],
+                                      valid ? valid + offsets[i] : nullptr, &tickets[i]) != EGTB_OK) {
+                    failed = true;
+                    break;
+                }
+                submitted.store(i + 1, std::memory_order_release);
+            }
+        });
+        uint64_t answered = 0;
+        bool timed_out = false;
+        for (; answered < n_req; ++answered) {
+            while (submitted.load(std::memory_order_acquire) <= answered && !failed) std::this_thread::yield();
+            if (submitted.load(std::memory_order_acquire) <= answered) break;
+            double lat = 0.0;
+            if (egtb_serve_wait(S, tickets[answered], 60000, &lat) != EGTB_OK) {
+                timed_out = true;
+                break;
+            }
+            latency_us[answered] = lat;
+        }
+        driver.join();
+        if (failed) throw Error(EGTB_ERR_ARG, "replay: a request was rejected");
+        if (timed_out)
+            throw Error(EGTB_ERR_TIMEOUT, "replay: request " + std::to_string(answered) + " not answered");
+        if (wall_us) *wall_us = std::chrono::duration<double, std::micro>(Clock::now() - t0).count();
+    });
+}
+
+extern "C" int egtb_serve_stop(egtb_server *S) {
+    return guarded([&] {
+        if (!S) return;
+        S->stop = true;
+        if (S->worker.joinable()) S->worker.join();
+        cudaSetDevice(S->device);
+        for (auto &sl : S->slots) {
+            if (sl.stream) cudaStreamSynchronize(sl.stream);
+            cudaFreeHost(sl.h_pos);
+            cudaFreeHost(sl.h_out);
+            cudaFreeHost(sl.h_valid);
+            cudaFree(sl.d_pos);
+            cudaFree(sl.d_out);
+            cudaFree(sl.d_valid);
+            if (sl.event) cudaEventDestroy(sl.event);
+            if (sl.stream) cudaStreamDestroy(sl.stream);
+        }
+        delete S;
+    });
+}

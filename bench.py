@@ -214,6 +214,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (default: --steps)")
     ap.add_argument("--profile-run", action="store_true",
                     help="one device-resident build and nothing else (for an ncu launch list)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serve-only", action="store_true", help="run the serving leg alone and print its JSON")
+    ap.add_argument("--serve-offered", type=float, default=1e8, help="offered lookups/s of the serving leg")
     ap.add_argument("--profile-sort", type=int, default=0,
                     help="one egtb_sort_unique_u64 of this many seeded random keys and nothing else (for ncu)")
     args = ap.parse_args()
@@ -255,6 +258,11 @@ def main():
                                              stream.cuda_stream))
         torch.cuda.synchronize()
         print(json.dumps({"profile_sort": args.profile_sort, "unique": int(cnt.item())}))
+        shutil.rmtree(work, ignore_errors=True)
+        return
+    if args.serve_only:
+        print(json.dumps({"serving": serving_leg(local, base, offered=args.serve_offered,
+                                                 cpu_reference=not args.no_cpu_baseline)}), flush=True)
         shutil.rmtree(work, ignore_errors=True)
         return
     if args.profile_run:
@@ -355,11 +363,132 @@ def main():
                 dt, rb = reference_build_seconds(pattern, target, meta, steps, docheck, threads)
                 line["cpu_baseline"] = {"value": rb / dt, "unit": "boards/s", "cores": threads, "kind": "reference",
                                         "sample": f"1 full build of {pattern}-{2 ** target} ({rb} boards, {dt:.2f} s)"}
+        if not args.no_serve and world == 1:
+            N.set_stream(local, None)
+            line["serving"] = serving_leg(local, base, offered=args.serve_offered,
+                                          cpu_reference=not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)
     shutil.rmtree(work, ignore_errors=True)
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
+
+
+SERVE_TABLES = (("L3", 8), ("442", 9))
+
+
+def reference_reader_rate(books, positions: np.ndarray, specs) -> dict | None:
+    """The reference's ClassicBookReader.move_on_dic (oracle/_ref, compiled
+    from its sources) answering sampled positions one call each on one host
+    thread (checker/baseline only)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reference as R  # noqa: E402
+
+    if not R.available():
+        return None
+    fcr = R.module()
+    per_book = len(positions) // len(books)
+    total_t, total_n = 0.0, 0
+    for b, (spec_b, book) in enumerate(zip(specs, books)):
+        spec = fcr.PatternSpec()
+        spec.name = spec_b.name
+        spec.pattern_masks = list(spec_b.pattern_masks)
+        spec.success_shifts = list(spec_b.success_shifts)
+        spec.symm_mode = int(spec_b.symm_mode)
+        reader = fcr.ClassicBookReader(spec, False)
+        path_list = [(book.directory + "/", book.dtype)]
+        boards = []
+        for p in positions[b * per_book:(b + 1) * per_book]:
+            p = int(p)
+            boards.append([[(1 << v) if (v := (p >> (4 * ((3 - r) * 4 + (3 - c)))) & 0xF) else 0 for c in range(4)]
+                           for r in range(4)])
+        reader.move_on_dic(boards[0], path_list, book.pattern_full, book.nums_adjust)  # first call opens files
+        t0 = time.perf_counter()
+        for bd in boards:
+            reader.move_on_dic(bd, path_list, book.pattern_full, book.nums_adjust)
+        total_t += time.perf_counter() - t0
+        total_n += len(boards)
+    return {"lookups_per_s": total_n / total_t, "cores": 1, "kind": "reference",
+            "sample": f"{total_n} move_on_dic calls over the same books, one position per call"}
+
+
+def serving_leg(local: int, base: str | None, seconds: float = 0.5, offered: float = 1e8,
+                cpu_reference: bool = True) -> dict:
+    """Serving: the L3-256 and 442-512 books resident in HBM, a Poisson stream
+    of 1..4096-position requests (positions sampled from the books' layers, 5%
+    perturbed by a random nibble change) replayed through the native serving
+    loop (continuous batching) and through the same loop limited to one
+    request per launch on one slot."""
+    import torch
+
+    S = importlib.import_module("2048endgametablebase_b200.serving")
+    N = importlib.import_module("2048endgametablebase_b200._native")
+    d = tempfile.mkdtemp(prefix="egtb_serve_", dir=base)
+    books, specs = [], []
+    try:
+        for pattern, target in SERVE_TABLES:
+            bd = os.path.join(d, f"{pattern}_{2 ** target}")
+            spec, full, adj = S.build_book(pattern, target, bd, device=local)
+            books.append(S.open_book(bd, full, "float32", spec, adj, local))
+            specs.append(spec)
+        book_keys = sum(os.path.getsize(os.path.join(b.directory, f)) // 12 for b in books
+                        for f in os.listdir(b.directory) if f.endswith(".book"))
+        # kernel only: one device-resident batch of 2^24 sampled positions per book
+        rng = np.random.default_rng(5)
+        stream = torch.cuda.current_stream(local)
+        kern = []
+        for b in books:
+            pos = S.perturb(S.sample_positions(b, 1 << 24, rng), 0.05, rng)
+            d_pos = torch.from_numpy(pos.view(np.int64)).cuda(local)
+            d_val = torch.empty((len(pos), 4), dtype=torch.float32, device=f"cuda:{local}")
+            d_ok = torch.empty(len(pos), dtype=torch.uint8, device=f"cuda:{local}")
+
+            def run():
+                N.check(N.lib().egtb_book_lookup_device(b.handle, d_pos.data_ptr(), len(pos), 0, d_val.data_ptr(),
+                                                        d_ok.data_ptr(), stream.cuda_stream))
+            for _ in range(3):
+                run()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(5):
+                run()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            kern.append(5 * len(pos) / (e0.elapsed_time(e1) / 1e3))
+            del d_pos, d_val, d_ok
+        mean_size = 2048.5
+        n_req = max(200, int(offered / mean_size * seconds))
+        rs = S.request_stream(books, n_req, offered / mean_size, seed=21)
+        sat = S.request_stream(books, 4000, 0.0, seed=22)
+        out = {"tables": [f"{p}-{2 ** t}" for p, t in SERVE_TABLES], "book_keys": int(book_keys),
+               "kernel_lookups_per_s": {f"{p}-{2 ** t}": k for (p, t), k in zip(SERVE_TABLES, kern)},
+               "request_positions": "1..4096 uniform, 5% perturbed", "offered_lookups_per_s": offered,
+               "requests": n_req, "positions": rs.positions}
+        with S.BookServer(books, slots=4, slot_positions=1 << 18) as srv:
+            srv.replay(sat)  # warm-up
+            _, _, _, w = srv.replay(sat)
+            out["saturation_lookups_per_s"] = sat.positions / (w / 1e6)
+            s0 = srv.stats()
+            _, _, lat, w = srv.replay(rs)
+            s1 = srv.stats()
+        out["lookups_per_s"] = rs.positions / (w / 1e6)
+        out.update(S.latency_summary(lat))
+        out["batches"] = s1["batches"] - s0["batches"]
+        out["launches"] = s1["launches"] - s0["launches"]
+        with S.BookServer(books, slots=1, slot_positions=4096, max_requests_per_batch=1) as srv:
+            _, _, lat1, w1 = srv.replay(rs)
+        out["unbatched"] = {"lookups_per_s": rs.positions / (w1 / 1e6), **S.latency_summary(lat1),
+                            "path": "same loop, one slot, one request per launch"}
+        if cpu_reference:
+            sample = S.perturb(np.concatenate([S.sample_positions(b, 10000, rng) for b in books]), 0.05, rng)
+            ref = reference_reader_rate(books, sample, specs)
+            if ref:
+                out["cpu_reference"] = ref
+        return out
+    finally:
+        for b in books:
+            b.close()
+        shutil.rmtree(d, ignore_errors=True)
 
 
 def roofline(prof, st, k, layer_boards, peak, peak_kind, pattern):

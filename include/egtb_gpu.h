@@ -260,6 +260,52 @@ EGTB_API int egtb_book_lookup_device(egtb_book *book, const uint64_t *d_position
 EGTB_API int egtb_find_classic_value(const char *pathname, const char *filename, uint64_t key, int32_t dtype,
                             int32_t device, double *value, int32_t *found);
 
+/* ---- serving loop ------------------------------------------------------
+ * Answers move_on_dic queries (last_op 0) against books resident in device
+ * memory, for many concurrent clients. No counterpart in the reference,
+ * which answers one position per Python call from files
+ * (ClassicBookReader.move_on_dic, native_core/src/ReaderRuntime.cpp:1050-1067;
+ * engine_core/BookReader.py:96-118); each answer equals that call's answer
+ * as float32 (egtb_book_lookup_device).
+ *
+ * A scheduler thread batches queued requests into `slots` in-flight batches
+ * (one CUDA stream, pinned buffers and device buffers of slot_positions
+ * positions each): a free slot takes queued requests in arrival order while
+ * they fit (continuous batching; admission by slot memory), so batches
+ * overlap on the GPU and a request waits for a running batch only when every
+ * slot is busy. max_requests_per_batch > 0 caps requests per batch (1 = one
+ * request per launch). Books must be loaded (egtb_book_load_all) and stay
+ * open while the server runs. */
+typedef struct egtb_server egtb_server;
+
+EGTB_API int egtb_serve_start(egtb_book *const *books, int32_t n_books, int32_t slots, uint64_t slot_positions,
+                              int32_t max_requests_per_batch, egtb_server **out);
+
+/* Queue one request of n (1..slot_positions) positions for books[book];
+ * positions, values4 (4 floats per position) and valid_mask (may be NULL)
+ * must stay valid until egtb_serve_wait returns for the ticket. */
+EGTB_API int egtb_serve_submit(egtb_server *server, int32_t book, const uint64_t *positions, uint64_t n,
+                               float *values4, uint8_t *valid_mask, uint64_t *ticket);
+
+/* Wait for a ticket (timeout_ms < 0: one hour); *latency_us = submit to
+ * answer. Every ticket must be waited for once. */
+EGTB_API int egtb_serve_wait(egtb_server *server, uint64_t ticket, int32_t timeout_ms, double *latency_us);
+
+EGTB_API int egtb_serve_stats(egtb_server *server, uint64_t *requests, uint64_t *positions, uint64_t *batches,
+                              uint64_t *launches);
+
+/* Replay a recorded request stream: request i arrives arrival_us[i]
+ * microseconds after the call, reads sizes[i] positions at pool + offsets[i]
+ * for books[book_of[i]] and answers into values4 + 4*offsets[i] and
+ * valid + offsets[i] (valid may be NULL); latency_us[i] gets its latency and
+ * *wall_us the time until the last answer. */
+EGTB_API int egtb_serve_replay(egtb_server *server, const uint64_t *pool, const double *arrival_us,
+                               const uint32_t *sizes, const uint64_t *offsets, const int32_t *book_of, uint64_t n_req,
+                               float *values4, uint8_t *valid, double *latency_us, double *wall_us);
+
+/* Stop the scheduler and free the slots (books stay open). */
+EGTB_API int egtb_serve_stop(egtb_server *server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,6 +18,10 @@ def pkg():
     return importlib.import_module("2048endgametablebase_b200")
 
 
+def serving():
+    return importlib.import_module("2048endgametablebase_b200.serving")
+
+
 def fc():
     return importlib.import_module("2048endgametablebase_b200.native_core.formation_core")
 
