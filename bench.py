@@ -507,17 +507,34 @@ def roofline(prof, st, k, layer_boards, peak, peak_kind, pattern):
         "sort_pass": 16 * layer_boards * passes,
         # compose (read key, write composite) + decompose (read, write)
         "layer_sort": 32 * layer_boards,
-        # solve: one board key + one rate per board, one 32-byte key sector and one 32-byte rate sector per probe
-        "solve": 12 * layer_boards + 64 * int(st.lookups),
+        # solve: one board key + one rate per board, one 16-byte {key, rate} index slot per probe
+        "solve": 12 * layer_boards + 16 * int(st.lookups),
         "book_pack": 12 * int(st.raw_boards) + 12 * int(st.book_entries),
         "rate_index": 28 * layer_boards,
         "final_layers": 12,
     }
     bytes_total = per_build.get(name, 0) * k
     achieved = bytes_total / (total / 1e3) / 1e9
-    return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-            "launches_per_step": count / k, "avg_launch_us": total / count * 1e3}
+    out = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+           "algorithmic_bytes_per_launch": bytes_total / count,
+           "launches_per_step": count / k, "avg_launch_us": total / count * 1e3}
+    cap = NCU_TRAFFIC.get((pattern, name))
+    if cap:
+        # DRAM bytes of one captured launch, scaled by parents to the mean launch
+        out["traffic"] = cap["bytes"] * (layer_boards / (count / k)) / cap["units"]
+        out["traffic_source"] = cap["source"]
+    return out
+
+
+# dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture per kernel
+# (profiles/), with the units (boards) that launch processed
+NCU_TRAFFIC = {
+    ("442", "expand"): {"bytes": 25.670656e6 + 0.801536e6, "units": 267258,
+                        "source": "profiles/expand_dedup_442-512.md: launch t=150, scaled by parents"},
+    ("442", "solve"): {"bytes": 31.505664e6, "units": 327456,
+                       "source": "profiles/solve_442-512.md: launch t=181, scaled by boards"},
+}
 
 
 if __name__ == "__main__":
