@@ -91,6 +91,46 @@ class KernelTimeC(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_uint64), ("total_ms", ctypes.c_double)]
 
 
+class BatchParamsC(ctypes.Structure):
+    _fields_ = [
+        ("expand_chunk", ctypes.c_int32),
+        ("expand_blocks_per_sm", ctypes.c_int32),
+        ("digit_nibbles", ctypes.c_int32),
+        ("index_load", ctypes.c_int32),
+        ("use_graphs", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
+class BatchStatsC(ctypes.Structure):
+    _fields_ = [
+        ("raw_boards", ctypes.c_uint64),
+        ("book_entries", ctypes.c_uint64),
+        ("candidates", ctypes.c_uint64),
+        ("lookups", ctypes.c_uint64),
+        ("tables", ctypes.c_int32),
+        ("max_steps", ctypes.c_int32),
+        ("retries", ctypes.c_int32),
+        ("graphs_used", ctypes.c_int32),
+        ("forward_ms", ctypes.c_double),
+        ("sort_ms", ctypes.c_double),
+        ("backward_ms", ctypes.c_double),
+        ("pack_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
+        ("kernel_launches", ctypes.c_uint64),
+        ("graph_launches", ctypes.c_uint64),
+        ("params", BatchParamsC),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_ if name != "params"}
+        d["params"] = self.params.as_dict()
+        return d
+
+
 # every entry point of include/egtb_gpu.h with its ctypes signature
 _P = ctypes.c_void_p
 _SIGS = {
@@ -125,6 +165,10 @@ _SIGS = {
     "egtb_find_classic_value": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int32,
                                                ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
                                                ctypes.POINTER(ctypes.c_int32)]),
+    "egtb_build_batch": (ctypes.c_int, [ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P]),
+    "egtb_batch_autotune": (ctypes.c_int, [ctypes.c_int32, _P, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_double)]),
+    "egtb_batch_book_copy": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32, ctypes.c_int32, _P, ctypes.c_size_t,
+                                            ctypes.POINTER(ctypes.c_size_t)]),
     "egtb_serve_start": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, ctypes.c_int32,
                                         ctypes.POINTER(_P)]),
     "egtb_serve_submit": (ctypes.c_int, [_P, ctypes.c_int32, _P, ctypes.c_uint64, _P, _P,

@@ -1303,6 +1303,25 @@ static void run_prim(int device, const uint64_t *boards, size_t n, size_t out_pe
     EGTB_CUDA(cudaStreamSynchronize(E.stream));
 }
 
+// ------------------------------------------- access for the batched build --
+
+EngineRef engine_ref(int device) {
+    Engine &E = engine_for(device);
+    return EngineRef{&E.mu, E.device, &E.stream, E.tab, E.sm_count, E.sweep_grid};
+}
+
+uint64_t pattern_pinned_nibbles(const egtb_pattern_spec &s) { return pinned_nibbles(s); }
+
+unsigned *build_progress_ptr() { return progress_device_ptr(); }
+
+void build_progress_set(uint32_t cur, uint32_t total) { set_progress(cur, total); }
+
+void write_stats_file(const egtb_run_options &o, int dtype, const std::vector<int> &layers,
+                      const std::vector<unsigned long long> &raw_len, const std::vector<unsigned long long> &book_len,
+                      const std::vector<unsigned long long> &maxbits, double seconds_per_layer) {
+    write_stats(o, dtype, layers, raw_len, book_len, maxbits, seconds_per_layer);
+}
+
 }  // namespace egtb
 
 // =================================================================== C ABI ===

@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -81,6 +82,29 @@ double round_to_2(double v);
 
 // Byte size of SuccessEntry<T> records, native_core/include/FormationRuntime.h:191-205.
 inline size_t record_size(int dtype) { return 8 + dtype_size(dtype); }
+
+// The per-device build engine (egtb_build.cu) as the batched build sees it:
+// its lock (builds on one device run one at a time), the stream in use, the
+// row table and the SM count.
+struct EngineRef {
+    std::mutex *mu;
+    int device;
+    cudaStream_t *stream;
+    const uint32_t *tab;
+    int sm_count;
+    int sweep_grid;
+};
+EngineRef engine_ref(int device);
+// Nibbles that are 0xF in every canonical key of the pattern.
+uint64_t pattern_pinned_nibbles(const egtb_pattern_spec &s);
+// Build progress (get_build_progress): the mapped word kernels write, and the host setter.
+unsigned *build_progress_ptr();
+void build_progress_set(uint32_t cur, uint32_t total);
+// stats.txt lines (ensure_stats_header + recalculate_process_impl,
+// native_core/src/BookSolver.cpp:286-293,569-581).
+void write_stats_file(const egtb_run_options &o, int dtype, const std::vector<int> &layers,
+                      const std::vector<unsigned long long> &raw_len, const std::vector<unsigned long long> &book_len,
+                      const std::vector<unsigned long long> &maxbits, double seconds_per_layer);
 
 // Simple fixed-size thread pool for file writes.
 class WriterPool {

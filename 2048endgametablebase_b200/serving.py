@@ -26,8 +26,8 @@ import numpy as np
 
 from . import _native as N
 
-__all__ = ["Book", "BookServer", "RequestStream", "open_book", "build_book", "sample_positions", "perturb",
-           "request_stream", "latency_summary"]
+__all__ = ["Book", "BookServer", "RequestStream", "open_book", "build_book", "sample_positions", "sample_book_keys",
+           "add_spawn", "perturb", "request_sizes", "request_stream", "latency_summary", "MEAN_REQUEST"]
 
 
 @dataclass
@@ -100,8 +100,17 @@ def build_book(pattern: str, target: int, directory: str, device: int = 0, dtype
 
 
 def sample_positions(book: Book, n: int, rng: np.random.Generator) -> np.ndarray:
-    """n boards drawn uniformly from the book's own records (every layer file,
-    weighted by its size)."""
+    """n positions to ask about, drawn like sample_classic_book_state
+    (native_core/src/ReaderRuntime.cpp:945-993): a book record chosen
+    uniformly over every layer file (weighted by its size), then one spawn (a
+    2 with probability 0.9, else a 4) in one of its empty cells, so the
+    position is one a player faces before moving."""
+    keys = sample_book_keys(book, n, rng)
+    return add_spawn(keys, rng)
+
+
+def sample_book_keys(book: Book, n: int, rng: np.random.Generator) -> np.ndarray:
+    """n boards drawn uniformly from the book's own records."""
     fc = importlib.import_module(__package__ + ".native_core.formation_core")
     rec = fc._record_dtype(book.dtype)
     files = []
@@ -131,18 +140,66 @@ def sample_positions(book: Book, n: int, rng: np.random.Generator) -> np.ndarray
     return out
 
 
+def _nibbles(b: np.ndarray) -> np.ndarray:
+    return ((b[:, None] >> (np.arange(16, dtype=np.uint64) * np.uint64(4))[None, :]) & np.uint64(0xF)).astype(np.int64)
+
+
+def _pick_where(mask: np.ndarray, rng: np.random.Generator) -> np.ndarray:
+    """A uniformly chosen True column per row (-1 for rows with none)."""
+    cnt = mask.sum(axis=1)
+    r = np.floor(rng.random(len(mask)) * np.maximum(cnt, 1)).astype(np.int64)
+    csum = np.cumsum(mask, axis=1)
+    col = np.argmax(csum > r[:, None], axis=1)
+    return np.where(cnt > 0, col, -1)
+
+
+def _chunked(fn):
+    """Apply a per-board transform in chunks (bounded temporary memory)."""
+    def run(boards: np.ndarray, *args):
+        out = np.empty_like(boards)
+        for a in range(0, len(boards), 1 << 20):
+            out[a:a + (1 << 20)] = fn(boards[a:a + (1 << 20)], *args)
+        return out
+    run.__doc__ = fn.__doc__
+    return run
+
+
+@_chunked
+def add_spawn(keys: np.ndarray, rng: np.random.Generator) -> np.ndarray:
+    """One spawn per board: a 2 (p 0.9) or a 4 in a uniformly chosen empty cell."""
+    pos = keys.copy()
+    cell = _pick_where(_nibbles(keys) == 0, rng)
+    tile = np.where(rng.random(len(keys)) < 0.9, 1, 2).astype(np.uint64)
+    ok = cell >= 0
+    pos[ok] |= tile[ok] << (cell[ok].astype(np.uint64) * np.uint64(4))
+    return pos
+
+
+@_chunked
 def perturb(positions: np.ndarray, frac: float, rng: np.random.Generator) -> np.ndarray:
-    """Change one random nibble of a `frac` share of the positions to another
-    random value (queries that mostly miss; a miss answers 0)."""
+    """Change one random free-cell nibble (a cell not pinned at 0xF) of a
+    `frac` share of the positions to another value in 0..14 (queries that
+    mostly miss; a miss answers 0)."""
     pos = positions.copy()
     sel = np.nonzero(rng.random(len(pos)) < frac)[0]
-    nib = rng.integers(0, 16, size=len(sel)).astype(np.uint64)
-    delta = rng.integers(1, 16, size=len(sel)).astype(np.uint64)
-    shift = nib * np.uint64(4)
-    old = (pos[sel] >> shift) & np.uint64(0xF)
-    new = (old + delta) & np.uint64(0xF)
-    pos[sel] = (pos[sel] & ~(np.uint64(0xF) << shift)) | (new << shift)
+    if not len(sel):
+        return pos
+    cell = _pick_where(_nibbles(pos[sel]) != 0xF, rng)
+    ok = cell >= 0
+    sel, cell = sel[ok], cell[ok].astype(np.uint64)
+    shift = cell * np.uint64(4)
+    old = ((pos[sel] >> shift) & np.uint64(0xF)).astype(np.int64)
+    new = (old + rng.integers(1, 15, size=len(sel))) % 15  # another value in 0..14
+    pos[sel] = (pos[sel] & ~(np.uint64(0xF) << shift)) | (new.astype(np.uint64) << shift)
     return pos
+
+
+def request_sizes(n: int, rng: np.random.Generator, max_size: int = 4096) -> np.ndarray:
+    """Log-uniform request sizes in 1..max_size."""
+    return np.clip(np.floor(np.exp(rng.random(n) * np.log(max_size + 1))), 1, max_size).astype(np.uint32)
+
+
+MEAN_REQUEST = float(np.mean(request_sizes(1 << 20, np.random.default_rng(0))))
 
 
 @dataclass
@@ -166,13 +223,13 @@ class RequestStream:
 def request_stream(books: list[Book], n_requests: int, rate_per_s: float, seed: int, miss_frac: float = 0.05,
                    max_size: int = 4096) -> RequestStream:
     """Poisson arrivals at `rate_per_s` requests per second (0: all at once);
-    sizes uniform in 1..max_size; each request asks one book (uniform), its
-    positions sampled from that book's own layers, `miss_frac` of them
-    perturbed by a random nibble change."""
+    sizes log-uniform in 1..max_size; each request asks one book (uniform),
+    its positions sampled from that book's own layers (sample_positions),
+    `miss_frac` of them perturbed on one free cell."""
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1e6 / rate_per_s, size=n_requests) if rate_per_s > 0 else np.zeros(n_requests)
     arrival = np.cumsum(gaps) - (gaps[0] if n_requests else 0.0)
-    sizes = rng.integers(1, max_size + 1, size=n_requests).astype(np.uint32)
+    sizes = request_sizes(n_requests, rng, max_size)
     book_of = rng.integers(0, len(books), size=n_requests).astype(np.int32)
     offsets = np.zeros(n_requests, dtype=np.uint64)
     if n_requests:

@@ -415,8 +415,8 @@ def reference_reader_rate(books, positions: np.ndarray, specs) -> dict | None:
 def serving_leg(local: int, base: str | None, seconds: float = 0.5, offered: float = 1e8,
                 cpu_reference: bool = True) -> dict:
     """Serving: the L3-256 and 442-512 books resident in HBM, a Poisson stream
-    of 1..4096-position requests (positions sampled from the books' layers, 5%
-    perturbed by a random nibble change) replayed through the native serving
+    of requests of log-uniform 1..4096 positions (a book record plus one
+    spawn, 5% perturbed on one free cell) replayed through the native serving
     loop (continuous batching) and through the same loop limited to one
     request per launch on one slot."""
     import torch
@@ -438,7 +438,7 @@ def serving_leg(local: int, base: str | None, seconds: float = 0.5, offered: flo
         stream = torch.cuda.current_stream(local)
         kern = []
         for b in books:
-            pos = S.perturb(S.sample_positions(b, 1 << 24, rng), 0.05, rng)
+            pos = S.perturb(S.sample_positions(b, 1 << 24, rng), 0.05, rng)  # 5 % perturbed on a free cell
             d_pos = torch.from_numpy(pos.view(np.int64)).cuda(local)
             d_val = torch.empty((len(pos), 4), dtype=torch.float32, device=f"cuda:{local}")
             d_ok = torch.empty(len(pos), dtype=torch.uint8, device=f"cuda:{local}")
@@ -456,13 +456,14 @@ def serving_leg(local: int, base: str | None, seconds: float = 0.5, offered: flo
             torch.cuda.synchronize()
             kern.append(5 * len(pos) / (e0.elapsed_time(e1) / 1e3))
             del d_pos, d_val, d_ok
-        mean_size = 2048.5
+        mean_size = S.MEAN_REQUEST
         n_req = max(200, int(offered / mean_size * seconds))
         rs = S.request_stream(books, n_req, offered / mean_size, seed=21)
         sat = S.request_stream(books, 4000, 0.0, seed=22)
         out = {"tables": [f"{p}-{2 ** t}" for p, t in SERVE_TABLES], "book_keys": int(book_keys),
                "kernel_lookups_per_s": {f"{p}-{2 ** t}": k for (p, t), k in zip(SERVE_TABLES, kern)},
-               "request_positions": "1..4096 uniform, 5% perturbed", "offered_lookups_per_s": offered,
+               "request_positions": "log-uniform 1..4096; book record + one spawn, 5% perturbed on a free cell",
+               "offered_lookups_per_s": offered,
                "requests": n_req, "positions": rs.positions}
         with S.BookServer(books, slots=4, slot_positions=1 << 18) as srv:
             srv.replay(sat)  # warm-up

@@ -260,6 +260,67 @@ EGTB_API int egtb_book_lookup_device(egtb_book *book, const uint64_t *d_position
 EGTB_API int egtb_find_classic_value(const char *pathname, const char *filename, uint64_t key, int32_t dtype,
                             int32_t device, double *value, int32_t *found);
 
+/* ---- batched build -----------------------------------------------------
+ * Many tables of uneven size built together: no counterpart in the
+ * reference, which builds one table per run_pattern_build call
+ * (native_core/src/BookSolver.cpp:823-832; engine_core/BookBuilder.py:264).
+ * Every table gives the same inputs as egtb_build (seeds, spec, options) and
+ * gets the same books, byte for byte; all tables advance one global layer
+ * step per kernel launch (forward: expand + dedup of layer t of every table;
+ * backward: solve + rate index of layer t of every table), the per-step
+ * loops replayed as CUDA graphs, one radix sort for every table's layers. */
+typedef struct egtb_batch_params {
+    int32_t expand_chunk;         /* parents per work item of the forward step: multiple of 32 in 32..4096 (0: tuned, else 128) */
+    int32_t expand_blocks_per_sm; /* blocks per SM of the forward step, 1..8 (0: tuned, else 4) */
+    int32_t digit_nibbles;        /* radix digit of the layer sort in nibbles, 1 or 2 (0: tuned, else 2) */
+    int32_t index_load;           /* rate-index slots per key of a table's largest layer, 2 or 4 (0: tuned, else 2) */
+    int32_t use_graphs;           /* 1: per-step loops replayed as CUDA graphs, -1: direct launches (0: tuned, else 1) */
+    int32_t reserved[3];
+} egtb_batch_params;
+
+typedef struct egtb_batch_stats {
+    uint64_t raw_boards;      /* all tables, as egtb_build_stats */
+    uint64_t book_entries;
+    uint64_t candidates;
+    uint64_t lookups;
+    int32_t tables;
+    int32_t max_steps;        /* global layer steps */
+    int32_t retries;          /* forward re-runs after capacity regrowth */
+    int32_t graphs_used;      /* 1 when the per-step loops ran as CUDA graphs */
+    double forward_ms;        /* device time of the phases */
+    double sort_ms;
+    double backward_ms;
+    double pack_ms;
+    double total_ms;          /* host wall time of the call */
+    uint64_t kernel_launches; /* kernels run (graph nodes counted one by one) */
+    uint64_t graph_launches;
+    egtb_batch_params params; /* the parameters used */
+} egtb_batch_stats;
+
+/* Build n_tables tables on options[0].device (all tables: same device and
+ * success_rate_dtype). Table i: seeds[i][0..n_seeds[i]), specs[i],
+ * options[i] (write_files per table). params may be NULL (tuned values for
+ * this set of tables when egtb_batch_autotune ran, else defaults).
+ * table_stats (n_tables entries) and stats may be NULL. The books of the last
+ * batch stay on the device for egtb_batch_book_copy. */
+EGTB_API int egtb_build_batch(int32_t n_tables, const uint64_t *const *seeds, const uint64_t *n_seeds,
+                              const egtb_pattern_spec *specs, const egtb_run_options *options,
+                              const egtb_batch_params *params, egtb_build_stats *table_stats, egtb_batch_stats *stats);
+
+/* Autotuner: builds the batch (books kept on the device) under candidate
+ * parameters, one parameter at a time (forward work-item size and blocks per
+ * SM, radix digit width, rate-index load), keeps the fastest by device time,
+ * remembers it for this set of tables and returns it in *best (*best_ms: its
+ * device time). */
+EGTB_API int egtb_batch_autotune(int32_t n_tables, const uint64_t *const *seeds, const uint64_t *n_seeds,
+                                 const egtb_pattern_spec *specs, const egtb_run_options *options,
+                                 egtb_batch_params *best, double *best_ms);
+
+/* Copy book layer `layer` of table `table` of the device's last batch (packed
+ * records) to host memory; *bytes = its size (dst may be NULL to ask). */
+EGTB_API int egtb_batch_book_copy(int device, int32_t table, int32_t layer, void *dst, size_t dst_bytes,
+                                  size_t *bytes);
+
 /* ---- serving loop ------------------------------------------------------
  * Answers move_on_dic queries (last_op 0) against books resident in device
  * memory, for many concurrent clients. No counterpart in the reference,

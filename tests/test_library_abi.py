@@ -45,6 +45,8 @@ def test_struct_layouts_match_header(tmp_path):
         "egtb_run_options": N.RunOptionsC,
         "egtb_build_stats": N.BuildStatsC,
         "egtb_kernel_time": N.KernelTimeC,
+        "egtb_batch_params": N.BatchParamsC,
+        "egtb_batch_stats": N.BatchStatsC,
     }
     lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void) {"]
     for cname, cls in fields.items():
