@@ -196,7 +196,7 @@ egtb_batch_params default_params() {
     egtb_batch_params p;
     std::memset(&p, 0, sizeof p);
     p.expand_chunk = 128;
-    p.expand_blocks_per_sm = 4;
+    p.expand_blocks_per_sm = 3;
     p.digit_nibbles = 2;
     p.index_load = 2;
     p.use_graphs = 1;
@@ -842,7 +842,7 @@ extern "C" int egtb_batch_autotune(int32_t n_tables, const uint64_t *const *seed
             }
         };
         try_field(&egtb_batch_params::expand_chunk, {32, 64, 128, 256, 512});
-        try_field(&egtb_batch_params::expand_blocks_per_sm, {2, 4, 6});
+        try_field(&egtb_batch_params::expand_blocks_per_sm, {2, 3, 6});
         try_field(&egtb_batch_params::digit_nibbles, {1, 2});
         try_field(&egtb_batch_params::index_load, {2, 4});
         Remembered &m = B.memory[batch_signature(tp)];

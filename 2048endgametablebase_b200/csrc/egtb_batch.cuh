@@ -94,7 +94,7 @@ __device__ __forceinline__ int seg_find(const unsigned long long *pre, int n, un
 // table's staging buffer t % 3.
 constexpr int kBatchThreads = 256;
 
-static __global__ void __launch_bounds__(kBatchThreads, 4)
+static __global__ void __launch_bounds__(kBatchThreads, 3)
 batch_expand_kernel(const BatchTable *__restrict__ T, BatchCtl *C, int n_tables, int t, uint64_t *__restrict__ arena,
                     unsigned long long *__restrict__ layer_off, unsigned long long *__restrict__ layer_len,
                     const uint32_t *__restrict__ tab, unsigned chunk, BatchSync *sync, unsigned *progress,
@@ -144,9 +144,9 @@ batch_expand_kernel(const BatchTable *__restrict__ T, BatchCtl *C, int n_tables,
     // flush the warp's staged keys of table cur
     auto flush_table = [&]() {
         const BatchTable &tb = T[cur];
-        stage_flush_dedup(stage[warp][0], cnt1, tb.stage[(t + 1) % 3], &C[cur].stage_count[(t + 1) % 3], tb.stage_cap,
+        stage_flush_dedup<false>(stage[warp][0], cnt1, tb.stage[(t + 1) % 3], &C[cur].stage_count[(t + 1) % 3], tb.stage_cap,
                           tb.set[(t + 1) & 1], tb.set_mask, tb.s0 + 2ll * (t + 1), bsum, &C[cur].err);
-        stage_flush_dedup(stage[warp][1], cnt2, tb.stage[(t + 2) % 3], &C[cur].stage_count[(t + 2) % 3], tb.stage_cap,
+        stage_flush_dedup<false>(stage[warp][1], cnt2, tb.stage[(t + 2) % 3], &C[cur].stage_count[(t + 2) % 3], tb.stage_cap,
                           tb.set[(t + 2) & 1], tb.set_mask, tb.s0 + 2ll * (t + 2), bsum, &C[cur].err);
         unsigned long long p = probes;
         for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xFFFFFFFFu, p, o);
@@ -190,21 +190,13 @@ batch_expand_kernel(const BatchTable *__restrict__ T, BatchCtl *C, int n_tables,
                 for (int v = 1; v <= 2; ++v) {
                     uint64_t *const sbuf = stage[warp][v - 1];
                     int c = v == 1 ? cnt1 : cnt2;
-                    uint64_t mv[4], s = 0;
-                    if (k >= 0) spawn_moves(tab, mc, k, (uint64_t)v, s, mv);
+                    uint64_t keys[4];
+                    const unsigned kept = spawn_children(tab, mc, k, (uint64_t)v, tb.spec, tb.filter, tb.filter_bits,
+                                                         keys, probes);
 #pragma unroll
                     for (int d = 0; d < 4; ++d) {
-                        bool keep = k >= 0 && mv[d] != s && is_pattern(mv[d], tb.spec);
-                        uint64_t key = 0;
-                        if (keep) {
-                            key = canonical(mv[d], tb.spec.symm);
-                            ++probes;
-                            if (tb.filter_bits) {
-                                const uint64_t slot = filter_slot(key, tb.filter_bits);
-                                if (tb.filter[slot] == key) keep = false;
-                                else tb.filter[slot] = key;
-                            }
-                        }
+                        const bool keep = kept >> d & 1u;
+                        const uint64_t key = keys[d];
                         const unsigned m = __ballot_sync(0xFFFFFFFFu, keep);
                         if (m) {
                             const int pos = c + __popc(m & ((1u << lane) - 1u));
@@ -213,7 +205,7 @@ batch_expand_kernel(const BatchTable *__restrict__ T, BatchCtl *C, int n_tables,
                             __syncwarp();
                             if (c > kStage - 32) {
                                 const int L = t + v;
-                                stage_flush_dedup(sbuf, c, tb.stage[L % 3], &C[i].stage_count[L % 3], tb.stage_cap,
+                                stage_flush_dedup<false>(sbuf, c, tb.stage[L % 3], &C[i].stage_count[L % 3], tb.stage_cap,
                                                   tb.set[L & 1], tb.set_mask, tb.s0 + 2ll * L, bsum, &C[i].err);
                             }
                         }
@@ -351,7 +343,7 @@ batch_final_kernel(const BatchTable *__restrict__ TB, BatchCtl *C, int n_tables,
 // native_core/src/BookSolver.cpp:413-470; same arithmetic as solve_kernel),
 // then layer t's live entries enter index plane t % 3 for steps t-1 and t-2.
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 batch_solve_kernel(const BatchTable *__restrict__ TB, BatchCtl *C, int n_tables, int t,
                    const uint64_t *__restrict__ arena, T *__restrict__ rates,
                    const unsigned long long *__restrict__ layer_off, const unsigned long long *__restrict__ layer_len,

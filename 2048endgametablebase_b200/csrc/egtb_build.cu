@@ -174,7 +174,7 @@ struct Engine {
     unsigned *tile_cnt = nullptr;
     unsigned long long *tile_off = nullptr;
     unsigned long long sort_tiles = 0, comp_tiles = 0;
-    uint64_t *dset[2] = {nullptr, nullptr};  // exact dedup sets of the layers under construction (by parity)
+    uint64_t *dset[3] = {nullptr, nullptr, nullptr};  // exact dedup sets: layer L in set L % 3
     unsigned long long dset_cap = 0;          // slots per set
     uint64_t *filter = nullptr;               // direct-mapped repeat filter in front of the sets
     int filter_bits = 20;
@@ -184,7 +184,7 @@ struct Engine {
     unsigned long long *layer_max = nullptr;  // ordered encoding of the largest rate per layer
     unsigned char *book = nullptr;
     unsigned long long book_cap_bytes = 0;
-    ulonglong2 *index[3] = {nullptr, nullptr, nullptr};  // rate index of layers L % 3
+    ulonglong2 *index[4] = {nullptr, nullptr, nullptr, nullptr};  // rate index of layer L in index[L % 4]
     unsigned long long index_cap = 0;                    // slots per index
     unsigned long long *first_tile = nullptr;            // all-layer packing: first tile of every layer
     DevCtl *ctl = nullptr;
@@ -215,6 +215,7 @@ struct Engine {
         EGTB_CUDA(cudaMalloc(&counters, sizeof(unsigned) * 16));
         int per_sm = 0;
         EGTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel, kSweepThreads, 0));
+        EGTB_CUDA(cudaFuncSetAttribute(expand_dedup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
         sweep_grid = sm_count * std::max(1, per_sm);
         progress_device_ptr();
     }
@@ -464,17 +465,16 @@ static void enqueue_sort_unique(Engine &E, const ForwardPlan &P, int x, int L, u
 // its staging buffer and set, layer_off[first_step-1] set.
 static void enqueue_forward(Engine &E, const ForwardPlan &P, unsigned *progress) {
     cudaStream_t s = E.stream;
-    const int g_exp = E.sm_count * 8;
+    const int g_exp = E.sm_count;  // one 1024-thread block per SM (the row table fills its shared memory)
     uint64_t *stage[3] = {E.cand[0], E.cand[1], E.tmp};
     for (int i = P.first_step; i < P.steps - 1; ++i) {
         const int t = i - 1;
         const int pe = E.prof_begin(K_EXPAND);
-        EGTB_LAUNCH(E, expand_dedup_kernel<<<g_exp, kExpandThreads, 0, s>>>(
+        EGTB_LAUNCH(E, expand_dedup_kernel<<<g_exp, kExpandThreads, kRowSmemBytes, s>>>(
                            stage[t % 3], stage[(t + 1) % 3], stage[(t + 2) % 3], t % 3, (t + 1) % 3, (t + 2) % 3,
                            E.arena, E.layer_off, E.layer_len, E.arena_cap, t, P.spec, i > P.docheck ? 1 : 0, E.tab,
-                           E.dset[(t + 1) & 1], E.dset[(t + 2) & 1], E.dset_cap - 1, P.s0 + 2ll * (t + 1),
-                           P.s0 + 2ll * (t + 2), E.cand_cap, E.filter, E.filter_bits, E.ctl, progress,
-                           (unsigned)i));
+                           E.dset[(t + 1) % 3], E.dset[(t + 2) % 3], E.dset_cap - 1, E.cand_cap, E.filter,
+                           E.filter_bits, E.dset[t % 3], E.ctl, progress, (unsigned)i));
         E.prof_end(pe);
     }
     for (int L = std::max(P.first_step, P.steps - 2); L < P.steps; ++L)
@@ -512,8 +512,8 @@ static void stage_start(Engine &E, const ForwardPlan &P, const uint64_t *base, s
     if (n_partial) {
         EGTB_CUDA(cudaMemcpyAsync(stage[t1 % 3], partial, sizeof(uint64_t) * n_partial, cudaMemcpyHostToDevice, s));
         EGTB_LAUNCH(E, set_u64_kernel<<<1, 1, 0, s>>>(&E.ctl->stage_count[t1 % 3], (unsigned long long)n_partial));
-        EGTB_LAUNCH(E, dedup_seed_kernel<<<E.sm_count * 4, 256, 0, s>>>(stage[t1 % 3], n_partial, E.dset[t1 & 1],
-                                                                          E.dset_cap - 1, P.s0 + 2ll * t1, E.ctl));
+        EGTB_LAUNCH(E, dedup_seed_kernel<<<E.sm_count * 4, 256, 0, s>>>(stage[t1 % 3], n_partial, E.dset[t1 % 3],
+                                                                          E.dset_cap - 1, E.ctl));
     }
     // the host buffers above may be pageable: finish the copies before returning
     EGTB_CUDA(cudaStreamSynchronize(s));
@@ -701,10 +701,10 @@ static void enqueue_index_at(Engine &E, int L, unsigned long long n, T zero, ulo
                                                                              E.layer_len, L, zero, idx, slots - 1, E.ctl));
 }
 
-// ... in index slot L % 3 (fused build: layers t, t+1, t+2 use distinct slots).
+// ... in index L % 4 (fused build).
 template <typename T>
 static void enqueue_index(Engine &E, int L, unsigned long long n, T zero) {
-    enqueue_index_at<T>(E, L, n, zero, E.index[L % 3]);
+    enqueue_index_at<T>(E, L, n, zero, E.index[L % 4]);
 }
 
 // Pack every layer's live entries as .book records in one pass; the book of
@@ -747,20 +747,23 @@ static void enqueue_backward(Engine &E, const BackwardPlan &B, const std::vector
     for (int t = B.steps - 2; t < B.steps; ++t)
         if (t >= 0) EGTB_LAUNCH(E, final_layer_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec, zero, maxv));
     for (int t = B.steps - 1; t >= B.steps - 2 && t >= 1; --t) enqueue_index<T>(E, t, len[t], zero);
+    // the solve of layer t reads the indexes of t+1 and t+2, fills layer t's
+    // (L % 4, cleared by the launch before) and clears the one of layer t-1
+    if (B.steps - 3 >= 1)
+        EGTB_CUDA(cudaMemsetAsync(E.index[(B.steps - 3) % 4], 0, sizeof(ulonglong2) * index_slots(len[B.steps - 3]), s));
     E.prof_end(pf);
     for (int t = B.steps - 3; t >= 0; --t) {
-        EGTB_LAUNCH(E, progress_kernel<<<1, 1, 0, s>>>(progress, total - (unsigned)t - 2u));
         const int ps = E.prof_begin(K_SOLVE);
+        ulonglong2 *idx0 = t >= 1 ? E.index[t % 4] : nullptr;
+        ulonglong2 *clear = t >= 2 ? E.index[(t - 1) % 4] : nullptr;
         EGTB_LAUNCH(E, solve_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec,
                                                          t > B.docheck ? 1 : 0, E.tab, B.p4, zero, maxv,
-                                                         E.index[(t + 1) % 3], index_slots(len[t + 1]) - 1,
-                                                         E.index[(t + 2) % 3], index_slots(len[t + 2]) - 1, E.ctl));
+                                                         E.index[(t + 1) % 4], index_slots(len[t + 1]) - 1,
+                                                         E.index[(t + 2) % 4], index_slots(len[t + 2]) - 1, E.ctl,
+                                                         idx0, index_slots(len[t]) - 1, clear,
+                                                         t >= 2 ? index_slots(len[t - 1]) : 0, progress,
+                                                         total - (unsigned)t - 2u));
         E.prof_end(ps);
-        if (t > 0) {
-            const int pi = E.prof_begin(K_INDEX);
-            enqueue_index<T>(E, t, len[t], zero);
-            E.prof_end(pi);
-        }
     }
     const int pp = E.prof_begin(K_PACK);
     enqueue_pack_all<T>(E, B.steps, len, zero);

@@ -129,6 +129,38 @@ __device__ __forceinline__ void move_all_dir(const uint32_t *__restrict__ tab, u
     out[3] = transpose(t ^ ur);
 }
 
+// Row-table accessors: rows(row) = left delta | right delta << 16.
+// GlobalRows reads the 65536-entry u32 table in global memory; SharedRows
+// reads a u16 table of left deltas staged in shared memory (128 KB) and gets
+// the right delta of a row as the reversed left delta of the reversed row.
+struct GlobalRows {
+    const uint32_t *__restrict__ t;
+    __device__ __forceinline__ uint32_t operator()(uint32_t row) const { return __ldg(t + row); }
+};
+
+__device__ __forceinline__ uint32_t reverse_row(uint32_t r) {
+    return ((r & 0xFu) << 12) | ((r & 0xF0u) << 4) | ((r >> 4) & 0xF0u) | (r >> 12);
+}
+
+struct SharedRows {
+    const uint16_t *t;
+    __device__ __forceinline__ uint32_t operator()(uint32_t row) const {
+        return (uint32_t)t[row] | (reverse_row(t[reverse_row(row)]) << 16);
+    }
+};
+
+// Copy the left halves of the u32 table into shared memory (every thread of
+// the block calls it; ends with a barrier).
+__device__ __forceinline__ void stage_rows(const uint32_t *__restrict__ tab, uint16_t *srows) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(tab);
+    uint2 *dst = reinterpret_cast<uint2 *>(srows);
+    for (int i = threadIdx.x; i < 65536 / 4; i += blockDim.x) {
+        const uint4 q = __ldg(src + i);
+        dst[i] = make_uint2((q.x & 0xFFFFu) | (q.y << 16), (q.z & 0xFFFFu) | (q.w << 16));
+    }
+    __syncthreads();
+}
+
 // Per-parent move context: the parent's row deltas (for left/right) and the
 // transposed board's row deltas (for up/down). A spawn touches one row and
 // one column, so a child's four moves need only the deltas of the touched
@@ -139,40 +171,51 @@ struct MoveCtx {
     uint64_t ul, ur;     // left/right deltas of t, all rows (= up/down of b)
 };
 
-__device__ __forceinline__ void move_ctx_init(const uint32_t *__restrict__ tab, uint64_t b, MoveCtx &c) {
+template <typename Rows>
+__device__ __forceinline__ void move_ctx_init(const Rows &rows, uint64_t b, MoveCtx &c) {
     c.b = b;
     c.t = transpose(b);
     c.dl = c.dr = c.ul = c.ur = 0;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        uint32_t d = row_delta(tab, (uint32_t)(b >> (16 * r)) & 0xFFFFu);
+        uint32_t d = rows((uint32_t)(b >> (16 * r)) & 0xFFFFu);
         c.dl |= (uint64_t)(d & 0xFFFFu) << (16 * r);
         c.dr |= (uint64_t)(d >> 16) << (16 * r);
-        uint32_t e = row_delta(tab, (uint32_t)(c.t >> (16 * r)) & 0xFFFFu);
+        uint32_t e = rows((uint32_t)(c.t >> (16 * r)) & 0xFFFFu);
         c.ul |= (uint64_t)(e & 0xFFFFu) << (16 * r);
         c.ur |= (uint64_t)(e >> 16) << (16 * r);
     }
+}
+
+__device__ __forceinline__ void move_ctx_init(const uint32_t *__restrict__ tab, uint64_t b, MoveCtx &c) {
+    move_ctx_init(GlobalRows{tab}, b, c);
 }
 
 // Transposed nibble index of nibble k: (r, c) -> (c, r) keeps k/4 <-> k%4.
 __device__ __forceinline__ int transposed_nibble(int k) { return ((k & 3) << 2) | (k >> 2); }
 
 // Moves of s = parent | v << 4k (nibble k empty in the parent).
-__device__ __forceinline__ void spawn_moves(const uint32_t *__restrict__ tab, const MoveCtx &c, int k, uint64_t v,
-                                            uint64_t &s, uint64_t out[4]) {
+template <typename Rows>
+__device__ __forceinline__ void spawn_moves(const Rows &rows, const MoveCtx &c, int k, uint64_t v, uint64_t &s,
+                                            uint64_t out[4]) {
     s = c.b | (v << (4 * k));
     const int row = k >> 2;
     const uint64_t rmask = 0xFFFFull << (16 * row);
-    const uint32_t d = row_delta(tab, (uint32_t)(s >> (16 * row)) & 0xFFFFu);
+    const uint32_t d = rows((uint32_t)(s >> (16 * row)) & 0xFFFFu);
     out[0] = s ^ ((c.dl & ~rmask) | ((uint64_t)(d & 0xFFFFu) << (16 * row)));
     out[1] = s ^ ((c.dr & ~rmask) | ((uint64_t)(d >> 16) << (16 * row)));
     const int kt = transposed_nibble(k);
     const uint64_t ts = c.t | (v << (4 * kt));
     const int trow = kt >> 2;
     const uint64_t tmask = 0xFFFFull << (16 * trow);
-    const uint32_t e = row_delta(tab, (uint32_t)(ts >> (16 * trow)) & 0xFFFFu);
+    const uint32_t e = rows((uint32_t)(ts >> (16 * trow)) & 0xFFFFu);
     out[2] = transpose(ts ^ ((c.ul & ~tmask) | ((uint64_t)(e & 0xFFFFu) << (16 * trow))));
     out[3] = transpose(ts ^ ((c.ur & ~tmask) | ((uint64_t)(e >> 16) << (16 * trow))));
+}
+
+__device__ __forceinline__ void spawn_moves(const uint32_t *__restrict__ tab, const MoveCtx &c, int k, uint64_t v,
+                                            uint64_t &s, uint64_t out[4]) {
+    spawn_moves(GlobalRows{tab}, c, k, v, s, out);
 }
 
 // Bit set in nibble k's low bit for every empty nibble of b.

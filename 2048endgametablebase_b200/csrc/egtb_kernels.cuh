@@ -86,8 +86,48 @@ __device__ __forceinline__ T block_excl_scan(T v, T *smem, T *total) {
 
 // --------------------------------------------------------- expand --------
 
-constexpr int kExpandThreads = 256;
+constexpr int kExpandThreads = 1024;                       // one block per SM
+constexpr int kRowSmemBytes = 65536 * (int)sizeof(uint16_t);  // dynamic shared memory: the row table
 constexpr int kStage = 64;  // per-warp staging slots per stream
+
+// Children of one spawn of the lane's parent (value v in empty nibble k; k < 0:
+// none): the four moves that moved the board and match the pattern,
+// canonicalised, minus the ones the direct-mapped repeat filter has already
+// seen (filter_bits 0: no filter). The four filter slots are read before any
+// is written, so their loads are in flight together. Returns the kept moves
+// as a 4-bit mask; *probes counts the children that reached the filter.
+template <typename Rows>
+__device__ __forceinline__ unsigned spawn_children(const Rows &rows, const MoveCtx &mc, int k, uint64_t v,
+                                                   const DevSpec &spec, uint64_t *filter, int filter_bits,
+                                                   uint64_t key[4], unsigned long long &probes) {
+    uint64_t mv[4], s = 0;
+    if (k >= 0) spawn_moves(rows, mc, k, v, s, mv);
+    unsigned keep = 0;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        key[d] = 0;
+        if (k >= 0 && mv[d] != s && is_pattern(mv[d], spec)) {
+            key[d] = canonical(mv[d], spec.symm);
+            keep |= 1u << d;
+        }
+    }
+    probes += __popc(keep);
+    if (filter_bits && keep) {
+        uint64_t slot[4], seen[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            slot[d] = filter_slot(key[d], filter_bits);
+            seen[d] = (keep >> d & 1u) ? filter[slot[d]] : ~key[d];
+        }
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            if (!(keep >> d & 1u)) continue;
+            if (seen[d] == key[d]) keep &= ~(1u << d);
+            else filter[slot[d]] = key[d];
+        }
+    }
+    return keep;
+}
 
 // Flush a warp's staging buffer to its candidate stream.
 __device__ __forceinline__ void stage_flush(uint64_t *stage, int &count, uint64_t *__restrict__ out,
@@ -159,10 +199,26 @@ __device__ __forceinline__ int dedup_insert(uint64_t *tab, unsigned long long ma
     return 0;
 }
 
+// 1 when key is new in a set whose free slots hold 0 (a set cleared before
+// its layer's first insert): one atomic per probed slot.
+__device__ __forceinline__ int dedup_insert_zero(uint64_t *tab, unsigned long long mask, uint64_t key, unsigned *err) {
+    unsigned long long h = mix64(key) & mask;
+    for (int probe = 0; probe < kMaxProbe; ++probe) {
+        const unsigned long long prev = atomicCAS((unsigned long long *)tab + h, 0ull, (unsigned long long)key);
+        if (prev == 0ull) return 1;
+        if (prev == key) return 0;
+        h = (h + 1) & mask;
+    }
+    atomicOr(err, kErrDedupOverflow);
+    return 0;
+}
+
 // Flush a warp's staged keys (children that passed the repeat filter): the
 // warp enters them in the layer's set 32 at a time, every lane busy, and
 // appends the ones that are new to the layer's staging buffer. Flags
-// kErrDedupOverflow when the layer passes half its set's capacity.
+// kErrDedupOverflow when the layer passes half its set's capacity. kZero:
+// the set's free slots hold 0 (else: a slot of another tile sum is free).
+template <bool kZero>
 __device__ __forceinline__ void stage_flush_dedup(uint64_t *stage, int &count, uint64_t *__restrict__ out,
                                                   unsigned long long *cnt, unsigned long long cap, uint64_t *set,
                                                   unsigned long long set_mask, long long want, const unsigned *bsum,
@@ -172,7 +228,11 @@ __device__ __forceinline__ void stage_flush_dedup(uint64_t *stage, int &count, u
     for (int b = 0; b < count; b += 32) {
         const int i = b + lane;
         const uint64_t key = i < count ? stage[i] : 0;
-        const bool fresh = i < count && dedup_insert(set, set_mask, key, want, bsum, err) != 0;
+        bool fresh = false;
+        if (i < count) {
+            if constexpr (kZero) fresh = dedup_insert_zero(set, set_mask, key, err) != 0;
+            else fresh = dedup_insert(set, set_mask, key, want, bsum, err) != 0;
+        }
         const unsigned m = __ballot_sync(0xFFFFFFFFu, fresh);
         if (m) {
             unsigned long long base = 0;
@@ -199,20 +259,29 @@ __device__ __forceinline__ void stage_flush_dedup(uint64_t *stage, int &count, u
 // layer t+v's staging buffer iff it is new in layer t+v's set. The same
 // kernel copies layer t into the arena at layer_off[t] and closes it (length,
 // next 16-aligned offset, capacity check); its last block empties layer t's
-// staging buffer for layer t+3.
-static __global__ void __launch_bounds__(kExpandThreads, 4)
+// staging buffer for layer t+3. Sets rotate over three buffers (layer L in
+// set L % 3): this step zeroes layer t's set, which layer t+3 fills next.
+static __global__ void __launch_bounds__(kExpandThreads, 1)
 expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ stage1, uint64_t *__restrict__ stage2,
                     int si_par, int si1, int si2, uint64_t *__restrict__ arena,
                     unsigned long long *__restrict__ layer_off, unsigned long long *__restrict__ layer_len,
                     unsigned long long arena_cap, int t, DevSpec spec, int do_check, const uint32_t *__restrict__ tab,
                     uint64_t *__restrict__ set1, uint64_t *__restrict__ set2, unsigned long long set_mask,
-                    long long sum1, long long sum2, unsigned long long stage_cap, uint64_t *filter,
-                    int filter_bits, DevCtl *ctl, unsigned *progress, unsigned progress_value) {
+                    unsigned long long stage_cap, uint64_t *filter, int filter_bits, uint64_t *__restrict__ clear_set,
+                    DevCtl *ctl, unsigned *progress, unsigned progress_value) {
     __shared__ uint64_t stage[kExpandThreads / 32][2][kStage];
-    __shared__ unsigned bsum[256];
     __shared__ int last_block;
+    extern __shared__ uint16_t srows[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    init_byte_sums(bsum);
+    stage_rows(tab, srows);
+    const SharedRows rows{srows};
+    {
+        uint4 *z = reinterpret_cast<uint4 *>(clear_set);
+        const unsigned long long nz = (set_mask + 1) / 2;
+        for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < nz;
+             i += (unsigned long long)gridDim.x * blockDim.x)
+            z[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
     // once this pass has overflowed a buffer it will be re-run: skip the work
     const unsigned long long n = (ctl->err & (kErrCandOverflow | kErrDedupOverflow)) ? 0 : ctl->stage_count[si_par];
     const unsigned long long off = layer_off[t];
@@ -241,7 +310,7 @@ expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ sta
         if (active && do_check && is_success(b, spec)) active = false;
         uint64_t empt = active ? empty_nibbles(b) : 0;
         MoveCtx mc;
-        move_ctx_init(tab, b, mc);
+        move_ctx_init(rows, b, mc);
         unsigned any = __ballot_sync(0xFFFFFFFFu, empt != 0);
         while (any) {
             // next empty nibble of this lane (lanes advance independently; the
@@ -254,24 +323,16 @@ expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ sta
 #pragma unroll 1
             for (int v = 1; v <= 2; ++v) {
                 uint64_t *const set = v == 1 ? set1 : set2;
-                const long long want = v == 1 ? sum1 : sum2;
                 uint64_t *const sbuf = stage[warp][v - 1];
                 int c = v == 1 ? cnt1 : cnt2;
-                uint64_t mv[4], s = 0;
-                if (k >= 0) spawn_moves(tab, mc, k, (uint64_t)v, s, mv);
+                // a direct-mapped filter drops most repeats with one load; a
+                // key it holds has already been staged for its set
+                uint64_t keys[4];
+                const unsigned kept = spawn_children(rows, mc, k, (uint64_t)v, spec, filter, filter_bits, keys, probes);
 #pragma unroll
                 for (int d = 0; d < 4; ++d) {
-                    bool keep = k >= 0 && mv[d] != s && is_pattern(mv[d], spec);
-                    uint64_t key = 0;
-                    if (keep) {
-                        key = canonical(mv[d], spec.symm);
-                        ++probes;
-                        // a direct-mapped filter drops most repeats with one load;
-                        // a key it holds has already been staged for its set
-                        const uint64_t slot = filter_slot(key, filter_bits);
-                        if (filter[slot] == key) keep = false;
-                        else filter[slot] = key;
-                    }
+                    const bool keep = kept >> d & 1u;
+                    const uint64_t key = keys[d];
                     const unsigned m = __ballot_sync(0xFFFFFFFFu, keep);
                     if (m) {
                         const int pos = c + __popc(m & ((1u << lane) - 1u));
@@ -279,8 +340,9 @@ expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ sta
                         c += __popc(m);
                         __syncwarp();
                         if (c > kStage - 32)
-                            stage_flush_dedup(sbuf, c, v == 1 ? stage1 : stage2, &ctl->stage_count[v == 1 ? si1 : si2],
-                                              stage_cap, set, set_mask, want, bsum, &ctl->err);
+                            stage_flush_dedup<true>(sbuf, c, v == 1 ? stage1 : stage2,
+                                                    &ctl->stage_count[v == 1 ? si1 : si2], stage_cap, set, set_mask,
+                                                    0, nullptr, &ctl->err);
                     }
                 }
                 if (v == 1) cnt1 = c; else cnt2 = c;
@@ -288,10 +350,10 @@ expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ sta
             any = __ballot_sync(0xFFFFFFFFu, empt != 0);
         }
     }
-    stage_flush_dedup(stage[warp][0], cnt1, stage1, &ctl->stage_count[si1], stage_cap, set1, set_mask, sum1, bsum,
-                      &ctl->err);
-    stage_flush_dedup(stage[warp][1], cnt2, stage2, &ctl->stage_count[si2], stage_cap, set2, set_mask, sum2, bsum,
-                      &ctl->err);
+    stage_flush_dedup<true>(stage[warp][0], cnt1, stage1, &ctl->stage_count[si1], stage_cap, set1, set_mask, 0,
+                            nullptr, &ctl->err);
+    stage_flush_dedup<true>(stage[warp][1], cnt2, stage2, &ctl->stage_count[si2], stage_cap, set2, set_mask, 0,
+                            nullptr, &ctl->err);
     for (int o = 16; o > 0; o >>= 1) probes += __shfl_xor_sync(0xFFFFFFFFu, probes, o);
     if (lane == 0 && probes) atomicAdd(&ctl->candidates, probes);
     // the last block to finish empties layer t's staging buffer
@@ -336,13 +398,10 @@ flush_layer_kernel(const uint64_t *__restrict__ stage_l, int si, uint64_t *__res
 // Insert keys already known to be in layer L (a resumed partial layer).
 static __global__ void __launch_bounds__(256)
 dedup_seed_kernel(const uint64_t *__restrict__ keys, unsigned long long n, uint64_t *set, unsigned long long mask,
-                  long long want_sum, DevCtl *ctl) {
-    __shared__ unsigned bsum[256];
-    init_byte_sums(bsum);
-    __syncthreads();
+                  DevCtl *ctl) {
     for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (unsigned long long)gridDim.x * blockDim.x)
-        dedup_insert(set, mask, keys[i], want_sum, bsum, &ctl->err);
+        dedup_insert_zero(set, mask, keys[i], &ctl->err);
 }
 
 // ------------------------------------------ sorting every layer at once ----
@@ -488,27 +547,56 @@ index_insert_kernel(const uint64_t *__restrict__ arena, const T *__restrict__ ra
     }
 }
 
+// {key, rate} into an index whose free slots hold key 0.
+template <typename T>
+__device__ __forceinline__ void index_insert_zero(ulonglong2 *slots, unsigned long long mask, uint64_t key, T r,
+                                                  unsigned *err) {
+    unsigned long long h = mix64(key) & mask;
+    for (int probe = 0; probe < kMaxProbe * 32; ++probe) {
+        const unsigned long long prev = atomicCAS(&slots[h].x, 0ull, (unsigned long long)key);
+        if (prev == 0ull || prev == key) {
+            slots[h].y = rate_bits<T>(r);
+            return;
+        }
+        h = (h + 1) & mask;
+    }
+    atomicOr(err, kErrIndexOverflow);
+}
+
 // Backward solve of layer t (recalculate_layer, native_core/src/BookSolver.cpp:
 // 413-470). Per board: success with do_check -> max; else for every empty
 // nibble ascending, best2 = max of layer t+1 rates over the kept moves of the
 // spawn-2 board, acc = fma(best2, 1-p4, acc); best4 likewise from layer t+2,
 // acc = fma(best4, p4, acc); rate = T(acc / #empty). The two fma() are the
 // reference's `+=` statements as its -Ofast x86-64-v3 build contracts them.
+// With idx0, layer t's live entries also enter its rate index (mask m0) for
+// the solves of layers t-1 and t-2; with clear_idx, this launch zeroes
+// clear_slots slots of another (unused) index for the next launch's inserts.
 template <typename T>
 __global__ void __launch_bounds__(256)
 solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
              const unsigned long long *__restrict__ layer_off, const unsigned long long *__restrict__ layer_len,
              int t, DevSpec spec, int do_check, const uint32_t *__restrict__ tab, double p4, T zero, T maxv,
              const ulonglong2 *__restrict__ idx1, unsigned long long m1, const ulonglong2 *__restrict__ idx2,
-             unsigned long long m2, DevCtl *ctl) {
+             unsigned long long m2, DevCtl *ctl, ulonglong2 *__restrict__ idx0 = nullptr, unsigned long long m0 = 0,
+             ulonglong2 *__restrict__ clear_idx = nullptr, unsigned long long clear_slots = 0,
+             unsigned *progress = nullptr, unsigned progress_value = 0) {
     const unsigned long long n0 = layer_len[t], o0 = layer_off[t];
     const double w2 = 1.0 - p4;
     unsigned long long looks = 0;
+    if (progress && blockIdx.x == 0 && threadIdx.x == 0) *(volatile unsigned *)progress = progress_value;
+    if (clear_idx) {
+        uint4 *z = reinterpret_cast<uint4 *>(clear_idx);
+        for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < clear_slots;
+             i += (unsigned long long)gridDim.x * blockDim.x)
+            z[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
     for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n0;
          i += (unsigned long long)gridDim.x * blockDim.x) {
         const uint64_t b = arena[o0 + i];
         if (do_check && is_success(b, spec)) {
             rates[o0 + i] = maxv;
+            if (idx0 && maxv > zero) index_insert_zero<T>(idx0, m0, b, maxv, &ctl->err);
             continue;
         }
         MoveCtx mc;
@@ -567,7 +655,9 @@ solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
             acc = fma((double)best2, w2, acc);
             acc = fma((double)best4, p4, acc);
         }
-        rates[o0 + i] = nempty > 0 ? cast_rate<T>(acc / (double)nempty) : zero;
+        const T r = nempty > 0 ? cast_rate<T>(acc / (double)nempty) : zero;
+        rates[o0 + i] = r;
+        if (idx0 && r > zero) index_insert_zero<T>(idx0, m0, b, r, &ctl->err);
     }
     // warp-aggregated statistics
     for (int o = 16; o > 0; o >>= 1) looks += __shfl_xor_sync(0xFFFFFFFFu, looks, o);

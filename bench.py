@@ -215,6 +215,8 @@ def main():
     ap.add_argument("--profile-run", action="store_true",
                     help="one device-resident build and nothing else (for an ncu launch list)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-build leg")
+    ap.add_argument("--batch-only", action="store_true", help="run the batched-build leg alone and print its JSON")
     ap.add_argument("--serve-only", action="store_true", help="run the serving leg alone and print its JSON")
     ap.add_argument("--serve-offered", type=float, default=1e8, help="offered lookups/s of the serving leg")
     ap.add_argument("--profile-sort", type=int, default=0,
@@ -258,6 +260,10 @@ def main():
                                              stream.cuda_stream))
         torch.cuda.synchronize()
         print(json.dumps({"profile_sort": args.profile_sort, "unique": int(cnt.item())}))
+        shutil.rmtree(work, ignore_errors=True)
+        return
+    if args.batch_only:
+        print(json.dumps({"batched": batch_leg(local, cpu_reference=not args.no_cpu_baseline)}), flush=True)
         shutil.rmtree(work, ignore_errors=True)
         return
     if args.serve_only:
@@ -367,6 +373,8 @@ def main():
             N.set_stream(local, None)
             line["serving"] = serving_leg(local, base, offered=args.serve_offered,
                                           cpu_reference=not args.no_cpu_baseline)
+        if not args.no_batch and world == 1:
+            line["batched"] = batch_leg(local, cpu_reference=not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)
     shutil.rmtree(work, ignore_errors=True)
     if pg is not None:
@@ -410,6 +418,82 @@ def reference_reader_rate(books, positions: np.ndarray, specs) -> dict | None:
         total_n += len(boards)
     return {"lookups_per_s": total_n / total_t, "cores": 1, "kind": "reference",
             "sample": f"{total_n} move_on_dic calls over the same books, one position per call"}
+
+
+def reference_batch_rate(tables, threads: int) -> dict | None:
+    """The reference's compiled classic path (oracle/_ref) building a sample
+    of the batch's tables one after another on the host cores
+    (checker/baseline only)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reference as R  # noqa: E402
+
+    if not R.available():
+        return None
+    base = "/dev/shm" if os.access("/dev/shm", os.W_OK) else None
+    total_t, boards, names = 0.0, 0, []
+    for t in tables:
+        d = tempfile.mkdtemp(prefix="egtb_refb_", dir=base) + "/"
+        try:
+            spec = t.spec()
+            s, o = R.make_spec_options(spec.pattern_masks, spec.success_shifts, 0, t.target, t.steps, t.docheck,
+                                       d + t.name + "_", "float32", t.spawn_rate4, threads)
+            t0 = time.perf_counter()
+            R.run_build(t.seeds, s, o)
+            total_t += time.perf_counter() - t0
+            lines = open(d + t.name + "_stats.txt").read().splitlines()[1:]
+            boards += sum(int(x.split(",")[1]) for x in lines if x)
+            names.append(t.name)
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+            lf = os.path.join(os.path.dirname(d.rstrip("/")), "length_factors_list.txt")
+            if os.path.exists(lf):
+                os.remove(lf)
+    return {"value": boards / total_t, "unit": "boards/s", "cores": threads, "kind": "reference",
+            "sample": f"{len(names)} of the 64 tables built one after another ({boards} boards, {total_t:.2f} s)"}
+
+
+def batch_leg(local: int, steps: int = 3, cpu_reference: bool = True) -> dict:
+    """Batched build: 64 seeded random tables (6-10 free cells anchored at the
+    bottom-right corner, targets 64..512) built in one batch (tuned launch
+    parameters, per-step loops as CUDA graphs) against the same tables built
+    one at a time by the plain path; books stay on the device in both."""
+    import torch
+
+    B = importlib.import_module("2048endgametablebase_b200.batch")
+    N = importlib.import_module("2048endgametablebase_b200._native")
+    tables = B.random_tables(64)
+    stream = torch.cuda.current_stream(local)
+    N.set_stream(local, stream.cuda_stream)
+
+    def timed(fn, k):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, e0.elapsed_time(e1) / k
+
+    B.build_batch(tables, device=local)  # capacities settle (regrowth) on the first build
+    tuned, _ = B.autotune(tables, device=local)
+    B.build_one_at_a_time(tables, device=local)
+    (ts, bs), batch_ms = timed(lambda: B.build_batch(tables, device=local), steps)
+    plain, plain_ms = timed(lambda: B.build_one_at_a_time(tables, device=local), 1)
+    N.set_stream(local, None)
+    boards = int(bs["raw_boards"])
+    out = {"workload": "64 random tables, 6-10 free cells, targets 64..512 (numpy default_rng(i) per table)",
+           "boards": boards, "batched_ms": batch_ms, "one_at_a_time_ms": plain_ms,
+           "batched_boards_per_s": boards / (batch_ms / 1e3), "one_at_a_time_boards_per_s": boards / (plain_ms / 1e3),
+           "speedup": plain_ms / batch_ms, "phases_ms": {k: bs[k] for k in ("forward_ms", "sort_ms", "backward_ms", "pack_ms")},
+           "kernel_launches": bs["kernel_launches"], "graph_launches": bs["graph_launches"],
+           "one_at_a_time_launches": int(sum(x["kernel_launches"] for x in plain)), "params": tuned, "steps": steps}
+    if cpu_reference:
+        small = sorted(tables, key=lambda t: len(t.cells) * 16 + t.target)[:16]
+        ref = reference_batch_rate(small, os.cpu_count() or 1)
+        if ref:
+            out["cpu_reference"] = ref
+    return out
 
 
 def serving_leg(local: int, base: str | None, seconds: float = 0.5, offered: float = 1e8,

@@ -271,7 +271,7 @@ EGTB_API int egtb_find_classic_value(const char *pathname, const char *filename,
  * loops replayed as CUDA graphs, one radix sort for every table's layers. */
 typedef struct egtb_batch_params {
     int32_t expand_chunk;         /* parents per work item of the forward step: multiple of 32 in 32..4096 (0: tuned, else 128) */
-    int32_t expand_blocks_per_sm; /* blocks per SM of the forward step, 1..8 (0: tuned, else 4) */
+    int32_t expand_blocks_per_sm; /* blocks per SM of the forward step, 1..8 (0: tuned, else 3) */
     int32_t digit_nibbles;        /* radix digit of the layer sort in nibbles, 1 or 2 (0: tuned, else 2) */
     int32_t index_load;           /* rate-index slots per key of a table's largest layer, 2 or 4 (0: tuned, else 2) */
     int32_t use_graphs;           /* 1: per-step loops replayed as CUDA graphs, -1: direct launches (0: tuned, else 1) */
