@@ -573,7 +573,7 @@ __device__ __forceinline__ void index_insert_zero(ulonglong2 *slots, unsigned lo
 // the solves of layers t-1 and t-2; with clear_idx, this launch zeroes
 // clear_slots slots of another (unused) index for the next launch's inserts.
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
              const unsigned long long *__restrict__ layer_off, const unsigned long long *__restrict__ layer_len,
              int t, DevSpec spec, int do_check, const uint32_t *__restrict__ tab, double p4, T zero, T maxv,

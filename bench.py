@@ -449,7 +449,7 @@ def reference_batch_rate(tables, threads: int) -> dict | None:
             if os.path.exists(lf):
                 os.remove(lf)
     return {"value": boards / total_t, "unit": "boards/s", "cores": threads, "kind": "reference",
-            "sample": f"{len(names)} of the 64 tables built one after another ({boards} boards, {total_t:.2f} s)"}
+            "sample": f"{len(names)} mid-sized tables of the 64 built one after another ({boards} boards, {total_t:.2f} s)"}
 
 
 def batch_leg(local: int, steps: int = 3, cpu_reference: bool = True) -> dict:
@@ -489,8 +489,9 @@ def batch_leg(local: int, steps: int = 3, cpu_reference: bool = True) -> dict:
            "kernel_launches": bs["kernel_launches"], "graph_launches": bs["graph_launches"],
            "one_at_a_time_launches": int(sum(x["kernel_launches"] for x in plain)), "params": tuned, "steps": steps}
     if cpu_reference:
-        small = sorted(tables, key=lambda t: len(t.cells) * 16 + t.target)[:16]
-        ref = reference_batch_rate(small, os.cpu_count() or 1)
+        by_size = sorted(range(len(tables)), key=lambda i: ts[i]["raw_boards"])
+        sample = [tables[i] for i in by_size[24:40]]  # 16 mid-sized tables
+        ref = reference_batch_rate(sample, os.cpu_count() or 1)
         if ref:
             out["cpu_reference"] = ref
     return out
