@@ -533,12 +533,12 @@ struct Run {
             for (int L = 0; L < t.steps; ++L) t.max_len = std::max(t.max_len, len[t.lbase + L]);
             t.index_slots = pow2_at_least((unsigned long long)prm.index_load * std::max(1ull, t.max_len), 64);
             t.index_off = index_total;
-            index_total += 3 * t.index_slots;
+            index_total += 4 * t.index_slots;
         }
         B.index.ensure(sizeof(ulonglong2) * index_total, "rate index");
         B.rates.ensure(sizeof(T) * arena_total, "rates");
         for (int i = 0; i < n; ++i) {
-            for (int k = 0; k < 3; ++k)
+            for (int k = 0; k < 4; ++k)
                 host_tables[i].index[k] = B.index.as<ulonglong2>() + tp[i].index_off + k * tp[i].index_slots;
             host_tables[i].index_mask = tp[i].index_slots - 1;
         }

@@ -37,7 +37,7 @@ struct BatchTable {
     uint64_t *set[2];              // exact dedup sets by layer parity
     unsigned long long set_mask;
     uint64_t *filter;
-    ulonglong2 *index[3];          // rate index planes: layer L in index[L % 3]
+    ulonglong2 *index[4];          // rate index planes: layer L in index[L % 4], zeroed by step L+1
     unsigned long long index_mask;
 };
 
@@ -271,40 +271,20 @@ batch_decompose_kernel(const BatchTable *__restrict__ T, const uint64_t *__restr
     }
 }
 
+// Zero `words` 16-byte words at p with every thread of the grid.
+__device__ __forceinline__ void grid_zero16(void *p, unsigned long long words) {
+    uint4 *z = reinterpret_cast<uint4 *>(p);
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < words;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        z[i] = make_uint4(0u, 0u, 0u, 0u);
+}
+
 // ------------------------------------------------------------ backward ----
 //
-// Rate-index planes are never cleared: layer L's entries go to plane L % 3,
-// which last held layers L+3, L+6, ... of other tile sums (or zeros). A slot
-// whose key has another tile sum than the layer's is free, exactly like the
-// forward's dedup sets; a lookup stops at the first free slot.
-
-// Insert {key, rate} of layer with tile sum want into a plane.
-template <typename T>
-__device__ __forceinline__ void plane_insert(ulonglong2 *slots, unsigned long long mask, uint64_t key, T r,
-                                             long long want, const unsigned *bsum, unsigned *err) {
-    unsigned long long h = mix64(key) & mask;
-    for (int probe = 0; probe < kMaxProbe * 32; ++probe) {
-        unsigned long long cur = __ldcg(&slots[h].x);
-        for (;;) {
-            if (cur == key) {
-                slots[h].y = rate_bits<T>(r);
-                return;
-            }
-            if (board_tile_sum(cur, bsum) != want) {
-                const unsigned long long prev = atomicCAS(&slots[h].x, cur, (unsigned long long)key);
-                if (prev == cur) {
-                    slots[h].y = rate_bits<T>(r);
-                    return;
-                }
-                cur = prev;
-                continue;
-            }
-            break;
-        }
-        h = (h + 1) & mask;
-    }
-    atomicOr(err, kErrIndexOverflow);
-}
+// Four rate-index planes per table (layer L in plane L % 4), all zeroed before
+// the backward pass; the solve of step t inserts layer t into plane t % 4 and
+// zeroes plane (t-1) % 4, whose last layer (t+3) was read by steps t+1 and
+// t+2, for the inserts of step t-1. A probe stops at a zero key.
 
 // Layers steps-2 and steps-1 of every table: success -> max, else zero
 // (final_situation_process, native_core/src/BookSolver.cpp:237-261); live
@@ -314,10 +294,8 @@ __global__ void __launch_bounds__(256)
 batch_final_kernel(const BatchTable *__restrict__ TB, BatchCtl *C, int n_tables, const uint64_t *__restrict__ arena,
                    T *__restrict__ rates, const unsigned long long *__restrict__ layer_off,
                    const unsigned long long *__restrict__ layer_len, T zero, T maxv) {
-    __shared__ unsigned bsum[256];
     __shared__ unsigned long long pre[2 * kMaxBatchTables + 1];
     __shared__ unsigned long long scan_sm[33];
-    init_byte_sums(bsum);
     const int nseg = 2 * n_tables;
     seg_prefix(nseg, pre, scan_sm, [&](int s) -> unsigned long long {
         const BatchTable &tb = TB[s >> 1];
@@ -335,13 +313,13 @@ batch_final_kernel(const BatchTable *__restrict__ TB, BatchCtl *C, int n_tables,
         const uint64_t b = arena[o];
         const T r = is_success(b, tb.spec) ? maxv : zero;
         rates[o] = r;
-        if (L >= 1 && r > zero) plane_insert<T>(tb.index[L % 3], tb.index_mask, b, r, tb.s0 + 2ll * L, bsum, &C[i].err);
+        if (L >= 1 && r > zero) index_insert_zero<T>(tb.index[L % 4], tb.index_mask, b, r, &C[i].err);
     }
 }
 
 // Backward step t of every table with t <= steps-3 (recalculate_layer,
 // native_core/src/BookSolver.cpp:413-470; same arithmetic as solve_kernel),
-// then layer t's live entries enter index plane t % 3 for steps t-1 and t-2.
+// then layer t's live entries enter index plane t % 4 for steps t-1 and t-2.
 template <typename T>
 __global__ void __launch_bounds__(256, 3)
 batch_solve_kernel(const BatchTable *__restrict__ TB, BatchCtl *C, int n_tables, int t,
@@ -349,13 +327,14 @@ batch_solve_kernel(const BatchTable *__restrict__ TB, BatchCtl *C, int n_tables,
                    const unsigned long long *__restrict__ layer_off, const unsigned long long *__restrict__ layer_len,
                    const uint32_t *__restrict__ tab, T zero, T maxv, BatchSync *sync, unsigned *progress,
                    unsigned progress_value) {
-    __shared__ unsigned bsum[256];
     __shared__ unsigned long long pre[kMaxBatchTables + 1];
     __shared__ unsigned long long scan_sm[33];
-    init_byte_sums(bsum);
     seg_prefix(n_tables, pre, scan_sm, [&](int i) -> unsigned long long {
         return t <= TB[i].steps - 3 ? layer_len[TB[i].lbase + t] : 0ull;
     });
+    if (t >= 2)
+        for (int i = 0; i < n_tables; ++i)
+            if (t <= TB[i].steps - 3) grid_zero16(TB[i].index[(t - 1) % 4], TB[i].index_mask + 1);
     if (progress && blockIdx.x == 0 && threadIdx.x == 0) *(volatile unsigned *)progress = progress_value;
     const unsigned long long total = pre[n_tables];
     unsigned long long looks = 0;
@@ -370,9 +349,8 @@ batch_solve_kernel(const BatchTable *__restrict__ TB, BatchCtl *C, int n_tables,
             r = maxv;
         } else {
             const double p4 = tb.p4, w2 = 1.0 - p4;
-            const ulonglong2 *idx1 = tb.index[(t + 1) % 3], *idx2 = tb.index[(t + 2) % 3];
+            const ulonglong2 *idx1 = tb.index[(t + 1) % 4], *idx2 = tb.index[(t + 2) % 4];
             const unsigned long long m = tb.index_mask;
-            const long long want1 = tb.s0 + 2ll * (t + 1), want2 = tb.s0 + 2ll * (t + 2);
             MoveCtx mc;
             move_ctx_init(tab, b, mc);
             uint64_t empt = empty_nibbles(b);
@@ -412,7 +390,7 @@ batch_solve_kernel(const BatchTable *__restrict__ TB, BatchCtl *C, int n_tables,
                             if (sl.x == key[j]) {
                                 got[j] = rate_from_bits<T>(sl.y);
                                 pend &= ~(1u << j);
-                            } else if (board_tile_sum(sl.x, bsum) != (j < 4 ? want1 : want2)) {
+                            } else if (sl.x == 0ull) {
                                 pend &= ~(1u << j);
                             } else {
                                 h[j] = (h[j] + 1) & m;
@@ -436,7 +414,7 @@ batch_solve_kernel(const BatchTable *__restrict__ TB, BatchCtl *C, int n_tables,
             r = nempty > 0 ? cast_rate<T>(acc / (double)nempty) : zero;
         }
         rates[o] = r;
-        if (t > 0 && r > zero) plane_insert<T>(tb.index[t % 3], tb.index_mask, b, r, tb.s0 + 2ll * t, bsum, &C[i].err);
+        if (t > 0 && r > zero) index_insert_zero<T>(tb.index[t % 4], tb.index_mask, b, r, &C[i].err);
     }
     for (int o = 16; o > 0; o >>= 1) looks += __shfl_xor_sync(0xFFFFFFFFu, looks, o);
     if ((threadIdx.x & 31) == 0 && looks) atomicAdd(&sync->lookups, looks);
