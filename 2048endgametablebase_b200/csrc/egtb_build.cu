@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstring>
 #include <fstream>
+#include <future>
 #include <memory>
 #include <mutex>
 #include <sstream>
@@ -163,6 +164,11 @@ struct Engine {
     size_t last_rec = 0;
     std::vector<unsigned long long> last_off, last_blen;
     uint64_t *split = nullptr;
+    // streamed forward: two sort buffers, a copy stream and its events
+    uint64_t *sort_buf[2] = {nullptr, nullptr};
+    unsigned long long sort_cap = 0;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_sorted = nullptr, ev_copied = nullptr;
     uint64_t *cand[2] = {nullptr, nullptr};
     uint64_t *tmp = nullptr;
     unsigned *hist = nullptr;               // digit histograms, kMaxPasses x 256
@@ -236,6 +242,18 @@ struct Engine {
         }
     }
 
+    // Run a grow step; if an allocation fails, forget the capacity (the
+    // buffers it released are gone) and rethrow.
+    template <typename F>
+    void grow(unsigned long long &cap, F &&f) {
+        try {
+            f();
+        } catch (...) {
+            cap = 0;
+            throw;
+        }
+    }
+
     void ensure_steps(int steps) {
         if (steps + 3 <= steps_cap) return;
         release(layer_off);
@@ -257,7 +275,9 @@ struct Engine {
         if (slots <= dset_cap) return;
         for (auto &p : dset) release(p);
         dset_cap = slots;
-        for (auto &p : dset) alloc_or_throw((void **)&p, sizeof(uint64_t) * dset_cap, "dedup set");
+        grow(dset_cap, [&] {
+            for (auto &p : dset) alloc_or_throw((void **)&p, sizeof(uint64_t) * dset_cap, "dedup set");
+        });
     }
 
     // look-back words for sorts of up to max(cand_cap, arena_cap) keys
@@ -277,7 +297,9 @@ struct Engine {
         if (slots <= index_cap) return;
         for (auto &p : index) release(p);
         index_cap = slots;
-        for (auto &p : index) alloc_or_throw((void **)&p, sizeof(ulonglong2) * index_cap, "rate index");
+        grow(index_cap, [&] {
+            for (auto &p : index) alloc_or_throw((void **)&p, sizeof(ulonglong2) * index_cap, "rate index");
+        });
     }
 
     void ensure_arena(unsigned long long cap) {
@@ -288,10 +310,12 @@ struct Engine {
         release(split);
         release(book);
         arena_cap = align16(cap);
-        alloc_or_throw((void **)&arena, sizeof(uint64_t) * arena_cap, "layer arena");
-        alloc_or_throw((void **)&split, sizeof(uint64_t) * (arena_cap / kSplitStride + 1), "splitters");
-        book_cap_bytes = arena_cap * 16ull;
-        alloc_or_throw((void **)&book, book_cap_bytes, "books");
+        grow(arena_cap, [&] {
+            alloc_or_throw((void **)&arena, sizeof(uint64_t) * arena_cap, "layer arena");
+            alloc_or_throw((void **)&split, sizeof(uint64_t) * (arena_cap / kSplitStride + 1), "splitters");
+            book_cap_bytes = arena_cap * 16ull;
+            alloc_or_throw((void **)&book, book_cap_bytes, "books");
+        });
         ensure_comp_tiles();
         ensure_status();
     }
@@ -302,7 +326,7 @@ struct Engine {
         if (need <= rates_bytes) return;
         release(rates);
         rates_bytes = need;
-        alloc_or_throw(&rates, need, "rates");
+        grow(rates_bytes, [&] { alloc_or_throw(&rates, need, "rates"); });
     }
 
     void ensure_cand(unsigned long long cap) {
@@ -312,9 +336,11 @@ struct Engine {
         release(cand[1]);
         release(tmp);
         cand_cap = cap;
-        alloc_or_throw((void **)&cand[0], sizeof(uint64_t) * cand_cap, "candidates");
-        alloc_or_throw((void **)&cand[1], sizeof(uint64_t) * cand_cap, "candidates");
-        alloc_or_throw((void **)&tmp, sizeof(uint64_t) * cand_cap, "sort buffer");
+        grow(cand_cap, [&] {
+            alloc_or_throw((void **)&cand[0], sizeof(uint64_t) * cand_cap, "candidates");
+            alloc_or_throw((void **)&cand[1], sizeof(uint64_t) * cand_cap, "candidates");
+            alloc_or_throw((void **)&tmp, sizeof(uint64_t) * cand_cap, "sort buffer");
+        });
         ensure_status();
         ensure_comp_tiles();
     }
@@ -327,6 +353,20 @@ struct Engine {
         comp_tiles = need;
         alloc_or_throw((void **)&tile_cnt, sizeof(unsigned) * comp_tiles, "tile counts");
         alloc_or_throw((void **)&tile_off, sizeof(unsigned long long) * comp_tiles, "tile offsets");
+    }
+
+    void ensure_sort_bufs(unsigned long long cap) {
+        if (cap <= sort_cap) return;
+        for (auto &p : sort_buf) release(p);
+        sort_cap = cap;
+        grow(sort_cap, [&] {
+            for (auto &p : sort_buf) alloc_or_throw((void **)&p, sizeof(uint64_t) * sort_cap, "layer sort buffer");
+        });
+        if (!copy_stream) {
+            EGTB_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+            EGTB_CUDA(cudaEventCreateWithFlags(&ev_sorted, cudaEventDisableTiming));
+            EGTB_CUDA(cudaEventCreateWithFlags(&ev_copied, cudaEventDisableTiming));
+        }
     }
 
     unsigned char *ensure_pinned(size_t bytes) {
@@ -624,6 +664,188 @@ static int run_forward(Engine &E, const ForwardPlan &P, const uint64_t *base, si
         if (c.err & kErrCandOverflow) E.ensure_cand(E.cand_cap * 2);
         if (c.err & kErrArenaOverflow) E.ensure_arena(E.arena_cap + E.arena_cap / 2);
         if (c.err & kErrDedupOverflow) E.ensure_dedup(E.dset_cap * 2);
+    }
+}
+
+// ------------------------------------------------------ streamed forward --
+//
+// Forward pass for tables larger than device memory: after step t expands
+// layer t, the layer (unique keys in its staging buffer) is radix-sorted on
+// the device, and while step t+1 runs it is copied on a second stream into
+// one of two pinned host buffers and written to the raw layer file
+// <pathname><t> by a host thread. The device holds the window of layers t..t+2
+// (staging buffers, dedup sets, two sort buffers) instead of the whole table.
+// The last two layers end sorted in the arena for the success-only books.
+
+static bool stream_layers_forced() {
+    const char *v = getenv("EGTB_STREAM_LAYERS");
+    return v && *v && std::strcmp(v, "0") != 0;
+}
+
+// Enqueue the sort of the n (*n_ptr, on the device) unique keys at src;
+// returns the buffer that holds them sorted.
+static uint64_t *enqueue_layer_sort(Engine &E, const SortPlan &sp, const uint64_t *src,
+                                    const unsigned long long *n_ptr) {
+    cudaStream_t s = E.stream;
+    EGTB_CUDA(cudaMemsetAsync(E.hist, 0, sizeof(unsigned) * kMaxPasses * 256, s));
+    EGTB_LAUNCH(E, sort_hist_kernel<<<E.sm_count * 2, 256, 0, s>>>(src, n_ptr, E.sort_cap, sp, E.hist, E.counters,
+                                                                   E.ctl));
+    const uint64_t *in = src;
+    uint64_t *out = E.sort_buf[0];
+    for (int q = 0; q < sp.passes; ++q) {
+        const int pi = E.prof_begin(K_SORT_PASS);
+        EGTB_LAUNCH(E, onesweep_kernel<<<E.sweep_grid, kSweepThreads, 0, s>>>(in, out, n_ptr, E.sort_cap, sp, q, E.hist,
+                                                                             E.counters, E.status, E.epoch++, E.ctl));
+        E.prof_end(pi);
+        in = out;
+        out = out == E.sort_buf[0] ? E.sort_buf[1] : E.sort_buf[0];
+    }
+    return const_cast<uint64_t *>(in);
+}
+
+// Returns the retries; off/len: the layers' arena offsets and lengths (only
+// the last two layers are in the arena).
+static int run_forward_streamed(Engine &E, const ForwardPlan &P, const uint64_t *base, size_t n_base,
+                                const uint64_t *partial, size_t n_partial, const std::string &prefix, float *ms,
+                                std::vector<unsigned long long> &off, std::vector<unsigned long long> &len) {
+    int retries = 0;
+    E.ensure_steps(P.steps);
+    // streamed tables are large: start at 16 Mi keys per layer buffer and
+    // grow 4x, since an overflow re-runs the pass from its first step
+    static const unsigned long long init_cand = env_keys("EGTB_INIT_CAND_KEYS", 1ull << 24);
+    static const unsigned long long init_set = env_keys("EGTB_INIT_SET_SLOTS", 1ull << 23);
+    E.ensure_cand(std::max<unsigned long long>(E.cand_cap, std::max<unsigned long long>(init_cand,
+                                                                                         2 * std::max(n_partial, n_base))));
+    unsigned long long set_need = init_set;
+    while (set_need < 4 * std::max<unsigned long long>(n_partial, 1)) set_need <<= 1;
+    E.ensure_dedup(std::max(E.dset_cap, set_need));
+    unsigned *progress = progress_device_ptr();
+    cudaStream_t s = E.stream;
+    const int steps = P.steps;
+    struct Small {
+        unsigned long long n;
+        DevCtl ctl;
+    };
+    Small *hs = nullptr;
+    EGTB_CUDA(cudaHostAlloc((void **)&hs, sizeof(Small), cudaHostAllocDefault));
+    std::unique_ptr<Small, void (*)(Small *)> hs_guard(hs, [](Small *q) { cudaFreeHost(q); });
+    cudaEvent_t ev_buf[2];
+    for (auto &e : ev_buf) EGTB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    std::unique_ptr<cudaEvent_t, void (*)(cudaEvent_t *)> ev_guard(ev_buf, [](cudaEvent_t *e) {
+        cudaEventDestroy(e[0]);
+        cudaEventDestroy(e[1]);
+    });
+    for (;;) {
+        E.ensure_sort_bufs(E.cand_cap);
+        E.ensure_status();
+        stage_start(E, P, base, n_base, partial, n_partial);
+        unsigned char *pin = E.ensure_pinned(2 * E.cand_cap * sizeof(uint64_t));
+        std::future<void> writer[2];
+        std::string write_error;
+        std::mutex write_mu;
+        uint64_t *stage[3] = {E.cand[0], E.cand[1], E.tmp};
+        len.assign(steps + 1, 0);
+        unsigned long long sorted_keys = 0;
+        unsigned err = 0;
+        int pending = -1;
+        uint64_t *pending_buf = nullptr;
+        bool copied_any = false;
+        EGTB_CUDA(cudaEventRecord(E.ev[0], s));
+        // ship layer t: its length, then the copy into pinned buffer t % 2 and the file write
+        auto ship = [&](int t, uint64_t *sorted) {
+            EGTB_CUDA(cudaEventSynchronize(E.ev_sorted));
+            err |= hs->ctl.err;
+            if (err) return;
+            const unsigned long long n = hs->n;
+            len[t] = n;
+            sorted_keys += n;
+            const int b = t & 1;
+            if (writer[b].valid()) writer[b].get();
+            unsigned char *dst = pin + (size_t)b * E.cand_cap * sizeof(uint64_t);
+            EGTB_CUDA(cudaStreamWaitEvent(E.copy_stream, E.ev_sorted, 0));
+            if (n) EGTB_CUDA(cudaMemcpyAsync(dst, sorted, n * 8, cudaMemcpyDeviceToHost, E.copy_stream));
+            EGTB_CUDA(cudaEventRecord(ev_buf[b], E.copy_stream));
+            EGTB_CUDA(cudaEventRecord(E.ev_copied, E.copy_stream));
+            copied_any = true;
+            const std::string path = prefix + std::to_string(t);
+            cudaEvent_t done = ev_buf[b];
+            const int dev = E.device;
+            writer[b] = std::async(std::launch::async, [=, &write_error, &write_mu] {
+                try {
+                    EGTB_CUDA(cudaSetDevice(dev));
+                    EGTB_CUDA(cudaEventSynchronize(done));
+                    write_file(path, dst, n * 8);
+                } catch (const std::exception &e) {
+                    std::lock_guard<std::mutex> lk(write_mu);
+                    write_error = e.what();
+                }
+            });
+        };
+        for (int i = P.first_step; i < steps - 1 && !err; ++i) {
+            const int t = i - 1;
+            const int pe = E.prof_begin(K_EXPAND);
+            EGTB_LAUNCH(E, expand_dedup_kernel<<<E.sm_count, kExpandThreads, kRowSmemBytes, s>>>(
+                               stage[t % 3], stage[(t + 1) % 3], stage[(t + 2) % 3], t % 3, (t + 1) % 3, (t + 2) % 3,
+                               nullptr, E.layer_off, E.layer_len, 0, t, P.spec, i > P.docheck ? 1 : 0, E.tab,
+                               E.dset[(t + 1) % 3], E.dset[(t + 2) % 3], E.dset_cap - 1, E.cand_cap, E.filter,
+                               E.filter_bits, E.dset[t % 3], E.ctl, progress, (unsigned)i));
+            E.prof_end(pe);
+            if (pending >= 0) {  // ship the layer sorted last step while this step runs
+                ship(pending, pending_buf);
+                pending = -1;
+            }
+            if (t >= P.first_step && t <= steps - 3) {
+                if (copied_any) EGTB_CUDA(cudaStreamWaitEvent(s, E.ev_copied, 0));  // sort buffers are free again
+                pending_buf = enqueue_layer_sort(E, P.sort, stage[t % 3], E.layer_len + t);
+                EGTB_CUDA(cudaMemcpyAsync(&hs->n, E.layer_len + t, 8, cudaMemcpyDeviceToHost, s));
+                EGTB_CUDA(cudaMemcpyAsync(&hs->ctl, E.ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, s));
+                EGTB_CUDA(cudaEventRecord(E.ev_sorted, s));
+                pending = t;
+            }
+        }
+        if (pending >= 0 && !err) ship(pending, pending_buf);
+        for (auto &w : writer)
+            if (w.valid()) w.get();
+        if (!write_error.empty()) throw Error(EGTB_ERR_IO, write_error);
+        EGTB_CUDA(cudaStreamSynchronize(E.copy_stream));
+        DevCtl c = read_ctl(E);
+        err |= c.err;
+        if (err == 0) {
+            // the last two layers: sorted into the arena for the final books
+            off.assign(steps + 1, 0);
+            std::vector<unsigned long long> nl(2, 0);
+            for (int k = 0; k < 2; ++k) nl[k] = c.stage_count[(steps - 2 + k) % 3];
+            E.ensure_arena(align16(nl[0]) + nl[1] + 16);
+            unsigned long long at = 0;
+            for (int k = 0; k < 2; ++k) {
+                const int L = steps - 2 + k;
+                off[L] = at;
+                len[L] = nl[k];
+                if (nl[k]) {
+                    uint64_t *sorted = enqueue_layer_sort(E, P.sort, stage[L % 3], &E.ctl->stage_count[L % 3]);
+                    EGTB_CUDA(cudaMemcpyAsync(E.arena + at, sorted, nl[k] * 8, cudaMemcpyDeviceToDevice, s));
+                    sorted_keys += nl[k];
+                }
+                at += align16(nl[k]);
+            }
+            EGTB_CUDA(cudaMemcpyAsync(E.layer_off, off.data(), sizeof(unsigned long long) * (steps + 1),
+                                      cudaMemcpyHostToDevice, s));
+            EGTB_CUDA(cudaMemcpyAsync(E.layer_len, len.data(), sizeof(unsigned long long) * (steps + 1),
+                                      cudaMemcpyHostToDevice, s));
+            EGTB_CUDA(cudaEventRecord(E.ev[1], s));
+            DevCtl c2 = read_ctl(E);
+            E.prof_resolve();
+            if (c2.err & kErrTimeout) throw Error(EGTB_ERR_TIMEOUT, "a bounded device wait gave up in a layer sort");
+            E.candidates = c2.candidates - sorted_keys;  // the sorts' histogram pass counts its keys too
+            EGTB_CUDA(cudaEventElapsedTime(ms, E.ev[0], E.ev[1]));
+            return retries;
+        }
+        E.prof_resolve();
+        if (err & kErrTimeout) throw Error(EGTB_ERR_TIMEOUT, "a bounded device wait gave up in the forward pass");
+        ++retries;
+        if (retries > 24) throw Error(EGTB_ERR_CAPACITY, "forward pass did not fit after repeated regrowth");
+        if (err & kErrCandOverflow) E.ensure_cand(E.cand_cap * 4);
+        if (err & kErrDedupOverflow) E.ensure_dedup(E.dset_cap * 4);
     }
 }
 
@@ -996,7 +1218,7 @@ static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const 
 
 template <typename T>
 static void generate_files(Engine &E, const uint64_t *seeds, size_t n_seeds, const egtb_pattern_spec &spec,
-                           const egtb_run_options &o, int *started, egtb_build_stats *st) {
+                           const egtb_run_options &o, int *started, egtb_build_stats *st, bool force_stream = false) {
     const auto t_start = std::chrono::steady_clock::now();
     const int steps = o.steps;
     const size_t rec = 8 + sizeof(T);
@@ -1025,13 +1247,27 @@ static void generate_files(Engine &E, const uint64_t *seeds, size_t n_seeds, con
         ForwardPlan P = make_forward_plan(spec, o, i0);
         P.s0 = n_seeds ? layer0_tile_sum(seeds, n_seeds)
                        : (base.empty() ? 0 : seed_tile_sum(base[0]) - 2ll * (i0 - 1));
-        retries = run_forward(E, P, base.data(), base.size(), partial.data(), partial.size(), &fwd_ms);
-        off = d2h_u64(E, E.layer_off, steps + 1);
-        len = d2h_u64(E, E.layer_len, steps + 1);
-        // raw layers i0 .. steps-3
+        // the whole table in device memory when it fits, else layers streamed to their files
+        bool streamed = force_stream || stream_layers_forced();
+        if (!streamed) {
+            try {
+                retries = run_forward(E, P, base.data(), base.size(), partial.data(), partial.size(), &fwd_ms);
+            } catch (const Error &e) {
+                if (e.code != EGTB_ERR_CAPACITY) throw;
+                streamed = true;
+            }
+        }
+        if (streamed)
+            retries += run_forward_streamed(E, P, base.data(), base.size(), partial.data(), partial.size(), p,
+                                            &fwd_ms, off, len);
+        else {
+            off = d2h_u64(E, E.layer_off, steps + 1);
+            len = d2h_u64(E, E.layer_len, steps + 1);
+        }
+        // raw layers i0 .. steps-3 (written already when streamed)
         std::vector<std::string> paths;
         std::vector<unsigned long long> doff, bytes;
-        for (int t = i0; t <= steps - 3; ++t) {
+        for (int t = i0; t <= steps - 3 && !streamed; ++t) {
             paths.push_back(p + std::to_string(t));
             doff.push_back(off[t] * 8);
             bytes.push_back(len[t] * 8);
@@ -1460,13 +1696,25 @@ extern "C" int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_patt
                 generate_files<T>(E, seeds, n_seeds, *spec, *options, &st, stats);
                 return;
             }
-            if (!resume) {
-                fused_build<T>(E, seeds, n_seeds, *spec, *options, stats);
-            } else {
+            bool streamed = false;
+            if (!resume && !(options->write_files && stream_layers_forced())) {
+                try {
+                    fused_build<T>(E, seeds, n_seeds, *spec, *options, stats);
+                    return;
+                } catch (const Error &e) {
+                    // the table does not fit in device memory: with files, build it
+                    // as the reference does (generate, then solve) with streamed layers
+                    if (e.code != EGTB_ERR_CAPACITY || !options->write_files) throw;
+                    streamed = true;
+                }
+            } else if (!resume) {
+                streamed = true;
+            }
+            {
                 int st = 0;
                 egtb_build_stats g;
                 std::memset(&g, 0, sizeof g);
-                generate_files<T>(E, seeds, n_seeds, *spec, *options, &st, &g);
+                generate_files<T>(E, seeds, n_seeds, *spec, *options, &st, &g, streamed);
                 solve_files<T>(E, nullptr, 0, nullptr, 0, *spec, *options, stats);
                 if (stats) {
                     stats->forward_ms = g.forward_ms;

@@ -285,8 +285,13 @@ expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ sta
     // once this pass has overflowed a buffer it will be re-run: skip the work
     const unsigned long long n = (ctl->err & (kErrCandOverflow | kErrDedupOverflow)) ? 0 : ctl->stage_count[si_par];
     const unsigned long long off = layer_off[t];
-    const bool fits = !(ctl->err & kErrArenaOverflow) && off + n <= arena_cap;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    // arena == nullptr: layers stream out of the device (the host sorts and
+    // ships layer t after this step); only the layer's length is recorded
+    const bool fits = arena && !(ctl->err & kErrArenaOverflow) && off + n <= arena_cap;
+    if (!arena && blockIdx.x == 0 && threadIdx.x == 0) {
+        layer_len[t] = n;
+        layer_off[t + 1] = 0;
+    } else if (blockIdx.x == 0 && threadIdx.x == 0) {
         const unsigned long long next = (off + n + kSplitStride - 1) & ~(unsigned long long)(kSplitStride - 1);
         if (!fits || next > arena_cap) {
             atomicOr(&ctl->err, kErrArenaOverflow);

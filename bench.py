@@ -47,6 +47,11 @@ WORKLOADS = {
     "442-512": ("442", 9),
     "L3-256": ("L3", 8),
 }
+# the 13-cell diagonal table at 1024 (560 steps, ~1e11 boards in all): the
+# first STREAM_STEPS steps of its forward pass, layers streamed to raw files
+STREAM_WORKLOAD = "4432-1024-stream"
+STREAM_STEPS = 130
+STREAM_REF_STEPS = 60  # the reference's CPU generate on a shorter prefix (a few minutes of host work)
 
 
 def load_peaks() -> tuple[float, str]:
@@ -209,7 +214,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="442-512", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="442-512", choices=sorted(WORKLOADS) + [STREAM_WORKLOAD])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (default: --steps)")
     ap.add_argument("--profile-run", action="store_true",
@@ -223,6 +228,9 @@ def main():
                     help="one egtb_sort_unique_u64 of this many seeded random keys and nothing else (for ncu)")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
+    if args.workload == STREAM_WORKLOAD:
+        stream_workload(args, world, rank, local, pg)
+        return
     if args.impl == "reference":
         run_reference_arm(args, world, rank, pg)
         if pg is not None:
@@ -380,6 +388,69 @@ def main():
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def stream_workload(args, world, rank, local, pg):
+    """Streamed forward pass of the 13-cell diagonal table at target 1024 (the
+    first STREAM_STEPS steps; layers sorted on the device and streamed through
+    pinned host memory to raw layer files on /dev/shm). The whole table does
+    not fit this machine, so the measured unit is its forward prefix; the
+    reference arm builds the same prefix with the reference's generate."""
+    fc = importlib.import_module("2048endgametablebase_b200.native_core.formation_core")
+    pats = importlib.import_module("2048endgametablebase_b200.patterns")
+    meta = pats.pattern_catalog["4432"]
+    s0 = -int(meta["nums_adjust"])
+    _, docheck = pats.steps_and_docheck(s0, 10, int(meta["extra_steps"]))
+    base = "/dev/shm" if os.access("/dev/shm", os.W_OK) else tempfile.gettempdir()
+    seeds = np.asarray(meta["seed_boards"], dtype=np.uint64)
+
+    def one(impl: str):
+        steps = STREAM_REF_STEPS if impl == "reference" else STREAM_STEPS
+        d = tempfile.mkdtemp(prefix=f"egtb_stream_r{rank}_", dir=base) + "/"
+        try:
+            if impl == "reference":
+                sys.path.insert(0, os.path.join(ROOT, "oracle"))
+                import reference as R  # noqa: E402
+                spec, o = R.make_spec_options(meta["pattern_masks"], meta["success_shifts"], R.SYMM["diagonal"], 10,
+                                              steps, docheck, d + "x_", "float32", 0.1, os.cpu_count() or 1)
+                t0 = time.perf_counter()
+                R.run_generate(seeds, spec, o)
+            else:
+                spec, o = make_spec_options(fc, "4432", 10, meta, steps, docheck, d + "x_", local)
+                os.environ["EGTB_STREAM_LAYERS"] = "1"
+                t0 = time.perf_counter()
+                fc.run_pattern_generate(seeds, spec, o)
+            dt = time.perf_counter() - t0
+            boards = sum(os.path.getsize(d + f"x_{t}") // 8 for t in range(steps - 2))
+            return dt, boards
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+
+    impl = args.impl
+    if impl == "reference" and rank != 0:
+        return
+    for _ in range(max(1, args.warmup if impl != "reference" else 0)):
+        one(impl)
+    total, boards = 0.0, 0
+    k = max(1, args.steps if impl != "reference" else 1)
+    for _ in range(k):
+        dt, boards = one(impl)
+        total += dt
+    v = boards * k / total
+    if rank == 0:
+        line = {"metric": "table-build boards/s (forward prefix, streamed layers)", "value": v, "unit": "boards/s",
+                "n_gpus": world, "steps": k, "warmup": args.warmup, "ms_per_step": total / k * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "u64 keys", "data": "synthetic (seeded table build, no input data)",
+                "config": {"workload": f"4432-1024 forward, first {STREAM_STEPS} of 560 steps, raw layers streamed to {base}",
+                           "boards_per_step": boards, "raw_bytes_per_step": boards * 8},
+                "e2e": {"value": v, "unit": "boards/s", "h2d_bytes_per_step": int(seeds.nbytes),
+                        "d2h_bytes_per_step": boards * 8}}
+        if impl == "reference":
+            line["impl"] = "reference"
+            line["cpu_baseline"] = {"value": v, "unit": "boards/s", "cores": os.cpu_count() or 1, "kind": "reference",
+                                    "sample": f"reference generate of the first {STREAM_REF_STEPS} steps"}
+        print(json.dumps(line), flush=True)
 
 
 SERVE_TABLES = (("L3", 8), ("442", 9))

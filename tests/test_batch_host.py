@@ -28,7 +28,7 @@ def test_random_tables_shape_and_determinism():
     b = B.random_tables(64)
     assert [t.name for t in a] == [t.name for t in b]
     assert all(np.array_equal(x.seeds, y.seeds) for x, y in zip(a, b))
-    pats = H.pkg().patterns
+    pats = __import__("importlib").import_module("2048endgametablebase_b200.patterns")
     sizes, targets = set(), set()
     for t in a:
         k = len(t.cells)
