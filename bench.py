@@ -161,6 +161,9 @@ def reference_build_seconds(pattern, target, meta, steps, docheck, threads) -> t
 
 
 def dist_setup():
+    """One process per GPU under torchrun: (world, rank, local rank, the
+    torch.distributed module or None). Backend NCCL, or EGTB_DIST_BACKEND
+    (gloo for CPU runs); a short timeout ends ranks that wait for one another."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -170,9 +173,26 @@ def dist_setup():
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = os.environ.get("EGTB_DIST_BACKEND", "nccl")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
         pg = dist
     return world, rank, local, pg
+
+
+def max_over_ranks(pg, value: float, device: str) -> float:
+    """The largest value over all ranks (the job's time is its slowest rank's)."""
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_rank: float, world: int, seconds_max: float) -> float:
+    """Whole-job throughput of N replicas: every rank's units over the slowest rank's time."""
+    return units_per_rank * world / seconds_max
 
 
 def run_reference_arm(args, world, rank, pg):
@@ -306,10 +326,7 @@ def main():
     prof = N.profile_read(local)
     N.profile(local, False)
     clocks = clk.summary()
-    if pg is not None:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(pg, ms, f"cuda:{local}")
     launches = int(sum(s.kernel_launches for s in stats))
 
     # ---- e2e: the drop-in API from host seeds to .book files
@@ -332,15 +349,12 @@ def main():
         wall += time.perf_counter() - t0
         book_bytes = sum(os.path.getsize(os.path.join(dirs[i], f)) for f in os.listdir(dirs[i]) if f.endswith(".book"))
         shutil.rmtree(dirs[i], ignore_errors=True)
-    if pg is not None:
-        t = torch.tensor([wall], device=f"cuda:{local}", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        wall = float(t.item())
+    wall = max_over_ranks(pg, wall, f"cuda:{local}")
 
     if rank == 0:
         layer_boards = int(stats[-1].raw_boards)
-        value = layer_boards * args.steps * world / (ms / 1e3)
-        e2e = layer_boards * e2e_steps * world / wall
+        value = replica_value(layer_boards * args.steps, world, ms / 1e3)
+        e2e = replica_value(layer_boards * e2e_steps, world, wall)
         peak, peak_kind = load_peaks()
         roof = roofline(prof, stats[-1], args.steps, layer_boards, peak, peak_kind, pattern)
         line = {
@@ -433,10 +447,14 @@ def stream_workload(args, world, rank, local, pg):
         one(impl)
     total, boards = 0.0, 0
     k = max(1, args.steps if impl != "reference" else 1)
+    if pg is not None and impl != "reference":
+        pg.barrier()
     for _ in range(k):
         dt, boards = one(impl)
         total += dt
-    v = boards * k / total
+    if impl != "reference":
+        total = max_over_ranks(pg, total, "cpu" if os.environ.get("EGTB_DIST_BACKEND") == "gloo" else f"cuda:{local}")
+    v = replica_value(boards * k, world if impl != "reference" else 1, total)
     if rank == 0:
         line = {"metric": "table-build boards/s (forward prefix, streamed layers)", "value": v, "unit": "boards/s",
                 "n_gpus": world, "steps": k, "warmup": args.warmup, "ms_per_step": total / k * 1e3,
