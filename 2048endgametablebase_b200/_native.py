@@ -174,6 +174,8 @@ _SIGS = {
     "egtb_serve_submit": (ctypes.c_int, [_P, ctypes.c_int32, _P, ctypes.c_uint64, _P, _P,
                                          ctypes.POINTER(ctypes.c_uint64)]),
     "egtb_serve_wait": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
+    "egtb_serve_register": (ctypes.c_int, [_P, _P, ctypes.c_uint64]),
+    "egtb_serve_unregister": (ctypes.c_int, [_P, _P]),
     "egtb_serve_stats": (ctypes.c_int, [_P] + [ctypes.POINTER(ctypes.c_uint64)] * 4),
     "egtb_serve_replay": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, ctypes.c_uint64, _P, _P, _P,
                                          ctypes.POINTER(ctypes.c_double)]),

@@ -220,62 +220,107 @@ __device__ __forceinline__ int adjusted_slot(int op, int m) {
     return (idx + (op & 3)) & 3;
 }
 
+// move_on_dic of one position (evaluate_classic_result_candidates,
+// native_core/src/ReaderRuntime.cpp:739-840): four values in direction order
+// up, right, down, left, the mask of directions with a value, and the op used.
+template <typename T, typename OutT>
+__device__ __forceinline__ void lookup_position(const LayerDesc *__restrict__ desc, int n_desc, uint64_t board,
+                                                long long nums_adjust, const DevSpec &spec,
+                                                const uint32_t *__restrict__ tab, int op_mode, double scale,
+                                                int round9, T zero, OutT out[4], uint8_t &mask, int &used) {
+#pragma unroll
+    for (int d = 0; d < 4; ++d) out[d] = 0;
+    mask = 0;
+    used = -1;
+    const long long nums = (tile_sum(board) + nums_adjust) / 2;  // C division, ReaderRuntime.cpp:749
+    if (nums < 0) {
+        used = -2;
+        return;
+    }
+    if (nums >= n_desc || !desc[nums].exists) {
+        used = -3;
+        return;
+    }
+    const LayerDesc L = desc[nums];
+    const T *rates = (const T *)L.rates;
+    // [last_op, 0..7] (operation_sequence, ReaderRuntime.cpp:171-182), or one op
+    const int single = op_mode >= 8 ? op_mode - 8 : -1;
+    const int count = single >= 0 ? 1 : 9;
+    for (int j = 0; j < count && used < 0; ++j) {
+        const int op = single >= 0 ? single : (j == 0 ? op_mode : j - 1);
+        const uint64_t tb = apply_sym(board, kOpSym[op]);
+        if (!is_pattern(tb, spec)) continue;
+        uint64_t mv[4];
+        move_all_dir(tab, tb, mv);
+        uint8_t m = 0;
+        OutT vals[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            if (mv[d] == tb || !is_pattern(mv[d], spec)) continue;
+            const uint64_t key = canonical(mv[d], spec.symm);
+            T r = zero;
+            if (L.sorted) {
+                r = layer_lookup<T>(L.keys, rates, L.n, L.split, key, zero);
+            } else {
+                T got;
+                if (probe_unsorted<T>(L.keys, rates, L.n, key, got)) r = got;
+            }
+            const int slot = adjusted_slot(op, d);
+            vals[slot] = (OutT)present<T>(r, scale, round9);
+            m |= (uint8_t)(1u << slot);
+        }
+        if (m) {
+            used = op;
+            mask = m;
+#pragma unroll
+            for (int d = 0; d < 4; ++d) out[d] = vals[d];
+        }
+    }
+}
+
 template <typename T, typename OutT>
 __global__ void __launch_bounds__(256)
 lookup_kernel(const LayerDesc *__restrict__ desc, int n_desc, const uint64_t *__restrict__ pos, size_t n,
               long long nums_adjust, DevSpec spec, const uint32_t *__restrict__ tab, int op_mode, double scale,
               int round9, T zero, OutT *__restrict__ values4, uint8_t *__restrict__ valid, int8_t *__restrict__ op_used) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const uint64_t board = pos[i];
-        OutT out[4] = {0, 0, 0, 0};
-        uint8_t mask = 0;
-        int used = -1;
-        const long long nums = (tile_sum(board) + nums_adjust) / 2;  // C division, ReaderRuntime.cpp:749
-        if (nums < 0) {
-            used = -2;
-        } else if (nums >= n_desc || !desc[nums].exists) {
-            used = -3;
-        } else {
-            const LayerDesc L = desc[nums];
-            const T *rates = (const T *)L.rates;
-            // [last_op, 0..7] (operation_sequence, ReaderRuntime.cpp:171-182), or one op
-            const int single = op_mode >= 8 ? op_mode - 8 : -1;
-            const int count = single >= 0 ? 1 : 9;
-            for (int j = 0; j < count && used < 0; ++j) {
-                const int op = single >= 0 ? single : (j == 0 ? op_mode : j - 1);
-                const uint64_t tb = apply_sym(board, kOpSym[op]);
-                if (!is_pattern(tb, spec)) continue;
-                uint64_t mv[4];
-                move_all_dir(tab, tb, mv);
-                uint8_t m = 0;
-                OutT vals[4] = {0, 0, 0, 0};
-#pragma unroll
-                for (int d = 0; d < 4; ++d) {
-                    if (mv[d] == tb || !is_pattern(mv[d], spec)) continue;
-                    const uint64_t key = canonical(mv[d], spec.symm);
-                    T r = zero;
-                    if (L.sorted) {
-                        r = layer_lookup<T>(L.keys, rates, L.n, L.split, key, zero);
-                    } else {
-                        T got;
-                        if (probe_unsorted<T>(L.keys, rates, L.n, key, got)) r = got;
-                    }
-                    const int slot = adjusted_slot(op, d);
-                    vals[slot] = (OutT)present<T>(r, scale, round9);
-                    m |= (uint8_t)(1u << slot);
-                }
-                if (m) {
-                    used = op;
-                    mask = m;
-#pragma unroll
-                    for (int d = 0; d < 4; ++d) out[d] = vals[d];
-                }
-            }
-        }
+        OutT out[4];
+        uint8_t mask;
+        int used;
+        lookup_position<T, OutT>(desc, n_desc, pos[i], nums_adjust, spec, tab, op_mode, scale, round9, zero, out,
+                                 mask, used);
 #pragma unroll
         for (int d = 0; d < 4; ++d) values4[4 * i + d] = out[d];
         valid[i] = mask;
         if (op_used) op_used[i] = (int8_t)used;
+    }
+}
+
+// The same over a list of requests whose positions and answers live in
+// caller memory the device can address (registered host memory): request r
+// covers work items prefix[r] .. prefix[r+1]-1.
+template <typename T>
+__global__ void __launch_bounds__(256)
+lookup_requests_kernel(const LayerDesc *__restrict__ desc, int n_desc, const ServeReq *__restrict__ reqs, int n_req,
+                       long long nums_adjust, DevSpec spec, const uint32_t *__restrict__ tab, int op_mode,
+                       double scale, int round9, T zero) {
+    const unsigned long long total = reqs[n_req].at;
+    for (unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+         g += (unsigned long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = n_req;  // largest r with reqs[r].at <= g
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (reqs[mid].at <= g) lo = mid; else hi = mid;
+        }
+        const ServeReq q = reqs[lo];
+        const unsigned long long i = g - q.at;
+        float out[4];
+        uint8_t mask;
+        int used;
+        lookup_position<T, float>(desc, n_desc, q.pos[i], nums_adjust, spec, tab, op_mode, scale, round9, zero, out,
+                                  mask, used);
+        reinterpret_cast<float4 *>(q.out)[i] = make_float4(out[0], out[1], out[2], out[3]);
+        if (q.valid) q.valid[i] = mask;
     }
 }
 
@@ -498,6 +543,42 @@ extern "C" int egtb_book_lookup_device(egtb_book *b, const uint64_t *d_positions
 
 namespace egtb {
 int book_device(const egtb_book *b) { return b->device; }
+
+// Enqueue move_on_dic (last_op 0) for n_req requests of this book listed at
+// d_reqs (n_req + 1 entries) covering `total` positions.
+void book_lookup_requests(egtb_book *b, const ServeReq *d_reqs, int n_req, unsigned long long total,
+                          cudaStream_t s) {
+    if (b->desc_dirty) {
+        std::lock_guard<std::mutex> lk(b->mu);
+        upload_desc(*b);
+    }
+    if (!b->d_desc) throw Error(EGTB_ERR_ARG, "no layers loaded (egtb_book_load_all)");
+    if (total == 0) return;
+    const uint32_t *tab = device_row_table();
+    const int grid = (int)std::min<unsigned long long>((total + 255) / 256, 148 * 8);
+    const double scale = scale_for(b->dtype);
+    const int r9 = round9_for(b->dtype) ? 1 : 0;
+    const int nd = (int)b->layers.size();
+    switch (b->dtype) {
+        case EGTB_DTYPE_UINT32:
+            lookup_requests_kernel<uint32_t><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
+                                                                 tab, 0, scale, r9, 0u);
+            break;
+        case EGTB_DTYPE_UINT64:
+            lookup_requests_kernel<uint64_t><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
+                                                                 tab, 0, scale, r9, 0ull);
+            break;
+        case EGTB_DTYPE_FLOAT32: case EGTB_DTYPE_1_FLOAT32:
+            lookup_requests_kernel<float><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
+                                                              tab, 0, scale, r9, (float)dtype_zero(b->dtype));
+            break;
+        default:
+            lookup_requests_kernel<double><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
+                                                               tab, 0, scale, r9, dtype_zero(b->dtype));
+            break;
+    }
+    EGTB_CUDA(cudaGetLastError());
+}
 }  // namespace egtb
 
 extern "C" int egtb_find_classic_value(const char *pathname, const char *filename, uint64_t key, int32_t dtype,

@@ -106,6 +106,16 @@ void write_stats_file(const egtb_run_options &o, int dtype, const std::vector<in
                       const std::vector<unsigned long long> &raw_len, const std::vector<unsigned long long> &book_len,
                       const std::vector<unsigned long long> &maxbits, double seconds_per_layer);
 
+// One request of the serving loop for the request-list lookup kernel: device
+// addresses of its positions and answers (registered caller memory) and its
+// first work item; one extra entry closes a list.
+struct ServeReq {
+    const uint64_t *pos;
+    float *out;
+    uint8_t *valid;
+    unsigned long long at;
+};
+
 // Simple fixed-size thread pool for file writes.
 class WriterPool {
 public:

@@ -9,7 +9,9 @@
 // position capacity (memory-based admission). Requests that arrive while
 // slots are on the GPU wait in the queue and join the next free slot, so up
 // to `slots` batches overlap on the device (copies and kernels of different
-// slots run concurrently).
+// slots run concurrently). Requests whose buffers lie in memory registered
+// with the server skip the staging copies: the slot passes the kernel a list
+// of {positions, answers} device addresses and the kernel works in place.
 //
 // The reference answers one position per call from files
 // (ClassicBookReader.move_on_dic, native_core/src/ReaderRuntime.cpp:1050-1067);
@@ -33,6 +35,7 @@
 // from egtb_book.cu
 namespace egtb {
 int book_device(const egtb_book *b);
+void book_lookup_requests(egtb_book *b, const ServeReq *d_reqs, int n_req, unsigned long long total, cudaStream_t s);
 }  // namespace egtb
 
 namespace egtb {
@@ -46,9 +49,21 @@ struct ServeRequest {
     size_t n = 0;
     float *out = nullptr;
     uint8_t *valid = nullptr;
+    // direct: every buffer lies in registered memory; the kernel reads and
+    // writes it through these device addresses (no staging copies)
+    bool direct = false;
+    const uint64_t *d_pos = nullptr;
+    float *d_out = nullptr;
+    uint8_t *d_valid = nullptr;
     Clock::time_point t_submit;
     double latency_us = 0.0;
     bool done = false;
+};
+
+// Caller memory registered with the server (page-locked and mapped).
+struct Registered {
+    uintptr_t begin, end;
+    uintptr_t dev;
 };
 
 struct Slot {
@@ -58,9 +73,11 @@ struct Slot {
     float *h_out = nullptr, *d_out = nullptr;
     uint8_t *h_valid = nullptr, *d_valid = nullptr;
     size_t cap = 0;
+    ServeReq *h_reqs = nullptr, *d_reqs = nullptr;  // request lists of the direct requests
+    size_t req_cap = 0;
     bool busy = false;
     std::vector<ServeRequest *> reqs;
-    std::vector<size_t> at;  // position offset of each request in the slot
+    std::vector<size_t> at;  // position offset of each staged request in the slot
 };
 
 }  // namespace egtb
@@ -74,6 +91,7 @@ struct egtb_server {
     std::condition_variable cv_done;
     std::deque<egtb::ServeRequest *> queue;
     std::unordered_map<uint64_t, std::unique_ptr<egtb::ServeRequest>> live;
+    std::vector<egtb::Registered> registered;
     uint64_t next_ticket = 1;
     std::atomic<bool> stop{false};
     std::thread worker;
@@ -99,8 +117,10 @@ static void serve_loop(egtb_server *S) {
                 const auto now = Clock::now();
                 for (size_t r = 0; r < sl.reqs.size(); ++r) {
                     ServeRequest *rq = sl.reqs[r];
-                    std::memcpy(rq->out, sl.h_out + 4 * sl.at[r], rq->n * 4 * sizeof(float));
-                    if (rq->valid) std::memcpy(rq->valid, sl.h_valid + sl.at[r], rq->n);
+                    if (!rq->direct) {
+                        std::memcpy(rq->out, sl.h_out + 4 * sl.at[r], rq->n * 4 * sizeof(float));
+                        if (rq->valid) std::memcpy(rq->valid, sl.h_valid + sl.at[r], rq->n);
+                    }
                     rq->latency_us = std::chrono::duration<double, std::micro>(now - rq->t_submit).count();
                     finished.push_back(rq);
                 }
@@ -124,43 +144,81 @@ static void serve_loop(egtb_server *S) {
                 {
                     std::lock_guard<std::mutex> lk(S->mu);
                     size_t used = 0;
+                    size_t n_direct = 0;
                     while (!S->queue.empty()) {
                         ServeRequest *rq = S->queue.front();
                         if (used + rq->n > sl.cap) break;  // does not fit: it opens the next slot
                         if (S->max_per_batch && take.size() >= S->max_per_batch) break;
+                        if (rq->direct && n_direct + S->books.size() + 1 > sl.req_cap) break;
                         take.push_back(rq);
                         used += rq->n;
+                        n_direct += rq->direct;
                         S->queue.pop_front();
                     }
                 }
                 if (take.empty()) break;
-                // group by book so every book gets one contiguous launch
-                std::stable_sort(take.begin(), take.end(),
-                                 [](const ServeRequest *a, const ServeRequest *b) { return a->book < b->book; });
-                size_t used = 0;
-                for (auto *rq : take) {
-                    sl.reqs.push_back(rq);
-                    sl.at.push_back(used);
-                    std::memcpy(sl.h_pos + used, rq->pos, rq->n * sizeof(uint64_t));
-                    used += rq->n;
-                }
-                EGTB_CUDA(cudaMemcpyAsync(sl.d_pos, sl.h_pos, used * sizeof(uint64_t), cudaMemcpyHostToDevice,
-                                          sl.stream));
-                size_t i = 0;
-                while (i < take.size()) {
+                // group by book so every book gets one contiguous launch per kind
+                std::stable_sort(take.begin(), take.end(), [](const ServeRequest *a, const ServeRequest *b) {
+                    return a->book != b->book ? a->book < b->book : a->direct < b->direct;
+                });
+                size_t used = 0, nd = 0;
+                std::vector<std::pair<size_t, size_t>> groups;  // staged: [first, last) of take per book
+                std::vector<std::pair<int, std::pair<size_t, size_t>>> dgroups;  // direct: book, entries
+                for (size_t i = 0; i < take.size();) {
                     size_t j = i;
-                    size_t cnt = 0;
-                    while (j < take.size() && take[j]->book == take[i]->book) cnt += take[j++]->n;
-                    const size_t a = sl.at[i];
-                    if (egtb_book_lookup_device(S->books[take[i]->book], sl.d_pos + a, cnt, 0, sl.d_out + 4 * a,
-                                                sl.d_valid + a, sl.stream) != EGTB_OK)
-                        throw Error(EGTB_ERR_CUDA, "book lookup launch failed");
-                    ++S->n_launches;
+                    const int book = take[i]->book;
+                    const bool direct = take[i]->direct;
+                    while (j < take.size() && take[j]->book == book && take[j]->direct == direct) ++j;
+                    if (!direct) {
+                        groups.push_back({i, j});
+                        for (size_t k = i; k < j; ++k) {
+                            ServeRequest *rq = take[k];
+                            sl.reqs.push_back(rq);
+                            sl.at.push_back(used);
+                            std::memcpy(sl.h_pos + used, rq->pos, rq->n * sizeof(uint64_t));
+                            used += rq->n;
+                        }
+                    } else {
+                        const size_t first = nd;
+                        unsigned long long at = 0;
+                        for (size_t k = i; k < j; ++k) {
+                            ServeRequest *rq = take[k];
+                            sl.reqs.push_back(rq);
+                            sl.at.push_back(0);
+                            sl.h_reqs[nd++] = ServeReq{rq->d_pos, rq->d_out, rq->d_valid, at};
+                            at += rq->n;
+                        }
+                        sl.h_reqs[nd++] = ServeReq{nullptr, nullptr, nullptr, at};  // closes the list
+                        dgroups.push_back({book, {first, j - i}});
+                        S->n_positions += at;
+                    }
                     i = j;
                 }
-                EGTB_CUDA(cudaMemcpyAsync(sl.h_out, sl.d_out, used * 4 * sizeof(float), cudaMemcpyDeviceToHost,
-                                          sl.stream));
-                EGTB_CUDA(cudaMemcpyAsync(sl.h_valid, sl.d_valid, used, cudaMemcpyDeviceToHost, sl.stream));
+                if (nd)
+                    EGTB_CUDA(cudaMemcpyAsync(sl.d_reqs, sl.h_reqs, nd * sizeof(ServeReq), cudaMemcpyHostToDevice,
+                                              sl.stream));
+                for (const auto &g : dgroups) {
+                    book_lookup_requests(S->books[g.first], sl.d_reqs + g.second.first, (int)g.second.second,
+                                         sl.h_reqs[g.second.first + g.second.second].at, sl.stream);
+                    ++S->n_launches;
+                }
+                if (used) {
+                    EGTB_CUDA(cudaMemcpyAsync(sl.d_pos, sl.h_pos, used * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                                              sl.stream));
+                    size_t a = 0;
+                    for (const auto &g : groups) {
+                        size_t cnt = 0;
+                        for (size_t k = g.first; k < g.second; ++k) cnt += take[k]->n;
+                        if (egtb_book_lookup_device(S->books[take[g.first]->book], sl.d_pos + a, cnt, 0,
+                                                    sl.d_out + 4 * a, sl.d_valid + a, sl.stream) != EGTB_OK)
+                            throw Error(EGTB_ERR_CUDA, "book lookup launch failed");
+                        ++S->n_launches;
+                        a += cnt;
+                    }
+                    EGTB_CUDA(cudaMemcpyAsync(sl.h_out, sl.d_out, used * 4 * sizeof(float), cudaMemcpyDeviceToHost,
+                                              sl.stream));
+                    EGTB_CUDA(cudaMemcpyAsync(sl.h_valid, sl.d_valid, used, cudaMemcpyDeviceToHost, sl.stream));
+                }
                 EGTB_CUDA(cudaEventRecord(sl.event, sl.stream));
                 sl.busy = true;
                 ++S->n_batches;
@@ -209,6 +267,9 @@ extern "C" int egtb_serve_start(egtb_book *const *books, int32_t n_books, int32_
             EGTB_CUDA(cudaMalloc(&sl.d_pos, slot_positions * 8));
             EGTB_CUDA(cudaMalloc(&sl.d_out, slot_positions * 16));
             EGTB_CUDA(cudaMalloc(&sl.d_valid, slot_positions));
+            sl.req_cap = std::min<size_t>(slot_positions, 65536) + 2 * S->books.size() + 2;
+            EGTB_CUDA(cudaHostAlloc((void **)&sl.h_reqs, sl.req_cap * sizeof(ServeReq), cudaHostAllocDefault));
+            EGTB_CUDA(cudaMalloc(&sl.d_reqs, sl.req_cap * sizeof(ServeReq)));
         }
         egtb_server *raw = S.release();
         raw->worker = std::thread(serve_loop, raw);
@@ -229,13 +290,63 @@ extern "C" int egtb_serve_submit(egtb_server *S, int32_t book, const uint64_t *p
         rq->n = n;
         rq->out = values4;
         rq->valid = valid_mask;
-        rq->t_submit = Clock::now();
         std::lock_guard<std::mutex> lk(S->mu);
         if (!S->error.empty()) throw Error(EGTB_ERR_CUDA, "server stopped: " + S->error);
+        // device address of [p, p + bytes) when it lies in registered memory
+        auto mapped = [&](const void *p, size_t bytes) -> uintptr_t {
+            const uintptr_t a = (uintptr_t)p;
+            for (const auto &r : S->registered)
+                if (a >= r.begin && a + bytes <= r.end) return r.dev + (a - r.begin);
+            return 0;
+        };
+        const uintptr_t dp = mapped(positions, n * 8), dout = mapped(values4, n * 16);
+        const uintptr_t dv = valid_mask ? mapped(valid_mask, n) : 0;
+        if (dp && dout && (dv || !valid_mask)) {
+            rq->direct = true;
+            rq->d_pos = (const uint64_t *)dp;
+            rq->d_out = (float *)dout;
+            rq->d_valid = (uint8_t *)dv;
+        }
+        rq->t_submit = Clock::now();
         rq->ticket = S->next_ticket++;
         *ticket = rq->ticket;
         S->queue.push_back(rq.get());
         S->live.emplace(rq->ticket, std::move(rq));
+    });
+}
+
+extern "C" int egtb_serve_register(egtb_server *S, void *ptr, uint64_t bytes) {
+    return guarded([&] {
+        if (!S || !ptr || !bytes) throw Error(EGTB_ERR_ARG, "NULL or empty range");
+        EGTB_CUDA(cudaSetDevice(S->device));
+        EGTB_CUDA(cudaHostRegister(ptr, bytes, cudaHostRegisterMapped | cudaHostRegisterPortable));
+        void *dev = nullptr;
+        const cudaError_t e = cudaHostGetDevicePointer(&dev, ptr, 0);
+        if (e != cudaSuccess) {
+            cudaHostUnregister(ptr);
+            EGTB_CUDA(e);
+        }
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->registered.push_back(Registered{(uintptr_t)ptr, (uintptr_t)ptr + bytes, (uintptr_t)dev});
+    });
+}
+
+extern "C" int egtb_serve_unregister(egtb_server *S, void *ptr) {
+    return guarded([&] {
+        if (!S || !ptr) throw Error(EGTB_ERR_ARG, "NULL argument");
+        std::lock_guard<std::mutex> lk(S->mu);
+        for (const auto &q : S->live)
+            if (q.second->direct && !q.second->done)
+                for (const auto &r : S->registered)
+                    if (r.begin == (uintptr_t)ptr && (uintptr_t)q.second->pos >= r.begin && (uintptr_t)q.second->pos < r.end)
+                        throw Error(EGTB_ERR_ARG, "a request in flight uses this range");
+        for (size_t i = 0; i < S->registered.size(); ++i)
+            if (S->registered[i].begin == (uintptr_t)ptr) {
+                EGTB_CUDA(cudaHostUnregister(ptr));
+                S->registered.erase(S->registered.begin() + (long)i);
+                return;
+            }
+        throw Error(EGTB_ERR_ARG, "range not registered");
     });
 }
 
@@ -274,6 +385,26 @@ extern "C" int egtb_serve_replay(egtb_server *S, const uint64_t *pool, const dou
         if (!S || !pool || !arrival_us || !sizes || !offsets || !books || !values4 || !latency_us)
             throw Error(EGTB_ERR_ARG, "NULL argument");
         std::vector<uint64_t> tickets(n_req, 0);
+        // the recorded stream's buffers are registered for the run: the kernel
+        // reads positions and writes answers in place
+        unsigned long long total = 0;
+        for (uint64_t i = 0; i < n_req; ++i) total = std::max<unsigned long long>(total, offsets[i] + sizes[i]);
+        std::vector<void *> reg;
+        auto reg_range = [&](void *p, uint64_t bytes) {
+            if (!p || !bytes) return;
+            if (egtb_serve_register(S, p, bytes) != EGTB_OK) throw Error(EGTB_ERR_CUDA, "replay: register failed");
+            reg.push_back(p);
+        };
+        struct Unreg {
+            egtb_server *S;
+            std::vector<void *> &v;
+            ~Unreg() {
+                for (void *p : v) egtb_serve_unregister(S, p);
+            }
+        } unreg{S, reg};
+        reg_range((void *)pool, total * 8);
+        reg_range(values4, total * 16);
+        reg_range(valid, total);
         const auto t0 = Clock::now();
         std::atomic<uint64_t> submitted{0};
         std::atomic<bool> failed{false};
@@ -325,9 +456,12 @@ extern "C" int egtb_serve_stop(egtb_server *S) {
             cudaFree(sl.d_pos);
             cudaFree(sl.d_out);
             cudaFree(sl.d_valid);
+            cudaFreeHost(sl.h_reqs);
+            cudaFree(sl.d_reqs);
             if (sl.event) cudaEventDestroy(sl.event);
             if (sl.stream) cudaStreamDestroy(sl.stream);
         }
+        for (auto &r : S->registered) cudaHostUnregister((void *)r.begin);
         delete S;
     });
 }

@@ -267,6 +267,7 @@ class BookServer:
                                          int(max_requests_per_batch), ctypes.byref(ptr)))
         self._h = ptr
         self._pending: dict[int, tuple] = {}
+        self._registered: dict[int, np.ndarray] = {}
 
     def __enter__(self):
         return self
@@ -279,10 +280,31 @@ class BookServer:
             N.check(N.lib().egtb_serve_stop(self._h))
             self._h = ctypes.c_void_p()
 
-    def submit(self, book: int, positions: np.ndarray) -> int:
+    def register(self, array: np.ndarray) -> None:
+        """Page-lock and map a C-contiguous array for the server: requests whose
+        positions and answer arrays all lie in registered arrays are answered
+        in place (no staging copies)."""
+        if not array.flags.c_contiguous:
+            raise ValueError("register needs a C-contiguous array")
+        N.check(N.lib().egtb_serve_register(self._h, array.ctypes.data, array.nbytes))
+        self._registered[array.ctypes.data] = array
+
+    def unregister(self, array: np.ndarray) -> None:
+        N.check(N.lib().egtb_serve_unregister(self._h, array.ctypes.data))
+        self._registered.pop(array.ctypes.data, None)
+
+    def submit(self, book: int, positions: np.ndarray, values: np.ndarray | None = None,
+               valid: np.ndarray | None = None) -> int:
+        """Queue one request; answers go to `values` ([n, 4] float32) and
+        `valid` ([n] uint8) when given (e.g. registered arrays), else to new
+        arrays that wait() returns."""
         pos = np.ascontiguousarray(positions, dtype=np.uint64)
-        vals = np.zeros((len(pos), 4), dtype=np.float32)
-        valid = np.zeros(len(pos), dtype=np.uint8)
+        vals = values if values is not None else np.zeros((len(pos), 4), dtype=np.float32)
+        valid = valid if valid is not None else np.zeros(len(pos), dtype=np.uint8)
+        if vals.shape != (len(pos), 4) or vals.dtype != np.float32 or not vals.flags.c_contiguous:
+            raise ValueError("values must be a C-contiguous float32 array of shape (n, 4)")
+        if valid.shape != (len(pos),) or valid.dtype != np.uint8:
+            raise ValueError("valid must be a uint8 array of shape (n,)")
         t = ctypes.c_uint64(0)
         N.check(N.lib().egtb_serve_submit(self._h, int(book), pos.ctypes.data, len(pos), vals.ctypes.data,
                                           valid.ctypes.data, ctypes.byref(t)))

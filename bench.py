@@ -243,7 +243,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-build leg")
     ap.add_argument("--batch-only", action="store_true", help="run the batched-build leg alone and print its JSON")
     ap.add_argument("--serve-only", action="store_true", help="run the serving leg alone and print its JSON")
-    ap.add_argument("--serve-offered", type=float, default=1e8, help="offered lookups/s of the serving leg")
+    ap.add_argument("--serve-offered", type=float, default=3e8, help="offered lookups/s of the serving leg")
     ap.add_argument("--profile-sort", type=int, default=0,
                     help="one egtb_sort_unique_u64 of this many seeded random keys and nothing else (for ncu)")
     args = ap.parse_args()
@@ -586,7 +586,7 @@ def batch_leg(local: int, steps: int = 3, cpu_reference: bool = True) -> dict:
     return out
 
 
-def serving_leg(local: int, base: str | None, seconds: float = 0.5, offered: float = 1e8,
+def serving_leg(local: int, base: str | None, seconds: float = 0.5, offered: float = 3e8,
                 cpu_reference: bool = True) -> dict:
     """Serving: the L3-256 and 442-512 books resident in HBM, a Poisson stream
     of requests of log-uniform 1..4096 positions (a book record plus one

@@ -348,6 +348,15 @@ EGTB_API int egtb_serve_start(egtb_book *const *books, int32_t n_books, int32_t 
 EGTB_API int egtb_serve_submit(egtb_server *server, int32_t book, const uint64_t *positions, uint64_t n,
                                float *values4, uint8_t *valid_mask, uint64_t *ticket);
 
+/* Register caller memory with the server (page-locked and mapped into the
+ * device's address space until egtb_serve_unregister or egtb_serve_stop). A
+ * request whose positions, values4 and valid_mask all lie in registered
+ * memory is answered in place: the lookup kernel reads its positions and
+ * writes its answers there, with no staging copy on the host.
+ * egtb_serve_replay registers its own buffers. */
+EGTB_API int egtb_serve_register(egtb_server *server, void *ptr, uint64_t bytes);
+EGTB_API int egtb_serve_unregister(egtb_server *server, void *ptr);
+
 /* Wait for a ticket (timeout_ms < 0: one hour); *latency_us = submit to
  * answer. Every ticket must be waited for once. */
 EGTB_API int egtb_serve_wait(egtb_server *server, uint64_t ticket, int32_t timeout_ms, double *latency_us);

@@ -101,3 +101,29 @@ def test_serve_rejects_bad_requests(books):
             srv.submit(0, np.zeros(0, dtype=np.uint64))
         v, m, _ = srv.wait(srv.submit(1, np.zeros(3, dtype=np.uint64)))
         assert v.shape == (3, 4)
+
+
+def test_registered_buffers_are_answered_in_place(books):
+    """Requests whose positions and answer arrays lie in registered memory are
+    answered by the kernel in place; the answers equal the staged path's."""
+    S = H.serving()
+    rs = S.request_stream(books, n_requests=80, rate_per_s=0, seed=9)
+    want_v, want_m = _reference_answers(books, rs)
+    pool = np.ascontiguousarray(rs.pool)
+    vals = np.zeros((len(pool), 4), dtype=np.float32)
+    valid = np.zeros(len(pool), dtype=np.uint8)
+    with S.BookServer(books, slots=2, slot_positions=1 << 16) as srv:
+        for a in (pool, vals, valid):
+            srv.register(a)
+        tickets = []
+        for i in range(len(rs.sizes)):
+            a, n = int(rs.offsets[i]), int(rs.sizes[i])
+            tickets.append(srv.submit(int(rs.book_of[i]), pool[a:a + n], vals[a:a + n], valid[a:a + n]))
+        for t in tickets:
+            srv.wait(t)
+        N = H.pkg()._native
+        with pytest.raises(N.NativeError):
+            srv.unregister(np.zeros(4))
+        for a in (pool, vals, valid):
+            srv.unregister(a)
+    assert np.array_equal(valid, want_m) and np.array_equal(vals.view(np.uint32), want_v.view(np.uint32))
