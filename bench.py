@@ -682,10 +682,10 @@ def roofline(prof, st, k, layer_boards, peak, peak_kind, pattern):
         "sort_pass": 16 * layer_boards * passes,
         # compose (read key, write composite) + decompose (read, write)
         "layer_sort": 32 * layer_boards,
-        # solve: one board key + one rate per board, one 16-byte {key, rate} index slot per probe
-        "solve": 12 * layer_boards + 16 * int(st.lookups),
+        # solve: one board key + one rate per board, its own 16-byte index insert, one 16-byte slot per probe
+        "solve": 28 * layer_boards + 16 * int(st.lookups),
         "book_pack": 12 * int(st.raw_boards) + 12 * int(st.book_entries),
-        "rate_index": 28 * layer_boards,
+        "rate_index": 28 * layer_boards,  # the last two layers only (the solve fills the others)
         "final_layers": 12,
     }
     bytes_total = per_build.get(name, 0) * k
@@ -705,9 +705,9 @@ def roofline(prof, st, k, layer_boards, peak, peak_kind, pattern):
 # dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture per kernel
 # (profiles/), with the units (boards) that launch processed
 NCU_TRAFFIC = {
-    ("442", "expand"): {"bytes": 25.670656e6 + 0.801536e6, "units": 267258,
+    ("442", "expand"): {"bytes": 23.3664e6 + 0.950016e6, "units": 267258,
                         "source": "profiles/expand_dedup_442-512.md: launch t=150, scaled by parents"},
-    ("442", "solve"): {"bytes": 31.505664e6, "units": 327456,
+    ("442", "solve"): {"bytes": 43.521536e6 + 1.717504e6, "units": 327456,
                        "source": "profiles/solve_442-512.md: launch t=181, scaled by boards"},
 }
 
