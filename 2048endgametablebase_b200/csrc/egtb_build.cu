@@ -1028,25 +1028,46 @@ static int writer_threads(const egtb_run_options &o) {
 }
 
 // Copy byte ranges [dev_off[i], +bytes[i]) of a device buffer to pinned host
-// memory and write them to files with a thread pool.
+// memory and write them to files with a thread pool; the copies go out in
+// groups of about 16 MB, and a group's files are written as soon as its copy
+// has landed, while the next groups are still crossing PCIe.
 static void write_ranges(Engine &E, const unsigned char *dev, const std::vector<std::string> &paths,
                          const std::vector<unsigned long long> &dev_off, const std::vector<unsigned long long> &bytes,
                          int threads) {
     unsigned long long total = 0;
     for (auto b : bytes) total += b;
     unsigned char *h = E.ensure_pinned(std::max<unsigned long long>(total, 1));
-    unsigned long long pos = 0;
-    std::vector<unsigned long long> hoff(paths.size());
+    std::vector<cudaEvent_t> events;
+    struct EventGuard {
+        std::vector<cudaEvent_t> &v;
+        ~EventGuard() {
+            for (auto e : v) cudaEventDestroy(e);
+        }
+    } guard{events};
+    WriterPool pool(threads);
+    unsigned long long pos = 0, group = 0;
+    size_t first = 0;
     for (size_t i = 0; i < paths.size(); ++i) {
-        hoff[i] = pos;
         if (bytes[i])
             EGTB_CUDA(cudaMemcpyAsync(h + pos, dev + dev_off[i], bytes[i], cudaMemcpyDeviceToHost, E.stream));
         pos += bytes[i];
+        group += bytes[i];
+        if (group >= (16ull << 20) || i + 1 == paths.size()) {
+            cudaEvent_t ev;
+            EGTB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            events.push_back(ev);
+            EGTB_CUDA(cudaEventRecord(ev, E.stream));
+            unsigned long long at = pos - group;
+            for (size_t k = first; k <= i; ++k) {
+                pool.submit(paths[k], h + at, bytes[k], ev, E.device);
+                at += bytes[k];
+            }
+            first = i + 1;
+            group = 0;
+        }
     }
-    EGTB_CUDA(cudaStreamSynchronize(E.stream));
-    WriterPool pool(threads);
-    for (size_t i = 0; i < paths.size(); ++i) pool.submit(paths[i], h + hoff[i], bytes[i]);
     pool.wait();
+    EGTB_CUDA(cudaStreamSynchronize(E.stream));
 }
 
 // ------------------------------------------------------------- restart ----

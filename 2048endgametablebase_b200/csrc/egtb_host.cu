@@ -239,6 +239,8 @@ struct WriterPool::Impl {
         std::string path;
         const void *data;
         size_t bytes;
+        cudaEvent_t ready;  // when set: the data is complete once this event has completed
+        int device;
     };
     std::mutex mu;
     std::condition_variable cv, done_cv;
@@ -266,6 +268,10 @@ WriterPool::WriterPool(int threads) : impl_(new Impl) {
                     ++s.active;
                 }
                 try {
+                    if (job.ready) {
+                        EGTB_CUDA(cudaSetDevice(job.device));
+                        EGTB_CUDA(cudaEventSynchronize(job.ready));
+                    }
                     write_file(job.path, job.data, job.bytes);
                 } catch (const Error &e) {
                     std::lock_guard<std::mutex> lk(s.mu);
@@ -294,10 +300,10 @@ WriterPool::~WriterPool() {
     delete impl_;
 }
 
-void WriterPool::submit(std::string path, const void *data, size_t bytes) {
+void WriterPool::submit(std::string path, const void *data, size_t bytes, cudaEvent_t ready, int device) {
     {
         std::lock_guard<std::mutex> lk(impl_->mu);
-        impl_->q.push_back({std::move(path), data, bytes});
+        impl_->q.push_back({std::move(path), data, bytes, ready, device});
     }
     impl_->cv.notify_one();
 }

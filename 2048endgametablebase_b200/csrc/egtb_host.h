@@ -121,7 +121,8 @@ class WriterPool {
 public:
     explicit WriterPool(int threads);
     ~WriterPool();
-    void submit(std::string path, const void *data, size_t bytes);
+    // ready (optional): the job waits for this event (on `device`) before writing
+    void submit(std::string path, const void *data, size_t bytes, cudaEvent_t ready = nullptr, int device = 0);
     void wait();  // rethrows the first failure
 
 private:
