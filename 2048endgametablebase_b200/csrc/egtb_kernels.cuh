@@ -213,11 +213,25 @@ __device__ __forceinline__ int dedup_insert_zero(uint64_t *tab, unsigned long lo
     return 0;
 }
 
+// Continue a zero-slot insert of key after its first probe found another key at h.
+__device__ __forceinline__ int dedup_insert_zero_from(uint64_t *tab, unsigned long long mask, uint64_t key,
+                                                      unsigned long long h, unsigned *err) {
+    for (int probe = 1; probe < kMaxProbe; ++probe) {
+        h = (h + 1) & mask;
+        const unsigned long long prev = atomicCAS((unsigned long long *)tab + h, 0ull, (unsigned long long)key);
+        if (prev == 0ull) return 1;
+        if (prev == key) return 0;
+    }
+    atomicOr(err, kErrDedupOverflow);
+    return 0;
+}
+
 // Flush a warp's staged keys (children that passed the repeat filter): the
 // warp enters them in the layer's set 32 at a time, every lane busy, and
 // appends the ones that are new to the layer's staging buffer. Flags
 // kErrDedupOverflow when the layer passes half its set's capacity. kZero:
-// the set's free slots hold 0 (else: a slot of another tile sum is free).
+// the set's free slots hold 0 (else: a slot of another tile sum is free);
+// then two keys per lane go at once, their first probes in flight together.
 template <bool kZero>
 __device__ __forceinline__ void stage_flush_dedup(uint64_t *stage, int &count, uint64_t *__restrict__ out,
                                                   unsigned long long *cnt, unsigned long long cap, uint64_t *set,
@@ -225,14 +239,41 @@ __device__ __forceinline__ void stage_flush_dedup(uint64_t *stage, int &count, u
                                                   unsigned *err) {
     const int lane = threadIdx.x & 31;
     const unsigned long long half = (set_mask + 1) / 2;
+    if constexpr (kZero) {
+        const unsigned below = (1u << lane) - 1u;
+        for (int b = 0; b < count; b += 64) {
+            const int i0 = b + lane, i1 = b + 32 + lane;
+            const bool v0 = i0 < count, v1 = i1 < count;
+            const uint64_t k0 = v0 ? stage[i0] : 0, k1 = v1 ? stage[i1] : 0;
+            const unsigned long long h0 = mix64(k0) & set_mask, h1 = mix64(k1) & set_mask;
+            const unsigned long long p0 = v0 ? atomicCAS((unsigned long long *)set + h0, 0ull, (unsigned long long)k0) : 1ull;
+            const unsigned long long p1 = v1 ? atomicCAS((unsigned long long *)set + h1, 0ull, (unsigned long long)k1) : 1ull;
+            bool f0 = v0 && p0 == 0ull, f1 = v1 && p1 == 0ull;
+            if (v0 && p0 != 0ull && p0 != k0) f0 = dedup_insert_zero_from(set, set_mask, k0, h0, err) != 0;
+            if (v1 && p1 != 0ull && p1 != k1) f1 = dedup_insert_zero_from(set, set_mask, k1, h1, err) != 0;
+            const unsigned m0 = __ballot_sync(0xFFFFFFFFu, f0), m1 = __ballot_sync(0xFFFFFFFFu, f1);
+            const unsigned n = __popc(m0) + __popc(m1);
+            if (n) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(cnt, (unsigned long long)n);
+                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                if (base + n > cap) {
+                    if (lane == 0) atomicOr(err, kErrCandOverflow);
+                } else {
+                    if (f0) out[base + __popc(m0 & below)] = k0;
+                    if (f1) out[base + __popc(m0) + __popc(m1 & below)] = k1;
+                }
+                if (lane == 0 && base + n > half) atomicOr(err, kErrDedupOverflow);
+            }
+        }
+        __syncwarp();
+        count = 0;
+        return;
+    }
     for (int b = 0; b < count; b += 32) {
         const int i = b + lane;
         const uint64_t key = i < count ? stage[i] : 0;
-        bool fresh = false;
-        if (i < count) {
-            if constexpr (kZero) fresh = dedup_insert_zero(set, set_mask, key, err) != 0;
-            else fresh = dedup_insert(set, set_mask, key, want, bsum, err) != 0;
-        }
+        const bool fresh = i < count && dedup_insert(set, set_mask, key, want, bsum, err) != 0;
         const unsigned m = __ballot_sync(0xFFFFFFFFu, fresh);
         if (m) {
             unsigned long long base = 0;
@@ -586,6 +627,7 @@ solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
              unsigned long long m2, DevCtl *ctl, ulonglong2 *__restrict__ idx0 = nullptr, unsigned long long m0 = 0,
              ulonglong2 *__restrict__ clear_idx = nullptr, unsigned long long clear_slots = 0,
              unsigned *progress = nullptr, unsigned progress_value = 0) {
+    const GlobalRows rows{tab};
     const unsigned long long n0 = layer_len[t], o0 = layer_off[t];
     const double w2 = 1.0 - p4;
     unsigned long long looks = 0;
@@ -605,7 +647,7 @@ solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
             continue;
         }
         MoveCtx mc;
-        move_ctx_init(tab, b, mc);
+        move_ctx_init(rows, b, mc);
         uint64_t empt = empty_nibbles(b);
         double acc = 0.0;
         int nempty = 0;
@@ -619,7 +661,7 @@ solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
 #pragma unroll
             for (int v = 1; v <= 2; ++v) {
                 uint64_t mv[4], s;
-                spawn_moves(tab, mc, k, (uint64_t)v, s, mv);
+                spawn_moves(rows, mc, k, (uint64_t)v, s, mv);
 #pragma unroll
                 for (int d = 0; d < 4; ++d) {
                     const int j = (v - 1) * 4 + d;
