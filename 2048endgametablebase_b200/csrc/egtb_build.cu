@@ -98,6 +98,11 @@ static const char *kKindNames[] = {"expand", "sort_pass", "layer_sort", "solve",
                                    "rate_index"};
 enum { K_EXPAND = 0, K_SORT_PASS, K_UNIQUE, K_SOLVE, K_PACK, K_FINAL, K_INDEX, K_NKINDS };
 
+static unsigned long long env_bytes(const char *name) {
+    const char *v = getenv(name);
+    return (v && *v) ? strtoull(v, nullptr, 10) : 0ull;
+}
+
 struct Engine {
     int device = 0;
     cudaStream_t stream = nullptr;      // stream in use
@@ -233,6 +238,14 @@ struct Engine {
     }
 
     void alloc_or_throw(void **p, size_t bytes, const char *what) {
+        // EGTB_MAX_ALLOC_BYTES: refuse larger single allocations, as a smaller
+        // device would (exercises the streamed fallback on any GPU)
+        static const unsigned long long max_alloc = env_bytes("EGTB_MAX_ALLOC_BYTES");
+        if (max_alloc && bytes > max_alloc) {
+            *p = nullptr;
+            throw Error(EGTB_ERR_CAPACITY, std::string("device allocation of ") + std::to_string(bytes >> 20) +
+                                               " MiB for " + what + " is above EGTB_MAX_ALLOC_BYTES");
+        }
         cudaError_t e = cudaMalloc(p, bytes);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -355,6 +368,13 @@ struct Engine {
         alloc_or_throw((void **)&tile_off, sizeof(unsigned long long) * comp_tiles, "tile offsets");
     }
 
+    void ensure_copy_stream() {
+        if (copy_stream) return;
+        EGTB_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+        EGTB_CUDA(cudaEventCreateWithFlags(&ev_sorted, cudaEventDisableTiming));
+        EGTB_CUDA(cudaEventCreateWithFlags(&ev_copied, cudaEventDisableTiming));
+    }
+
     void ensure_sort_bufs(unsigned long long cap) {
         if (cap <= sort_cap) return;
         for (auto &p : sort_buf) release(p);
@@ -362,11 +382,7 @@ struct Engine {
         grow(sort_cap, [&] {
             for (auto &p : sort_buf) alloc_or_throw((void **)&p, sizeof(uint64_t) * sort_cap, "layer sort buffer");
         });
-        if (!copy_stream) {
-            EGTB_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
-            EGTB_CUDA(cudaEventCreateWithFlags(&ev_sorted, cudaEventDisableTiming));
-            EGTB_CUDA(cudaEventCreateWithFlags(&ev_copied, cudaEventDisableTiming));
-        }
+        ensure_copy_stream();
     }
 
     unsigned char *ensure_pinned(size_t bytes) {
@@ -952,6 +968,29 @@ static void enqueue_pack_all(Engine &E, int steps, const std::vector<unsigned lo
                                                                    E.tile_off, E.book, E.book_cap_bytes, E.ctl));
 }
 
+// Pack the books of layers l0 .. l1-1 (the same kernels over a range of layers).
+template <typename T>
+static void enqueue_pack_range(Engine &E, int l0, int l1, const std::vector<unsigned long long> &len, T zero) {
+    cudaStream_t s = E.stream;
+    const int nl = l1 - l0;
+    std::vector<unsigned long long> ft(nl + 1, 0);
+    for (int k = 0; k < nl; ++k) ft[k + 1] = ft[k] + (len[l0 + k] + kTileKeys - 1) / kTileKeys;
+    const unsigned long long n_tiles = ft[nl];
+    if (n_tiles > E.comp_tiles) throw Error(EGTB_ERR_CAPACITY, "tile buffers too small for packing");
+    // stream-ordered after the previous range's kernels, which read the same buffer
+    EGTB_CUDA(cudaMemcpyAsync(E.first_tile, ft.data(), sizeof(unsigned long long) * (nl + 1), cudaMemcpyHostToDevice, s));
+    const int g = E.sm_count * 4;
+    EGTB_LAUNCH(E, book_count_all_kernel<T><<<g, kSortThreads, 0, s>>>((const T *)E.rates, E.layer_off + l0,
+                                                                   E.layer_len + l0, E.first_tile, nl, n_tiles, zero,
+                                                                   E.tile_cnt, E.layer_max + l0));
+    EGTB_LAUNCH(E, scan_tiles_kernel<<<1, 1024, 0, s>>>(E.tile_cnt, n_tiles, E.tile_off, &E.ctl->n_unique));
+    EGTB_LAUNCH(E, book_lens_kernel<<<(nl + 255) / 256, 256, 0, s>>>(E.first_tile, nl, n_tiles, E.tile_off,
+                                                                    &E.ctl->n_unique, E.book_len + l0));
+    EGTB_LAUNCH(E, book_write_all_kernel<T><<<g, kSortThreads, 0, s>>>(E.arena, (const T *)E.rates, E.layer_off + l0,
+                                                                   E.layer_len + l0, E.first_tile, nl, n_tiles, zero,
+                                                                   E.tile_off, E.book, E.book_cap_bytes, E.ctl));
+}
+
 // Solve every layer on the device-resident arena (layers 0..steps-1 present)
 // and pack all books.
 template <typename T>
@@ -990,6 +1029,128 @@ static void enqueue_backward(Engine &E, const BackwardPlan &B, const std::vector
     const int pp = E.prof_begin(K_PACK);
     enqueue_pack_all<T>(E, B.steps, len, zero);
     E.prof_end(pp);
+}
+
+static int writer_threads(const egtb_run_options &o);
+
+// The same solve, with the books packed in groups of layers as the solve
+// finishes them: while the device solves the next layers, the host copies
+// each finished group (second stream) into pinned memory and writer threads
+// write its .book files. Returns the book lengths and rate maxima.
+template <typename T>
+static void backward_write_books(Engine &E, const BackwardPlan &B, const std::vector<unsigned long long> &len,
+                                 const std::vector<unsigned long long> &off, const egtb_run_options &o,
+                                 std::vector<unsigned long long> &blen, std::vector<unsigned long long> &maxb,
+                                 float *bwd_ms) {
+    cudaStream_t s = E.stream;
+    const int steps = B.steps;
+    const T zero = (T)dtype_zero(B.dtype), maxv = (T)dtype_max(B.dtype);
+    const int g = E.sm_count * 8;
+    T *rates = (T *)E.rates;
+    const uint32_t total = (uint32_t)(steps * 2);
+    unsigned *progress = progress_device_ptr();
+    const size_t rec = 8 + sizeof(T);
+    unsigned long long biggest = 0, raw_total = 0;
+    for (int L = 0; L < steps; ++L) {
+        biggest = std::max(biggest, len[L]);
+        raw_total += len[L];
+    }
+    E.ensure_index(index_slots(biggest));
+    E.ensure_copy_stream();
+    struct Group {
+        int l0, l1;
+        cudaEvent_t packed;
+    };
+    std::vector<Group> groups;
+    struct GroupGuard {
+        std::vector<Group> &v;
+        ~GroupGuard() {
+            for (auto &q : v) cudaEventDestroy(q.packed);
+        }
+    } gguard{groups};
+    auto close_group = [&](int l0, int l1) {
+        const int pp = E.prof_begin(K_PACK);
+        enqueue_pack_range<T>(E, l0, l1, len, zero);
+        E.prof_end(pp);
+        cudaEvent_t ev;
+        EGTB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        EGTB_CUDA(cudaEventRecord(ev, s));
+        groups.push_back({l0, l1, ev});
+    };
+    EGTB_CUDA(cudaEventRecord(E.ev[2], s));
+    EGTB_CUDA(cudaMemsetAsync(E.layer_max, 0, sizeof(unsigned long long) * steps, s));
+    const int pf = E.prof_begin(K_FINAL);
+    for (int t = steps - 2; t < steps; ++t)
+        if (t >= 0) EGTB_LAUNCH(E, final_layer_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec, zero, maxv));
+    for (int t = steps - 1; t >= steps - 2 && t >= 1; --t) enqueue_index<T>(E, t, len[t], zero);
+    if (steps - 3 >= 1)
+        EGTB_CUDA(cudaMemsetAsync(E.index[(steps - 3) % 4], 0, sizeof(ulonglong2) * index_slots(len[steps - 3]), s));
+    E.prof_end(pf);
+    close_group(std::max(0, steps - 2), steps);
+    constexpr int kGroup = 16;  // layers per packed group
+    int hi = steps - 2;         // the current group is [t, hi)
+    for (int t = steps - 3; t >= 0; --t) {
+        const int ps = E.prof_begin(K_SOLVE);
+        ulonglong2 *idx0 = t >= 1 ? E.index[t % 4] : nullptr;
+        ulonglong2 *clear = t >= 2 ? E.index[(t - 1) % 4] : nullptr;
+        EGTB_LAUNCH(E, solve_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec,
+                                                         t > B.docheck ? 1 : 0, E.tab, B.p4, zero, maxv,
+                                                         E.index[(t + 1) % 4], index_slots(len[t + 1]) - 1,
+                                                         E.index[(t + 2) % 4], index_slots(len[t + 2]) - 1, E.ctl,
+                                                         idx0, index_slots(len[t]) - 1, clear,
+                                                         t >= 2 ? index_slots(len[t - 1]) : 0, progress,
+                                                         total - (unsigned)t - 2u));
+        E.prof_end(ps);
+        if (hi - t == kGroup || t == 0) {
+            close_group(t, hi);
+            hi = t;
+        }
+    }
+    EGTB_CUDA(cudaEventRecord(E.ev[3], s));
+    // copy and write each group as soon as it is packed
+    blen.assign(steps, 0);
+    maxb.assign(steps, 0);
+    unsigned char *pin = E.ensure_pinned(std::max<unsigned long long>(raw_total * rec, 1));
+    std::vector<cudaEvent_t> copied;
+    struct EventGuard {
+        std::vector<cudaEvent_t> &v;
+        ~EventGuard() {
+            for (auto e : v) cudaEventDestroy(e);
+        }
+    } cguard{copied};
+    WriterPool pool(writer_threads(o));
+    unsigned long long pos = 0;
+    for (const Group &q : groups) {
+        const int nl = q.l1 - q.l0;
+        EGTB_CUDA(cudaStreamWaitEvent(E.copy_stream, q.packed, 0));
+        EGTB_CUDA(cudaMemcpyAsync(blen.data() + q.l0, E.book_len + q.l0, sizeof(unsigned long long) * nl,
+                                  cudaMemcpyDeviceToHost, E.copy_stream));
+        EGTB_CUDA(cudaMemcpyAsync(maxb.data() + q.l0, E.layer_max + q.l0, sizeof(unsigned long long) * nl,
+                                  cudaMemcpyDeviceToHost, E.copy_stream));
+        EGTB_CUDA(cudaStreamSynchronize(E.copy_stream));
+        cudaEvent_t ev;
+        EGTB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        copied.push_back(ev);
+        std::vector<std::pair<int, unsigned long long>> at;
+        for (int L = q.l0; L < q.l1; ++L) {
+            const unsigned long long bytes = blen[L] * rec;
+            if (pos + bytes > E.pinned_cap) throw Error(EGTB_ERR_CAPACITY, "book larger than its raw layer");
+            if (bytes)
+                EGTB_CUDA(cudaMemcpyAsync(pin + pos, E.book + off[L] * rec, bytes, cudaMemcpyDeviceToHost,
+                                          E.copy_stream));
+            at.push_back({L, pos});
+            pos += bytes;
+        }
+        EGTB_CUDA(cudaEventRecord(ev, E.copy_stream));
+        for (const auto &a : at)
+            pool.submit(std::string(o.pathname) + std::to_string(a.first) + ".book", pin + a.second,
+                        blen[a.first] * rec, ev, E.device);
+    }
+    pool.wait();
+    EGTB_CUDA(cudaStreamSynchronize(E.copy_stream));
+    EGTB_CUDA(cudaStreamSynchronize(s));
+    EGTB_CUDA(cudaGetLastError());
+    EGTB_CUDA(cudaEventElapsedTime(bwd_ms, E.ev[2], E.ev[3]));
 }
 
 // ---------------------------------------------------------------- output --
@@ -1183,32 +1344,31 @@ static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const 
     std::vector<unsigned long long> len = d2h_u64(E, E.layer_len, steps + 1);
     BackwardPlan B{steps, o.docheck_step, o.success_rate_dtype, o.spawn_rate4, P.spec};
     E.ensure_rates(sizeof(T));
-    EGTB_CUDA(cudaEventRecord(E.ev[2], E.stream));
-    enqueue_backward<T>(E, B, len, progress_device_ptr());
-    EGTB_CUDA(cudaEventRecord(E.ev[3], E.stream));
-    EGTB_CUDA(cudaStreamSynchronize(E.stream));
-    EGTB_CUDA(cudaGetLastError());
-    EGTB_CUDA(cudaEventElapsedTime(&bwd_ms, E.ev[2], E.ev[3]));
+    std::vector<unsigned long long> blen, maxb;
+    if (o.write_files) {
+        backward_write_books<T>(E, B, len, off, o, blen, maxb, &bwd_ms);
+    } else {
+        EGTB_CUDA(cudaEventRecord(E.ev[2], E.stream));
+        enqueue_backward<T>(E, B, len, progress_device_ptr());
+        EGTB_CUDA(cudaEventRecord(E.ev[3], E.stream));
+        EGTB_CUDA(cudaStreamSynchronize(E.stream));
+        EGTB_CUDA(cudaGetLastError());
+        EGTB_CUDA(cudaEventElapsedTime(&bwd_ms, E.ev[2], E.ev[3]));
+    }
     E.prof_resolve();
     DevCtl c = read_ctl(E);
     if (c.err & kErrIndexOverflow) throw Error(EGTB_ERR_CAPACITY, "rate index probe chain too long");
     if (c.err) throw Error(EGTB_ERR_CAPACITY, "book buffer overflow");
-    std::vector<unsigned long long> blen = d2h_u64(E, E.book_len, steps);
-    std::vector<unsigned long long> maxb = d2h_u64(E, E.layer_max, steps);
+    if (!o.write_files) {
+        blen = d2h_u64(E, E.book_len, steps);
+        maxb = d2h_u64(E, E.layer_max, steps);
+    }
     const size_t rec = 8 + sizeof(T);
     E.last_steps = steps;
     E.last_rec = rec;
     E.last_off = off;
     E.last_blen = blen;
     if (o.write_files) {
-        std::vector<std::string> paths;
-        std::vector<unsigned long long> doff, bytes;
-        for (int t = 0; t < steps; ++t) {
-            paths.push_back(std::string(o.pathname) + std::to_string(t) + ".book");
-            doff.push_back(off[t] * rec);
-            bytes.push_back(blen[t] * rec);
-        }
-        write_ranges(E, E.book, paths, doff, bytes, writer_threads(o));
         std::vector<int> order;
         for (int t = steps - 3; t >= 0; --t) order.push_back(t);
         write_stats(o, o.success_rate_dtype, order, len, blen, maxb,

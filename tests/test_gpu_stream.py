@@ -76,3 +76,42 @@ def test_streamed_diagonal_1024_prefix_matches_128(tmp_root, streamed):
     for t in range(57, 60):
         assert os.path.getsize(d + f"4432_1024_{t}") // 8 >= ref["raw_len"][t], t
     shutil.rmtree(d, ignore_errors=True)
+
+
+def test_build_falls_back_to_streamed_layers_when_the_table_does_not_fit(tmp_root):
+    """A build whose layer arena cannot be allocated is built with streamed
+    layers by itself (generate + solve through files), books unchanged. The
+    allocation limit stands in for a smaller device; it is read once per
+    process, so the build runs in a child process."""
+    import json
+    import subprocess
+    import sys
+    key = "L3_256_float32"
+    case = H.cases()[key]
+    d = H.fresh(os.path.join(tmp_root, "fallback_" + key) + "/")
+    code = f"""
+import json, sys
+sys.path.insert(0, {H.ROOT!r}); sys.path.insert(0, {os.path.join(H.ROOT, "tests")!r})
+import helpers as H
+import ctypes
+case = H.cases()[{key!r}]
+F = H.fc()
+N = H.pkg()._native
+spec, o = H.spec_options(case, {d!r} + case["pattern_full"] + "_")
+# without files there is no streamed path: under the limit the table must not fit
+seeds = H.seeds(case)
+c_spec, c_opt = spec.to_c(), o.to_c(write_files=False)
+rc = N.lib().egtb_build(seeds.ctypes.data, len(seeds), ctypes.byref(c_spec), ctypes.byref(c_opt), None)
+assert rc == -5, rc
+F.run_pattern_build(seeds, spec, o)
+print(json.dumps(F.last_build_stats()))
+"""
+    env = dict(os.environ, EGTB_MAX_ALLOC_BYTES=str(512 << 20))
+    env.pop("EGTB_STREAM_LAYERS", None)
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=900)
+    assert out.returncode == 0, out.stderr[-2000:]
+    name = case["pattern_full"]
+    for t in range(case["steps"]):
+        assert H.sha(d + f"{name}_{t}.book") == case["book_sha256"][t], t
+    assert not any(os.path.exists(d + f"{name}_{t}") for t in range(case["steps"]))
+    shutil.rmtree(d, ignore_errors=True)
