@@ -79,10 +79,6 @@ static uint32_t read_progress() {
     return cur;
 }
 
-__global__ void progress_kernel(unsigned *p, unsigned v) {
-    if (p) *(volatile unsigned *)p = v;
-}
-
 // ---------------------------------------------------------------- engine ---
 
 static unsigned long long align16(unsigned long long x) { return (x + 15ull) & ~15ull; }
@@ -490,30 +486,6 @@ struct ForwardPlan {
     long long s0;      // tile sum of layer 0; layer t has tile sum s0 + 2t
     FreeNibbles free;  // nibbles that vary between keys
 };
-
-// Sort the candidates of buffer x and unique them into the arena as layer L:
-// one histogram kernel, one onesweep kernel per pass, one unique kernel.
-static void enqueue_sort_unique(Engine &E, const ForwardPlan &P, int x, int L, unsigned *progress) {
-    cudaStream_t s = E.stream;
-    unsigned long long *n_ptr = &E.ctl->cand_count[x];
-    EGTB_LAUNCH(E, sort_hist_kernel<<<E.sm_count * 2, 256, 0, s>>>(E.cand[x], n_ptr, E.cand_cap, P.sort, E.hist,
-                                                                   E.counters, E.ctl));
-    uint64_t *src = E.cand[x], *dst = E.tmp;
-    for (int p = 0; p < P.sort.passes; ++p) {
-        const int pi = E.prof_begin(K_SORT_PASS);
-        EGTB_LAUNCH(E, onesweep_kernel<<<E.sweep_grid, kSweepThreads, 0, s>>>(src, dst, n_ptr, E.cand_cap, P.sort, p,
-                                                                             E.hist, E.counters, E.status, E.epoch++,
-                                                                             E.ctl));
-        E.prof_end(pi);
-        std::swap(src, dst);
-    }
-    const int pu = E.prof_begin(K_UNIQUE);
-    EGTB_LAUNCH(E, unique_layer_kernel<<<E.sweep_grid, kSortThreads, 0, s>>>(src, x, E.cand_cap, E.arena, E.layer_off,
-                                                                             E.layer_len, L, E.arena_cap, E.counters,
-                                                                             E.ustatus, E.epoch++, E.hist, E.ctl,
-                                                                             progress));
-    E.prof_end(pu);
-}
 
 // Enqueue forward steps first_step .. steps-2 (one fused expand + dedup
 // kernel each) and close the last two layers. Preconditions on the device:
