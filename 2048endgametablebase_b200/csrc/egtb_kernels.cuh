@@ -266,26 +266,24 @@ __device__ __forceinline__ void stage_flush_dedup(uint64_t *stage, int &count, u
                 if (lane == 0 && base + n > half) atomicOr(err, kErrDedupOverflow);
             }
         }
-        __syncwarp();
-        count = 0;
-        return;
-    }
-    for (int b = 0; b < count; b += 32) {
-        const int i = b + lane;
-        const uint64_t key = i < count ? stage[i] : 0;
-        const bool fresh = i < count && dedup_insert(set, set_mask, key, want, bsum, err) != 0;
-        const unsigned m = __ballot_sync(0xFFFFFFFFu, fresh);
-        if (m) {
-            unsigned long long base = 0;
-            if (lane == 0) base = atomicAdd(cnt, (unsigned long long)__popc(m));
-            base = __shfl_sync(0xFFFFFFFFu, base, 0);
-            const unsigned long long pos = base + __popc(m & ((1u << lane) - 1u));
-            if (base + __popc(m) > cap) {
-                if (lane == 0) atomicOr(err, kErrCandOverflow);
-            } else if (fresh) {
-                out[pos] = key;
+    } else {
+        for (int b = 0; b < count; b += 32) {
+            const int i = b + lane;
+            const uint64_t key = i < count ? stage[i] : 0;
+            const bool fresh = i < count && dedup_insert(set, set_mask, key, want, bsum, err) != 0;
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, fresh);
+            if (m) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(cnt, (unsigned long long)__popc(m));
+                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                const unsigned long long pos = base + __popc(m & ((1u << lane) - 1u));
+                if (base + __popc(m) > cap) {
+                    if (lane == 0) atomicOr(err, kErrCandOverflow);
+                } else if (fresh) {
+                    out[pos] = key;
+                }
+                if (lane == 0 && base + __popc(m) > half) atomicOr(err, kErrDedupOverflow);
             }
-            if (lane == 0 && base + __popc(m) > half) atomicOr(err, kErrDedupOverflow);
         }
     }
     __syncwarp();
