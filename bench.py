@@ -697,6 +697,11 @@ def roofline(prof, st, k, layer_boards, peak, peak_kind, pattern):
            "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
            "algorithmic_bytes_per_launch": bytes_total / count,
            "launches_per_step": count / k, "avg_launch_us": total / count * 1e3}
+    out["limit"] = {
+        "expand": "latency of L2 round trips (repeat filter, set CAS): ncu long_scoreboard stalls, DRAM 3 %",
+        "solve": "latency of L2 index probes: ncu long_scoreboard stalls",
+        "sort_pass": "issue and barrier bound at ~1.6 TB/s; DRAM traffic equals the algorithmic bytes",
+    }.get(name, "")
     cap = NCU_TRAFFIC.get((pattern, name))
     if cap:
         # DRAM bytes of one captured launch, scaled by parents to the mean launch
