@@ -239,6 +239,8 @@ std::vector<TablePlan> make_plans(int n, const uint64_t *const *seeds, const uin
         if (o.compress || o.optimal_branch_only)
             throw Error(EGTB_ERR_UNSUPPORTED, "compress / optimal_branch_only post-passes are not built");
         if (o.steps < 3 || o.steps > (1 << 16)) throw Error(EGTB_ERR_ARG, "steps of a batched table must be 3..65536");
+        if (o.deletion_threshold > 0.0)
+            throw Error(EGTB_ERR_UNSUPPORTED, "deletion_threshold: build such a table with egtb_build");
         if (specs[i].symm_mode < 0 || specs[i].symm_mode > 3)
             throw Error(EGTB_ERR_UNSUPPORTED, "symmetry modes min33/min24/min34 are not built");
         if (n_seeds[i] == 0 || !seeds[i]) throw Error(EGTB_ERR_ARG, "every table needs seed boards");

@@ -1850,7 +1850,12 @@ extern "C" int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_patt
                 return;
             }
             bool streamed = false;
-            if (!resume && !(options->write_files && stream_layers_forced())) {
+            // a deletion threshold rewrites the book of layer i+2 after solving
+            // layer i (BookSolver.cpp:589-593): the layer-by-layer solve does that
+            const bool layered = options->deletion_threshold > 0.0;
+            if (layered && !options->write_files)
+                throw Error(EGTB_ERR_UNSUPPORTED, "deletion_threshold rewrites book files: build with write_files");
+            if (!resume && !layered && !(options->write_files && stream_layers_forced())) {
                 try {
                     fused_build<T>(E, seeds, n_seeds, *spec, *options, stats);
                     return;
@@ -1860,8 +1865,8 @@ extern "C" int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_patt
                     if (e.code != EGTB_ERR_CAPACITY || !options->write_files) throw;
                     streamed = true;
                 }
-            } else if (!resume) {
-                streamed = true;
+            } else if (!resume && !layered) {
+                streamed = true;  // EGTB_STREAM_LAYERS
             }
             {
                 int st = 0;

@@ -80,7 +80,8 @@ def pattern_params(entry: dict, target: int):
     return masks, shifts, symm, seeds, steps, docheck, s0
 
 
-def make_spec_options(masks, shifts, symm, target, steps, docheck, pathname, dtype="float32", p4=0.1, threads=0):
+def make_spec_options(masks, shifts, symm, target, steps, docheck, pathname, dtype="float32", p4=0.1, threads=0,
+                      deletion_threshold=0.0):
     fc = module()
     spec = fc.PatternSpec()
     spec.name = "oracle"
@@ -96,6 +97,7 @@ def make_spec_options(masks, shifts, symm, target, steps, docheck, pathname, dty
     o.spawn_rate4 = float(p4)
     o.direct_io = False
     o.num_threads = int(threads or os.cpu_count() or 4)
+    o.deletion_threshold = float(deletion_threshold)
     return spec, o
 
 

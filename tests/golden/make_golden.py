@@ -80,6 +80,9 @@ def custom_patterns() -> dict:
     return pats
 
 
+# builds whose books are rewritten with a deletion threshold (BookSolver.cpp:589-593)
+DELETION_CASES = [("L3", 5, "float32", 0.3), ("442", 6, "uint32", 0.5), ("diag9", 6, "float64", 0.7)]
+
 SMALL_CASES = [
     ("44", 6, "float32"), ("44", 7, "uint32"),
     ("L3", 5, "float32"), ("L3", 5, "uint32"), ("L3", 5, "uint64"), ("L3", 5, "float64"),
@@ -101,12 +104,13 @@ def sha(path: str) -> str:
     return h.hexdigest()
 
 
-def run_case(catalog, pat, target, dtype):
+def run_case(catalog, pat, target, dtype, deletion=0.0):
     masks, shifts, symm, seeds, steps, docheck, s0 = R.pattern_params(catalog[pat], target)
     T = 2 ** target
     name = f"{pat}_{T}"
-    gdir = R.fresh_dir(os.path.join(WORK, f"{name}_{dtype}", "gen") + "/")
-    bdir = R.fresh_dir(os.path.join(WORK, f"{name}_{dtype}", "build") + "/")
+    tag = f"{name}_{dtype}" + (f"_del{deletion}" if deletion else "")
+    gdir = R.fresh_dir(os.path.join(WORK, tag, "gen") + "/")
+    bdir = R.fresh_dir(os.path.join(WORK, tag, "build") + "/")
     spec, o = R.make_spec_options(masks, shifts, symm, target, steps, docheck, gdir + name + "_", dtype)
     started, last0, last1 = R.run_generate(seeds, spec, o)
     raw_len, raw_sha = [], []
@@ -114,7 +118,8 @@ def run_case(catalog, pat, target, dtype):
         p = gdir + f"{name}_{t}"
         raw_len.append(os.path.getsize(p) // 8)
         raw_sha.append(sha(p))
-    spec, o = R.make_spec_options(masks, shifts, symm, target, steps, docheck, bdir + name + "_", dtype)
+    spec, o = R.make_spec_options(masks, shifts, symm, target, steps, docheck, bdir + name + "_", dtype,
+                                  deletion_threshold=deletion)
     R.run_build(seeds, spec, o)
     book_len, book_sha = [], []
     rec = 12 if dtype in ("uint32", "float32", "1-float32") else 16
@@ -131,6 +136,10 @@ def run_case(catalog, pat, target, dtype):
         "partial_len": [int(last0.size), int(last1.size)],
         "book_len": book_len, "book_sha256": book_sha,
     }
+    if deletion:
+        case["deletion_threshold"] = deletion
+        lines = open(bdir + name + "_stats.txt").read().splitlines()
+        case["stats_columns"] = [",".join(x.split(",")[:3]) for x in lines]
     if (pat, target, dtype) in HUGE_CASES:
         import shutil
         shutil.rmtree(gdir, ignore_errors=True)
@@ -257,6 +266,14 @@ def main():
                 raw = bdir + f"free5_32_{t}.book"
                 data[f"book_{t}"] = np.fromfile(raw, dtype=np.uint8)
             np.savez_compressed(os.path.join(GOLDEN, "free5_32.npz"), **data)
+    for pat, target, dtype, thr in DELETION_CASES:
+        key = f"{pat}_{2 ** target}_{dtype}_del{thr}"
+        if only and key not in only:
+            continue
+        print("case", key, flush=True)
+        case, _ = run_case(catalog, pat, target, dtype, thr)
+        case["size_class"] = "deletion"
+        cases[key] = case
     json.dump(cases, open(cases_path, "w"), indent=0)
     if reader:
         rpath = os.path.join(GOLDEN, "reader.json")

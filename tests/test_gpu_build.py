@@ -174,3 +174,32 @@ def test_huge_build_in_memory_bit_exact(key):
     for t in range(case["steps"]):
         N.check(N.lib().egtb_book_layer_copy(0, t, buf.ctypes.data, buf.nbytes, ctypes.byref(size)))
         assert hashlib.sha256(buf[: size.value].tobytes()).hexdigest() == case["book_sha256"][t], t
+
+
+@pytest.mark.parametrize("key", [k for k, v in H.cases().items() if v.get("size_class") == "deletion"])
+def test_deletion_threshold_books_bit_exact(key, tmp_root):
+    """deletion_threshold > 0: after layer i is solved, the book of layer i+2
+    keeps only rates above the threshold (BookSolver.cpp:589-593); the books
+    and the stats.txt columns must equal the reference's."""
+    case = H.cases()[key]
+    F = H.fc()
+    d = H.fresh(os.path.join(tmp_root, "del_" + key) + "/")
+    spec, o = H.spec_options(case, d + case["pattern_full"] + "_")
+    o.deletion_threshold = case["deletion_threshold"]
+    F.run_pattern_build(H.seeds(case), spec, o)
+    name = case["pattern_full"]
+    for t in range(case["steps"]):
+        assert H.sha(d + f"{name}_{t}.book") == case["book_sha256"][t], (key, t)
+    lines = open(d + f"{name}_stats.txt").read().splitlines()
+    assert [",".join(x.split(",")[:3]) for x in lines] == case["stats_columns"]
+
+
+def test_deletion_threshold_needs_files():
+    import ctypes
+    case = H.cases()["L3_32_float32"]
+    N = H.pkg()._native
+    spec, o = H.spec_options(case, "/nonexistent/unused_")
+    o.deletion_threshold = 0.3
+    c_spec, c_opt = spec.to_c(), o.to_c(write_files=False)
+    s = H.seeds(case)
+    assert N.lib().egtb_build(s.ctypes.data, len(s), ctypes.byref(c_spec), ctypes.byref(c_opt), None) == -7
