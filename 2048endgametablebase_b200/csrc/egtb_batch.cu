@@ -236,11 +236,11 @@ std::vector<TablePlan> make_plans(int n, const uint64_t *const *seeds, const uin
             throw Error(EGTB_ERR_ARG, "all tables of a batch must use one success_rate_dtype");
         dtype_size(o.success_rate_dtype);
         if (o.is_variant) throw Error(EGTB_ERR_UNSUPPORTED, "variant boards (wall-merge mover) are not built");
-        if (o.compress || o.optimal_branch_only)
-            throw Error(EGTB_ERR_UNSUPPORTED, "compress / optimal_branch_only post-passes are not built");
+        if (o.compress) throw Error(EGTB_ERR_UNSUPPORTED, "compressed books (compress) are not built");
         if (o.steps < 3 || o.steps > (1 << 16)) throw Error(EGTB_ERR_ARG, "steps of a batched table must be 3..65536");
-        if (o.deletion_threshold > 0.0)
-            throw Error(EGTB_ERR_UNSUPPORTED, "deletion_threshold: build such a table with egtb_build");
+        if (o.deletion_threshold > 0.0 || o.optimal_branch_only)
+            throw Error(EGTB_ERR_UNSUPPORTED,
+                        "deletion_threshold / optimal_branch_only rewrite book files: build such a table with egtb_build");
         if (specs[i].symm_mode < 0 || specs[i].symm_mode > 3)
             throw Error(EGTB_ERR_UNSUPPORTED, "symmetry modes min33/min24/min34 are not built");
         if (n_seeds[i] == 0 || !seeds[i]) throw Error(EGTB_ERR_ARG, "every table needs seed boards");

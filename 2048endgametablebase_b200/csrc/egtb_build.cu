@@ -1251,8 +1251,7 @@ static void check_common(const uint64_t *seeds, size_t n_seeds, const egtb_patte
     if (!spec || !o) throw Error(EGTB_ERR_ARG, "spec and options are required");
     if (n_seeds && !seeds) throw Error(EGTB_ERR_ARG, "seeds pointer is NULL");
     if (o->is_variant) throw Error(EGTB_ERR_UNSUPPORTED, "variant boards (wall-merge mover) are not built");
-    if (o->compress || o->optimal_branch_only)
-        throw Error(EGTB_ERR_UNSUPPORTED, "compress / optimal_branch_only post-passes are not built");
+    if (o->compress) throw Error(EGTB_ERR_UNSUPPORTED, "compressed books (compress) are not built");
     dtype_size(o->success_rate_dtype);
     if (o->steps > (1 << 20)) throw Error(EGTB_ERR_ARG, "steps out of range");
 }
@@ -1657,6 +1656,135 @@ static void solve_files(Engine &E, const void *d1_recs, size_t n1, const void *d
     }
 }
 
+// ---------------------------------------------- optimal-branch pass --------
+
+// keep_only_optimal_branches_impl (native_core/src/BookSolver.cpp:688-735) on
+// the book files the solve wrote: for i = 21 .. steps-1, book i keeps only
+// the entries that are the best move of a position of the thinned book i-2
+// plus a 4 or of the thinned book i-1 plus a 2 (optimal_mark_kernel), in
+// order, and is rewritten. Three layers live on the device (keys + rates),
+// with a {key, position} index and a mark byte per entry of book i.
+template <typename T>
+static void optimal_branch_files(Engine &E, const egtb_pattern_spec &spec, const egtb_run_options &o) {
+    const int steps = o.steps;
+    const std::string p = o.pathname;
+    const size_t rec = 8 + sizeof(T);
+    const T zero = (T)dtype_zero(o.success_rate_dtype);
+    cudaStream_t s = E.stream;
+    const uint32_t total = (uint32_t)(steps * 3);
+    if (steps <= 21) {  // the pass thins layers 21 and up only
+        if (file_exists(p + "optlayer")) std::remove((p + "optlayer").c_str());
+        set_progress(total, total);
+        return;
+    }
+    const DevSpec ds = make_dev_spec(spec, o.target);
+    unsigned long long cap = 16;
+    for (int i = 19; i < steps; ++i) cap = std::max<unsigned long long>(cap, file_size(p + std::to_string(i) + ".book") / rec);
+    unsigned long long slots = 64;
+    while (slots < 2 * cap) slots <<= 1;
+    const unsigned long long tiles = cap / kTileKeys + 2;
+    // one block: keys[3] | rates[3] | index | marks | records | tile counts |
+    // tile offsets | total, every part starting on a 256-byte boundary
+    auto r256 = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t part[7] = {r256(cap * 8),  r256(cap * sizeof(T)), r256(slots * sizeof(ulonglong2)), r256(cap),
+                            r256(cap * rec), r256(tiles * 4),       r256(tiles * 8)};
+    const size_t bytes = 3 * part[0] + 3 * part[1] + part[2] + part[3] + part[4] + part[5] + part[6] + 256;
+    unsigned char *base = nullptr;
+    E.alloc_or_throw((void **)&base, bytes, "optimal-branch pass");
+    std::unique_ptr<unsigned char, void (*)(unsigned char *)> guard(base, [](unsigned char *q) { cudaFree(q); });
+    size_t at = 0;
+    auto take = [&](size_t n) {
+        unsigned char *q = base + at;
+        at += n;
+        return q;
+    };
+    uint64_t *keys[3];
+    T *rates[3];
+    for (int k = 0; k < 3; ++k) keys[k] = (uint64_t *)take(part[0]);
+    for (int k = 0; k < 3; ++k) rates[k] = (T *)take(part[1]);
+    ulonglong2 *index = (ulonglong2 *)take(part[2]);
+    uint8_t *marks = take(part[3]);
+    unsigned char *recs = take(part[4]);
+    unsigned *tile_cnt = (unsigned *)take(part[5]);
+    unsigned long long *tile_off = (unsigned long long *)take(part[6]);
+    unsigned long long *d_total = (unsigned long long *)take(256);
+    const int g = E.sm_count * 4;
+    // book L's records -> keys[slot], rates[slot] (staged through `recs`)
+    auto load = [&](int L, int slot) -> unsigned long long {
+        std::vector<unsigned char> h = read_file(p + std::to_string(L) + ".book");
+        const unsigned long long n = h.size() / rec;
+        if (n > cap) throw Error(EGTB_ERR_CAPACITY, "book larger than measured");
+        if (n) {
+            EGTB_CUDA(cudaMemcpyAsync(recs, h.data(), n * rec, cudaMemcpyHostToDevice, s));
+            EGTB_LAUNCH(E, unpack_records_kernel<T><<<g, 256, 0, s>>>(recs, n, keys[slot], rates[slot]));
+        }
+        EGTB_CUDA(cudaStreamSynchronize(s));
+        return n;
+    };
+    int s0 = 0, s1 = 1, s2 = 2;  // slots of books i-2, i-1 (thinned) and i
+    unsigned long long n0 = 0, n1 = 0;
+    // handle_restart_opt_only (BookSolver.cpp:648-683): "<path>optlayer" holds
+    // the last layer already thinned; the pass starts after it, from books
+    // i-2 and i-1 as they are on disk, and rewrites the marker before each
+    // later layer.
+    const std::string marker = p + "optlayer";
+    bool started = false;
+    for (int i = 0; i < steps; ++i) {
+        set_progress((uint32_t)(2 * steps + i + 1), total);
+        if (started) {
+            const std::string last = std::to_string(i - 1);
+            write_file(marker, last.data(), last.size());
+        } else {
+            int current = i - 1;
+            if (file_exists(marker)) {
+                const std::vector<unsigned char> text = read_file(marker);
+                std::istringstream in(std::string(text.begin(), text.end()));
+                in >> current;
+            }
+            const std::string b0 = p + std::to_string(i - 2) + ".book", b1 = p + std::to_string(i - 1) + ".book";
+            if (current >= i || i <= 20 || !file_exists(b0) || !file_exists(b1)) continue;
+            n0 = load(i - 2, s0);
+            n1 = load(i - 1, s1);
+            started = true;
+        }
+        const unsigned long long n2 = load(i, s2);
+        unsigned long long kept = 0;
+        if (n2) {
+            unsigned long long sl = 64;
+            while (sl < 2 * n2) sl <<= 1;
+            EGTB_CUDA(cudaMemsetAsync(index, 0, sl * sizeof(ulonglong2), s));
+            EGTB_LAUNCH(E, pos_index_kernel<<<g, 256, 0, s>>>(keys[s2], n2, index, sl - 1));
+            EGTB_CUDA(cudaMemsetAsync(marks, 0, n2, s));
+            if (n0)
+                EGTB_LAUNCH(E, optimal_mark_kernel<T><<<g, 256, 0, s>>>(keys[s0], n0, 2ull, ds, E.tab, index, sl - 1,
+                                                                      rates[s2], n2, zero, marks));
+            if (n1)
+                EGTB_LAUNCH(E, optimal_mark_kernel<T><<<g, 256, 0, s>>>(keys[s1], n1, 1ull, ds, E.tab, index, sl - 1,
+                                                                      rates[s2], n2, zero, marks));
+            const unsigned long long nt = (n2 + kTileKeys - 1) / kTileKeys;
+            EGTB_LAUNCH(E, mark_count_kernel<<<g, kSortThreads, 0, s>>>(marks, n2, tile_cnt));
+            EGTB_LAUNCH(E, scan_tiles_kernel<<<1, 1024, 0, s>>>(tile_cnt, nt, tile_off, d_total));
+            // the thinned book i goes to the slot of book i-2, which is no longer needed
+            EGTB_LAUNCH(E, mark_write_kernel<T><<<g, kSortThreads, 0, s>>>(keys[s2], rates[s2], marks, n2, tile_off,
+                                                                        keys[s0], rates[s0], recs));
+            EGTB_CUDA(cudaMemcpyAsync(&kept, d_total, 8, cudaMemcpyDeviceToHost, s));
+            EGTB_CUDA(cudaStreamSynchronize(s));
+            EGTB_CUDA(cudaGetLastError());
+        }
+        std::vector<unsigned char> out(kept * rec);
+        if (kept) EGTB_CUDA(cudaMemcpy(out.data(), recs, kept * rec, cudaMemcpyDeviceToHost));
+        write_file(p + std::to_string(i) + ".book", out.data(), out.size());
+        // books i-1 and i (thinned) are the parents of book i+1
+        const int thinned = s0;
+        s0 = s1;
+        s1 = thinned;
+        n0 = n1;
+        n1 = kept;
+    }
+    if (file_exists(marker)) std::remove(marker.c_str());
+    set_progress(total, total);
+}
+
 // ------------------------------------------------------ primitives -------
 
 __global__ void prim_moves_kernel(const uint32_t *tab, const uint64_t *in, size_t n, uint64_t *out4) {
@@ -1828,6 +1956,7 @@ extern "C" int egtb_solve(const void *d1_records, size_t n1, const void *d2_reco
         dispatch_dtype(options->success_rate_dtype, [&](auto z) {
             using T = decltype(z);
             solve_files<T>(E, d1_records, n1, d2_records, n2, *spec, *options, stats);
+            if (options->optimal_branch_only) optimal_branch_files<T>(E, *spec, *options);  // run_pattern_solve_impl
         });
     });
 }
@@ -1837,7 +1966,9 @@ extern "C" int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_patt
     return guarded([&] {
         check_common(seeds, n_seeds, spec, options);
         // run_pattern_build_cpp resets the progress first (BookSolver.cpp:828)
-        egtb_reset_build_progress((uint32_t)(options->steps > 0 ? options->steps * 2 : 0));
+        // classic_build_progress_total (FormationRuntime.h:48-54)
+        egtb_reset_build_progress((uint32_t)(options->steps > 0 ? options->steps * (options->optimal_branch_only ? 3 : 2)
+                                                                : 0));
         Engine &E = engine_for(options->device);
         std::lock_guard<std::mutex> lk(E.mu);
         if (stats) std::memset(stats, 0, sizeof *stats);
@@ -1853,11 +1984,13 @@ extern "C" int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_patt
             // a deletion threshold rewrites the book of layer i+2 after solving
             // layer i (BookSolver.cpp:589-593): the layer-by-layer solve does that
             const bool layered = options->deletion_threshold > 0.0;
-            if (layered && !options->write_files)
-                throw Error(EGTB_ERR_UNSUPPORTED, "deletion_threshold rewrites book files: build with write_files");
+            if ((layered || options->optimal_branch_only) && !options->write_files)
+                throw Error(EGTB_ERR_UNSUPPORTED,
+                            "deletion_threshold and optimal_branch_only rewrite book files: build with write_files");
             if (!resume && !layered && !(options->write_files && stream_layers_forced())) {
                 try {
                     fused_build<T>(E, seeds, n_seeds, *spec, *options, stats);
+                    if (options->optimal_branch_only) optimal_branch_files<T>(E, *spec, *options);
                     return;
                 } catch (const Error &e) {
                     // the table does not fit in device memory: with files, build it
@@ -1874,6 +2007,7 @@ extern "C" int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_patt
                 std::memset(&g, 0, sizeof g);
                 generate_files<T>(E, seeds, n_seeds, *spec, *options, &st, &g, streamed);
                 solve_files<T>(E, nullptr, 0, nullptr, 0, *spec, *options, stats);
+                if (options->optimal_branch_only) optimal_branch_files<T>(E, *spec, *options);
                 if (stats) {
                     stats->forward_ms = g.forward_ms;
                     stats->candidates = g.candidates;

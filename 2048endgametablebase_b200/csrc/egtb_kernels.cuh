@@ -929,4 +929,132 @@ book_write_all_kernel(const uint64_t *__restrict__ arena, const T *__restrict__ 
     }
 }
 
+// ------------------------------------------------ optimal-branch pass ----
+//
+// keep_only_optimal_branches_impl (native_core/src/BookSolver.cpp:688-735):
+// for layer i >= 21, entry e of book i stays only when some position of book
+// i-2 plus a 4 (or of book i-1 plus a 2) has e as its best move (first
+// strictly largest rate over the moves left, right, up, down). Books i-2 and
+// i-1 are the already-thinned ones.
+
+// {key, position} index of a sorted book layer (key 0 = empty slot).
+static __global__ void __launch_bounds__(256)
+pos_index_kernel(const uint64_t *__restrict__ keys, unsigned long long n, ulonglong2 *__restrict__ slots,
+                 unsigned long long mask) {
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const uint64_t key = keys[i];
+        unsigned long long h = mix64(key) & mask;
+        for (unsigned long long probe = 0; probe <= mask; ++probe) {  // at most half full
+            const unsigned long long prev = atomicCAS(&slots[h].x, 0ull, (unsigned long long)key);
+            if (prev == 0ull || prev == key) {
+                slots[h].y = i;
+                break;
+            }
+            h = (h + 1) & mask;
+        }
+    }
+}
+
+// find_optimal_branches (BookSolver.cpp:611-645): mark the best move's entry
+// of book i for every position b | v << 4k of the parent book (empty k
+// ascending). As the reference, a position with no move above zero marks
+// entry 0.
+template <typename T>
+__global__ void __launch_bounds__(256)
+optimal_mark_kernel(const uint64_t *__restrict__ par, unsigned long long n_par, uint64_t v, DevSpec spec,
+                    const uint32_t *__restrict__ tab, const ulonglong2 *__restrict__ slots, unsigned long long mask,
+                    const T *__restrict__ rates2, unsigned long long n2, T zero, uint8_t *__restrict__ marks) {
+    for (unsigned long long r = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; r < n_par;
+         r += (unsigned long long)gridDim.x * blockDim.x) {
+        const uint64_t b = par[r];
+        for (int k = 0; k < 16; ++k) {
+            if ((b >> (4 * k)) & 0xFull) continue;
+            const uint64_t spawned = b | (v << (4 * k));
+            uint64_t mv[4];
+            move_all_dir(tab, spawned, mv);
+            T best = zero;
+            unsigned long long best_index = 0;
+#pragma unroll
+            for (int d = 0; d < 4; ++d) {
+                if (mv[d] == spawned || !is_pattern(mv[d], spec)) continue;
+                const uint64_t key = canonical(mv[d], spec.symm);
+                unsigned long long h = mix64(key) & mask;
+                for (unsigned long long probe = 0; probe <= mask; ++probe) {
+                    const ulonglong2 sl = __ldg(slots + h);
+                    if (sl.x == key) {
+                        const T rate = rates2[sl.y];
+                        if (rate > best) {
+                            best = rate;
+                            best_index = sl.y;
+                        }
+                        break;
+                    }
+                    if (sl.x == 0ull) break;
+                    h = (h + 1) & mask;
+                }
+            }
+            if (best_index < n2) marks[best_index] = 1;
+        }
+    }
+}
+
+// Order-preserving compaction of the marked entries: per 4096-entry tile
+// counts, then (after a scan) the write of the kept keys and rates (SoA) and
+// of their packed records.
+static __global__ void __launch_bounds__(kSortThreads)
+mark_count_kernel(const uint8_t *__restrict__ marks, unsigned long long n, unsigned *__restrict__ tile_cnt) {
+    __shared__ unsigned long long sm[33];
+    const unsigned long long ntiles = (n + kTileKeys - 1) / kTileKeys;
+    for (unsigned long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        unsigned long long c = 0;
+        const unsigned long long base = tile * kTileKeys + threadIdx.x;
+        for (int i = 0; i < kKeysPerThread; ++i) {
+            const unsigned long long idx = base + (unsigned long long)i * kSortThreads;
+            if (idx < n) c += marks[idx] != 0;
+        }
+        unsigned long long tot;
+        block_excl_scan<unsigned long long>(c, sm, &tot);
+        if (threadIdx.x == 0) tile_cnt[tile] = (unsigned)tot;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSortThreads)
+mark_write_kernel(const uint64_t *__restrict__ keys, const T *__restrict__ rates, const uint8_t *__restrict__ marks,
+                  unsigned long long n, const unsigned long long *__restrict__ tile_off, uint64_t *__restrict__ keys_out,
+                  T *__restrict__ rates_out, unsigned char *__restrict__ recs) {
+    __shared__ unsigned long long sm[33];
+    constexpr int rec = 8 + (int)sizeof(T);
+    const unsigned long long ntiles = (n + kTileKeys - 1) / kTileKeys;
+    for (unsigned long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const unsigned long long base = tile * kTileKeys + (unsigned long long)threadIdx.x * kKeysPerThread;
+        unsigned keep = 0, c = 0;
+        for (int i = 0; i < kKeysPerThread; ++i) {
+            const bool k = base + i < n && marks[base + i] != 0;
+            keep |= (unsigned)k << i;
+            c += k;
+        }
+        unsigned long long tot;
+        unsigned long long pos = tile_off[tile] + block_excl_scan<unsigned long long>(c, sm, &tot);
+        for (int i = 0; i < kKeysPerThread; ++i) {
+            if (!(keep >> i & 1u)) continue;
+            const uint64_t key = keys[base + i];
+            const T r = rates[base + i];
+            keys_out[pos] = key;
+            rates_out[pos] = r;
+            if constexpr (rec == 16) {
+                *reinterpret_cast<uint64_t *>(recs + pos * rec) = key;
+                *reinterpret_cast<T *>(recs + pos * rec + 8) = r;
+            } else {
+                uint32_t *w = reinterpret_cast<uint32_t *>(recs + pos * rec);
+                w[0] = (uint32_t)key;
+                w[1] = (uint32_t)(key >> 32);
+                w[2] = *reinterpret_cast<const uint32_t *>(&r);
+            }
+            ++pos;
+        }
+    }
+}
+
 }  // namespace egtb

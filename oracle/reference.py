@@ -81,7 +81,7 @@ def pattern_params(entry: dict, target: int):
 
 
 def make_spec_options(masks, shifts, symm, target, steps, docheck, pathname, dtype="float32", p4=0.1, threads=0,
-                      deletion_threshold=0.0):
+                      deletion_threshold=0.0, optimal_branch_only=False):
     fc = module()
     spec = fc.PatternSpec()
     spec.name = "oracle"
@@ -98,6 +98,7 @@ def make_spec_options(masks, shifts, symm, target, steps, docheck, pathname, dty
     o.direct_io = False
     o.num_threads = int(threads or os.cpu_count() or 4)
     o.deletion_threshold = float(deletion_threshold)
+    o.optimal_branch_only = bool(optimal_branch_only)
     return spec, o
 
 

@@ -82,6 +82,8 @@ def custom_patterns() -> dict:
 
 # builds whose books are rewritten with a deletion threshold (BookSolver.cpp:589-593)
 DELETION_CASES = [("L3", 5, "float32", 0.3), ("442", 6, "uint32", 0.5), ("diag9", 6, "float64", 0.7)]
+# builds followed by the optimal-branch pass (keep_only_optimal_branches_impl, BookSolver.cpp:688-735)
+OPTIMAL_CASES = [("L3", 6, "float32"), ("442", 6, "uint32"), ("diag9", 6, "float64"), ("44", 6, "1-float32")]
 
 SMALL_CASES = [
     ("44", 6, "float32"), ("44", 7, "uint32"),
@@ -104,11 +106,11 @@ def sha(path: str) -> str:
     return h.hexdigest()
 
 
-def run_case(catalog, pat, target, dtype, deletion=0.0):
+def run_case(catalog, pat, target, dtype, deletion=0.0, optimal=False):
     masks, shifts, symm, seeds, steps, docheck, s0 = R.pattern_params(catalog[pat], target)
     T = 2 ** target
     name = f"{pat}_{T}"
-    tag = f"{name}_{dtype}" + (f"_del{deletion}" if deletion else "")
+    tag = f"{name}_{dtype}" + (f"_del{deletion}" if deletion else "") + ("_opt" if optimal else "")
     gdir = R.fresh_dir(os.path.join(WORK, tag, "gen") + "/")
     bdir = R.fresh_dir(os.path.join(WORK, tag, "build") + "/")
     spec, o = R.make_spec_options(masks, shifts, symm, target, steps, docheck, gdir + name + "_", dtype)
@@ -119,7 +121,7 @@ def run_case(catalog, pat, target, dtype, deletion=0.0):
         raw_len.append(os.path.getsize(p) // 8)
         raw_sha.append(sha(p))
     spec, o = R.make_spec_options(masks, shifts, symm, target, steps, docheck, bdir + name + "_", dtype,
-                                  deletion_threshold=deletion)
+                                  deletion_threshold=deletion, optimal_branch_only=optimal)
     R.run_build(seeds, spec, o)
     book_len, book_sha = [], []
     rec = 12 if dtype in ("uint32", "float32", "1-float32") else 16
@@ -136,6 +138,8 @@ def run_case(catalog, pat, target, dtype, deletion=0.0):
         "partial_len": [int(last0.size), int(last1.size)],
         "book_len": book_len, "book_sha256": book_sha,
     }
+    if optimal:
+        case["optimal_branch_only"] = True
     if deletion:
         case["deletion_threshold"] = deletion
         lines = open(bdir + name + "_stats.txt").read().splitlines()
@@ -273,6 +277,14 @@ def main():
         print("case", key, flush=True)
         case, _ = run_case(catalog, pat, target, dtype, thr)
         case["size_class"] = "deletion"
+        cases[key] = case
+    for pat, target, dtype in OPTIMAL_CASES:
+        key = f"{pat}_{2 ** target}_{dtype}_opt"
+        if only and key not in only:
+            continue
+        print("case", key, flush=True)
+        case, _ = run_case(catalog, pat, target, dtype, optimal=True)
+        case["size_class"] = "optimal"
         cases[key] = case
     json.dump(cases, open(cases_path, "w"), indent=0)
     if reader:

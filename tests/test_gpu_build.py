@@ -203,3 +203,62 @@ def test_deletion_threshold_needs_files():
     c_spec, c_opt = spec.to_c(), o.to_c(write_files=False)
     s = H.seeds(case)
     assert N.lib().egtb_build(s.ctypes.data, len(s), ctypes.byref(c_spec), ctypes.byref(c_opt), None) == -7
+
+
+OPTIMAL_CASES = [k for k, v in H.cases().items() if v.get("size_class") == "optimal"]
+
+
+@pytest.mark.parametrize("key", OPTIMAL_CASES)
+def test_optimal_branch_books_bit_exact(key, tmp_root):
+    """optimal_branch_only: after the solve, book i (i >= 21) keeps only the
+    entries that are the best move of a position of thinned book i-2 plus a
+    4 or of thinned book i-1 plus a 2 (BookSolver.cpp:611-735); every book
+    must equal the reference's, and the progress counts 3 * steps."""
+    case = H.cases()[key]
+    F = H.fc()
+    d = H.fresh(os.path.join(tmp_root, "opt_" + key) + "/")
+    spec, o = H.spec_options(case, d + case["pattern_full"] + "_")
+    o.optimal_branch_only = True
+    F.reset_build_progress(0)
+    F.run_pattern_build(H.seeds(case), spec, o)
+    cur, tot = F.get_build_progress()
+    assert tot == 3 * case["steps"] and cur == tot
+    name = case["pattern_full"]
+    for t in range(case["steps"]):
+        assert H.sha(d + f"{name}_{t}.book") == case["book_sha256"][t], (key, t)
+    assert not os.path.exists(d + name + "_optlayer")
+
+
+def test_optimal_branch_resumes_after_marker(tmp_root):
+    """An interrupted pass leaves "<path>optlayer" with the last thinned
+    layer: a rerun solves nothing and thins only the layers above it."""
+    case = H.cases()["L3_64_float32_opt"]
+    F = H.fc()
+    name = case["pattern_full"]
+    done = H.fresh(os.path.join(tmp_root, "opt_done") + "/")
+    spec, o = H.spec_options(case, done + name + "_")
+    o.optimal_branch_only = True
+    F.run_pattern_build(H.seeds(case), spec, o)
+    d = H.fresh(os.path.join(tmp_root, "opt_resume") + "/")
+    spec, o = H.spec_options(case, d + name + "_")
+    F.run_pattern_build(H.seeds(case), spec, o)  # books not thinned
+    for t in range(21, 41):
+        os.replace(done + f"{name}_{t}.book", d + f"{name}_{t}.book")
+    with open(d + name + "_optlayer", "w") as f:
+        f.write("40")
+    o.optimal_branch_only = True
+    F.run_pattern_solve(F.PatternLayer(), F.PatternLayer(), spec, o)
+    for t in range(case["steps"]):
+        assert H.sha(d + f"{name}_{t}.book") == case["book_sha256"][t], t
+    assert not os.path.exists(d + name + "_optlayer")
+
+
+def test_optimal_branch_needs_files():
+    import ctypes
+    case = H.cases()["L3_32_float32"]
+    N = H.pkg()._native
+    spec, o = H.spec_options(case, "/nonexistent/unused_")
+    o.optimal_branch_only = True
+    c_spec, c_opt = spec.to_c(), o.to_c(write_files=False)
+    s = H.seeds(case)
+    assert N.lib().egtb_build(s.ctypes.data, len(s), ctypes.byref(c_spec), ctypes.byref(c_opt), None) == -7
