@@ -509,7 +509,7 @@ struct Run {
                                                  lbits, fbits, src);
         EGTB_CUDA(cudaMemsetAsync(B.hist.p, 0, sizeof(unsigned) * kMaxPasses * 256, s()));
         batch_set_count_kernel<<<1, 1, 0, s()>>>(&dc->cand_count[0], total);
-        sort_hist_kernel<<<R.sm_count * 2, 256, 0, s()>>>(src, &dc->cand_count[0], total, sp, B.hist.as<unsigned>(),
+        sort_hist_kernel<<<R.sm_count * 2, kHistThreads, 0, s()>>>(src, &dc->cand_count[0], total, sp, B.hist.as<unsigned>(),
                                                           B.counters.as<unsigned>(), dc);
         launches += 3;
         for (int q = 0; q < sp.passes; ++q) {

@@ -583,7 +583,7 @@ static void enqueue_sort_layers(Engine &E, const ForwardPlan &P, const std::vect
                                                                       comp));
         EGTB_CUDA(cudaMemsetAsync(E.hist, 0, sizeof(unsigned) * kMaxPasses * 256, s));
         EGTB_LAUNCH(E, set_u64_kernel<<<1, 1, 0, s>>>(&E.ctl->cand_count[0], total));
-        EGTB_LAUNCH(E, sort_hist_kernel<<<E.sm_count * 2, 256, 0, s>>>(comp, &E.ctl->cand_count[0], E.arena_cap, sp,
+        EGTB_LAUNCH(E, sort_hist_kernel<<<E.sm_count * 2, kHistThreads, 0, s>>>(comp, &E.ctl->cand_count[0], E.arena_cap, sp,
                                                                        E.hist, E.counters, E.ctl));
         uint64_t *src = comp, *dst = other;
         for (int q = 0; q < sp.passes; ++q) {
@@ -676,7 +676,7 @@ static uint64_t *enqueue_layer_sort(Engine &E, const SortPlan &sp, const uint64_
                                     const unsigned long long *n_ptr) {
     cudaStream_t s = E.stream;
     EGTB_CUDA(cudaMemsetAsync(E.hist, 0, sizeof(unsigned) * kMaxPasses * 256, s));
-    EGTB_LAUNCH(E, sort_hist_kernel<<<E.sm_count * 2, 256, 0, s>>>(src, n_ptr, E.sort_cap, sp, E.hist, E.counters,
+    EGTB_LAUNCH(E, sort_hist_kernel<<<E.sm_count * 2, kHistThreads, 0, s>>>(src, n_ptr, E.sort_cap, sp, E.hist, E.counters,
                                                                    E.ctl));
     const uint64_t *in = src;
     uint64_t *out = E.sort_buf[0];

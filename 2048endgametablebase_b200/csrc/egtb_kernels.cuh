@@ -31,6 +31,7 @@ struct DevCtl {
     unsigned long long n_unique;        // result of the last unique / compaction
     unsigned long long candidates;      // statistics: keys that reached a sort
     unsigned long long lookups;         // statistics: exact searches in the backward pass
+    unsigned long long expand_next;     // next 32-parent chunk of the running expand launch
     unsigned int err;
     unsigned int pad;
 };
@@ -344,9 +345,13 @@ expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ sta
     __syncthreads();
     int cnt1 = 0, cnt2 = 0;  // keys staged in this warp for layers t+1 and t+2
     unsigned long long probes = 0;
-    const unsigned long long nwarps = (unsigned long long)gridDim.x * (kExpandThreads / 32);
-    for (unsigned long long base = ((unsigned long long)blockIdx.x * (kExpandThreads / 32) + warp) * 32; base < n;
-         base += nwarps * 32) {
+    // warps claim 32-parent chunks as they go, so a warp whose parents have
+    // few empty cells takes more of them (the last block resets the counter)
+    for (;;) {
+        unsigned long long chunk = 0;
+        if (lane == 0) chunk = atomicAdd(&ctl->expand_next, 1ull);
+        const unsigned long long base = __shfl_sync(0xFFFFFFFFu, chunk, 0) * 32;
+        if (base >= n) break;
         const unsigned long long p = base + lane;
         bool active = p < n;
         uint64_t b = active ? stage_par[p] : 0;
@@ -409,6 +414,7 @@ expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ sta
     if (last_block && threadIdx.x == 0) {
         ctl->stage_count[si_par] = 0;
         ctl->blocks_done = 0;
+        ctl->expand_next = 0;
         if (progress) *(volatile unsigned *)progress = progress_value;
     }
 }

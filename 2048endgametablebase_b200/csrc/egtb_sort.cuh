@@ -94,8 +94,14 @@ __device__ __forceinline__ unsigned long long look_back(const unsigned long long
 }
 
 // Digit histograms of every pass; also resets the tile counters of the coming
-// passes and counts the candidates.
-static __global__ void __launch_bounds__(256)
+// passes and counts the candidates. Each thread has kHistKeys loads in flight
+// (coalesced across the block); a digit shared by the whole warp - the common
+// case for the layer digits of composite keys - is counted with one
+// shared-memory atomic, other digits with one atomic per lane.
+constexpr int kHistThreads = 512;
+constexpr int kHistKeys = 8;
+
+static __global__ void __launch_bounds__(kHistThreads, 2)
 sort_hist_kernel(const uint64_t *__restrict__ keys, const unsigned long long *n_ptr, unsigned long long cap, SortPlan sp,
                  unsigned *__restrict__ hist, unsigned *__restrict__ counters, DevCtl *ctl) {
     __shared__ unsigned h[kMaxPasses][256];
@@ -108,15 +114,26 @@ sort_hist_kernel(const uint64_t *__restrict__ keys, const unsigned long long *n_
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const unsigned long long step = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < n; base += step) {
-        const unsigned long long i = base + threadIdx.x;
-        const bool valid = i < n;
-        const uint64_t k = valid ? keys[i] : 0;
-        for (int p = 0; p < sp.passes; ++p) {
-            const unsigned d = valid ? sort_digit(k, sp, p) : 256u;
-            const unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
-            if (valid && (__ffs(peers) - 1) == lane) atomicAdd(&h[p][d], (unsigned)__popc(peers));
+    const unsigned long long span = (unsigned long long)kHistThreads * kHistKeys;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * span; base < n; base += (unsigned long long)gridDim.x * span) {
+        uint64_t k[kHistKeys];
+#pragma unroll
+        for (int r = 0; r < kHistKeys; ++r) {
+            const unsigned long long i = base + (unsigned long long)r * kHistThreads + threadIdx.x;
+            k[r] = i < n ? keys[i] : 0;
+        }
+#pragma unroll
+        for (int r = 0; r < kHistKeys; ++r) {
+            const bool valid = base + (unsigned long long)r * kHistThreads + threadIdx.x < n;
+            for (int p = 0; p < sp.passes; ++p) {
+                const unsigned d = valid ? sort_digit(k[r], sp, p) : 256u;
+                const unsigned d0 = __shfl_sync(0xFFFFFFFFu, d, 0);
+                if (__all_sync(0xFFFFFFFFu, d == d0)) {
+                    if (lane == 0 && d0 < 256u) atomicAdd(&h[p][d0], 32u);
+                } else if (valid) {
+                    atomicAdd(&h[p][d], 1u);
+                }
+            }
         }
     }
     __syncthreads();

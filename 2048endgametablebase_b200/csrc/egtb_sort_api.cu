@@ -89,7 +89,7 @@ static void enqueue_sort_unique_u64(const uint64_t *d_in, size_t n, uint64_t *d_
     else
         EGTB_CUDA(cudaMemcpyAsync(&s.ctl->cand_count[0], &nn, sizeof nn, cudaMemcpyHostToDevice, st));
     const SortPlan sp = full_key_plan();
-    sort_hist_kernel<<<grid, 256, 0, st>>>(d_in, &s.ctl->cand_count[0], n, sp, s.hist, s.counters, s.ctl);
+    sort_hist_kernel<<<grid, kHistThreads, 0, st>>>(d_in, &s.ctl->cand_count[0], n, sp, s.hist, s.counters, s.ctl);
     // 8 passes: in -> out -> tmp -> out ... -> tmp, then unique tmp -> out
     const uint64_t *src = d_in;
     for (int p = 0; p < sp.passes; ++p) {
