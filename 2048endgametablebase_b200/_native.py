@@ -9,7 +9,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libegtb_gpu.so")
+# EGTB_LIB_PATH: load another build of the library (a build kept beside this one)
+LIB_PATH = os.environ.get("EGTB_LIB_PATH") or os.path.join(HERE, "_lib", "libegtb_gpu.so")
 
 EGTB_OK = 0
 ERR_NAMES = {

@@ -52,6 +52,7 @@ struct BatchCtl {
 // Batch-wide counters.
 struct BatchSync {
     unsigned long long blocks_done;
+    unsigned long long next_item;  // next work item of the running expand launch (reset by its last block)
     unsigned long long lookups;
     unsigned err;
     unsigned pad;
@@ -133,11 +134,6 @@ batch_expand_kernel(const BatchTable *__restrict__ T, BatchCtl *C, int n_tables,
         }
     }
     const unsigned long long total = pre[n_tables];
-    const unsigned long long nw = (unsigned long long)gridDim.x * (kBatchThreads / 32);
-    const unsigned long long gw = (unsigned long long)blockIdx.x * (kBatchThreads / 32) + warp;
-    const unsigned long long per = (total + nw - 1) / nw;
-    unsigned long long it = gw * per;
-    const unsigned long long it_end = it + per < total ? it + per : total;
     int cur = -1;
     int cnt1 = 0, cnt2 = 0;
     unsigned long long probes = 0;
@@ -153,8 +149,14 @@ batch_expand_kernel(const BatchTable *__restrict__ T, BatchCtl *C, int n_tables,
         if (lane == 0 && p) atomicAdd(&C[cur].candidates, p);
         probes = 0;
     };
-    for (; it < it_end; ++it) {
-        const int i = (cur >= 0 && it < pre[cur + 1]) ? cur : seg_find(pre, n_tables, it);
+    // warps claim work items (a chunk of one table's parents) as they go, in
+    // increasing order, so consecutive claims mostly stay in one table
+    for (;;) {
+        unsigned long long claim = 0;
+        if (lane == 0) claim = atomicAdd(&sync->next_item, 1ull);
+        const unsigned long long it = __shfl_sync(0xFFFFFFFFu, claim, 0);
+        if (it >= total) break;
+        const int i = (cur >= 0 && it >= pre[cur] && it < pre[cur + 1]) ? cur : seg_find(pre, n_tables, it);
         if (i != cur) {
             if (cur >= 0 && T[cur].steps - 3 >= t) flush_table();
             cur = i;
@@ -228,6 +230,7 @@ batch_expand_kernel(const BatchTable *__restrict__ T, BatchCtl *C, int n_tables,
             if (t < T[i].steps) C[i].stage_count[sp] = 0;
         if (threadIdx.x == 0) {
             sync->blocks_done = 0;
+            sync->next_item = 0;
             if (progress) *(volatile unsigned *)progress = progress_value;
         }
     }
