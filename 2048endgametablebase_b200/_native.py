@@ -155,11 +155,13 @@ _SIGS = {
     "egtb_book_layer_copy": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32, _P, ctypes.c_size_t,
                                             ctypes.POINTER(ctypes.c_uint64)]),
     "egtb_move_all_dir": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, _P]),
+    "egtb_move_all_dir_variant": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, _P]),
     "egtb_canonical": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, ctypes.c_int32, _P]),
     "egtb_apply_sym": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, ctypes.c_int32, _P]),
     "egtb_book_open": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(PatternSpecC),
                                       ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(_P)]),
     "egtb_book_close": (ctypes.c_int, [_P]),
+    "egtb_book_set_variant": (ctypes.c_int, [_P, ctypes.c_int32]),
     "egtb_book_load_all": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
     "egtb_book_lookup": (ctypes.c_int, [_P, _P, ctypes.c_size_t, ctypes.c_int32, _P, _P, _P]),
     "egtb_book_lookup_device": (ctypes.c_int, [_P, _P, ctypes.c_size_t, ctypes.c_int32, _P, _P, _P]),

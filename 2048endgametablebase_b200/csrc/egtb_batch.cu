@@ -235,7 +235,8 @@ std::vector<TablePlan> make_plans(int n, const uint64_t *const *seeds, const uin
         if (o.success_rate_dtype != opts[0].success_rate_dtype)
             throw Error(EGTB_ERR_ARG, "all tables of a batch must use one success_rate_dtype");
         dtype_size(o.success_rate_dtype);
-        if (o.is_variant) throw Error(EGTB_ERR_UNSUPPORTED, "variant boards (wall-merge mover) are not built");
+        if (o.is_variant)
+            throw Error(EGTB_ERR_UNSUPPORTED, "variant boards (wall-merge mover) are built one at a time: use egtb_build");
         if (o.compress) throw Error(EGTB_ERR_UNSUPPORTED, "compressed books (compress) are not built");
         if (o.steps < 3 || o.steps > (1 << 16)) throw Error(EGTB_ERR_ARG, "steps of a batched table must be 3..65536");
         if (o.deletion_threshold > 0.0 || o.optimal_branch_only)

@@ -193,7 +193,7 @@ batch_expand_kernel(const BatchTable *__restrict__ T, BatchCtl *C, int n_tables,
                     uint64_t *const sbuf = stage[warp][v - 1];
                     int c = v == 1 ? cnt1 : cnt2;
                     uint64_t keys[4];
-                    const unsigned kept = spawn_children(tab, mc, k, (uint64_t)v, tb.spec, tb.filter, tb.filter_bits,
+                    const unsigned kept = spawn_children<false>(tab, mc, k, (uint64_t)v, tb.spec, tb.filter, tb.filter_bits,
                                                          keys, probes);
 #pragma unroll
                     for (int d = 0; d < 4; ++d) {
@@ -372,7 +372,7 @@ batch_solve_kernel(const BatchTable *__restrict__ TB, BatchCtl *C, int n_tables,
 #pragma unroll
                     for (int d = 0; d < 4; ++d) {
                         const int j = (v - 1) * 4 + d;
-                        key[j] = canonical(mv[d], tb.spec.symm);
+                        key[j] = canonical<false>(mv[d], tb.spec.symm);  // batched tables: modes 0-3
                         if (mv[d] != s && is_pattern(mv[d], tb.spec)) pend |= 1u << j;
                     }
                 }

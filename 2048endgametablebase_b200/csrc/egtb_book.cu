@@ -11,6 +11,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "egtb_host.h"
@@ -100,6 +101,7 @@ struct egtb_book {
     int dtype = 0;
     int device = 0;
     long long nums_adjust = 0;
+    bool variant = false;  // variant boards: wall-merge moves, the board as given only
     egtb::DevSpec spec;
     std::vector<egtb::BookLayer> layers;
     egtb::LayerDesc *d_desc = nullptr;
@@ -306,7 +308,7 @@ __device__ __forceinline__ int adjusted_slot(int op, int m) {
 // move_on_dic of one position (evaluate_classic_result_candidates,
 // native_core/src/ReaderRuntime.cpp:739-840): four values in direction order
 // up, right, down, left, the mask of directions with a value, and the op used.
-template <typename T, typename OutT>
+template <typename T, typename OutT, bool kVariantModes>
 __device__ __forceinline__ void lookup_position(const LayerDesc *__restrict__ desc, int n_desc, uint64_t board,
                                                 long long nums_adjust, const DevSpec &spec,
                                                 const uint32_t *__restrict__ tab, int op_mode, double scale,
@@ -340,7 +342,7 @@ __device__ __forceinline__ void lookup_position(const LayerDesc *__restrict__ de
 #pragma unroll
         for (int d = 0; d < 4; ++d) {
             if (mv[d] == tb || !is_pattern(mv[d], spec)) continue;
-            const uint64_t key = canonical(mv[d], spec.symm);
+            const uint64_t key = canonical<kVariantModes>(mv[d], spec.symm);
             T r = zero;
             if (L.sorted) {
                 r = L.index ? index_lookup<T>(L.index, L.index_mask, key, zero)
@@ -362,7 +364,7 @@ __device__ __forceinline__ void lookup_position(const LayerDesc *__restrict__ de
     }
 }
 
-template <typename T, typename OutT>
+template <typename T, typename OutT, bool kVariantModes>
 __global__ void __launch_bounds__(256)
 lookup_kernel(const LayerDesc *__restrict__ desc, int n_desc, const uint64_t *__restrict__ pos, size_t n,
               long long nums_adjust, DevSpec spec, const uint32_t *__restrict__ tab, int op_mode, double scale,
@@ -371,7 +373,7 @@ lookup_kernel(const LayerDesc *__restrict__ desc, int n_desc, const uint64_t *__
         OutT out[4];
         uint8_t mask;
         int used;
-        lookup_position<T, OutT>(desc, n_desc, pos[i], nums_adjust, spec, tab, op_mode, scale, round9, zero, out,
+        lookup_position<T, OutT, kVariantModes>(desc, n_desc, pos[i], nums_adjust, spec, tab, op_mode, scale, round9, zero, out,
                                  mask, used);
 #pragma unroll
         for (int d = 0; d < 4; ++d) values4[4 * i + d] = out[d];
@@ -383,7 +385,7 @@ lookup_kernel(const LayerDesc *__restrict__ desc, int n_desc, const uint64_t *__
 // The same over a list of requests whose positions and answers live in
 // caller memory the device can address (registered host memory): request r
 // covers work items prefix[r] .. prefix[r+1]-1.
-template <typename T>
+template <typename T, bool kVariantModes>
 __global__ void __launch_bounds__(256)
 lookup_requests_kernel(const LayerDesc *__restrict__ desc, int n_desc, const ServeReq *__restrict__ reqs, int n_req,
                        long long nums_adjust, DevSpec spec, const uint32_t *__restrict__ tab, int op_mode,
@@ -401,7 +403,7 @@ lookup_requests_kernel(const LayerDesc *__restrict__ desc, int n_desc, const Ser
         float out[4];
         uint8_t mask;
         int used;
-        lookup_position<T, float>(desc, n_desc, q.pos[i], nums_adjust, spec, tab, op_mode, scale, round9, zero, out,
+        lookup_position<T, float, kVariantModes>(desc, n_desc, q.pos[i], nums_adjust, spec, tab, op_mode, scale, round9, zero, out,
                                   mask, used);
         reinterpret_cast<float4 *>(q.out)[i] = make_float4(out[0], out[1], out[2], out[3]);
         if (q.valid) q.valid[i] = mask;
@@ -423,30 +425,39 @@ static double scale_for(int dtype) {
 template <typename OutT>
 static void launch_lookup(egtb_book &b, const uint64_t *d_pos, size_t n, int op_mode, OutT *d_vals, uint8_t *d_valid,
                           int8_t *d_op, cudaStream_t s) {
-    const uint32_t *tab = device_row_table();
+    const uint32_t *tab = device_row_table(b.variant);
+    // a variant reader tries the board as given only (operation_sequence,
+    // ReaderRuntime.cpp:171-182): single operation 0
+    if (b.variant) op_mode = 8;
     const int grid = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
     if (n == 0) return;
     const double scale = scale_for(b.dtype);
     const int r9 = round9_for(b.dtype) ? 1 : 0;
     const int nd = (int)b.layers.size();
-    switch (b.dtype) {
-        case EGTB_DTYPE_UINT32:
-            lookup_kernel<uint32_t, OutT><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
-                                                               scale, r9, 0u, d_vals, d_valid, d_op);
-            break;
-        case EGTB_DTYPE_UINT64:
-            lookup_kernel<uint64_t, OutT><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
-                                                               scale, r9, 0ull, d_vals, d_valid, d_op);
-            break;
-        case EGTB_DTYPE_FLOAT32: case EGTB_DTYPE_1_FLOAT32:
-            lookup_kernel<float, OutT><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
-                                                            scale, r9, (float)dtype_zero(b.dtype), d_vals, d_valid, d_op);
-            break;
-        default:
-            lookup_kernel<double, OutT><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
-                                                             scale, r9, dtype_zero(b.dtype), d_vals, d_valid, d_op);
-            break;
-    }
+    // the kernel build with the variant symmetry modes only for tables that use them
+    auto run = [&](auto variant_modes) {
+        constexpr bool W = decltype(variant_modes)::value;
+        switch (b.dtype) {
+            case EGTB_DTYPE_UINT32:
+                lookup_kernel<uint32_t, OutT, W><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
+                                                                   scale, r9, 0u, d_vals, d_valid, d_op);
+                break;
+            case EGTB_DTYPE_UINT64:
+                lookup_kernel<uint64_t, OutT, W><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
+                                                                   scale, r9, 0ull, d_vals, d_valid, d_op);
+                break;
+            case EGTB_DTYPE_FLOAT32: case EGTB_DTYPE_1_FLOAT32:
+                lookup_kernel<float, OutT, W><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
+                                                                scale, r9, (float)dtype_zero(b.dtype), d_vals, d_valid, d_op);
+                break;
+            default:
+                lookup_kernel<double, OutT, W><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
+                                                                 scale, r9, dtype_zero(b.dtype), d_vals, d_valid, d_op);
+                break;
+        }
+    };
+    if (b.spec.symm >= 4) run(std::true_type{});
+    else run(std::false_type{});
     EGTB_CUDA(cudaGetLastError());
 }
 
@@ -522,6 +533,14 @@ extern "C" int egtb_book_open(const char *dir, const char *pattern_full, int32_t
         b->spec = make_dev_spec(*spec, 0);
         EGTB_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
         *out = b.release();
+    });
+}
+
+extern "C" int egtb_book_set_variant(egtb_book *b, int32_t is_variant) {
+    return guarded([&] {
+        if (!b) throw Error(EGTB_ERR_ARG, "NULL book");
+        std::lock_guard<std::mutex> lk(b->mu);
+        b->variant = is_variant != 0;
     });
 }
 
@@ -639,29 +658,35 @@ void book_lookup_requests(egtb_book *b, const ServeReq *d_reqs, int n_req, unsig
     }
     if (!b->d_desc) throw Error(EGTB_ERR_ARG, "no layers loaded (egtb_book_load_all)");
     if (total == 0) return;
-    const uint32_t *tab = device_row_table();
+    const uint32_t *tab = device_row_table(b->variant);
+    const int op_mode = b->variant ? 8 : 0;  // variant: the board as given only
     const int grid = (int)std::min<unsigned long long>((total + 255) / 256, 148 * 8);
     const double scale = scale_for(b->dtype);
     const int r9 = round9_for(b->dtype) ? 1 : 0;
     const int nd = (int)b->layers.size();
-    switch (b->dtype) {
-        case EGTB_DTYPE_UINT32:
-            lookup_requests_kernel<uint32_t><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
-                                                                 tab, 0, scale, r9, 0u);
-            break;
-        case EGTB_DTYPE_UINT64:
-            lookup_requests_kernel<uint64_t><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
-                                                                 tab, 0, scale, r9, 0ull);
-            break;
-        case EGTB_DTYPE_FLOAT32: case EGTB_DTYPE_1_FLOAT32:
-            lookup_requests_kernel<float><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
-                                                              tab, 0, scale, r9, (float)dtype_zero(b->dtype));
-            break;
-        default:
-            lookup_requests_kernel<double><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
-                                                               tab, 0, scale, r9, dtype_zero(b->dtype));
-            break;
-    }
+    auto run = [&](auto variant_modes) {
+        constexpr bool W = decltype(variant_modes)::value;
+        switch (b->dtype) {
+            case EGTB_DTYPE_UINT32:
+                lookup_requests_kernel<uint32_t, W><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
+                                                                     tab, op_mode, scale, r9, 0u);
+                break;
+            case EGTB_DTYPE_UINT64:
+                lookup_requests_kernel<uint64_t, W><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
+                                                                     tab, op_mode, scale, r9, 0ull);
+                break;
+            case EGTB_DTYPE_FLOAT32: case EGTB_DTYPE_1_FLOAT32:
+                lookup_requests_kernel<float, W><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
+                                                                  tab, op_mode, scale, r9, (float)dtype_zero(b->dtype));
+                break;
+            default:
+                lookup_requests_kernel<double, W><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
+                                                                   tab, op_mode, scale, r9, dtype_zero(b->dtype));
+                break;
+        }
+    };
+    if (b->spec.symm >= 4) run(std::true_type{});
+    else run(std::false_type{});
     EGTB_CUDA(cudaGetLastError());
 }
 }  // namespace egtb

@@ -150,8 +150,12 @@ struct Engine {
         }
         prof_pending.clear();
     }
-    const uint32_t *tab = nullptr;
+    const uint32_t *tab = nullptr;                     // row table of the running build
+    const uint32_t *classic_tab = nullptr, *variant_tab = nullptr;
     std::mutex mu;
+
+    // Select the mover of the next build: classic, or the variant boards' wall merge.
+    void use_mover(bool variant) { tab = variant ? variant_tab : classic_tab; }
 
     // capacities (elements)
     unsigned long long arena_cap = 0, cand_cap = 0;
@@ -208,7 +212,9 @@ struct Engine {
         EGTB_CUDA(cudaSetDevice(dev));
         EGTB_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
         stream = own_stream;
-        tab = device_row_table();
+        classic_tab = device_row_table(false);
+        variant_tab = device_row_table(true);
+        tab = classic_tab;
         cudaDeviceProp prop;
         EGTB_CUDA(cudaGetDeviceProperties(&prop, dev));
         sm_count = prop.multiProcessorCount;
@@ -222,7 +228,8 @@ struct Engine {
         EGTB_CUDA(cudaMalloc(&counters, sizeof(unsigned) * 16));
         int per_sm = 0;
         EGTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel, kSweepThreads, 0));
-        EGTB_CUDA(cudaFuncSetAttribute(expand_dedup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
+        EGTB_CUDA(cudaFuncSetAttribute(expand_dedup_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
+        EGTB_CUDA(cudaFuncSetAttribute(expand_dedup_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
         sweep_grid = sm_count * std::max(1, per_sm);
         progress_device_ptr();
     }
@@ -487,6 +494,18 @@ struct ForwardPlan {
     FreeNibbles free;  // nibbles that vary between keys
 };
 
+// The expand and solve kernels come in two builds: with the variant boards'
+// symmetry modes (min33/min24/min34) and without; a table takes the one its
+// mode needs, so the classic tables' kernels carry no variant code.
+static auto expand_kernel_for(const DevSpec &spec) {
+    return spec.symm >= 4 ? expand_dedup_kernel<true> : expand_dedup_kernel<false>;
+}
+
+template <typename T>
+static auto solve_kernel_for(const DevSpec &spec) {
+    return spec.symm >= 4 ? solve_kernel<T, true> : solve_kernel<T, false>;
+}
+
 // Enqueue forward steps first_step .. steps-2 (one fused expand + dedup
 // kernel each) and close the last two layers. Preconditions on the device:
 // layer first_step-1 in its staging buffer, layer first_step's keys so far in
@@ -495,10 +514,11 @@ static void enqueue_forward(Engine &E, const ForwardPlan &P, unsigned *progress)
     cudaStream_t s = E.stream;
     const int g_exp = E.sm_count;  // one 1024-thread block per SM (the row table fills its shared memory)
     uint64_t *stage[3] = {E.cand[0], E.cand[1], E.tmp};
+    const auto expand = expand_kernel_for(P.spec);
     for (int i = P.first_step; i < P.steps - 1; ++i) {
         const int t = i - 1;
         const int pe = E.prof_begin(K_EXPAND);
-        EGTB_LAUNCH(E, expand_dedup_kernel<<<g_exp, kExpandThreads, kRowSmemBytes, s>>>(
+        EGTB_LAUNCH(E, expand<<<g_exp, kExpandThreads, kRowSmemBytes, s>>>(
                            stage[t % 3], stage[(t + 1) % 3], stage[(t + 2) % 3], t % 3, (t + 1) % 3, (t + 2) % 3,
                            E.arena, E.layer_off, E.layer_len, E.arena_cap, t, P.spec, i > P.docheck ? 1 : 0, E.tab,
                            E.dset[(t + 1) % 3], E.dset[(t + 2) % 3], E.dset_cap - 1, E.cand_cap, E.filter,
@@ -769,10 +789,11 @@ static int run_forward_streamed(Engine &E, const ForwardPlan &P, const uint64_t 
                 }
             });
         };
+        const auto expand = expand_kernel_for(P.spec);
         for (int i = P.first_step; i < steps - 1 && !err; ++i) {
             const int t = i - 1;
             const int pe = E.prof_begin(K_EXPAND);
-            EGTB_LAUNCH(E, expand_dedup_kernel<<<E.sm_count, kExpandThreads, kRowSmemBytes, s>>>(
+            EGTB_LAUNCH(E, expand<<<E.sm_count, kExpandThreads, kRowSmemBytes, s>>>(
                                stage[t % 3], stage[(t + 1) % 3], stage[(t + 2) % 3], t % 3, (t + 1) % 3, (t + 2) % 3,
                                nullptr, E.layer_off, E.layer_len, 0, t, P.spec, i > P.docheck ? 1 : 0, E.tab,
                                E.dset[(t + 1) % 3], E.dset[(t + 2) % 3], E.dset_cap - 1, E.cand_cap, E.filter,
@@ -989,7 +1010,7 @@ static void enqueue_backward(Engine &E, const BackwardPlan &B, const std::vector
         const int ps = E.prof_begin(K_SOLVE);
         ulonglong2 *idx0 = t >= 1 ? E.index[t % 4] : nullptr;
         ulonglong2 *clear = t >= 2 ? E.index[(t - 1) % 4] : nullptr;
-        EGTB_LAUNCH(E, solve_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec,
+        EGTB_LAUNCH(E, solve_kernel_for<T>(B.spec)<<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec,
                                                          t > B.docheck ? 1 : 0, E.tab, B.p4, zero, maxv,
                                                          E.index[(t + 1) % 4], index_slots(len[t + 1]) - 1,
                                                          E.index[(t + 2) % 4], index_slots(len[t + 2]) - 1, E.ctl,
@@ -1065,7 +1086,7 @@ static void backward_write_books(Engine &E, const BackwardPlan &B, const std::ve
         const int ps = E.prof_begin(K_SOLVE);
         ulonglong2 *idx0 = t >= 1 ? E.index[t % 4] : nullptr;
         ulonglong2 *clear = t >= 2 ? E.index[(t - 1) % 4] : nullptr;
-        EGTB_LAUNCH(E, solve_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec,
+        EGTB_LAUNCH(E, solve_kernel_for<T>(B.spec)<<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec,
                                                          t > B.docheck ? 1 : 0, E.tab, B.p4, zero, maxv,
                                                          E.index[(t + 1) % 4], index_slots(len[t + 1]) - 1,
                                                          E.index[(t + 2) % 4], index_slots(len[t + 2]) - 1, E.ctl,
@@ -1250,7 +1271,6 @@ static void check_common(const uint64_t *seeds, size_t n_seeds, const egtb_patte
                          const egtb_run_options *o) {
     if (!spec || !o) throw Error(EGTB_ERR_ARG, "spec and options are required");
     if (n_seeds && !seeds) throw Error(EGTB_ERR_ARG, "seeds pointer is NULL");
-    if (o->is_variant) throw Error(EGTB_ERR_UNSUPPORTED, "variant boards (wall-merge mover) are not built");
     if (o->compress) throw Error(EGTB_ERR_UNSUPPORTED, "compressed books (compress) are not built");
     dtype_size(o->success_rate_dtype);
     if (o->steps > (1 << 20)) throw Error(EGTB_ERR_ARG, "steps out of range");
@@ -1586,10 +1606,10 @@ static void solve_files(Engine &E, const void *d1_recs, size_t n1, const void *d
             enqueue_index_at<T>(E, 2, dlen2, zero, E.index[idx_of[2]]);
             index_fresh = true;
         }
-        EGTB_LAUNCH(E, solve_kernel<T><<<E.sm_count * 8, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, 0, ds,
-                                                                    i > o.docheck_step ? 1 : 0, E.tab, o.spawn_rate4, zero, maxv,
-                                                                    E.index[idx_of[1]], index_slots(dlen1) - 1,
-                                                                    E.index[idx_of[2]], index_slots(dlen2) - 1, E.ctl));
+        EGTB_LAUNCH(E, solve_kernel_for<T>(ds)<<<E.sm_count * 8, 256, 0, s>>>(
+                           E.arena, rates, E.layer_off, E.layer_len, 0, ds, i > o.docheck_step ? 1 : 0, E.tab,
+                           o.spawn_rate4, zero, maxv, E.index[idx_of[1]], index_slots(dlen1) - 1, E.index[idx_of[2]],
+                           index_slots(dlen2) - 1, E.ctl, nullptr, 0, nullptr, 0, nullptr, 0));
         if (i > 0) enqueue_index_at<T>(E, 0, n0, zero, E.index[idx_of[0]]);
         EGTB_LAUNCH(E, splitters_kernel<<<E.sm_count, 256, 0, s>>>(k0, n0, E.split + slot_of[0] * slot / kSplitStride));
         enqueue_pack<T>(E, 0, zero);
@@ -1827,7 +1847,8 @@ static void run_prim(int device, const uint64_t *boards, size_t n, size_t out_pe
 
 EngineRef engine_ref(int device) {
     Engine &E = engine_for(device);
-    return EngineRef{&E.mu, E.device, &E.stream, E.tab, E.sm_count, E.sweep_grid};
+    // the batched build moves every table with the classic rule
+    return EngineRef{&E.mu, E.device, &E.stream, E.classic_tab, E.sm_count, E.sweep_grid};
 }
 
 uint64_t pattern_pinned_nibbles(const egtb_pattern_spec &s) { return pinned_nibbles(s); }
@@ -1935,6 +1956,7 @@ extern "C" int egtb_generate(const uint64_t *seeds, size_t n_seeds, const egtb_p
         check_common(seeds, n_seeds, spec, options);
         Engine &E = engine_for(options->device);
         std::lock_guard<std::mutex> lk(E.mu);
+        E.use_mover(options->is_variant != 0);  // VBoardMover for variant boards (BookSolver.cpp:792-819)
         int st = 0;
         if (stats) std::memset(stats, 0, sizeof *stats);
         dispatch_dtype(options->success_rate_dtype, [&](auto z) {
@@ -1952,6 +1974,7 @@ extern "C" int egtb_solve(const void *d1_records, size_t n1, const void *d2_reco
         if ((n1 && !d1_records) || (n2 && !d2_records)) throw Error(EGTB_ERR_ARG, "NULL record buffer");
         Engine &E = engine_for(options->device);
         std::lock_guard<std::mutex> lk(E.mu);
+        E.use_mover(options->is_variant != 0);  // VBoardMover for variant boards (BookSolver.cpp:792-819)
         if (stats) std::memset(stats, 0, sizeof *stats);
         dispatch_dtype(options->success_rate_dtype, [&](auto z) {
             using T = decltype(z);
@@ -1971,6 +1994,7 @@ extern "C" int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_patt
                                                                 : 0));
         Engine &E = engine_for(options->device);
         std::lock_guard<std::mutex> lk(E.mu);
+        E.use_mover(options->is_variant != 0);  // VBoardMover for variant boards (BookSolver.cpp:792-819)
         if (stats) std::memset(stats, 0, sizeof *stats);
         const bool resume = options->write_files && any_layer_file(*options);
         dispatch_dtype(options->success_rate_dtype, [&](auto z) {
@@ -2035,14 +2059,22 @@ extern "C" int egtb_book_layer_copy(int device, int32_t layer, void *dst, size_t
 extern "C" int egtb_move_all_dir(int device, const uint64_t *boards, size_t n, uint64_t *out4) {
     return guarded([&] {
         run_prim(device, boards, n, 4, out4, [&](Engine &E, uint64_t *din, uint64_t *dout) {
-            EGTB_LAUNCH(E, prim_moves_kernel<<<E.sm_count * 4, 256, 0, E.stream>>>(E.tab, din, n, dout));
+            EGTB_LAUNCH(E, prim_moves_kernel<<<E.sm_count * 4, 256, 0, E.stream>>>(E.classic_tab, din, n, dout));
+        });
+    });
+}
+
+extern "C" int egtb_move_all_dir_variant(int device, const uint64_t *boards, size_t n, uint64_t *out4) {
+    return guarded([&] {
+        run_prim(device, boards, n, 4, out4, [&](Engine &E, uint64_t *din, uint64_t *dout) {
+            EGTB_LAUNCH(E, prim_moves_kernel<<<E.sm_count * 4, 256, 0, E.stream>>>(E.variant_tab, din, n, dout));
         });
     });
 }
 
 extern "C" int egtb_canonical(int device, const uint64_t *boards, size_t n, int32_t symm_mode, uint64_t *out) {
     return guarded([&] {
-        if (symm_mode < 0 || symm_mode > 3) throw Error(EGTB_ERR_UNSUPPORTED, "symmetry mode not built");
+        if (symm_mode < 0 || symm_mode > 6) throw Error(EGTB_ERR_ARG, "symmetry mode out of range");
         run_prim(device, boards, n, 1, out, [&](Engine &E, uint64_t *din, uint64_t *dout) {
             EGTB_LAUNCH(E, prim_canonical_kernel<<<E.sm_count * 4, 256, 0, E.stream>>>(din, n, symm_mode, dout));
         });

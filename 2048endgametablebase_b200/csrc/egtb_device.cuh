@@ -75,12 +75,68 @@ __device__ __forceinline__ uint64_t apply_sym(uint64_t b, int idx) {
     }
 }
 
+// Swap rows 0 and 2 (row 0 is the high 16 bits), all four columns.
+__device__ __forceinline__ uint64_t swap_rows02(uint64_t b) {
+    return (b & 0x0000FFFF0000FFFFull) | ((b >> 32) & 0x00000000FFFF0000ull) | ((b << 32) & 0xFFFF000000000000ull);
+}
+
+// Swap columns 0 and 2 (column 0 is the high nibble of a row), all four rows.
+__device__ __forceinline__ uint64_t swap_cols02(uint64_t b) {
+    return (b & 0x0F0F0F0F0F0F0F0Full) | ((b >> 8) & 0x00F000F000F000F0ull) | ((b << 8) & 0xF000F000F000F000ull);
+}
+
+// Bit offset of cell (r, c): row r (0 = high 16 bits), column c (0 = high nibble).
+__host__ __device__ constexpr int cell_shift(int r, int c) { return 60 - 16 * r - 4 * c; }
+
+// A symmetry of the top-left 3x3 block, every other cell fixed: kind 0 the
+// transpose (r,c)->(c,r), 1 the anti-transpose (2-c,2-r), 2 the half turn
+// (2-r,2-c), 3 and 4 the quarter turns (c,2-r) and (2-c,r).
+template <int kKind>
+__device__ __forceinline__ uint64_t block33(uint64_t b) {
+    uint64_t o = b & 0x000F000F000FFFFFull;  // column 3 of rows 0-2 and row 3
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int R = kKind == 0 ? c : kKind == 1 ? 2 - c : kKind == 2 ? 2 - r : kKind == 3 ? c : 2 - c;
+            const int C = kKind == 0 ? r : kKind == 1 ? 2 - r : kKind == 2 ? 2 - c : kKind == 3 ? 2 - r : r;
+            o |= ((b >> cell_shift(r, c)) & 0xFull) << cell_shift(R, C);
+        }
+    }
+    return o;
+}
+
 // Minimum over the symmetry group (canonical_by_mode,
-// native_core/include/SymmetryUtils.h:31-49).
+// native_core/include/SymmetryUtils.h:31-49; the min33/min24/min34 groups of
+// the variant boards, native_core/include/Calculator.h:192-203): 4 min33, the
+// eight symmetries of the 3x3 block (its row and column swaps over whole
+// rows and columns); 5 min24, the mirrors and half turn of the whole board;
+// 6 min34, the column mirror and the row-0/row-2 swap of the 3x4 block and
+// their product.
+// Modes 4-6 (variant boards only).
+__device__ __forceinline__ uint64_t canonical_variant(uint64_t b, int symm) {
+    if (symm == 4) {
+        uint64_t m = umin(b, umin(swap_cols02(b), swap_rows02(b)));
+        m = umin(m, umin(block33<0>(b), block33<1>(b)));
+        m = umin(m, block33<2>(b));
+        return umin(m, umin(block33<3>(b), block33<4>(b)));
+    }
+    const uint64_t c = mirror_cols(b);
+    if (symm == 5) return umin(umin(b, c), umin(mirror_rows(b), mirror_rows(c)));
+    return umin(umin(b, c), umin(swap_rows02(b), swap_rows02(c)));
+}
+
+// kVariantModes = false leaves modes 4-6 out of the code (the hot kernels
+// are instantiated both ways and launched by the table's mode): the caller
+// then guarantees symm < 4.
+template <bool kVariantModes = true>
 __device__ __forceinline__ uint64_t canonical(uint64_t b, int symm) {
     if (symm == 0) return b;
     if (symm == 2) return umin(b, transpose(b));
     if (symm == 3) return umin(b, mirror_cols(b));
+    if constexpr (kVariantModes) {
+        if (symm >= 4) return canonical_variant(b, symm);
+    }
     // full group: b and its transpose, each with the four row/column mirrors
     uint64_t t = transpose(b);
     uint64_t m = umin(b, t);

@@ -34,28 +34,44 @@ extern "C" int egtb_last_error(char *buf, size_t len) {
 
 namespace egtb {
 
-// One row moved toward column 0 (reverse = false) or column 3: slide the
-// tiles, merge each adjacent equal pair once, first pair first; 0xF (32768)
-// never merges (native_core/include/BoardMover.h:6-55).
-static uint32_t row_after_move(uint32_t row, bool reverse) {
+// One row moved toward column 0 (reverse = false) or column 3.
+// Classic (walls = false): slide the tiles, merge each adjacent equal pair
+// once, first pair first; 0xF (32768) slides but never merges
+// (native_core/include/BoardMover.h:6-55).
+// Variant (walls = true): 0xF cells are walls that stay put; the tiles of
+// each stretch between walls slide and merge within it the same way
+// (WallMergePolicy, native_core/include/VBoardMover.h:7-76).
+static uint32_t row_after_move(uint32_t row, bool reverse, bool walls) {
     int cell[4];
     for (int i = 0; i < 4; ++i) cell[i] = (row >> (12 - 4 * i)) & 0xF;  // column 0 first
     if (reverse) {
         std::swap(cell[0], cell[3]);
         std::swap(cell[1], cell[2]);
     }
-    int out[4] = {0, 0, 0, 0}, m = 0, pending = 0;
-    for (int i = 0; i < 4; ++i) {
-        if (!cell[i]) continue;
-        if (pending && pending == cell[i] && pending != 0xF) {
-            out[m++] = pending + 1;
-            pending = 0;
-        } else {
-            if (pending) out[m++] = pending;
-            pending = cell[i];
+    int out[4] = {0, 0, 0, 0};
+    int seg = 0;  // first cell of the current stretch
+    while (seg < 4) {
+        if (walls && cell[seg] == 0xF) {
+            out[seg] = 0xF;
+            ++seg;
+            continue;
         }
+        int end = seg;
+        while (end < 4 && !(walls && cell[end] == 0xF)) ++end;
+        int m = seg, pending = 0;
+        for (int i = seg; i < end; ++i) {
+            if (!cell[i]) continue;
+            if (pending && pending == cell[i] && pending != 0xF) {
+                out[m++] = pending + 1;
+                pending = 0;
+            } else {
+                if (pending) out[m++] = pending;
+                pending = cell[i];
+            }
+        }
+        if (pending) out[m++] = pending;
+        seg = end;
     }
-    if (pending) out[m++] = pending;
     if (reverse) {
         std::swap(out[0], out[3]);
         std::swap(out[1], out[2]);
@@ -65,33 +81,35 @@ static uint32_t row_after_move(uint32_t row, bool reverse) {
     return r;
 }
 
-const std::vector<uint32_t> &host_row_tables() {
-    static const std::vector<uint32_t> tab = [] {
+const std::vector<uint32_t> &host_row_tables(bool variant) {
+    auto make = [](bool walls) {
         std::vector<uint32_t> t(65536);
         for (uint32_t r = 0; r < 65536; ++r) {
-            const uint32_t l = row_after_move(r, false) ^ r;
-            const uint32_t rr = row_after_move(r, true) ^ r;
+            const uint32_t l = row_after_move(r, false, walls) ^ r;
+            const uint32_t rr = row_after_move(r, true, walls) ^ r;
             t[r] = l | (rr << 16);
         }
         return t;
-    }();
-    return tab;
+    };
+    static const std::vector<uint32_t> classic = make(false), walled = make(true);
+    return variant ? walled : classic;
 }
 
-const uint32_t *device_row_table() {
+const uint32_t *device_row_table(bool variant) {
     static std::mutex mu;
-    static std::vector<uint32_t *> per_device;
+    static std::vector<uint32_t *> per_device[2];
     int dev = 0;
     EGTB_CUDA(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lk(mu);
-    if ((int)per_device.size() <= dev) per_device.resize(dev + 1, nullptr);
-    if (!per_device[dev]) {
+    std::vector<uint32_t *> &v = per_device[variant ? 1 : 0];
+    if ((int)v.size() <= dev) v.resize(dev + 1, nullptr);
+    if (!v[dev]) {
         uint32_t *p = nullptr;
         EGTB_CUDA(cudaMalloc(&p, 65536 * sizeof(uint32_t)));
-        EGTB_CUDA(cudaMemcpy(p, host_row_tables().data(), 65536 * sizeof(uint32_t), cudaMemcpyHostToDevice));
-        per_device[dev] = p;
+        EGTB_CUDA(cudaMemcpy(p, host_row_tables(variant).data(), 65536 * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        v[dev] = p;
     }
-    return per_device[dev];
+    return v[dev];
 }
 
 DevSpec make_dev_spec(const egtb_pattern_spec &s, int target) {
@@ -99,9 +117,8 @@ DevSpec make_dev_spec(const egtb_pattern_spec &s, int target) {
     std::memset(&d, 0, sizeof d);
     if (s.n_masks < 0 || s.n_masks > kMaxMasks) throw Error(EGTB_ERR_ARG, "n_masks out of range");
     if (s.n_shifts < 0 || s.n_shifts > 16) throw Error(EGTB_ERR_ARG, "n_shifts out of range");
-    if (s.symm_mode < 0 || s.symm_mode > 3)
-        throw Error(EGTB_ERR_UNSUPPORTED, "symmetry mode " + std::to_string(s.symm_mode) +
-                                              " (min33/min24/min34 belong to the variant boards) is not built");
+    if (s.symm_mode < 0 || s.symm_mode > 6)
+        throw Error(EGTB_ERR_ARG, "symmetry mode " + std::to_string(s.symm_mode) + " out of range");
     d.n_masks = s.n_masks;
     for (int i = 0; i < s.n_masks; ++i) d.masks[i] = s.pattern_masks[i];
     d.symm = s.symm_mode;

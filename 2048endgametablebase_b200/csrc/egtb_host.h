@@ -53,11 +53,13 @@ int guarded(F &&f) {
 }
 
 // Row-move XOR delta table (low 16 bits toward column 0, high 16 toward
-// column 3) from the merge rule of native_core/include/BoardMover.h:6-55.
-const std::vector<uint32_t> &host_row_tables();
+// column 3) from the classic merge rule (native_core/include/BoardMover.h:6-55)
+// or, with variant, the wall-merge rule of the variant boards
+// (native_core/include/VBoardMover.h:7-76).
+const std::vector<uint32_t> &host_row_tables(bool variant = false);
 
-// Device copy of the row table on the current device (created once per device).
-const uint32_t *device_row_table();
+// Device copy of a row table on the current device (created once per device).
+const uint32_t *device_row_table(bool variant = false);
 
 DevSpec make_dev_spec(const egtb_pattern_spec &s, int target);
 

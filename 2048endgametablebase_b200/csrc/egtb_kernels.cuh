@@ -97,7 +97,7 @@ constexpr int kStage = 64;  // per-warp staging slots per stream
 // seen (filter_bits 0: no filter). The four filter slots are read before any
 // is written, so their loads are in flight together. Returns the kept moves
 // as a 4-bit mask; *probes counts the children that reached the filter.
-template <typename Rows>
+template <bool kVariantModes, typename Rows>
 __device__ __forceinline__ unsigned spawn_children(const Rows &rows, const MoveCtx &mc, int k, uint64_t v,
                                                    const DevSpec &spec, uint64_t *filter, int filter_bits,
                                                    uint64_t key[4], unsigned long long &probes) {
@@ -108,7 +108,7 @@ __device__ __forceinline__ unsigned spawn_children(const Rows &rows, const MoveC
     for (int d = 0; d < 4; ++d) {
         key[d] = 0;
         if (k >= 0 && mv[d] != s && is_pattern(mv[d], spec)) {
-            key[d] = canonical(mv[d], spec.symm);
+            key[d] = canonical<kVariantModes>(mv[d], spec.symm);
             keep |= 1u << d;
         }
     }
@@ -301,7 +301,8 @@ __device__ __forceinline__ void stage_flush_dedup(uint64_t *stage, int &count, u
 // next 16-aligned offset, capacity check); its last block empties layer t's
 // staging buffer for layer t+3. Sets rotate over three buffers (layer L in
 // set L % 3): this step zeroes layer t's set, which layer t+3 fills next.
-static __global__ void __launch_bounds__(kExpandThreads, 1)
+template <bool kVariantModes>
+__global__ void __launch_bounds__(kExpandThreads, 1)
 expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ stage1, uint64_t *__restrict__ stage2,
                     int si_par, int si1, int si2, uint64_t *__restrict__ arena,
                     unsigned long long *__restrict__ layer_off, unsigned long long *__restrict__ layer_len,
@@ -377,7 +378,8 @@ expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ sta
                 // a direct-mapped filter drops most repeats with one load; a
                 // key it holds has already been staged for its set
                 uint64_t keys[4];
-                const unsigned kept = spawn_children(rows, mc, k, (uint64_t)v, spec, filter, filter_bits, keys, probes);
+                const unsigned kept =
+                    spawn_children<kVariantModes>(rows, mc, k, (uint64_t)v, spec, filter, filter_bits, keys, probes);
 #pragma unroll
                 for (int d = 0; d < 4; ++d) {
                     const bool keep = kept >> d & 1u;
@@ -622,7 +624,7 @@ __device__ __forceinline__ void index_insert_zero(ulonglong2 *slots, unsigned lo
 // With idx0, layer t's live entries also enter its rate index (mask m0) for
 // the solves of layers t-1 and t-2; with clear_idx, this launch zeroes
 // clear_slots slots of another (unused) index for the next launch's inserts.
-template <typename T>
+template <typename T, bool kVariantModes>
 __global__ void __launch_bounds__(256, 4)
 solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
              const unsigned long long *__restrict__ layer_off, const unsigned long long *__restrict__ layer_len,
@@ -669,7 +671,7 @@ solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
 #pragma unroll
                 for (int d = 0; d < 4; ++d) {
                     const int j = (v - 1) * 4 + d;
-                    key[j] = canonical(mv[d], spec.symm);
+                    key[j] = canonical<kVariantModes>(mv[d], spec.symm);
                     if (mv[d] != s && is_pattern(mv[d], spec)) pend |= 1u << j;
                 }
             }

@@ -294,12 +294,11 @@ class ClassicBookReader:
         self.is_variant_ = bool(is_variant)
         self.prefer_max_result_ = pattern_spec.name in ("4442ff", "4442f", "4tiler")
         self.last_operation_index_ = 0
-        if self.is_variant_:
-            raise RuntimeError("variant boards (wall-merge mover) are not built")
 
     def _book(self, directory: str, pattern_full: str, dtype: str, nums_adjust: int):
         key = (os.path.abspath(directory), pattern_full, dtype_code(dtype), int(nums_adjust),
-               tuple(int(m) for m in self.spec_.pattern_masks), int(self.spec_.symm_mode), _device())
+               tuple(int(m) for m in self.spec_.pattern_masks), int(self.spec_.symm_mode), _device(),
+               self.is_variant_)
         h = ClassicBookReader._books.get(key)
         if h is None:
             spec = self.spec_.to_c()
@@ -307,6 +306,8 @@ class ClassicBookReader:
             N.check(N.lib().egtb_book_open(directory.encode(), pattern_full.encode(), dtype_code(dtype),
                                            ctypes.byref(spec), int(nums_adjust), _device(), ctypes.byref(ptr)))
             h = ptr
+            if self.is_variant_:
+                N.check(N.lib().egtb_book_set_variant(h, 1))
             ClassicBookReader._books[key] = h
         return h
 
@@ -355,7 +356,8 @@ class ClassicBookReader:
                     self.last_operation_index_ = op
                     return dict(self._sorted_entries(op, vals, mask)), dtype
                 continue
-            for op_index in [self.last_operation_index_] + list(range(8)):
+            ops = [0] if self.is_variant_ else [self.last_operation_index_] + list(range(8))
+            for op_index in ops:
                 vals, mask, op = self._evaluate(book, encoded, 8 + op_index)
                 if op < 0:
                     continue

@@ -197,6 +197,11 @@ EGTB_API int egtb_book_layer_copy(int device, int32_t layer, void *dst, size_t d
  * (move_all_dir native_core/include/CommonMover.h:136-139; canonical_by_mode
  * SymmetryUtils.h:31-49; apply_sym_like SymmetryUtils.h:9-29). */
 EGTB_API int egtb_move_all_dir(int device, const uint64_t *boards, size_t n, uint64_t *out4);
+/* move_all_dir of the variant boards' mover (VBoardMover,
+ * native_core/include/VBoardMover.h:79 over CommonMover.h:136-139): 0xF cells
+ * are walls, tiles slide and merge between them. */
+EGTB_API int egtb_move_all_dir_variant(int device, const uint64_t *boards, size_t n, uint64_t *out4);
+/* symm_mode 0-6: identity, full, diagonal, horizontal, min33, min24, min34. */
 EGTB_API int egtb_canonical(int device, const uint64_t *boards, size_t n, int32_t symm_mode, uint64_t *out);
 EGTB_API int egtb_apply_sym(int device, const uint64_t *boards, size_t n, int32_t symm_index, uint64_t *out);
 
@@ -233,6 +238,13 @@ typedef struct egtb_book egtb_book;
 EGTB_API int egtb_book_open(const char *dir, const char *pattern_full, int32_t dtype, const egtb_pattern_spec *spec,
                    int64_t nums_adjust, int32_t device, egtb_book **out);
 EGTB_API int egtb_book_close(egtb_book *book);
+
+/* Mark the book as one of variant boards (ClassicBookReader(spec, is_variant),
+ * native_core/src/ReaderRuntime.cpp:1050-1067): its lookups move with the
+ * wall-merge rule (VBoardMover, native_core/include/VBoardMover.h) and try
+ * the board as given only (operation_sequence, ReaderRuntime.cpp:171-182),
+ * whatever last_op says. */
+EGTB_API int egtb_book_set_variant(egtb_book *book, int32_t is_variant);
 
 /* Load every book layer of the table now (otherwise loaded on first lookup). */
 EGTB_API int egtb_book_load_all(egtb_book *book, int32_t *layers_loaded);

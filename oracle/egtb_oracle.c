@@ -20,30 +20,45 @@
 
 /* ---------------------------------------------------------------- rows --- */
 
-static uint16_t g_left[65536], g_right[65536];
+static uint16_t g_left[2][65536], g_right[2][65536];  /* [0] classic, [1] variant */
 static int g_tables_ready = 0;
 
 /* One row moved toward column 0 (reverse=0) or column 3 (reverse=1).
- * Restates StandardMergePolicy::_internal_merge, native_core/include/BoardMover.h:6-55:
- * slide non-empty cells, merge each adjacent equal pair once (first pair
- * first), the 32768 tile (nibble 0xF) never merges. Works on log2 nibbles. */
-static uint16_t row_move(uint16_t row, int reverse) {
-    int line[4], nz[4], out[4] = {0, 0, 0, 0};
-    int n = 0, m = 0;
+ * walls=0 restates StandardMergePolicy::_internal_merge,
+ * native_core/include/BoardMover.h:6-55: slide non-empty cells, merge each
+ * adjacent equal pair once (first pair first), the 32768 tile (nibble 0xF)
+ * never merges. walls=1 restates WallMergePolicy::_internal_merge,
+ * native_core/include/VBoardMover.h:7-76: 0xF cells stay where they are and
+ * split the row into stretches, each moved like a row of its own.
+ * Works on log2 nibbles. */
+static uint16_t row_move(uint16_t row, int reverse, int walls) {
+    int line[4], out[4] = {0, 0, 0, 0};
     for (int i = 0; i < 4; ++i) line[i] = (row >> (4 * (3 - i))) & 0xF;
     if (reverse) {
         int t = line[0]; line[0] = line[3]; line[3] = t;
         t = line[1]; line[1] = line[2]; line[2] = t;
     }
-    for (int i = 0; i < 4; ++i)
-        if (line[i]) nz[n++] = line[i];
-    for (int i = 0; i < n; ++i) {
-        if (i + 1 < n && nz[i] == nz[i + 1] && nz[i] != 0xF) {
-            out[m++] = nz[i] + 1;
-            ++i;
-        } else {
-            out[m++] = nz[i];
+    int lo = 0;
+    while (lo < 4) {
+        if (walls && line[lo] == 0xF) {
+            out[lo] = 0xF;
+            ++lo;
+            continue;
         }
+        int hi = lo, nz[4], n = 0, m = lo;
+        while (hi < 4 && !(walls && line[hi] == 0xF)) {
+            if (line[hi]) nz[n++] = line[hi];
+            ++hi;
+        }
+        for (int i = 0; i < n; ++i) {
+            if (i + 1 < n && nz[i] == nz[i + 1] && nz[i] != 0xF) {
+                out[m++] = nz[i] + 1;
+                ++i;
+            } else {
+                out[m++] = nz[i];
+            }
+        }
+        lo = hi;
     }
     if (reverse) {
         int t = out[0]; out[0] = out[3]; out[3] = t;
@@ -57,17 +72,24 @@ static uint16_t row_move(uint16_t row, int reverse) {
 /* XOR-delta row tables, native_core/include/CommonMover.h:87-94 */
 static void init_tables(void) {
     if (g_tables_ready) return;
-    for (uint32_t r = 0; r < 65536; ++r) {
-        g_left[r] = (uint16_t)(row_move((uint16_t)r, 0) ^ r);
-        g_right[r] = (uint16_t)(row_move((uint16_t)r, 1) ^ r);
-    }
+    for (int w = 0; w < 2; ++w)
+        for (uint32_t r = 0; r < 65536; ++r) {
+            g_left[w][r] = (uint16_t)(row_move((uint16_t)r, 0, w) ^ r);
+            g_right[w][r] = (uint16_t)(row_move((uint16_t)r, 1, w) ^ r);
+        }
     g_tables_ready = 1;
 }
 
 void or_row_tables(uint16_t *left_xor, uint16_t *right_xor) {
     init_tables();
-    memcpy(left_xor, g_left, sizeof g_left);
-    memcpy(right_xor, g_right, sizeof g_right);
+    memcpy(left_xor, g_left[0], sizeof g_left[0]);
+    memcpy(right_xor, g_right[0], sizeof g_right[0]);
+}
+
+void or_row_tables_variant(uint16_t *left_xor, uint16_t *right_xor) {
+    init_tables();
+    memcpy(left_xor, g_left[1], sizeof g_left[1]);
+    memcpy(right_xor, g_right[1], sizeof g_right[1]);
 }
 
 /* ------------------------------------------------------------ symmetry --- */
@@ -100,12 +122,53 @@ uint64_t or_apply_sym(uint64_t b, int idx) {
     return o;
 }
 
+/* A cell map on the board: cell (r,c) goes to (R,C) = f(r,c); cells the map
+ * does not move keep their value. */
+static uint64_t cell_map(uint64_t b, int kind) {
+    uint64_t o = 0;
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            int R = r, C = c;
+            const int in33 = r < 3 && c < 3;
+            switch (kind) {
+                case 0: if (c == 0) C = 2; else if (c == 2) C = 0; break;       /* columns 0 <-> 2 */
+                case 1: if (r == 0) R = 2; else if (r == 2) R = 0; break;       /* rows 0 <-> 2 */
+                case 2: if (in33) { R = c; C = r; } break;                      /* 3x3 transpose */
+                case 3: if (in33) { R = 2 - c; C = 2 - r; } break;              /* 3x3 anti-transpose */
+                case 4: if (in33) { R = 2 - r; C = 2 - c; } break;              /* 3x3 half turn */
+                case 5: if (in33) { R = c; C = 2 - r; } break;                  /* 3x3 quarter turn */
+                case 6: if (in33) { R = 2 - c; C = r; } break;                  /* 3x3 quarter turn */
+                default: break;
+            }
+            o |= put(nib(b, r, c), R, C);
+        }
+    return o;
+}
+
+static inline uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+
 /* canonical_by_mode, native_core/include/SymmetryUtils.h:31-49 with
- * Calculator::canonical_{identity,full,diagonal,horizontal}
- * (native_core/include/Calculator.h:80-97): the minimum over the group. */
+ * Calculator::canonical_{identity,full,diagonal,horizontal,min33,min24,min34}
+ * (native_core/include/Calculator.h:80-97, 192-203): the minimum over the
+ * group. min33: the eight symmetries of the top-left 3x3 block, its column
+ * and row swaps taken over whole columns and rows; min24: the mirrors and
+ * half turn of the board; min34: the column mirror, the swap of rows 0 and
+ * 2, and both. */
 uint64_t or_canonical(uint64_t b, int mode) {
     uint64_t m = b, t;
     switch (mode) {
+        case OR_SYM_MIN33:
+            for (int k = 0; k < 7; ++k) m = umin64(m, cell_map(b, k));
+            return m;
+        case OR_SYM_MIN24:
+            m = umin64(m, or_apply_sym(b, 1));
+            m = umin64(m, or_apply_sym(b, 2));
+            return umin64(m, or_apply_sym(b, 5));
+        case OR_SYM_MIN34:
+            t = or_apply_sym(b, 1);
+            m = umin64(m, t);
+            m = umin64(m, cell_map(b, 1));
+            return umin64(m, cell_map(t, 1));
         case OR_SYM_FULL:
             for (int i = 1; i < 8; ++i) {
                 t = or_apply_sym(b, i);
@@ -134,18 +197,26 @@ static inline uint64_t rows_apply(uint64_t b, const uint16_t *tab) {
     return o;
 }
 
-/* move_all_dir: {left, right, up, down}, native_core/include/CommonMover.h:136-139 */
-void or_move_all_dir(uint64_t b, uint64_t out[4]) {
+/* move_all_dir: {left, right, up, down}, native_core/include/CommonMover.h:136-139,
+ * with the classic (BoardMover) or the variant (VBoardMover) row rule */
+static void move_all_dir_w(uint64_t b, uint64_t out[4], int variant) {
     init_tables();
+    const int w = variant ? 1 : 0;
     uint64_t t = transpose(b);
-    out[0] = rows_apply(b, g_left);
-    out[1] = rows_apply(b, g_right);
-    out[2] = transpose(rows_apply(t, g_left));
-    out[3] = transpose(rows_apply(t, g_right));
+    out[0] = rows_apply(b, g_left[w]);
+    out[1] = rows_apply(b, g_right[w]);
+    out[2] = transpose(rows_apply(t, g_left[w]));
+    out[3] = transpose(rows_apply(t, g_right[w]));
 }
 
+void or_move_all_dir(uint64_t b, uint64_t out[4]) { move_all_dir_w(b, out, 0); }
+
 void or_move_all_dir_batch(const uint64_t *b, size_t n, uint64_t *out4) {
-    for (size_t i = 0; i < n; ++i) or_move_all_dir(b[i], out4 + 4 * i);
+    for (size_t i = 0; i < n; ++i) move_all_dir_w(b[i], out4 + 4 * i, 0);
+}
+
+void or_move_all_dir_variant_batch(const uint64_t *b, size_t n, uint64_t *out4) {
+    for (size_t i = 0; i < n; ++i) move_all_dir_w(b[i], out4 + 4 * i, 1);
 }
 
 void or_canonical_batch(const uint64_t *b, size_t n, int mode, uint64_t *out) {
@@ -187,7 +258,7 @@ size_t or_expand(const uint64_t *parents, size_t n, const or_spec *spec, int tar
             if ((b >> (4 * i)) & 0xF) continue;
             for (uint64_t v = 1; v <= 2; ++v) {
                 uint64_t s = b | (v << (4 * i));
-                or_move_all_dir(s, mv);
+                move_all_dir_w(s, mv, spec->is_variant);
                 for (int d = 0; d < 4; ++d) {
                     if (mv[d] == s || !or_is_pattern(mv[d], spec)) continue;
                     uint64_t k = or_canonical(mv[d], spec->symm_mode);
@@ -391,7 +462,7 @@ DEFINE_LOOKUP(double, lookup_f64)
                 for (uint64_t v = 1; v <= 2; ++v) {                                              \
                     uint64_t s = b | (v << (4 * i));                                             \
                     T best = zero;                                                               \
-                    or_move_all_dir(s, mv);                                                      \
+                    move_all_dir_w(s, mv, spec->is_variant);                                     \
                     for (int d = 0; d < 4; ++d) {                                                \
                         if (mv[d] == s || !or_is_pattern(mv[d], spec)) continue;                 \
                         uint64_t key = or_canonical(mv[d], spec->symm_mode);                     \

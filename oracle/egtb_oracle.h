@@ -25,7 +25,10 @@ extern "C" {
 enum { OR_U32 = 0, OR_U64 = 1, OR_F32 = 2, OR_F64 = 3, OR_1F32 = 4, OR_1F64 = 5 };
 
 /* symmetry modes, native_core/include/FormationRuntime.h:13 */
-enum { OR_SYM_IDENTITY = 0, OR_SYM_FULL = 1, OR_SYM_DIAGONAL = 2, OR_SYM_HORIZONTAL = 3 };
+enum {
+    OR_SYM_IDENTITY = 0, OR_SYM_FULL = 1, OR_SYM_DIAGONAL = 2, OR_SYM_HORIZONTAL = 3,
+    OR_SYM_MIN33 = 4, OR_SYM_MIN24 = 5, OR_SYM_MIN34 = 6
+};
 
 typedef struct {
     const uint64_t *masks;
@@ -33,10 +36,13 @@ typedef struct {
     const uint8_t *shifts;
     int n_shifts;
     int symm_mode;
+    int is_variant; /* 1: the variant boards' wall-merge mover */
 } or_spec;
 
 /* board primitives */
 void or_move_all_dir(uint64_t b, uint64_t out[4]);
+void or_move_all_dir_variant_batch(const uint64_t *b, size_t n, uint64_t *out4);
+void or_row_tables_variant(uint16_t *left_xor, uint16_t *right_xor);
 uint64_t or_apply_sym(uint64_t b, int idx);
 uint64_t or_canonical(uint64_t b, int mode);
 int or_is_pattern(uint64_t b, const or_spec *s);

@@ -26,6 +26,7 @@ class _Spec(ctypes.Structure):
         ("shifts", ctypes.POINTER(ctypes.c_uint8)),
         ("n_shifts", ctypes.c_int),
         ("symm_mode", ctypes.c_int),
+        ("is_variant", ctypes.c_int),
     ]
 
 
@@ -65,6 +66,8 @@ def lib():
         L.or_move_all_dir_batch.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
         L.or_canonical_batch.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p]
         L.or_row_tables.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.or_row_tables_variant.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.or_move_all_dir_variant_batch.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
         L.or_expand.restype = ctypes.c_size_t
         L.or_expand.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(_Spec), ctypes.c_int, ctypes.c_int,
                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
@@ -79,7 +82,7 @@ def lib():
 class Spec:
     """Holds the C spec struct and keeps its arrays alive."""
 
-    def __init__(self, masks, shifts, symm_mode):
+    def __init__(self, masks, shifts, symm_mode, is_variant=False):
         self.masks = np.ascontiguousarray(np.asarray(list(masks), dtype=np.uint64))
         self.shifts = np.ascontiguousarray(np.asarray(list(shifts), dtype=np.uint8))
         self.c = _Spec(
@@ -88,13 +91,15 @@ class Spec:
             self.shifts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
             len(self.shifts),
             int(symm_mode),
+            int(bool(is_variant)),
         )
 
 
-def move_all_dir(boards: np.ndarray) -> np.ndarray:
+def move_all_dir(boards: np.ndarray, variant: bool = False) -> np.ndarray:
     b = np.ascontiguousarray(boards, dtype=np.uint64)
     out = np.zeros((len(b), 4), dtype=np.uint64)
-    lib().or_move_all_dir_batch(b.ctypes.data, len(b), out.ctypes.data)
+    fn = lib().or_move_all_dir_variant_batch if variant else lib().or_move_all_dir_batch
+    fn(b.ctypes.data, len(b), out.ctypes.data)
     return out
 
 
@@ -109,10 +114,10 @@ def apply_sym(board: int, idx: int) -> int:
     return int(lib().or_apply_sym(int(board), int(idx)))
 
 
-def row_tables():
+def row_tables(variant: bool = False):
     left = np.zeros(65536, dtype=np.uint16)
     right = np.zeros(65536, dtype=np.uint16)
-    lib().or_row_tables(left.ctypes.data, right.ctypes.data)
+    (lib().or_row_tables_variant if variant else lib().or_row_tables)(left.ctypes.data, right.ctypes.data)
     return left, right
 
 

@@ -3,7 +3,9 @@
 // infrastructure only: it exposes the reference's own move tables and
 // symmetry functions to the parity tests and to the golden-vector script.
 //
-//   move_all_dir      native_core/include/CommonMover.h:136-139
+//   move_all_dir      native_core/include/CommonMover.h:136-139 (classic
+//                     BoardMover and the variant VBoardMover,
+//                     native_core/include/VBoardMover.h)
 //   row tables        native_core/include/CommonMover.h:87-94,
 //                     native_core/include/BoardMover.h:6-55
 //   canonical_by_mode native_core/include/SymmetryUtils.h:31-49
@@ -15,6 +17,7 @@
 #include <vector>
 
 #include "BoardMover.h"
+#include "VBoardMover.h"
 #include "Formation.h"
 #include "SymmetryUtils.h"
 
@@ -53,6 +56,23 @@ void ref_row_tables(uint16_t *left_xor, uint16_t *right_xor) {
     for (uint32_t r = 0; r < 65536; ++r) {
         left_xor[r] = BoardMover::row_move_table[r].movel;
         right_xor[r] = BoardMover::row_move_table[r].mover;
+    }
+}
+
+void ref_move_all_dir_variant_batch(const uint64_t *boards, size_t n, uint64_t *out4) {
+    for (size_t i = 0; i < n; ++i) {
+        auto m = VBoardMover::move_all_dir(boards[i]);
+        out4[4 * i + 0] = std::get<0>(m);
+        out4[4 * i + 1] = std::get<1>(m);
+        out4[4 * i + 2] = std::get<2>(m);
+        out4[4 * i + 3] = std::get<3>(m);
+    }
+}
+
+void ref_row_tables_variant(uint16_t *left_xor, uint16_t *right_xor) {
+    for (uint32_t r = 0; r < 65536; ++r) {
+        left_xor[r] = VBoardMover::row_move_table[r].movel;
+        right_xor[r] = VBoardMover::row_move_table[r].mover;
     }
 }
 

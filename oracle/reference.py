@@ -81,7 +81,7 @@ def pattern_params(entry: dict, target: int):
 
 
 def make_spec_options(masks, shifts, symm, target, steps, docheck, pathname, dtype="float32", p4=0.1, threads=0,
-                      deletion_threshold=0.0, optimal_branch_only=False):
+                      deletion_threshold=0.0, optimal_branch_only=False, is_variant=False):
     fc = module()
     spec = fc.PatternSpec()
     spec.name = "oracle"
@@ -99,6 +99,7 @@ def make_spec_options(masks, shifts, symm, target, steps, docheck, pathname, dty
     o.num_threads = int(threads or os.cpu_count() or 4)
     o.deletion_threshold = float(deletion_threshold)
     o.optimal_branch_only = bool(optimal_branch_only)
+    o.is_variant = bool(is_variant)
     return spec, o
 
 

@@ -7,8 +7,9 @@ fixtures are outputs of the reference itself, run in this container:
   cases.json   per build case: the PatternSpec/RunOptions inputs, every raw
                layer's length and SHA-256 (run_pattern_generate writes them) and
                every .book file's SHA-256 (run_pattern_build writes them)
-  prims.npz    board primitives on seeded random boards: move_all_dir,
-               canonical_by_mode for modes 0-3, apply_sym_like 0-7, row tables
+  prims.npz    board primitives on seeded random boards: move_all_dir (classic
+               and variant movers), canonical_by_mode for modes 0-6,
+               apply_sym_like 0-7, row tables of both movers
   reader.json  ClassicBookReader.move_on_dic answers on positions sampled from
                the books of the small cases
   free5_32.npz one complete small build (raw layers and books) as data
@@ -84,6 +85,9 @@ def custom_patterns() -> dict:
 DELETION_CASES = [("L3", 5, "float32", 0.3), ("442", 6, "uint32", 0.5), ("diag9", 6, "float64", 0.7)]
 # builds followed by the optimal-branch pass (keep_only_optimal_branches_impl, BookSolver.cpp:688-735)
 OPTIMAL_CASES = [("L3", 6, "float32"), ("442", 6, "uint32"), ("diag9", 6, "float64"), ("44", 6, "1-float32")]
+# variant boards (wall-merge mover, VBoardMover) of the catalog's "variant"
+# category, each with its own symmetry mode (min24, min33, min34)
+VARIANT_CASES = [("2x4", 7, "float32"), ("2x4", 8, "uint32"), ("3x3", 7, "float64"), ("3x4", 7, "float32")]
 
 SMALL_CASES = [
     ("44", 6, "float32"), ("44", 7, "uint32"),
@@ -106,14 +110,15 @@ def sha(path: str) -> str:
     return h.hexdigest()
 
 
-def run_case(catalog, pat, target, dtype, deletion=0.0, optimal=False):
+def run_case(catalog, pat, target, dtype, deletion=0.0, optimal=False, variant=False):
     masks, shifts, symm, seeds, steps, docheck, s0 = R.pattern_params(catalog[pat], target)
     T = 2 ** target
     name = f"{pat}_{T}"
     tag = f"{name}_{dtype}" + (f"_del{deletion}" if deletion else "") + ("_opt" if optimal else "")
     gdir = R.fresh_dir(os.path.join(WORK, tag, "gen") + "/")
     bdir = R.fresh_dir(os.path.join(WORK, tag, "build") + "/")
-    spec, o = R.make_spec_options(masks, shifts, symm, target, steps, docheck, gdir + name + "_", dtype)
+    spec, o = R.make_spec_options(masks, shifts, symm, target, steps, docheck, gdir + name + "_", dtype,
+                                  is_variant=variant)
     started, last0, last1 = R.run_generate(seeds, spec, o)
     raw_len, raw_sha = [], []
     for t in range(steps - 2):
@@ -121,7 +126,7 @@ def run_case(catalog, pat, target, dtype, deletion=0.0, optimal=False):
         raw_len.append(os.path.getsize(p) // 8)
         raw_sha.append(sha(p))
     spec, o = R.make_spec_options(masks, shifts, symm, target, steps, docheck, bdir + name + "_", dtype,
-                                  deletion_threshold=deletion, optimal_branch_only=optimal)
+                                  deletion_threshold=deletion, optimal_branch_only=optimal, is_variant=variant)
     R.run_build(seeds, spec, o)
     book_len, book_sha = [], []
     rec = 12 if dtype in ("uint32", "float32", "1-float32") else 16
@@ -140,6 +145,8 @@ def run_case(catalog, pat, target, dtype, deletion=0.0, optimal=False):
     }
     if optimal:
         case["optimal_branch_only"] = True
+    if variant:
+        case["is_variant"] = True
     if deletion:
         case["deletion_threshold"] = deletion
         lines = open(bdir + name + "_stats.txt").read().splitlines()
@@ -164,7 +171,10 @@ def prims_fixture():
     mv = np.zeros(n * 4, dtype=np.uint64)
     L.ref_move_all_dir_batch(boards.ctypes.data, ctypes.c_size_t(n), mv.ctypes.data)
     out["moves"] = mv.reshape(n, 4)
-    for mode in range(4):
+    mv = np.zeros(n * 4, dtype=np.uint64)
+    L.ref_move_all_dir_variant_batch(boards.ctypes.data, ctypes.c_size_t(n), mv.ctypes.data)
+    out["moves_variant"] = mv.reshape(n, 4)
+    for mode in range(7):
         c = np.zeros(n, dtype=np.uint64)
         L.ref_canonical_batch(boards.ctypes.data, ctypes.c_size_t(n), mode, c.ctypes.data)
         out[f"canonical_{mode}"] = c
@@ -177,6 +187,11 @@ def prims_fixture():
     L.ref_row_tables(left.ctypes.data, right.ctypes.data)
     out["row_left"] = left
     out["row_right"] = right
+    left = np.zeros(65536, dtype=np.uint16)
+    right = np.zeros(65536, dtype=np.uint16)
+    L.ref_row_tables_variant(left.ctypes.data, right.ctypes.data)
+    out["row_left_variant"] = left
+    out["row_right_variant"] = right
     np.savez_compressed(os.path.join(GOLDEN, "prims.npz"), **out)
 
 
@@ -195,7 +210,8 @@ def reader_fixture(case, bdir, rng, n_pos=60):
     spec.pattern_masks = [int(m, 16) for m in case["masks"]]
     spec.success_shifts = case["shifts"]
     spec.symm_mode = case["symm_mode"]
-    reader = fc.ClassicBookReader(spec, False)
+    variant = bool(case.get("is_variant"))
+    reader = fc.ClassicBookReader(spec, variant)
     rec = 12 if case["dtype"] in ("uint32", "float32", "1-float32") else 16
     path_list = [(bdir, case["dtype"])]
     out = []
@@ -217,7 +233,9 @@ def reader_fixture(case, bdir, rng, n_pos=60):
             j = int(rng.integers(16))
             if (pos >> (4 * j)) & 0xF != 0xF:
                 pos = (pos & ~(0xF << (4 * j))) | (int(rng.integers(0, 6)) << (4 * j))
-        op = int(rng.integers(8))
+        # a variant reader tries the board as given only (operation_sequence,
+        # ReaderRuntime.cpp:171-182): most variant positions stay unrotated
+        op = int(rng.integers(8)) if not variant or rng.random() < 0.25 else 0
         board = decode(pos)
         b = np.array(board)
         if op in (1, 5):
@@ -286,6 +304,15 @@ def main():
         case, _ = run_case(catalog, pat, target, dtype, optimal=True)
         case["size_class"] = "optimal"
         cases[key] = case
+    for pat, target, dtype in VARIANT_CASES:
+        key = f"{pat}_{2 ** target}_{dtype}"
+        if only and key not in only:
+            continue
+        print("case", key, flush=True)
+        case, bdir = run_case(catalog, pat, target, dtype, variant=True)
+        case["size_class"] = "variant"
+        cases[key] = case
+        reader[key] = reader_fixture(case, bdir, rng)
     json.dump(cases, open(cases_path, "w"), indent=0)
     if reader:
         rpath = os.path.join(GOLDEN, "reader.json")

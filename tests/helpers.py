@@ -64,6 +64,7 @@ def spec_options(case: dict, pathname: str):
     o.pathname = pathname
     o.success_rate_dtype = case["dtype"]
     o.spawn_rate4 = case["spawn_rate4"]
+    o.is_variant = bool(case.get("is_variant", False))
     return spec, o
 
 
@@ -81,3 +82,7 @@ def fresh(path: str) -> str:
 SMALL_CPU_CASES = [k for k, v in cases().items() if v.get("size_class") == "small" and sum(v["raw_len"]) < 3_000_000]
 SMALL_CASES = [k for k, v in cases().items() if v.get("size_class") == "small"]
 FULL_CASES = [k for k, v in cases().items() if v.get("size_class") == "full"]
+# variant boards (wall-merge mover, min24/min33/min34 symmetry); the CPU oracle
+# takes the ones it finishes in seconds
+VARIANT_CASES = [k for k, v in cases().items() if v.get("size_class") == "variant"]
+VARIANT_CPU_CASES = [k for k in VARIANT_CASES if sum(cases()[k]["raw_len"]) < 3_000_000]

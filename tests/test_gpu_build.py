@@ -17,7 +17,7 @@ def _generate(case, d):
     return started, l0, l1
 
 
-@pytest.mark.parametrize("key", H.SMALL_CASES)
+@pytest.mark.parametrize("key", H.SMALL_CASES + H.VARIANT_CPU_CASES)
 def test_generate_raw_layers_bit_exact(key, tmp_root):
     case = H.cases()[key]
     d = H.fresh(os.path.join(tmp_root, "gen_" + key) + "/")
@@ -38,7 +38,7 @@ def test_generate_raw_layers_bit_exact(key, tmp_root):
     assert l0.size == case["book_len"][steps - 2] and l1.size == case["book_len"][steps - 1]
 
 
-@pytest.mark.parametrize("key", H.SMALL_CASES)
+@pytest.mark.parametrize("key", H.SMALL_CASES + H.VARIANT_CASES)
 def test_build_books_bit_exact(key, tmp_root):
     case = H.cases()[key]
     F = H.fc()
@@ -144,13 +144,28 @@ def test_invalid_options_raise(tmp_root):
     F = H.fc()
     case = H.cases()["44_64_float32"]
     spec, o = H.spec_options(case, os.path.join(tmp_root, "bad_"))
-    o.is_variant = True
-    with pytest.raises(RuntimeError, match="variant"):
+    o.compress = True
+    with pytest.raises(RuntimeError, match="compress"):
         F.run_pattern_build(H.seeds(case), spec, o)
-    o.is_variant = False
-    spec.symm_mode = 4
+    o.compress = False
+    spec.symm_mode = 7
     with pytest.raises(RuntimeError, match="symmetry"):
         F.run_pattern_build(H.seeds(case), spec, o)
+
+
+def test_variant_tables_are_refused_by_the_batched_build():
+    """The batched build moves every table with the classic rule: a variant
+    table in a batch is an error (build it with egtb_build)."""
+    import ctypes
+    import importlib
+    B = importlib.import_module("2048endgametablebase_b200.batch")
+    N = H.pkg()._native
+    a = B._Args(B.random_tables(2, seed=3), "float32", 0, None)
+    a.opts[1].is_variant = 1
+    ts = (N.BuildStatsC * a.n)()
+    bs = N.BatchStatsC()
+    rc = N.lib().egtb_build_batch(a.n, a.seed_ptrs, a.n_seeds, a.specs, a.opts, None, ts, ctypes.byref(bs))
+    assert rc == -7 and "variant" in N.last_error()
 
 
 @pytest.mark.slow

@@ -31,7 +31,13 @@ def test_moves():
     assert np.array_equal(_call("egtb_move_all_dir", p["boards"], width=4), p["moves"])
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_variant_moves():
+    """The variant boards' wall-merge mover (VBoardMover)."""
+    p = H.prims()
+    assert np.array_equal(_call("egtb_move_all_dir_variant", p["boards"], width=4), p["moves_variant"])
+
+
+@pytest.mark.parametrize("mode", range(7))
 def test_canonical(mode):
     p = H.prims()
     assert np.array_equal(_call("egtb_canonical", p["boards"], mode), p[f"canonical_{mode}"])
@@ -43,9 +49,9 @@ def test_symmetries(idx):
     assert np.array_equal(_call("egtb_apply_sym", p["boards"], idx), p[f"sym_{idx}"])
 
 
-def test_unsupported_mode_is_an_error():
+def test_unknown_mode_is_an_error():
     N = H.pkg()._native
     b = np.zeros(4, dtype=np.uint64)
     out = np.zeros(4, dtype=np.uint64)
-    rc = N.lib().egtb_canonical(0, b.ctypes.data, 4, 5, out.ctypes.data)
-    assert rc == -7 and "symmetry" in N.last_error()
+    rc = N.lib().egtb_canonical(0, b.ctypes.data, 4, 7, out.ctypes.data)
+    assert rc == -1 and "symmetry" in N.last_error()

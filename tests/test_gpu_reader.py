@@ -30,7 +30,7 @@ def test_move_on_dic_matches_reference(key, built):
     F = H.fc()
     case = H.cases()[key]
     spec, _ = H.spec_options(case, "")
-    reader = F.ClassicBookReader(spec, False)
+    reader = F.ClassicBookReader(spec, bool(case.get("is_variant", False)))
     path_list = [(built[key].rstrip("/"), case["dtype"])]
     for i, entry in enumerate(H.reader_cases()[key]):
         res, dt = reader.move_on_dic(entry["board"], path_list, case["pattern_full"], -case["tile_sum0"])

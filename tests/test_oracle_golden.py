@@ -20,7 +20,16 @@ def test_moves_match_reference():
     assert np.array_equal(O.move_all_dir(p["boards"]), p["moves"])
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_variant_row_tables_and_moves_match_reference():
+    """The variant boards' wall-merge mover (VBoardMover)."""
+    p = H.prims()
+    left, right = O.row_tables(variant=True)
+    assert np.array_equal(left, p["row_left_variant"])
+    assert np.array_equal(right, p["row_right_variant"])
+    assert np.array_equal(O.move_all_dir(p["boards"], variant=True), p["moves_variant"])
+
+
+@pytest.mark.parametrize("mode", range(7))
 def test_canonical_match_reference(mode):
     p = H.prims()
     assert np.array_equal(O.canonical(p["boards"], mode), p[f"canonical_{mode}"])
@@ -35,11 +44,12 @@ def test_symmetries_match_reference(idx):
 
 
 def _build(case):
-    spec = O.Spec([int(m, 16) for m in case["masks"]], case["shifts"], case["symm_mode"])
+    spec = O.Spec([int(m, 16) for m in case["masks"]], case["shifts"], case["symm_mode"],
+                  case.get("is_variant", False))
     return O.Build(H.seeds(case), spec, case["target"], case["steps"], case["docheck_step"])
 
 
-@pytest.mark.parametrize("key", H.SMALL_CPU_CASES)
+@pytest.mark.parametrize("key", H.SMALL_CPU_CASES + H.VARIANT_CPU_CASES)
 def test_oracle_raw_layers_and_books(key):
     case = H.cases()[key]
     b = _build(case)
