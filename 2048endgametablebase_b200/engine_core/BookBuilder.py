@@ -118,6 +118,45 @@ def _run_with_single_resume_retry(build_label: str, build_fn) -> None:
             logger.warning("%s interrupted (%s); re-entering build once.", build_label, exc)
 
 
+def generate_free_inits(t32ks: int, t2s: int) -> np.ndarray:
+    """Seed boards of a free pattern (generate_free_inits,
+    engine_core/BookBuilder.py:149-182): every board with t32ks 32768 tiles
+    and t2s 2-tiles (combinations in lexicographic order, at most 10^6),
+    sorted and unique; then, board by board in that order, its four moves
+    (left, right, up, down) that are their own full-symmetry canonical form,
+    stopping after the board at which at least (boards - 3) have been
+    collected; the result sorted and unique. The moves and canonical forms
+    are the device primitives (egtb_move_all_dir, egtb_canonical)."""
+    from itertools import combinations
+
+    from . import Calculator as C
+
+    cap = 1_000_000
+    boards = []
+    for walls in combinations(range(16), t32ks):
+        base = 0
+        for p in walls:
+            base |= 0xF << (4 * p)
+        rest = [p for p in range(16) if p not in walls]
+        for twos in combinations(rest, t2s):
+            if len(boards) >= cap:
+                break
+            b = base
+            for p in twos:
+                b |= 1 << (4 * p)
+            boards.append(b)
+    gen = np.unique(np.array(boards, dtype=np.uint64))
+    if len(gen) == 0:
+        return gen
+    moved = C.move_all_dir(gen)                                    # (n, 4)
+    keep = moved == C.canonical_full(moved.reshape(-1)).reshape(moved.shape)
+    # collected after each board, in order; stop at the first board that reaches n - 3
+    cum = np.cumsum(keep.sum(axis=1))
+    hit = np.nonzero(cum >= len(gen) - 3)[0]
+    last = int(hit[0]) if len(hit) else len(gen) - 1
+    return np.unique(moved[: last + 1][keep[: last + 1]])
+
+
 def start_build(pattern: str, target: int, pathname: str) -> bool:
     """start_build, engine_core/BookBuilder.py:264-317 (classic algorithm)."""
     config = SingletonConfig().config
@@ -129,16 +168,23 @@ def start_build(pattern: str, target: int, pathname: str) -> bool:
     is_variant = pattern in patterns.category_info.get("variant", [])
     save_config_to_txt(pathname + "config.txt")
     if pattern.startswith("free"):
-        raise RuntimeError("free-pattern seed generation is not built")
-    arr_init = seed_boards
-    masks = patterns.pattern_catalog[pattern]["pattern_masks"]
-    inter = 0
-    if masks:
-        inter = ~0 & 0xFFFFFFFFFFFFFFFF
-        for m in masks:
-            inter &= int(m)
-    fixed = patterns.find_f_nibble_positions(inter) if masks else []
-    is_free = (len(fixed) < 4) and (tile_sum < 180000)
+        # BookBuilder.py:275-283: the seeds of a free pattern are generated
+        # when its extra tiles are all 2s that fit the free cells
+        seed = int(seed_boards[0])
+        num_32k = sum(1 for k in range(16) if (seed >> (4 * k)) & 0xF == 0xF)
+        extra = tile_sum - 32768 * num_32k
+        arr_init = generate_free_inits(num_32k, extra // 2) if extra <= (15 - num_32k) * 2 else seed_boards
+        is_free = True
+    else:
+        arr_init = seed_boards
+        masks = patterns.pattern_catalog[pattern]["pattern_masks"]
+        inter = 0
+        if masks:
+            inter = ~0 & 0xFFFFFFFFFFFFFFFF
+            for m in masks:
+                inter &= int(m)
+        fixed = patterns.find_f_nibble_positions(inter) if masks else []
+        is_free = (len(fixed) < 4) and (tile_sum < 180000)
     _run_with_single_resume_retry(
         f"Classic build {pattern}_{2 ** target}",
         lambda: _run_classic_build(pattern, arr_init, target, steps, pathname, docheck_step, is_free, is_variant,

@@ -77,11 +77,35 @@ def canonical_horizontal(board):
     return _canon(board, 3)
 
 
+def canonical_min33(board):
+    """Minimum over the eight symmetries of the 3x3 board (Calculator.py:315-317)."""
+    return _canon(board, 4)
+
+
+def canonical_min24(board):
+    """Minimum over the mirrors and half turn of the 2x4 board (Calculator.py:319-321)."""
+    return _canon(board, 5)
+
+
+def canonical_min34(board):
+    """Minimum over the symmetries of the 3x4 board (Calculator.py:323-325)."""
+    return _canon(board, 6)
+
+
 def move_all_dir(boards):
     """{left, right, up, down} of every board (CommonMover.h:136-139)."""
     a, scalar = _batch(boards)
     out = np.zeros((len(a), 4), dtype=np.uint64)
     N.check(N.lib().egtb_move_all_dir(_dev(), a.ctypes.data, len(a), out.ctypes.data))
+    return tuple(np.uint64(x) for x in out[0]) if scalar else out
+
+
+def move_all_dir_variant(boards):
+    """move_all_dir of the variant boards' mover: 0xF cells are walls
+    (VBoardMover, native_core/include/VBoardMover.h)."""
+    a, scalar = _batch(boards)
+    out = np.zeros((len(a), 4), dtype=np.uint64)
+    N.check(N.lib().egtb_move_all_dir_variant(_dev(), a.ctypes.data, len(a), out.ctypes.data))
     return tuple(np.uint64(x) for x in out[0]) if scalar else out
 
 

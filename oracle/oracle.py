@@ -192,3 +192,30 @@ class Build:
             lib().or_free(self.h)
         except Exception:
             pass
+
+
+def free_inits(t32ks: int, t2s: int) -> np.ndarray:
+    """generate_free_inits (engine_core/BookBuilder.py:149-182) restated on the
+    oracle's primitives: boards with t32ks 32768 tiles and t2s 2-tiles (at most
+    10^6, combinations in lexicographic order), sorted and unique; then board
+    by board the moves {left, right, up, down} that equal their full-symmetry
+    canonical form, stopping once (boards - 3) are collected; sorted, unique."""
+    from itertools import combinations
+    boards = []
+    for walls in combinations(range(16), t32ks):
+        base = sum(0xF << (4 * p) for p in walls)
+        for twos in combinations([p for p in range(16) if p not in walls], t2s):
+            if len(boards) >= 1_000_000:
+                break
+            boards.append(base | sum(1 << (4 * p) for p in twos))
+    gen = np.unique(np.array(boards, dtype=np.uint64))
+    moves = move_all_dir(gen)
+    canon = canonical(moves.reshape(-1), 1).reshape(moves.shape)
+    out = []
+    for i in range(len(gen)):
+        for d in range(4):
+            if moves[i, d] == canon[i, d]:
+                out.append(moves[i, d])
+        if len(out) >= len(gen) - 3:
+            break
+    return np.unique(np.array(out, dtype=np.uint64))
