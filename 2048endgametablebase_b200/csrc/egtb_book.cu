@@ -81,17 +81,35 @@ book_index_kernel(const uint64_t *__restrict__ keys, const T *__restrict__ rates
     }
 }
 
+// The four move lookups of one position at once: every first slot load is
+// issued before any is compared, so a thread has up to four misses in flight
+// instead of one dependent chain after another.
 template <typename T>
-__device__ __forceinline__ T index_lookup(const ulonglong2 *__restrict__ slots, unsigned long long mask, uint64_t key,
-                                          T zero) {
-    unsigned long long h = mix64(key) & mask;
-    for (unsigned long long probe = 0; probe <= mask; ++probe) {
-        const ulonglong2 sl = __ldg(slots + h);
-        if (sl.x == key) return book_rate_from_bits<T>(sl.y);
-        if (sl.x == 0ull) return zero;
-        h = (h + 1) & mask;
+__device__ __forceinline__ void index_lookup4(const ulonglong2 *__restrict__ slots, unsigned long long mask,
+                                              const uint64_t key[4], unsigned pend, T zero, T r[4]) {
+    unsigned long long h[4];
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        r[d] = zero;
+        h[d] = mix64(key[d]) & mask;
     }
-    return zero;
+    for (unsigned long long probe = 0; pend && probe <= mask; ++probe) {
+        ulonglong2 sl[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) sl[d] = (pend >> d & 1u) ? __ldg(slots + h[d]) : make_ulonglong2(0ull, 0ull);
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            if (!(pend >> d & 1u)) continue;
+            if (sl[d].x == key[d]) {
+                r[d] = book_rate_from_bits<T>(sl[d].y);
+                pend &= ~(1u << d);
+            } else if (sl[d].x == 0ull) {
+                pend &= ~(1u << d);
+            } else {
+                h[d] = (h[d] + 1) & mask;
+            }
+        }
+    }
 }
 
 }  // namespace egtb
@@ -335,24 +353,39 @@ __device__ __forceinline__ void lookup_position(const LayerDesc *__restrict__ de
         const int op = single >= 0 ? single : (j == 0 ? op_mode : j - 1);
         const uint64_t tb = apply_sym(board, kOpSym[op]);
         if (!is_pattern(tb, spec)) continue;
-        uint64_t mv[4];
+        uint64_t mv[4], key[4];
         move_all_dir(tab, tb, mv);
+        unsigned live = 0;  // moves that moved and stay in the pattern
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            key[d] = 0;
+            if (mv[d] == tb || !is_pattern(mv[d], spec)) continue;
+            key[d] = canonical<kVariantModes>(mv[d], spec.symm);
+            live |= 1u << d;
+        }
+        T r[4];
+        if (L.sorted && L.index) {
+            index_lookup4<T>(L.index, L.index_mask, key, live, zero, r);
+        } else {
+#pragma unroll
+            for (int d = 0; d < 4; ++d) {
+                r[d] = zero;
+                if (!(live >> d & 1u)) continue;
+                if (L.sorted) {
+                    r[d] = layer_lookup<T>(L.keys, rates, L.n, L.split, key[d], zero);
+                } else {
+                    T got;
+                    if (probe_unsorted<T>(L.keys, rates, L.n, key[d], got)) r[d] = got;
+                }
+            }
+        }
         uint8_t m = 0;
         OutT vals[4] = {0, 0, 0, 0};
 #pragma unroll
         for (int d = 0; d < 4; ++d) {
-            if (mv[d] == tb || !is_pattern(mv[d], spec)) continue;
-            const uint64_t key = canonical<kVariantModes>(mv[d], spec.symm);
-            T r = zero;
-            if (L.sorted) {
-                r = L.index ? index_lookup<T>(L.index, L.index_mask, key, zero)
-                            : layer_lookup<T>(L.keys, rates, L.n, L.split, key, zero);
-            } else {
-                T got;
-                if (probe_unsorted<T>(L.keys, rates, L.n, key, got)) r = got;
-            }
+            if (!(live >> d & 1u)) continue;
             const int slot = adjusted_slot(op, d);
-            vals[slot] = (OutT)present<T>(r, scale, round9);
+            vals[slot] = (OutT)present<T>(r[d], scale, round9);
             m |= (uint8_t)(1u << slot);
         }
         if (m) {
