@@ -168,6 +168,23 @@ def _seeds(arr_init) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.uint64)
 
 
+# The reference's message when a build runs out of room
+# (native_core/src/BookGenerator.cpp:371), which
+# BookBuilder._should_retry_build_resume (engine_core/BookBuilder.py:237-243)
+# answers with one resumed retry.
+CAPACITY_MESSAGE = "The length multiplier is not big enough. Please restart."
+
+
+def _check_build(rc: int) -> None:
+    """N.check for the build calls: a table that does not fit even after the
+    library's own regrowth and streamed fallback (EGTB_ERR_CAPACITY) raises
+    with the reference's capacity message; the library's detail is chained."""
+    if rc == -5:
+        detail = N.NativeError(rc, f"EGTB_ERR_CAPACITY: {N.last_error()}")
+        raise N.NativeError(rc, CAPACITY_MESSAGE) from detail
+    N.check(rc)
+
+
 def run_pattern_generate(arr_init, pattern_spec: PatternSpec, run_options: RunOptions):
     """run_pattern_generate (native_core/src/BookSolver.cpp:766-782): raw layer files
     plus the success-only books of the last two layers; returns
@@ -177,7 +194,7 @@ def run_pattern_generate(arr_init, pattern_spec: PatternSpec, run_options: RunOp
     opts = run_options.to_c()
     started = ctypes.c_int32(0)
     st = N.BuildStatsC()
-    N.check(N.lib().egtb_generate(seeds.ctypes.data, len(seeds), ctypes.byref(spec), ctypes.byref(opts),
+    _check_build(N.lib().egtb_generate(seeds.ctypes.data, len(seeds), ctypes.byref(spec), ctypes.byref(opts),
                                   ctypes.byref(started), ctypes.byref(st)))
     _last_stats.clear()
     _last_stats.update(st.as_dict())
@@ -201,7 +218,7 @@ def run_pattern_solve(d1: PatternLayer, d2: PatternLayer, pattern_spec: PatternS
     r1 = np.ascontiguousarray(d1.records.astype(rdt, copy=False)) if d1 is not None else np.zeros(0, rdt)
     r2 = np.ascontiguousarray(d2.records.astype(rdt, copy=False)) if d2 is not None else np.zeros(0, rdt)
     st = N.BuildStatsC()
-    N.check(N.lib().egtb_solve(r1.ctypes.data if len(r1) else None, len(r1), r2.ctypes.data if len(r2) else None,
+    _check_build(N.lib().egtb_solve(r1.ctypes.data if len(r1) else None, len(r1), r2.ctypes.data if len(r2) else None,
                                len(r2), ctypes.byref(spec), ctypes.byref(opts), ctypes.byref(st)))
     _last_stats.clear()
     _last_stats.update(st.as_dict())
@@ -213,7 +230,7 @@ def run_pattern_build(arr_init, pattern_spec: PatternSpec, run_options: RunOptio
     spec = pattern_spec.to_c()
     opts = run_options.to_c()
     st = N.BuildStatsC()
-    N.check(N.lib().egtb_build(seeds.ctypes.data, len(seeds), ctypes.byref(spec), ctypes.byref(opts),
+    _check_build(N.lib().egtb_build(seeds.ctypes.data, len(seeds), ctypes.byref(spec), ctypes.byref(opts),
                                ctypes.byref(st)))
     _last_stats.clear()
     _last_stats.update(st.as_dict())

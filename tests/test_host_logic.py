@@ -82,3 +82,33 @@ def test_reader_fixture_ordering_rules(key):
         assert vals == sorted(vals, reverse=True)
         kinds = [isinstance(v, float) for _, v in entry["result"]]
         assert kinds == sorted(kinds, reverse=True)
+
+
+def test_capacity_failure_raises_the_reference_message(monkeypatch):
+    """A build that cannot fit even after regrowth and the streamed fallback
+    (EGTB_ERR_CAPACITY) raises the reference's "length multiplier" message, so
+    BookBuilder's one resumed retry still applies; other errors keep theirs."""
+    F = H.fc()
+    N = H.pkg()._native
+    bb = __import__("importlib").import_module("2048endgametablebase_b200.engine_core.BookBuilder")
+
+    class FakeLib:
+        def __init__(self, rc):
+            self.rc = rc
+
+        def egtb_build(self, *args):
+            return self.rc
+
+        def egtb_last_error(self, buf, n):
+            return 0
+
+    case = H.cases()["L3_32_float32"]
+    spec, o = H.spec_options(case, "/nonexistent/unused_")
+    for rc, retry in ((-5, True), (-7, False)):
+        monkeypatch.setattr(N, "lib", lambda rc=rc: FakeLib(rc))
+        with pytest.raises(N.NativeError) as ei:
+            F.run_pattern_build(H.seeds(case), spec, o)
+        assert ei.value.code == rc
+        assert bb._should_retry_build_resume(ei.value) is retry
+        if retry:
+            assert str(ei.value) == F.CAPACITY_MESSAGE
