@@ -4,12 +4,13 @@
 // board primitives).
 //
 // Fused build (egtb_build with no layer files on disk): every raw layer stays
-// in one device arena (16-aligned offsets, splitter every 16 keys) for the
-// whole build. Forward step i expands layer i-1 into two candidate buffers
-// (spawn-2 children for layer i, spawn-4 children for layer i+1; a layer's
-// candidates always live in buffer layer&1), then radix-sorts and uniques
-// buffer i&1 into the arena as layer i. All sizes stay on the device, so the
-// host enqueues the whole forward without waiting; capacity overflows are
+// in one device arena (16-aligned offsets) for the whole build. Forward step
+// i is one kernel: it expands layer i-1 and enters the spawn-2 children of
+// layer i and the spawn-4 children of layer i+1 into those layers' hash sets
+// (exact dedup), appending the new keys to the layers' staging buffers; it
+// copies layer i-1 into the arena. After the last step every layer is sorted
+// in its own region (enqueue_sort_layers). All sizes stay on the device, so
+// the host enqueues the whole forward without waiting; capacity overflows are
 // flagged by the kernels and the forward is re-run with larger buffers.
 // Backward solve runs layer by layer on the same arena, then every layer is
 // packed into .book records on the device and written by a thread pool.
@@ -189,7 +190,10 @@ struct Engine {
     unsigned long long dset_cap = 0;          // slots per set
     uint64_t *filter = nullptr;               // direct-mapped repeat filter in front of the sets
     int filter_bits = 20;
-    unsigned long long *dense_off = nullptr;  // layer sort: dense offsets of the layers
+    int *seg_tab = nullptr;                    // per-layer sort: tile -> layer, then layer -> first tile
+    unsigned long long seg_tab_cap = 0;
+    unsigned *seg_hist = nullptr;              // per-layer sort: digit histograms, layer x pass x 256
+    unsigned long long seg_hist_cap = 0;
     unsigned long long candidates = 0;        // children probed by the last forward pass
     unsigned long long *layer_off = nullptr, *layer_len = nullptr, *book_len = nullptr;
     unsigned long long *layer_max = nullptr;  // ordered encoding of the largest rate per layer
@@ -283,8 +287,6 @@ struct Engine {
         alloc_or_throw((void **)&layer_max, sizeof(unsigned long long) * steps_cap, "layer maxima");
         release(first_tile);
         alloc_or_throw((void **)&first_tile, sizeof(unsigned long long) * steps_cap, "tile map");
-        release(dense_off);
-        alloc_or_throw((void **)&dense_off, sizeof(unsigned long long) * steps_cap, "dense offsets");
     }
 
     void ensure_dedup(unsigned long long slots) {
@@ -296,9 +298,24 @@ struct Engine {
         });
     }
 
-    // look-back words for sorts of up to max(cand_cap, arena_cap) keys
-    void ensure_status() {
-        const unsigned long long need = std::max(cand_cap, arena_cap) / kTileKeys + 2;
+    // per-layer sort tables: `tiles` tile entries + `layers` layer entries, histograms of `layers` layers
+    void ensure_seg(unsigned long long tiles, unsigned long long layers) {
+        if (tiles + layers > seg_tab_cap) {
+            release(seg_tab);
+            seg_tab_cap = tiles + layers + (tiles + layers) / 4 + 64;
+            alloc_or_throw((void **)&seg_tab, sizeof(int) * seg_tab_cap, "layer sort tile map");
+        }
+        if (layers * kMaxPasses * 256 > seg_hist_cap) {
+            release(seg_hist);
+            seg_hist_cap = layers * kMaxPasses * 256;
+            alloc_or_throw((void **)&seg_hist, sizeof(unsigned) * seg_hist_cap, "layer sort histograms");
+        }
+        ensure_status(tiles);
+    }
+
+    // look-back words for sorts of up to max(cand_cap, arena_cap) keys (and at least `tiles` tiles)
+    void ensure_status(unsigned long long tiles = 0) {
+        const unsigned long long need = std::max(std::max(cand_cap, arena_cap) / kTileKeys + 2, tiles);
         if (need <= sort_tiles) return;
         release(status);
         release(ustatus);
@@ -574,55 +591,55 @@ static unsigned long long env_keys(const char *name, unsigned long long dflt) {
     return x ? x : dflt;
 }
 
-// Sort layers 1 .. steps-1 in place (layer 0 keeps the seeds' order): one
-// radix sort over composite keys when layer index and free nibbles fit 64
-// bits, else one sort per layer. len: host copy of the layer lengths.
+// Sort layers 1 .. steps-1 in place (layer 0 keeps the seeds' order), each in
+// its own arena region by its free nibbles: one digit-histogram kernel for
+// every layer and pass, then one segmented onesweep kernel per pass (tiles
+// aligned to layers), ping-ponging with the book buffer, which is free until
+// the solve. len: host copy of the layer lengths.
 static void enqueue_sort_layers(Engine &E, const ForwardPlan &P, const std::vector<unsigned long long> &len) {
     cudaStream_t s = E.stream;
     const int steps = P.steps;
     if (steps < 2) return;
-    std::vector<unsigned long long> doff(steps + 1, 0);
-    for (int L = 0; L < steps; ++L) doff[L + 1] = doff[L] + len[L];
-    EGTB_CUDA(cudaMemcpyAsync(E.dense_off, doff.data(), sizeof(unsigned long long) * (steps + 1),
-                              cudaMemcpyHostToDevice, s));
-    int lb = 0;
-    while ((1ull << lb) < (unsigned long long)(steps - 1)) ++lb;
-    const int F = P.free.count;
-    uint64_t *comp = (uint64_t *)E.book, *other = comp + E.arena_cap;
-    auto sort_range = [&](int l0, int l1, int nibbles) {
-        const unsigned long long total = doff[l1] - doff[l0];
-        if (total < 2) return;
-        SortPlan sp;
-        std::memset(&sp, 0, sizeof sp);
-        sp.passes = (nibbles + 1) / 2;
-        for (int q = 0; q < sp.passes; ++q) {
-            sp.lo[q] = 2 * q;
-            sp.hi[q] = 2 * q + 1 < nibbles ? 2 * q + 1 : -1;
-        }
-        EGTB_LAUNCH(E, compose_kernel<<<E.sm_count * 8, 256, 0, s>>>(E.arena, E.layer_off, E.dense_off, l0, l1, P.free,
-                                                                      comp));
-        EGTB_CUDA(cudaMemsetAsync(E.hist, 0, sizeof(unsigned) * kMaxPasses * 256, s));
-        EGTB_LAUNCH(E, set_u64_kernel<<<1, 1, 0, s>>>(&E.ctl->cand_count[0], total));
-        EGTB_LAUNCH(E, sort_hist_kernel<<<E.sm_count * 2, kHistThreads, 0, s>>>(comp, &E.ctl->cand_count[0], E.arena_cap, sp,
-                                                                       E.hist, E.counters, E.ctl));
-        uint64_t *src = comp, *dst = other;
-        for (int q = 0; q < sp.passes; ++q) {
-            const int pi = E.prof_begin(K_SORT_PASS);
-            EGTB_LAUNCH(E, onesweep_kernel<<<E.sweep_grid, kSweepThreads, 0, s>>>(src, dst, &E.ctl->cand_count[0],
-                                                                                 E.arena_cap, sp, q, E.hist, E.counters,
-                                                                                 E.status, E.epoch++, E.ctl));
-            E.prof_end(pi);
-            std::swap(src, dst);
-        }
-        EGTB_LAUNCH(E, decompose_kernel<<<E.sm_count * 8, 256, 0, s>>>(src, E.layer_off, E.dense_off, l0, l1, P.free,
-                                                                        E.arena));
-    };
-    const int pu = E.prof_begin(K_UNIQUE);
-    if (4 * F + lb <= 64 && F < 16) {
-        sort_range(1, steps, F + (lb + 3) / 4);
-    } else {
-        for (int L = 1; L < steps; ++L) sort_range(L, L + 1, F);
+    // layers 1..steps-1 (layer 0 keeps the seeds as given), each sorted in its own
+    // arena region by its free nibbles: tiles never straddle two layers
+    std::vector<int> tab;
+    std::vector<int> tile0(steps, 0);
+    for (int L = 1; L < steps; ++L) {
+        tile0[L] = (int)tab.size();
+        const unsigned long long nt = (len[L] + kTileKeys - 1) / kTileKeys;
+        for (unsigned long long j = 0; j < nt; ++j) tab.push_back(L);
     }
+    const unsigned ntiles = (unsigned)tab.size();
+    if (ntiles == 0) return;
+    tab.insert(tab.end(), tile0.begin(), tile0.end());
+    E.ensure_seg(ntiles, (unsigned long long)steps);
+    EGTB_CUDA(cudaMemcpyAsync(E.seg_tab, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice, s));
+    const int *tile_layer = E.seg_tab, *layer_tile0 = E.seg_tab + ntiles;
+    const int F = P.free.count;
+    SortPlan sp;
+    std::memset(&sp, 0, sizeof sp);
+    sp.passes = (F + 1) / 2;
+    for (int q = 0; q < sp.passes; ++q) {
+        sp.lo[q] = P.free.idx[2 * q];
+        sp.hi[q] = 2 * q + 1 < F ? P.free.idx[2 * q + 1] : -1;
+    }
+    const int pu = E.prof_begin(K_UNIQUE);
+    EGTB_CUDA(cudaMemsetAsync(E.seg_hist, 0, sizeof(unsigned) * (size_t)steps * kMaxPasses * 256, s));
+    EGTB_LAUNCH(E, seg_hist_kernel<<<E.sm_count * 2, kHistThreads, 0, s>>>(E.arena, tile_layer, layer_tile0, E.layer_off,
+                                                                         E.layer_len, ntiles, sp, E.seg_hist,
+                                                                         E.counters));
+    uint64_t *src = E.arena, *dst = (uint64_t *)E.book;  // the book buffer is free until the solve
+    for (int q = 0; q < sp.passes; ++q) {
+        const int pi = E.prof_begin(K_SORT_PASS);
+        EGTB_LAUNCH(E, seg_onesweep_kernel<<<E.sweep_grid, kSweepThreads, 0, s>>>(
+                           src, dst, tile_layer, layer_tile0, E.layer_off, E.layer_len, ntiles, sp, q, E.seg_hist,
+                           E.counters, E.status, E.epoch++, E.ctl));
+        E.prof_end(pi);
+        std::swap(src, dst);
+    }
+    if (src != E.arena)
+        EGTB_LAUNCH(E, seg_copy_kernel<<<E.sm_count * 8, 256, 0, s>>>(src, E.arena, tile_layer, layer_tile0, E.layer_off,
+                                                                     E.layer_len, ntiles));
     E.prof_end(pu);
 }
 

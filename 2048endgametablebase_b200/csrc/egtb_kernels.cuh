@@ -456,12 +456,13 @@ dedup_seed_kernel(const uint64_t *__restrict__ keys, unsigned long long n, uint6
         dedup_insert_zero(set, mask, keys[i], &ctl->err);
 }
 
-// ------------------------------------------ sorting every layer at once ----
+// ------------------------------------------------- layer sort helpers ----
 //
-// After the forward pass each layer holds its unique keys in arrival order.
-// All layers but layer 0 (the seeds, kept as given) are sorted together by
-// composite keys (layer << 4F) | (the layer key's F free nibbles): one radix
-// sort, then every key goes back to its layer's region in ascending order.
+// After the forward pass each layer holds its unique keys in arrival order;
+// the layers are sorted by their free nibbles (the others are 0xF in every
+// key of the pattern): the plain build sorts each layer in its own region
+// (seg_* kernels, egtb_sort.cuh), the batched build sorts composite keys
+// (table, layer, compacted free nibbles) with these helpers.
 
 struct FreeNibbles {
     int count;
@@ -490,35 +491,6 @@ __device__ __forceinline__ int layer_of_dense(const unsigned long long *doff, in
         if (doff[mid] <= j) lo = mid; else hi = mid;
     }
     return lo;
-}
-
-static __global__ void __launch_bounds__(256)
-compose_kernel(const uint64_t *__restrict__ arena, const unsigned long long *__restrict__ layer_off,
-               const unsigned long long *__restrict__ doff, int l0, int l1, FreeNibbles fn,
-               uint64_t *__restrict__ comp) {
-    const unsigned long long total = doff[l1] - doff[l0];
-    for (unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; j < total;
-         j += (unsigned long long)gridDim.x * blockDim.x) {
-        const unsigned long long g = doff[l0] + j;
-        const int L = layer_of_dense(doff, l0, l1, g);
-        const uint64_t key = arena[layer_off[L] + (g - doff[L])];
-        const uint64_t layer_part = fn.count < 16 ? ((uint64_t)(L - l0) << (4 * fn.count)) : 0ull;
-        comp[j] = layer_part | compact_key(key, fn);
-    }
-}
-
-static __global__ void __launch_bounds__(256)
-decompose_kernel(const uint64_t *__restrict__ comp, const unsigned long long *__restrict__ layer_off,
-                 const unsigned long long *__restrict__ doff, int l0, int l1, FreeNibbles fn,
-                 uint64_t *__restrict__ arena) {
-    const unsigned long long total = doff[l1] - doff[l0];
-    for (unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; j < total;
-         j += (unsigned long long)gridDim.x * blockDim.x) {
-        const uint64_t c = comp[j];
-        const int L = l0 + (fn.count < 16 ? (int)(c >> (4 * fn.count)) : 0);
-        const unsigned long long g = doff[l0] + j;
-        arena[layer_off[L] + (g - doff[L])] = expand_key(fn.count < 16 ? c & ((1ull << (4 * fn.count)) - 1) : c, fn);
-    }
 }
 
 // Single block: exclusive scan of the tile counts; total -> *total_out.

@@ -245,6 +245,202 @@ onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, co
     }
 }
 
+// ------------------------------------------- per-layer (segmented) sort ----
+//
+// Every layer of the arena sorted in place of its own region, by its free
+// nibbles only (the other nibbles are 0xF in every key of a layer): tiles of
+// kTileKeys keys never straddle two layers (tile_layer[j] is tile j's layer,
+// layer_tile0[L] the first tile of layer L), each layer has its own digit
+// histograms (hist_l[(L * kMaxPasses + p) * 256 + d]), and the look-back of a
+// tile stops at its layer's first tile, which publishes its counts as a
+// prefix. The layer digits of a composite (layer, key) sort are not needed.
+
+// A tile's layer, its first key in the arena and its key count.
+struct SegTile {
+    int layer;
+    unsigned long long first;
+    unsigned n;
+    bool head;  // first tile of its layer
+};
+
+__device__ __forceinline__ SegTile seg_tile(unsigned tile, const int *__restrict__ tile_layer,
+                                            const int *__restrict__ layer_tile0,
+                                            const unsigned long long *__restrict__ layer_off,
+                                            const unsigned long long *__restrict__ layer_len) {
+    SegTile t;
+    t.layer = tile_layer[tile];
+    const unsigned lt = tile - (unsigned)layer_tile0[t.layer];
+    const unsigned long long done = (unsigned long long)lt * kTileKeys;
+    const unsigned long long rem = layer_len[t.layer] - done;
+    t.first = layer_off[t.layer] + done;
+    t.n = rem < (unsigned long long)kTileKeys ? (unsigned)rem : (unsigned)kTileKeys;
+    t.head = lt == 0;
+    return t;
+}
+
+// Digit histograms of every pass, per layer. Block b takes a contiguous run
+// of tiles (mostly of one layer) and adds its counts to the layer's
+// histograms when the layer changes. Also resets the tile counters.
+static __global__ void __launch_bounds__(kHistThreads, 2)
+seg_hist_kernel(const uint64_t *__restrict__ keys, const int *__restrict__ tile_layer,
+                const int *__restrict__ layer_tile0, const unsigned long long *__restrict__ layer_off,
+                const unsigned long long *__restrict__ layer_len, unsigned ntiles, SortPlan sp,
+                unsigned *__restrict__ hist_l, unsigned *__restrict__ counters) {
+    __shared__ unsigned h[kMaxPasses][256];
+    for (int i = threadIdx.x; i < kMaxPasses * 256; i += blockDim.x) (&h[0][0])[i] = 0;
+    if (blockIdx.x == 0 && threadIdx.x < 16) counters[threadIdx.x] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const unsigned per = (ntiles + gridDim.x - 1) / gridDim.x;
+    const unsigned t0 = blockIdx.x * per;
+    const unsigned t1 = t0 + per < ntiles ? t0 + per : ntiles;
+    int cur = -1;
+    auto flush = [&]() {
+        __syncthreads();
+        unsigned *out = hist_l + (size_t)cur * kMaxPasses * 256;
+        for (int i = threadIdx.x; i < sp.passes * 256; i += blockDim.x) {
+            const unsigned c = (&h[0][0])[i];
+            if (c) {
+                atomicAdd(out + i, c);
+                (&h[0][0])[i] = 0;
+            }
+        }
+        __syncthreads();
+    };
+    for (unsigned tile = t0; tile < t1; ++tile) {
+        const SegTile t = seg_tile(tile, tile_layer, layer_tile0, layer_off, layer_len);
+        if (t.layer != cur) {
+            if (cur >= 0) flush();
+            cur = t.layer;
+        }
+        uint64_t k[kHistKeys];
+#pragma unroll
+        for (int r = 0; r < kHistKeys; ++r) {
+            const unsigned i = (unsigned)r * kHistThreads + threadIdx.x;
+            k[r] = i < t.n ? keys[t.first + i] : 0;
+        }
+#pragma unroll
+        for (int r = 0; r < kHistKeys; ++r) {
+            const bool valid = (unsigned)r * kHistThreads + threadIdx.x < t.n;
+            for (int p = 0; p < sp.passes; ++p) {
+                const unsigned d = valid ? sort_digit(k[r], sp, p) : 256u;
+                const unsigned d0 = __shfl_sync(0xFFFFFFFFu, d, 0);
+                if (__all_sync(0xFFFFFFFFu, d == d0)) {
+                    if (lane == 0 && d0 < 256u) atomicAdd(&h[p][d0], 32u);
+                } else if (valid) {
+                    atomicAdd(&h[p][d], 1u);
+                }
+            }
+        }
+    }
+    if (cur >= 0) flush();
+}
+
+// One pass of the per-layer sort: src -> dst (same layout) ordered by digit p
+// within every layer, stable. The same tile work as onesweep_kernel.
+static __global__ void __launch_bounds__(kSweepThreads, 2)
+seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, const int *__restrict__ tile_layer,
+                    const int *__restrict__ layer_tile0, const unsigned long long *__restrict__ layer_off,
+                    const unsigned long long *__restrict__ layer_len, unsigned ntiles, SortPlan sp, int p,
+                    const unsigned *__restrict__ hist_l, unsigned *__restrict__ counters,
+                    unsigned long long *__restrict__ status, unsigned epoch, DevCtl *ctl) {
+    __shared__ uint64_t tkeys[kTileKeys];
+    __shared__ unsigned short wcnt[kSweepWarps][256];
+    __shared__ unsigned loff[256];
+    __shared__ unsigned long long gbase[256];
+    __shared__ unsigned long long sm[33];
+    __shared__ unsigned tile_sh;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int d = threadIdx.x;  // digit owned by this thread when d < 256
+    for (;;) {
+        if (threadIdx.x == 0) tile_sh = atomicAdd(&counters[p], 1u);
+        for (int i = threadIdx.x; i < kSweepWarps * 256; i += kSweepThreads) (&wcnt[0][0])[i] = 0;
+        __syncthreads();
+        const unsigned tile = tile_sh;
+        if (tile >= ntiles) break;
+        const SegTile t = seg_tile(tile, tile_layer, layer_tile0, layer_off, layer_len);
+        // start of every digit of this layer in the layer's region
+        unsigned long long ghist_d;
+        {
+            unsigned long long tot;
+            const unsigned long long hd = d < 256 ? hist_l[((size_t)t.layer * kMaxPasses + p) * 256 + d] : 0ull;
+            ghist_d = block_excl_scan<unsigned long long>(hd, sm, &tot);
+        }
+        const unsigned base = (unsigned)warp * (kTileKeys / kSweepWarps);
+        uint64_t k[kSweepKeys];
+        unsigned rd[kSweepKeys];  // rank in the warp (low 16 bits) | digit << 16 (256 = no key)
+#pragma unroll
+        for (int r = 0; r < kSweepKeys; ++r) {
+            const unsigned idx = base + (unsigned)r * 32 + lane;
+            k[r] = idx < t.n ? src[t.first + idx] : 0;
+        }
+#pragma unroll
+        for (int r = 0; r < kSweepKeys; ++r) {
+            const unsigned idx = base + (unsigned)r * 32 + lane;
+            const bool valid = idx < t.n;
+            const unsigned dg = valid ? sort_digit(k[r], sp, p) : 256u;
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, dg);
+            const unsigned before = __popc(peers & ((1u << lane) - 1u));
+            unsigned c = 0;
+            if (valid) c = wcnt[warp][dg];
+            rd[r] = (c + before) | (dg << 16);
+            __syncwarp();
+            if (valid && before == 0) wcnt[warp][dg] = (unsigned short)(c + __popc(peers));
+            __syncwarp();
+        }
+        __syncthreads();
+        unsigned cnt = 0;
+        unsigned long long excl = 0;
+        if (d < 256) {
+#pragma unroll
+            for (int w = 0; w < kSweepWarps; ++w) {
+                const unsigned c = wcnt[w][d];
+                wcnt[w][d] = (unsigned short)cnt;
+                cnt += c;
+            }
+            unsigned long long *my = status + (size_t)tile * 256 + d;
+            if (t.head) {
+                publish_status(my, status_word(epoch, kFlagPrefix, cnt));
+            } else {
+                publish_status(my, status_word(epoch, kFlagAgg, cnt));
+                // stops at the first prefix: at the latest the layer's first tile
+                excl = look_back(status + d, 256, (long long)tile, epoch, ctl);
+                publish_status(my, status_word(epoch, kFlagPrefix, (unsigned)(excl + cnt)));
+            }
+            gbase[d] = layer_off[t.layer] + ghist_d + excl;
+        }
+        {
+            unsigned long long tot;
+            const unsigned long long lo = block_excl_scan<unsigned long long>((unsigned long long)cnt, sm, &tot);
+            if (d < 256) loff[d] = (unsigned)lo;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kSweepKeys; ++r) {
+            const unsigned dg = rd[r] >> 16;
+            if (dg < 256u) tkeys[loff[dg] + wcnt[warp][dg] + (rd[r] & 0xFFFFu)] = k[r];
+        }
+        __syncthreads();
+        for (unsigned i = threadIdx.x; i < t.n; i += kSweepThreads) {
+            const uint64_t key = tkeys[i];
+            const unsigned dg = sort_digit(key, sp, p);
+            dst[gbase[dg] + (i - loff[dg])] = key;
+        }
+        __syncthreads();
+    }
+}
+
+// Copy every layer's keys (tile by tile) from src to dst.
+static __global__ void __launch_bounds__(256)
+seg_copy_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, const int *__restrict__ tile_layer,
+                const int *__restrict__ layer_tile0, const unsigned long long *__restrict__ layer_off,
+                const unsigned long long *__restrict__ layer_len, unsigned ntiles) {
+    for (unsigned tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const SegTile t = seg_tile(tile, tile_layer, layer_tile0, layer_off, layer_len);
+        for (unsigned i = threadIdx.x; i < t.n; i += blockDim.x) dst[t.first + i] = src[t.first + i];
+    }
+}
+
 // Unique + layer write + layer close, single pass. keys: sorted candidates
 // of buffer x; layer L goes to arena[layer_off[L] ..]. The last tile records
 // layer_len[L] and the next 16-aligned offset, resets the buffer's count and
