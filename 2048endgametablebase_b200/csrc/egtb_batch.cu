@@ -105,8 +105,8 @@ struct BatchEngine {
     cudaStream_t cap_stream = nullptr;  // capture only: graphs are launched on the build stream
     cudaEvent_t ev[6];
     DevBuf arena, rates, stage, sets, filters, index, book, comp, status, seeds;
-    DevBuf layer_off, layer_len, book_len, layer_max, first_tile, tile_cnt, tile_off, doff, layer_table;
-    DevBuf tables, ctl, sync, devctl, hist, counters, seed_at;
+    DevBuf layer_off, layer_len, book_len, layer_max, first_tile, tile_cnt, tile_off;
+    DevBuf tables, ctl, sync, devctl, hist, counters, seed_at, seg_tab, seg_hist;
     unsigned char *pinned = nullptr;
     size_t pinned_cap = 0;
     unsigned epoch = 1;
@@ -270,7 +270,6 @@ __global__ void batch_seed_kernel(const BatchTable *__restrict__ T, int n, const
         for (unsigned long long j = at[i] + threadIdx.x; j < at[i + 1]; j += blockDim.x) T[i].stage[0][j - at[i]] = seeds[j];
 }
 
-__global__ void batch_set_count_kernel(unsigned long long *p, unsigned long long v) { *p = v; }
 
 struct Run {
     BatchEngine &B;
@@ -453,76 +452,82 @@ struct Run {
     }
     std::vector<unsigned long long> cand_;
 
-    // One radix sort of the keys of layers 1..steps-1 of every table.
+    // Layers 1..steps-1 of every table sorted, each in its own arena region,
+    // by the free nibbles of its table (per-layer digit positions), digit
+    // width digit_nibbles (1 or 2 nibbles).
     void sort_layers() {
         len.assign(G + 1, 0);
         EGTB_CUDA(cudaMemcpyAsync(len.data(), B.layer_len.p, sizeof(unsigned long long) * (G + 1),
                                   cudaMemcpyDeviceToHost, s()));
         EGTB_CUDA(cudaStreamSynchronize(s()));
-        std::vector<unsigned long long> doff(G + 1, 0);
-        std::vector<int> lt(G, 0);
+        std::vector<int> lt(G + 1, 0);
         int fmax = 0;
         for (int i = 0; i < n; ++i) {
             const TablePlan &t = tp[i];
             fmax = std::max(fmax, t.fn.count);
             for (int L = 0; L <= t.steps; ++L) lt[t.lbase + L] = i;
         }
+        std::vector<int> tab;
+        std::vector<int> tile0(G, 0);
         for (int g = 0; g < G; ++g) {
             const int i = lt[g];
             const int L = g - tp[i].lbase;
-            doff[g + 1] = doff[g] + ((L >= 1 && L < tp[i].steps) ? len[g] : 0ull);
+            if (L < 1 || L >= tp[i].steps) continue;
+            tile0[g] = (int)tab.size();
+            const unsigned long long nt = (len[g] + kTileKeys - 1) / kTileKeys;
+            for (unsigned long long j = 0; j < nt; ++j) tab.push_back(g);
         }
-        const unsigned long long total = doff[G];
-        int tbits = 0, lbits = 0;
-        while ((1 << tbits) < n) ++tbits;
-        while ((1 << lbits) < max_steps) ++lbits;
-        const int fbits = 4 * fmax;
-        if (tbits + lbits + fbits > 64)
-            throw Error(EGTB_ERR_UNSUPPORTED, "table, layer and free-cell bits of this batch exceed 64; build such tables "
-                                              "one at a time");
-        if (total < 2) return;
-        const int nib = (tbits + lbits + fbits + 3) / 4;
-        int dn = prm.digit_nibbles;
-        if ((nib + dn - 1) / dn > kMaxPasses) dn = 2;
-        SortPlan sp;
-        std::memset(&sp, 0, sizeof sp);
-        sp.passes = (nib + dn - 1) / dn;
-        for (int q = 0; q < sp.passes; ++q) {
-            sp.lo[q] = dn * q;
-            sp.hi[q] = (dn == 2 && dn * q + 1 < nib) ? dn * q + 1 : -1;
+        const unsigned ntiles = (unsigned)tab.size();
+        if (ntiles == 0) return;
+        tab.reserve(tab.size() + tile0.size());
+    for (const int v : tile0) tab.push_back(v);
+        int dn = prm.digit_nibbles == 1 ? 1 : 2;
+        if ((fmax + dn - 1) / dn > kMaxPasses) dn = 2;
+        const int passes = (fmax + dn - 1) / dn;
+        std::vector<unsigned short> nib((size_t)G * kMaxPasses, 0xFFFFu);
+        for (int g = 0; g < G; ++g) {
+            const FreeNibbles &fn = tp[lt[g]].fn;
+            for (int q = 0; q < passes; ++q) {
+                const int a = dn * q, b = dn * q + 1;
+                const unsigned lo = a < fn.count ? (unsigned)fn.idx[a] : 0xFFu;
+                const unsigned hi = (dn == 2 && b < fn.count) ? (unsigned)fn.idx[b] : 0xFFu;
+                nib[(size_t)g * kMaxPasses + q] = (unsigned short)(lo | (hi << 8));
+            }
         }
-        B.doff.ensure(sizeof(unsigned long long) * (G + 1), "dense offsets");
-        B.layer_table.ensure(sizeof(int) * G, "layer map");
-        B.comp.ensure(sizeof(uint64_t) * 2 * total, "sort buffers");
-        const unsigned long long tiles = total / kTileKeys + 2;
-        if (B.status.bytes < sizeof(unsigned long long) * 256 * tiles) {
-            B.status.ensure(sizeof(unsigned long long) * 256 * tiles, "sort look-back");
+        const size_t hist_words = (size_t)G * kMaxPasses * 256;
+        B.seg_tab.ensure(sizeof(int) * tab.size(), "layer sort tile map");
+        B.seg_hist.ensure(sizeof(unsigned) * hist_words + sizeof(unsigned short) * nib.size(), "layer sort histograms");
+        B.comp.ensure(sizeof(uint64_t) * std::max<unsigned long long>(arena_total, 1), "sort buffer");
+        if (B.status.bytes < sizeof(unsigned long long) * 256 * ((size_t)ntiles + 2)) {
+            B.status.ensure(sizeof(unsigned long long) * 256 * ((size_t)ntiles + 2), "sort look-back");
             EGTB_CUDA(cudaMemsetAsync(B.status.p, 0, B.status.bytes, s()));
         }
-        EGTB_CUDA(cudaMemcpyAsync(B.doff.p, doff.data(), sizeof(unsigned long long) * (G + 1), cudaMemcpyHostToDevice, s()));
-        EGTB_CUDA(cudaMemcpyAsync(B.layer_table.p, lt.data(), sizeof(int) * G, cudaMemcpyHostToDevice, s()));
-        uint64_t *src = B.comp.as<uint64_t>(), *dst = src + total;
-        const int g = R.sm_count * 8;
+        const int *tile_layer = B.seg_tab.as<int>(), *layer_tile0 = tile_layer + ntiles;
+        unsigned *hist = B.seg_hist.as<unsigned>();
+        unsigned short *seg_nib = reinterpret_cast<unsigned short *>(hist + hist_words);
+        EGTB_CUDA(cudaMemcpyAsync(B.seg_tab.p, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice, s()));
+        EGTB_CUDA(cudaMemcpyAsync(seg_nib, nib.data(), sizeof(unsigned short) * nib.size(), cudaMemcpyHostToDevice, s()));
+        EGTB_CUDA(cudaMemsetAsync(hist, 0, sizeof(unsigned) * hist_words, s()));
         DevCtl *dc = B.devctl.as<DevCtl>();
         EGTB_CUDA(cudaMemsetAsync(dc, 0, sizeof(DevCtl), s()));
-        batch_compose_kernel<<<g, 256, 0, s()>>>(B.tables.as<BatchTable>(), B.layer_table.as<int>(), B.arena.as<uint64_t>(),
-                                                 B.layer_off.as<unsigned long long>(), B.doff.as<unsigned long long>(), G,
-                                                 lbits, fbits, src);
-        EGTB_CUDA(cudaMemsetAsync(B.hist.p, 0, sizeof(unsigned) * kMaxPasses * 256, s()));
-        batch_set_count_kernel<<<1, 1, 0, s()>>>(&dc->cand_count[0], total);
-        sort_hist_kernel<<<R.sm_count * 2, kHistThreads, 0, s()>>>(src, &dc->cand_count[0], total, sp, B.hist.as<unsigned>(),
-                                                          B.counters.as<unsigned>(), dc);
-        launches += 3;
-        for (int q = 0; q < sp.passes; ++q) {
-            onesweep_kernel<<<R.sweep_grid, kSweepThreads, 0, s()>>>(src, dst, &dc->cand_count[0], total, sp, q,
-                                                                    B.hist.as<unsigned>(), B.counters.as<unsigned>(),
-                                                                    B.status.as<unsigned long long>(), B.epoch++, dc);
+        const unsigned long long *loff = B.layer_off.as<unsigned long long>(), *llen = B.layer_len.as<unsigned long long>();
+        seg_hist_kernel<<<R.sm_count * 2, kHistThreads, 0, s()>>>(B.arena.as<uint64_t>(), tile_layer, layer_tile0, loff, llen,
+                                                                  ntiles, passes, seg_nib, hist, B.counters.as<unsigned>());
+        ++launches;
+        uint64_t *src = B.arena.as<uint64_t>(), *dst = B.comp.as<uint64_t>();
+        for (int q = 0; q < passes; ++q) {
+            seg_onesweep_kernel<<<R.sweep_grid, kSweepThreads, 0, s()>>>(src, dst, tile_layer, layer_tile0, loff, llen,
+                                                                        ntiles, seg_nib, q, hist,
+                                                                        B.counters.as<unsigned>(),
+                                                                        B.status.as<unsigned long long>(), B.epoch++, dc);
             std::swap(src, dst);
             ++launches;
         }
-        batch_decompose_kernel<<<g, 256, 0, s()>>>(B.tables.as<BatchTable>(), src, B.layer_off.as<unsigned long long>(),
-                                                   B.doff.as<unsigned long long>(), G, lbits, fbits, B.arena.as<uint64_t>());
-        ++launches;
+        if (src != B.arena.as<uint64_t>()) {
+            seg_copy_kernel<<<R.sm_count * 8, 256, 0, s()>>>(src, B.arena.as<uint64_t>(), tile_layer, layer_tile0, loff,
+                                                             llen, ntiles);
+            ++launches;
+        }
         EGTB_CUDA(cudaGetLastError());
     }
 

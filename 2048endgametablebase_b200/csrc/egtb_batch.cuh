@@ -236,44 +236,6 @@ batch_expand_kernel(const BatchTable *__restrict__ T, BatchCtl *C, int n_tables,
     }
 }
 
-// -------------------------------------------- sorting every table's layers --
-//
-// After the forward pass the keys of layers 1..steps-1 of every table are
-// sorted by one radix sort of composite keys
-// (table << (lbits + 4*F)) | (layer << 4*F) | (free nibbles of the key),
-// F the largest free-cell count of the batch: the order groups by table, then
-// layer, then key, which is each layer's ascending order.
-
-static __global__ void __launch_bounds__(256)
-batch_compose_kernel(const BatchTable *__restrict__ T, const int *__restrict__ layer_table, const uint64_t *__restrict__ arena,
-                     const unsigned long long *__restrict__ layer_off, const unsigned long long *__restrict__ doff,
-                     int n_layers, int lbits, int fbits, uint64_t *__restrict__ comp) {
-    const unsigned long long total = doff[n_layers];
-    for (unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; j < total;
-         j += (unsigned long long)gridDim.x * blockDim.x) {
-        const int g = layer_of_dense(doff, 0, n_layers, j);
-        const int i = layer_table[g];
-        const BatchTable &tb = T[i];
-        const uint64_t key = arena[layer_off[g] + (j - doff[g])];
-        comp[j] = ((uint64_t)i << (lbits + fbits)) | ((uint64_t)(g - tb.lbase) << fbits) | compact_key(key, tb.fn);
-    }
-}
-
-static __global__ void __launch_bounds__(256)
-batch_decompose_kernel(const BatchTable *__restrict__ T, const uint64_t *__restrict__ comp,
-                       const unsigned long long *__restrict__ layer_off, const unsigned long long *__restrict__ doff,
-                       int n_layers, int lbits, int fbits, uint64_t *__restrict__ arena) {
-    const unsigned long long total = doff[n_layers];
-    for (unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; j < total;
-         j += (unsigned long long)gridDim.x * blockDim.x) {
-        const uint64_t c = comp[j];
-        const int i = (int)(c >> (lbits + fbits));
-        const BatchTable &tb = T[i];
-        const int g = tb.lbase + (int)((c >> fbits) & ((1ull << lbits) - 1));
-        arena[layer_off[g] + (j - doff[g])] = expand_key(c & ((1ull << fbits) - 1), tb.fn);
-    }
-}
-
 // Zero `words` 16-byte words at p with every thread of the grid.
 __device__ __forceinline__ void grid_zero16(void *p, unsigned long long words) {
     uint4 *z = reinterpret_cast<uint4 *>(p);

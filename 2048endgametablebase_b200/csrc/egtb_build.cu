@@ -192,7 +192,7 @@ struct Engine {
     int filter_bits = 20;
     int *seg_tab = nullptr;                    // per-layer sort: tile -> layer, then layer -> first tile
     unsigned long long seg_tab_cap = 0;
-    unsigned *seg_hist = nullptr;              // per-layer sort: digit histograms, layer x pass x 256
+    unsigned *seg_hist = nullptr;              // per-layer sort: digit histograms (layer x pass x 256), digit positions
     unsigned long long seg_hist_cap = 0;
     unsigned long long candidates = 0;        // children probed by the last forward pass
     unsigned long long *layer_off = nullptr, *layer_len = nullptr, *book_len = nullptr;
@@ -305,9 +305,11 @@ struct Engine {
             seg_tab_cap = tiles + layers + (tiles + layers) / 4 + 64;
             alloc_or_throw((void **)&seg_tab, sizeof(int) * seg_tab_cap, "layer sort tile map");
         }
-        if (layers * kMaxPasses * 256 > seg_hist_cap) {
+        // histograms (layer x pass x 256) followed by the digit positions (layer x pass, u16)
+        const unsigned long long hist_words = layers * kMaxPasses * 256 + (layers * kMaxPasses + 1) / 2;
+        if (hist_words > seg_hist_cap) {
             release(seg_hist);
-            seg_hist_cap = layers * kMaxPasses * 256;
+            seg_hist_cap = hist_words;
             alloc_or_throw((void **)&seg_hist, sizeof(unsigned) * seg_hist_cap, "layer sort histograms");
         }
         ensure_status(tiles);
@@ -611,28 +613,31 @@ static void enqueue_sort_layers(Engine &E, const ForwardPlan &P, const std::vect
     }
     const unsigned ntiles = (unsigned)tab.size();
     if (ntiles == 0) return;
-    tab.insert(tab.end(), tile0.begin(), tile0.end());
+    tab.reserve(tab.size() + tile0.size());
+    for (const int v : tile0) tab.push_back(v);
     E.ensure_seg(ntiles, (unsigned long long)steps);
     EGTB_CUDA(cudaMemcpyAsync(E.seg_tab, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice, s));
     const int *tile_layer = E.seg_tab, *layer_tile0 = E.seg_tab + ntiles;
+    // digit positions of every pass (two free nibbles each), the same for every layer
     const int F = P.free.count;
-    SortPlan sp;
-    std::memset(&sp, 0, sizeof sp);
-    sp.passes = (F + 1) / 2;
-    for (int q = 0; q < sp.passes; ++q) {
-        sp.lo[q] = P.free.idx[2 * q];
-        sp.hi[q] = 2 * q + 1 < F ? P.free.idx[2 * q + 1] : -1;
-    }
+    const int passes = (F + 1) / 2;
+    std::vector<unsigned short> nib((size_t)steps * kMaxPasses, 0xFFFFu);
+    for (int L = 0; L < steps; ++L)
+        for (int q = 0; q < passes; ++q)
+            nib[(size_t)L * kMaxPasses + q] =
+                (unsigned short)(P.free.idx[2 * q] | ((2 * q + 1 < F ? P.free.idx[2 * q + 1] : 0xFF) << 8));
+    unsigned short *seg_nib = reinterpret_cast<unsigned short *>(E.seg_hist + (size_t)steps * kMaxPasses * 256);
+    EGTB_CUDA(cudaMemcpyAsync(seg_nib, nib.data(), sizeof(unsigned short) * nib.size(), cudaMemcpyHostToDevice, s));
     const int pu = E.prof_begin(K_UNIQUE);
     EGTB_CUDA(cudaMemsetAsync(E.seg_hist, 0, sizeof(unsigned) * (size_t)steps * kMaxPasses * 256, s));
     EGTB_LAUNCH(E, seg_hist_kernel<<<E.sm_count * 2, kHistThreads, 0, s>>>(E.arena, tile_layer, layer_tile0, E.layer_off,
-                                                                         E.layer_len, ntiles, sp, E.seg_hist,
-                                                                         E.counters));
+                                                                         E.layer_len, ntiles, passes, seg_nib,
+                                                                         E.seg_hist, E.counters));
     uint64_t *src = E.arena, *dst = (uint64_t *)E.book;  // the book buffer is free until the solve
-    for (int q = 0; q < sp.passes; ++q) {
+    for (int q = 0; q < passes; ++q) {
         const int pi = E.prof_begin(K_SORT_PASS);
         EGTB_LAUNCH(E, seg_onesweep_kernel<<<E.sweep_grid, kSweepThreads, 0, s>>>(
-                           src, dst, tile_layer, layer_tile0, E.layer_off, E.layer_len, ntiles, sp, q, E.seg_hist,
+                           src, dst, tile_layer, layer_tile0, E.layer_off, E.layer_len, ntiles, seg_nib, q, E.seg_hist,
                            E.counters, E.status, E.epoch++, E.ctl));
         E.prof_end(pi);
         std::swap(src, dst);

@@ -456,42 +456,18 @@ dedup_seed_kernel(const uint64_t *__restrict__ keys, unsigned long long n, uint6
         dedup_insert_zero(set, mask, keys[i], &ctl->err);
 }
 
-// ------------------------------------------------- layer sort helpers ----
+// ------------------------------------------------------ free nibbles ----
 //
 // After the forward pass each layer holds its unique keys in arrival order;
 // the layers are sorted by their free nibbles (the others are 0xF in every
-// key of the pattern): the plain build sorts each layer in its own region
-// (seg_* kernels, egtb_sort.cuh), the batched build sorts composite keys
-// (table, layer, compacted free nibbles) with these helpers.
+// key of the pattern), each in its own arena region (seg_* kernels,
+// egtb_sort.cuh), in the plain and the batched build alike.
 
 struct FreeNibbles {
     int count;
     int idx[16];       // free nibble positions, least significant first
     uint64_t pinned;   // every other nibble is 0xF
 };
-
-__device__ __forceinline__ uint64_t compact_key(uint64_t key, const FreeNibbles &fn) {
-    uint64_t c = 0;
-#pragma unroll 16
-    for (int k = 0; k < fn.count; ++k) c |= ((key >> (4 * fn.idx[k])) & 0xFull) << (4 * k);
-    return c;
-}
-
-__device__ __forceinline__ uint64_t expand_key(uint64_t c, const FreeNibbles &fn) {
-    uint64_t key = fn.pinned;
-#pragma unroll 16
-    for (int k = 0; k < fn.count; ++k) key |= ((c >> (4 * k)) & 0xFull) << (4 * fn.idx[k]);
-    return key;
-}
-
-// dense index j -> layer L with doff[L] <= j < doff[L+1]
-__device__ __forceinline__ int layer_of_dense(const unsigned long long *doff, int lo, int hi, unsigned long long j) {
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (doff[mid] <= j) lo = mid; else hi = mid;
-    }
-    return lo;
-}
 
 // Single block: exclusive scan of the tile counts; total -> *total_out.
 static __global__ void __launch_bounds__(1024)

@@ -251,9 +251,20 @@ onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, co
 // nibbles only (the other nibbles are 0xF in every key of a layer): tiles of
 // kTileKeys keys never straddle two layers (tile_layer[j] is tile j's layer,
 // layer_tile0[L] the first tile of layer L), each layer has its own digit
-// histograms (hist_l[(L * kMaxPasses + p) * 256 + d]), and the look-back of a
-// tile stops at its layer's first tile, which publishes its counts as a
-// prefix. The layer digits of a composite (layer, key) sort are not needed.
+// histograms (hist_l[(L * kMaxPasses + p) * 256 + d]) and its own digit
+// positions (seg_nib[L * kMaxPasses + p]: the less significant nibble in the
+// low byte, the more significant one in the high byte, 0xFF for none, so the
+// layers of tables with different free cells sort together), and the
+// look-back of a tile stops at its layer's first tile, which publishes its
+// counts as a prefix. The layer digits of a composite (layer, key) sort are
+// not needed.
+
+__device__ __forceinline__ unsigned seg_digit(uint64_t key, unsigned nib2) {
+    const unsigned lo = nib2 & 0xFFu, hi = nib2 >> 8;
+    unsigned d = lo != 0xFFu ? (unsigned)(key >> (4 * lo)) & 0xFu : 0u;
+    if (hi != 0xFFu) d |= ((unsigned)(key >> (4 * hi)) & 0xFu) << 4;
+    return d;
+}
 
 // A tile's layer, its first key in the arena and its key count.
 struct SegTile {
@@ -284,9 +295,11 @@ __device__ __forceinline__ SegTile seg_tile(unsigned tile, const int *__restrict
 static __global__ void __launch_bounds__(kHistThreads, 2)
 seg_hist_kernel(const uint64_t *__restrict__ keys, const int *__restrict__ tile_layer,
                 const int *__restrict__ layer_tile0, const unsigned long long *__restrict__ layer_off,
-                const unsigned long long *__restrict__ layer_len, unsigned ntiles, SortPlan sp,
-                unsigned *__restrict__ hist_l, unsigned *__restrict__ counters) {
+                const unsigned long long *__restrict__ layer_len, unsigned ntiles, int passes,
+                const unsigned short *__restrict__ seg_nib, unsigned *__restrict__ hist_l,
+                unsigned *__restrict__ counters) {
     __shared__ unsigned h[kMaxPasses][256];
+    __shared__ unsigned nib[kMaxPasses];
     for (int i = threadIdx.x; i < kMaxPasses * 256; i += blockDim.x) (&h[0][0])[i] = 0;
     if (blockIdx.x == 0 && threadIdx.x < 16) counters[threadIdx.x] = 0;
     __syncthreads();
@@ -298,7 +311,7 @@ seg_hist_kernel(const uint64_t *__restrict__ keys, const int *__restrict__ tile_
     auto flush = [&]() {
         __syncthreads();
         unsigned *out = hist_l + (size_t)cur * kMaxPasses * 256;
-        for (int i = threadIdx.x; i < sp.passes * 256; i += blockDim.x) {
+        for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
             const unsigned c = (&h[0][0])[i];
             if (c) {
                 atomicAdd(out + i, c);
@@ -312,6 +325,8 @@ seg_hist_kernel(const uint64_t *__restrict__ keys, const int *__restrict__ tile_
         if (t.layer != cur) {
             if (cur >= 0) flush();
             cur = t.layer;
+            if (threadIdx.x < kMaxPasses) nib[threadIdx.x] = seg_nib[(size_t)cur * kMaxPasses + threadIdx.x];
+            __syncthreads();
         }
         uint64_t k[kHistKeys];
 #pragma unroll
@@ -322,8 +337,8 @@ seg_hist_kernel(const uint64_t *__restrict__ keys, const int *__restrict__ tile_
 #pragma unroll
         for (int r = 0; r < kHistKeys; ++r) {
             const bool valid = (unsigned)r * kHistThreads + threadIdx.x < t.n;
-            for (int p = 0; p < sp.passes; ++p) {
-                const unsigned d = valid ? sort_digit(k[r], sp, p) : 256u;
+            for (int p = 0; p < passes; ++p) {
+                const unsigned d = valid ? seg_digit(k[r], nib[p]) : 256u;
                 const unsigned d0 = __shfl_sync(0xFFFFFFFFu, d, 0);
                 if (__all_sync(0xFFFFFFFFu, d == d0)) {
                     if (lane == 0 && d0 < 256u) atomicAdd(&h[p][d0], 32u);
@@ -341,8 +356,9 @@ seg_hist_kernel(const uint64_t *__restrict__ keys, const int *__restrict__ tile_
 static __global__ void __launch_bounds__(kSweepThreads, 2)
 seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, const int *__restrict__ tile_layer,
                     const int *__restrict__ layer_tile0, const unsigned long long *__restrict__ layer_off,
-                    const unsigned long long *__restrict__ layer_len, unsigned ntiles, SortPlan sp, int p,
-                    const unsigned *__restrict__ hist_l, unsigned *__restrict__ counters,
+                    const unsigned long long *__restrict__ layer_len, unsigned ntiles,
+                    const unsigned short *__restrict__ seg_nib, int p, const unsigned *__restrict__ hist_l,
+                    unsigned *__restrict__ counters,
                     unsigned long long *__restrict__ status, unsigned epoch, DevCtl *ctl) {
     __shared__ uint64_t tkeys[kTileKeys];
     __shared__ unsigned short wcnt[kSweepWarps][256];
@@ -359,6 +375,7 @@ seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst
         const unsigned tile = tile_sh;
         if (tile >= ntiles) break;
         const SegTile t = seg_tile(tile, tile_layer, layer_tile0, layer_off, layer_len);
+        const unsigned nib2 = seg_nib[(size_t)t.layer * kMaxPasses + p];
         // start of every digit of this layer in the layer's region
         unsigned long long ghist_d;
         {
@@ -378,7 +395,7 @@ seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst
         for (int r = 0; r < kSweepKeys; ++r) {
             const unsigned idx = base + (unsigned)r * 32 + lane;
             const bool valid = idx < t.n;
-            const unsigned dg = valid ? sort_digit(k[r], sp, p) : 256u;
+            const unsigned dg = valid ? seg_digit(k[r], nib2) : 256u;
             const unsigned peers = __match_any_sync(0xFFFFFFFFu, dg);
             const unsigned before = __popc(peers & ((1u << lane) - 1u));
             unsigned c = 0;
@@ -423,7 +440,7 @@ seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst
         __syncthreads();
         for (unsigned i = threadIdx.x; i < t.n; i += kSweepThreads) {
             const uint64_t key = tkeys[i];
-            const unsigned dg = sort_digit(key, sp, p);
+            const unsigned dg = seg_digit(key, nib2);
             dst[gbase[dg] + (i - loff[dg])] = key;
         }
         __syncthreads();
