@@ -95,8 +95,8 @@ __device__ __forceinline__ unsigned long long look_back(const unsigned long long
 
 // Digit histograms of every pass; also resets the tile counters of the coming
 // passes and counts the candidates. Each thread has kHistKeys loads in flight
-// (coalesced across the block); a digit shared by the whole warp - the common
-// case for the layer digits of composite keys - is counted with one
+// (coalesced across the block); a digit shared by the whole warp (common for
+// the high nibbles of sorted or clustered keys) is counted with one
 // shared-memory atomic, other digits with one atomic per lane.
 constexpr int kHistThreads = 512;
 constexpr int kHistKeys = 8;

@@ -280,7 +280,8 @@ EGTB_API int egtb_find_classic_value(const char *pathname, const char *filename,
  * gets the same books, byte for byte; all tables advance one global layer
  * step per kernel launch (forward: expand + dedup of layer t of every table;
  * backward: solve + rate index of layer t of every table), the per-step
- * loops replayed as CUDA graphs, one radix sort for every table's layers. */
+ * loops replayed as CUDA graphs, one radix sort pass at a time over every
+ * table's layers, each layer in its own region. */
 typedef struct egtb_batch_params {
     int32_t expand_chunk;         /* parents per work item of the forward step: multiple of 32 in 32..4096 (0: tuned, else 128) */
     int32_t expand_blocks_per_sm; /* blocks per SM of the forward step, 1..8 (0: tuned, else 3) */
