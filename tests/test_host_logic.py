@@ -112,3 +112,32 @@ def test_capacity_failure_raises_the_reference_message(monkeypatch):
         assert bb._should_retry_build_resume(ei.value) is retry
         if retry:
             assert str(ei.value) == F.CAPACITY_MESSAGE
+
+
+# The catalog entries of the reference's variant patterns (its
+# patterns_config.json format), parsed as the build reads them.
+_VARIANT_ENTRIES = {
+    "2x4": {"category": "variant", "valid pattern": [], "target pos": "0xffffffff0000", "canonical mode": "min24",
+            "seed boards": ["0xffff00000000ffff"], "extra steps": 48},
+    "3x3": {"category": "variant", "valid pattern": [], "target pos": "0xfff0fff0fff00000", "canonical mode": "min33",
+            "seed boards": ["0x000f000f000fffff"], "extra steps": 60},
+    "3x4": {"category": "variant", "valid pattern": [], "target pos": "0xffffffffffff0000", "canonical mode": "min34",
+            "seed boards": ["0x000000000000ffff"], "extra steps": 60},
+}
+
+
+@pytest.mark.parametrize("key", H.VARIANT_CASES)
+def test_variant_catalog_entries_match_golden_cases(key):
+    """Masks, success shifts, symmetry mode, seeds, steps and docheck of the
+    variant patterns as the golden cases (made by the reference) hold them."""
+    P = patterns()
+    case = H.cases()[key]
+    meta = P.parse_entry(case["pattern"], _VARIANT_ENTRIES[case["pattern"]])
+    assert [hex(int(m)) for m in meta["pattern_masks"]] == case["masks"]
+    assert list(meta["success_shifts"]) == case["shifts"]
+    assert P.SYMM_MODES[meta["canonical_mode"]] == case["symm_mode"]
+    assert [hex(int(s)) for s in meta["seed_boards"]] == case["seeds"]
+    assert -meta["nums_adjust"] == case["tile_sum0"]
+    steps, docheck = P.steps_and_docheck(case["tile_sum0"], case["target"], meta["extra_steps"])
+    assert (steps, docheck) == (case["steps"], case["docheck_step"])
+    assert case.get("is_variant") is True
