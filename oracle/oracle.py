@@ -187,11 +187,100 @@ class Build:
         rec["rate"] = rates[live]
         return rec.tobytes()
 
+    def live(self, t: int, dtype: str):
+        """(keys, rates) of book t: the entries with rate > zero."""
+        keys, rates = self.layer(t), self.rates(t)
+        live = rates > rates.dtype.type(_ZERO[dtype])
+        return keys[live], rates[live]
+
+    def books(self, dtype: str, deletion: float = 0.0, optimal: bool = False, variant: bool = False) -> list:
+        """Every .book's bytes with the reference's post-passes applied.
+
+        deletion > 0 (BookSolver.cpp:589-593): after solving layer i the book of
+        layer i+2 keeps only rates above T(deletion * (max - zero) + zero), so
+        books 2..steps-1 are thinned (books 0 and 1 never are; a thinned book is
+        never read by a later solve).
+        optimal (keep_only_optimal_branches_impl, BookSolver.cpp:611-735): for
+        i = 21..steps-1, book i keeps the entries that are the best move of a
+        position of the (already thinned) book i-2 plus a 4 or of book i-1 plus
+        a 2: first strictly largest rate over the moves left, right, up, down
+        that moved and stay in the pattern; no move above zero marks entry 0."""
+        steps = self.steps
+        books = [self.live(t, dtype) for t in range(steps)]
+        if deletion > 0.0:
+            T = books[0][1].dtype.type
+            thr = _threshold(T, deletion, dtype)
+            for t in range(2, steps):
+                k, r = books[t]
+                keep = r > thr
+                books[t] = (k[keep], r[keep])
+        if optimal:
+            zero = books[0][1].dtype.type(_ZERO[dtype])
+            for i in range(21, steps):
+                k2, r2 = books[i]
+                mark = np.zeros(len(k2), dtype=bool)
+                if len(k2):
+                    for parents, v in ((books[i - 2][0], 2), (books[i - 1][0], 1)):
+                        _mark_best_moves(parents, v, k2, r2, zero, self.spec, variant, mark)
+                books[i] = (k2[mark], r2[mark])
+        out = []
+        for k, r in books:
+            rec = np.zeros(len(k), dtype=[("board", "<u8"), ("rate", r.dtype)])
+            rec["board"] = k
+            rec["rate"] = r
+            out.append(rec.tobytes())
+        return out
+
     def __del__(self):
         try:
             lib().or_free(self.h)
         except Exception:
             pass
+
+
+_ZERO = {"uint32": 0, "uint64": 0, "float32": 0.0, "float64": 0.0, "1-float32": -1.0, "1-float64": -1.0}
+_MAX = {"uint32": 4e9, "uint64": 1.6e18, "float32": 1.0, "float64": 1.0, "1-float32": 0.0, "1-float64": 0.0}
+
+
+def _threshold(T, deletion: float, dtype: str):
+    """static_cast<T>(deletion * double(max - zero) + double(zero)): truncation for
+    the integer kinds, rounding to nearest for float."""
+    x = deletion * (_MAX[dtype] - _ZERO[dtype]) + _ZERO[dtype]
+    return T(int(x)) if np.issubdtype(T, np.integer) else T(x)
+
+
+def _is_pattern(boards: np.ndarray, masks: np.ndarray) -> np.ndarray:
+    if len(masks) == 0:
+        return np.ones(boards.shape, dtype=bool)
+    ok = np.zeros(boards.shape, dtype=bool)
+    for m in masks:
+        ok |= (boards & np.uint64(m)) == np.uint64(m)
+    return ok
+
+
+def _mark_best_moves(parents, v, k2, r2, zero, spec, variant, mark):
+    """find_optimal_branches (BookSolver.cpp:611-645) over one parent book."""
+    parents = np.asarray(parents, dtype=np.uint64)
+    n2 = len(k2)
+    for cell in range(16):
+        sel = parents[((parents >> np.uint64(4 * cell)) & np.uint64(0xF)) == 0]
+        if len(sel) == 0:
+            continue
+        spawned = sel | np.uint64(v << (4 * cell))
+        mv = move_all_dir(spawned, variant)                                  # (n, 4)
+        valid = (mv != spawned[:, None]) & _is_pattern(mv, spec.masks)
+        key = canonical(mv.reshape(-1), int(spec.c.symm_mode)).reshape(mv.shape)
+        pos = np.searchsorted(k2, key)
+        posc = np.minimum(pos, n2 - 1)
+        found = valid & (pos < n2) & (k2[posc] == key)
+        rate = np.where(found, r2[posc], zero)
+        best = np.full(len(sel), zero, dtype=r2.dtype)
+        best_index = np.zeros(len(sel), dtype=np.int64)
+        for d in range(4):
+            up = found[:, d] & (rate[:, d] > best)
+            best = np.where(up, rate[:, d], best)
+            best_index = np.where(up, posc[:, d], best_index)
+        mark[best_index] = True
 
 
 def free_inits(t32ks: int, t2s: int) -> np.ndarray:

@@ -73,3 +73,19 @@ def test_free5_book_data_fixture():
     b.solve("float32", 0.1)
     for t in range(case["steps"]):
         assert b.book(t, "float32") == data[f"book_{t}"].tobytes(), t
+
+
+POST_PASS_CASES = [k for k, v in H.cases().items() if v.get("size_class") in ("deletion", "optimal")]
+
+
+@pytest.mark.parametrize("key", POST_PASS_CASES)
+def test_oracle_post_pass_books(key):
+    """The oracle's restated post-passes (deletion threshold, optimal branch)
+    give the reference's books byte for byte."""
+    case = H.cases()[key]
+    b = _build(case)
+    b.solve(case["dtype"], case["spawn_rate4"])
+    books = b.books(case["dtype"], case.get("deletion_threshold", 0.0), case.get("optimal_branch_only", False),
+                    case.get("is_variant", False))
+    for t in range(case["steps"]):
+        assert H.sha_bytes(books[t]) == case["book_sha256"][t], (key, t)
