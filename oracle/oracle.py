@@ -7,6 +7,7 @@ this module.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 
@@ -308,3 +309,134 @@ def free_inits(t32ks: int, t2s: int) -> np.ndarray:
         if len(out) >= len(gen) - 3:
             break
     return np.unique(np.array(out, dtype=np.uint64))
+
+
+# ------------------------------------------------------------------ reader --
+# ClassicBookReader.move_on_dic restated (native_core/src/ReaderRuntime.cpp).
+
+_DIRECTION_NAMES = ("up", "right", "down", "left")      # kDirectionNames, :32
+_ORDERED_KEYS = ("down", "right", "left", "up")         # kOrderedResultKeys, :33
+_DTYPE_INFO = {"uint32": (4e9, 0.0), "uint64": (1.6e18, 0.0), "float32": (1.0, 0.0), "float64": (1.0, 0.0),
+               "1-float32": (0.0, -1.0), "1-float64": (0.0, -1.0)}  # dtype_info_for_name, :190-206
+_REC = {"uint32": "<u4", "uint64": "<u8", "float32": "<f4", "float64": "<f8", "1-float32": "<f4", "1-float64": "<f8"}
+
+
+def _apply_operation(m, op: int):
+    """apply_operation (:127-147) on a 4x4 list matrix."""
+    a = np.array(m, dtype=np.int64)
+    left = lambda x: np.array([[x[r][3 - c] for r in range(4)] for c in range(4)])   # rotated[3-c][r] = x[r][c]
+    right = lambda x: np.array([[x[3 - r][c] for r in range(4)] for c in range(4)])  # rotated[c][3-r] = x[r][c]
+    half = lambda x: x[::-1, ::-1]
+    flip = lambda x: x[:, ::-1]
+    out = {0: a, 1: left(a), 2: half(a), 3: right(a), 4: flip(a), 5: flip(left(a)), 6: flip(half(a)),
+           7: flip(right(a))}[op]
+    return out.tolist()
+
+
+def _encode(m) -> int:
+    """encode_board_matrix (BoardCodec.h:20-29): log2 of each tile, row 0 high."""
+    b = 0
+    for r in range(4):
+        for c in range(4):
+            v = int(m[r][c])
+            b |= (v.bit_length() - 1 if v >= 2 else 0) << (4 * ((3 - r) * 4 + (3 - c)))
+    return b
+
+
+def _adjust_direction(op: int, name: str) -> str:
+    """adjust_direction (:149-169)."""
+    if op >= 4 and name in ("left", "right"):
+        name = "right" if name == "left" else "left"
+    idx = {"up": 0, "right": 1, "down": 2, "left": 3}[name]
+    return _DIRECTION_NAMES[(idx + op % 4) % 4]
+
+
+def _round_half_away(x: float) -> float:
+    f = math.floor(abs(x))
+    r = f + (1.0 if abs(x) - f >= 0.5 else 0.0)
+    return math.copysign(r, x)
+
+
+def _present(raw, dtype: str) -> float:
+    """normalize_raw_value + maybe_round_value (:208-214, :271-277); the -Ofast
+    build divides by 10^9 as a multiplication by its reciprocal."""
+    max_scale = _DTYPE_INFO[dtype][0]
+    v = float(raw)
+    if np.issubdtype(np.dtype(_REC[dtype]), np.integer) and max_scale > 1.0:
+        v = v / max_scale
+    if "32" in dtype and abs(v) > 1e-7:
+        v = _round_half_away(v * 1e9) * (1.0 / 1e9)
+    return v
+
+
+def _file_lookup(path: str, key: int, dtype: str):
+    """find_success_entry_in_file (:279-316): binary search over the records as
+    they lie in the file; a miss reads as the dtype's zero."""
+    rec = np.fromfile(path, dtype=[("board", "<u8"), ("rate", _REC[dtype])])
+    n = len(rec)
+    left, right = 0, n - 1
+    while n and left <= right:
+        mid = (left + right) // 2
+        b = int(rec["board"][mid])
+        if b == key:
+            return _present(rec["rate"][mid], dtype)
+        if b < key:
+            left = mid + 1
+        else:
+            if mid == 0:
+                break
+            right = mid - 1
+    return _present(_DTYPE_INFO[dtype][1], dtype)
+
+
+class Reader:
+    """ClassicBookReader (:1050-1067) with move_on_dic (evaluate_classic_result_candidates, :739-840)."""
+
+    def __init__(self, masks, symm_mode: int, is_variant: bool = False, prefer_max: bool = False):
+        self.masks = np.asarray(list(masks), dtype=np.uint64)
+        self.symm = int(symm_mode)
+        self.variant = bool(is_variant)
+        self.prefer_max = bool(prefer_max)
+        self.last_op = 0
+
+    def move_on_dic(self, board, path_list, pattern_full: str, nums_adjust: int):
+        if not path_list:
+            return [("?", "?")], ""
+        s = sum(int(v) for row in board for v in row) + int(nums_adjust)
+        nums = int(s / 2) if s >= 0 else -((-s) // 2)  # C++ division
+        blank = [("down", ""), ("right", ""), ("left", ""), ("up", "")]
+        if nums < 0:
+            return blank, ""
+        final, best, dt_out = blank, 0.0, ""
+        ops = [0] if self.variant else [self.last_op] + list(range(8))  # operation_sequence, :171-182
+        for directory, dtype in path_list:
+            path = os.path.join(directory, f"{pattern_full}_{nums}.book")
+            if not os.path.exists(directory) or best > 0.0 or not os.path.exists(path):
+                continue
+            for op in ops:
+                enc = _encode(_apply_operation(board, op))
+                if not _is_pattern(np.array([enc], dtype=np.uint64), self.masks)[0]:
+                    continue
+                mv = move_all_dir(np.array([enc], dtype=np.uint64), self.variant)[0]
+                values = [None] * 4  # in _ORDERED_KEYS order
+                slot_of_move = (2, 1, 3, 0)  # left, right, up, down -> down/right/left/up slots
+                for d in range(4):
+                    m = int(mv[d])
+                    if m == enc or not _is_pattern(np.array([m], dtype=np.uint64), self.masks)[0]:
+                        continue
+                    key = int(canonical(np.array([m], dtype=np.uint64), self.symm)[0])
+                    values[slot_of_move[d]] = _file_lookup(path, key, dtype)
+                entries = [(_adjust_direction(op, k), values[i]) for i, k in enumerate(_ORDERED_KEYS)]
+                numeric = [e for e in entries if e[1] is not None]
+                others = [e for e in entries if e[1] is None]
+                numeric.sort(key=lambda e: -e[1])  # stable, descending (sort_adjusted_entries, :244-269)
+                if not numeric:
+                    continue
+                self.last_op = op
+                result = numeric + others
+                if self.prefer_max:
+                    if numeric[0][1] > best:
+                        best, final, dt_out = numeric[0][1], result, dtype
+                else:
+                    return result, dtype
+        return final, dt_out

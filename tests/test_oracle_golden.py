@@ -89,3 +89,25 @@ def test_oracle_post_pass_books(key):
                     case.get("is_variant", False))
     for t in range(case["steps"]):
         assert H.sha_bytes(books[t]) == case["book_sha256"][t], (key, t)
+
+
+READER_CPU_CASES = sorted(k for k in H.reader_cases() if k in set(H.SMALL_CPU_CASES + H.VARIANT_CPU_CASES))
+
+
+@pytest.mark.parametrize("key", READER_CPU_CASES)
+def test_oracle_reader_answers(key, tmp_path):
+    """The oracle's move_on_dic over the oracle's own books gives the reference
+    reader's answers, position after position (the reader's last operation
+    carries over, as in the reference)."""
+    case = H.cases()[key]
+    b = _build(case)
+    b.solve(case["dtype"], case["spawn_rate4"])
+    books = b.books(case["dtype"])
+    name = case["pattern_full"]
+    for t, data in enumerate(books):
+        (tmp_path / f"{name}_{t}.book").write_bytes(data)
+    reader = O.Reader([int(m, 16) for m in case["masks"]], case["symm_mode"], case.get("is_variant", False))
+    for i, entry in enumerate(H.reader_cases()[key]):
+        res, dt = reader.move_on_dic(entry["board"], [(str(tmp_path), case["dtype"])], name, -case["tile_sum0"])
+        assert [[k, v] for k, v in res] == entry["result"], (key, i, entry["board"])
+        assert dt == entry["dtype"], (key, i)
