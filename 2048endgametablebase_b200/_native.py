@@ -142,6 +142,7 @@ _SIGS = {
     "egtb_profile": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
     "egtb_profile_read": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(KernelTimeC), ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_int)]),
+    "egtb_set_spin_limit": (ctypes.c_int, [ctypes.c_uint32]),
     "egtb_get_build_progress": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
     "egtb_reset_build_progress": (ctypes.c_int, [ctypes.c_uint32]),
     "egtb_build": (ctypes.c_int, [_P, ctypes.c_size_t, ctypes.POINTER(PatternSpecC), ctypes.POINTER(RunOptionsC),

@@ -26,7 +26,7 @@ import numpy as np
 from . import _native as N
 
 __all__ = ["Table", "random_tables", "build_batch", "build_one_at_a_time", "autotune", "batch_book",
-           "plain_book", "region_mask"]
+           "plain_book", "region_mask", "batch_mismatches"]
 
 
 def _nibble(r: int, c: int) -> int:
@@ -209,3 +209,19 @@ def plain_book(layer: int, device: int = 0) -> bytes:
     buf = ctypes.create_string_buffer(max(1, n.value))
     N.check(N.lib().egtb_book_layer_copy(int(device), int(layer), buf, n.value, ctypes.byref(n)))
     return buf.raw[:n.value]
+
+
+def batch_mismatches(tables: list[Table], dtype: str = "float32", device: int = 0) -> list[str]:
+    """Check the device's last batch (built from `tables`) against the plain
+    path: every table is rebuilt alone by egtb_build and each of its books is
+    compared byte for byte with the batch's. Returns the names of the tables
+    whose books differ (empty: the batch is exact). The batch's books stay on
+    the device through the plain builds (they live in the batch's own buffers)."""
+    bad = []
+    for i, t in enumerate(tables):
+        build_one_at_a_time([t], dtype, device)
+        for L in range(t.steps):
+            if batch_book(i, L, device) != plain_book(L, device):
+                bad.append(t.name)
+                break
+    return bad

@@ -519,7 +519,8 @@ struct Run {
             seg_onesweep_kernel<<<R.sweep_grid, kSweepThreads, 0, s()>>>(src, dst, tile_layer, layer_tile0, loff, llen,
                                                                         ntiles, seg_nib, q, hist,
                                                                         B.counters.as<unsigned>(),
-                                                                        B.status.as<unsigned long long>(), B.epoch++, dc);
+                                                                        B.status.as<unsigned long long>(), B.epoch++, dc,
+                                                                        look_back_spin_limit());
             std::swap(src, dst);
             ++launches;
         }

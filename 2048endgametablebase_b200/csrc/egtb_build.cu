@@ -638,7 +638,7 @@ static void enqueue_sort_layers(Engine &E, const ForwardPlan &P, const std::vect
         const int pi = E.prof_begin(K_SORT_PASS);
         EGTB_LAUNCH(E, seg_onesweep_kernel<<<E.sweep_grid, kSweepThreads, 0, s>>>(
                            src, dst, tile_layer, layer_tile0, E.layer_off, E.layer_len, ntiles, seg_nib, q, E.seg_hist,
-                           E.counters, E.status, E.epoch++, E.ctl));
+                           E.counters, E.status, E.epoch++, E.ctl, look_back_spin_limit()));
         E.prof_end(pi);
         std::swap(src, dst);
     }
@@ -725,7 +725,7 @@ static uint64_t *enqueue_layer_sort(Engine &E, const SortPlan &sp, const uint64_
     for (int q = 0; q < sp.passes; ++q) {
         const int pi = E.prof_begin(K_SORT_PASS);
         EGTB_LAUNCH(E, onesweep_kernel<<<E.sweep_grid, kSweepThreads, 0, s>>>(in, out, n_ptr, E.sort_cap, sp, q, E.hist,
-                                                                             E.counters, E.status, E.epoch++, E.ctl));
+                                                                             E.counters, E.status, E.epoch++, E.ctl, look_back_spin_limit()));
         E.prof_end(pi);
         in = out;
         out = out == E.sort_buf[0] ? E.sort_buf[1] : E.sort_buf[0];

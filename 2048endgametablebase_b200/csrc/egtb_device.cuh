@@ -10,6 +10,10 @@
 
 namespace egtb {
 
+// Default number of polls of a bounded wait on another block (sort look-back).
+constexpr unsigned kSpinLimit = 1u << 22;
+
+
 constexpr int kMaxMasks = 32;
 
 // Pattern parameters handed to every kernel by value.

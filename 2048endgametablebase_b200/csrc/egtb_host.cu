@@ -5,6 +5,7 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <atomic>
 #include <cerrno>
 #include <cmath>
 #include <condition_variable>
@@ -21,7 +22,19 @@ static thread_local std::string g_last_error;
 void set_last_error(const std::string &msg) { g_last_error = msg; }
 void clear_last_error() { g_last_error.clear(); }
 
+static std::atomic<unsigned> g_spin_limit{0};  // 0: kSpinLimit
+
+unsigned look_back_spin_limit() {
+    const unsigned v = g_spin_limit.load(std::memory_order_relaxed);
+    return v ? v : kSpinLimit;
+}
+
 }  // namespace egtb
+
+extern "C" int egtb_set_spin_limit(uint32_t polls) {
+    egtb::g_spin_limit.store(polls, std::memory_order_relaxed);
+    return EGTB_OK;
+}
 
 extern "C" int egtb_last_error(char *buf, size_t len) {
     if (!buf || len == 0) return EGTB_ERR_ARG;

@@ -82,6 +82,10 @@ std::string parent_dir(const std::string &path);
 std::string now_string();
 double round_to_2(double v);
 
+// Polls a sort look-back wait makes before it gives up (egtb_set_spin_limit;
+// process-wide, read at every launch).
+unsigned look_back_spin_limit();
+
 // Byte size of SuccessEntry<T> records, native_core/include/FormationRuntime.h:191-205.
 inline size_t record_size(int dtype) { return 8 + dtype_size(dtype); }
 

@@ -56,6 +56,10 @@ struct ServeRequest {
     float *d_out = nullptr;
     uint8_t *d_valid = nullptr;
     Clock::time_point t_submit;
+    // latency is measured from here: the submit time, or for a replayed
+    // stream the request's scheduled arrival (so time a late driver thread
+    // spent behind the schedule counts as queueing)
+    Clock::time_point t_arrival;
     double latency_us = 0.0;
     bool done = false;
 };
@@ -121,7 +125,7 @@ static void serve_loop(egtb_server *S) {
                         std::memcpy(rq->out, sl.h_out + 4 * sl.at[r], rq->n * 4 * sizeof(float));
                         if (rq->valid) std::memcpy(rq->valid, sl.h_valid + sl.at[r], rq->n);
                     }
-                    rq->latency_us = std::chrono::duration<double, std::micro>(now - rq->t_submit).count();
+                    rq->latency_us = std::chrono::duration<double, std::micro>(now - rq->t_arrival).count();
                     finished.push_back(rq);
                 }
                 sl.reqs.clear();
@@ -277,8 +281,11 @@ extern "C" int egtb_serve_start(egtb_book *const *books, int32_t n_books, int32_
     });
 }
 
-extern "C" int egtb_serve_submit(egtb_server *S, int32_t book, const uint64_t *positions, uint64_t n, float *values4,
-                                 uint8_t *valid_mask, uint64_t *ticket) {
+namespace egtb {
+
+// egtb_serve_submit with the time its latency is measured from (arrival <= now).
+static int serve_submit_at(egtb_server *S, int32_t book, const uint64_t *positions, uint64_t n, float *values4,
+                           uint8_t *valid_mask, uint64_t *ticket, const Clock::time_point *arrival) {
     return guarded([&] {
         if (!S || !ticket) throw Error(EGTB_ERR_ARG, "NULL argument");
         if (book < 0 || book >= (int)S->books.size()) throw Error(EGTB_ERR_ARG, "book index out of range");
@@ -308,11 +315,25 @@ extern "C" int egtb_serve_submit(egtb_server *S, int32_t book, const uint64_t *p
             rq->d_valid = (uint8_t *)dv;
         }
         rq->t_submit = Clock::now();
+        rq->t_arrival = arrival ? std::min(*arrival, rq->t_submit) : rq->t_submit;
         rq->ticket = S->next_ticket++;
         *ticket = rq->ticket;
         S->queue.push_back(rq.get());
         S->live.emplace(rq->ticket, std::move(rq));
     });
+}
+
+// [a, a + bytes) overlaps [r.begin, r.end)
+static bool overlaps(const void *a, size_t bytes, const Registered &r) {
+    const uintptr_t x = (uintptr_t)a;
+    return a && bytes && x < r.end && x + bytes > r.begin;
+}
+
+}  // namespace egtb
+
+extern "C" int egtb_serve_submit(egtb_server *S, int32_t book, const uint64_t *positions, uint64_t n, float *values4,
+                                 uint8_t *valid_mask, uint64_t *ticket) {
+    return serve_submit_at(S, book, positions, n, values4, valid_mask, ticket, nullptr);
 }
 
 extern "C" int egtb_serve_register(egtb_server *S, void *ptr, uint64_t bytes) {
@@ -335,11 +356,16 @@ extern "C" int egtb_serve_unregister(egtb_server *S, void *ptr) {
     return guarded([&] {
         if (!S || !ptr) throw Error(EGTB_ERR_ARG, "NULL argument");
         std::lock_guard<std::mutex> lk(S->mu);
-        for (const auto &q : S->live)
-            if (q.second->direct && !q.second->done)
-                for (const auto &r : S->registered)
-                    if (r.begin == (uintptr_t)ptr && (uintptr_t)q.second->pos >= r.begin && (uintptr_t)q.second->pos < r.end)
-                        throw Error(EGTB_ERR_ARG, "a request in flight uses this range");
+        // a direct request that is not done (queued or on the GPU) reads its
+        // positions and writes its answers through the mapped addresses
+        for (const auto &q : S->live) {
+            const ServeRequest &rq = *q.second;
+            if (!rq.direct || rq.done) continue;
+            for (const auto &r : S->registered)
+                if (r.begin == (uintptr_t)ptr &&
+                    (overlaps(rq.pos, rq.n * 8, r) || overlaps(rq.out, rq.n * 16, r) || overlaps(rq.valid, rq.n, r)))
+                    throw Error(EGTB_ERR_ARG, "a request in flight uses this range");
+        }
         for (size_t i = 0; i < S->registered.size(); ++i)
             if (S->registered[i].begin == (uintptr_t)ptr) {
                 EGTB_CUDA(cudaHostUnregister(ptr));
@@ -407,15 +433,16 @@ extern "C" int egtb_serve_replay(egtb_server *S, const uint64_t *pool, const dou
         reg_range(valid, total);
         const auto t0 = Clock::now();
         std::atomic<uint64_t> submitted{0};
-        std::atomic<bool> failed{false};
-        // the driver thread submits every request at its arrival time
+        std::atomic<bool> failed{false}, halt{false};
+        // the driver thread submits every request at its arrival time; each
+        // request's latency counts from its scheduled arrival
         std::thread driver([&] {
-            for (uint64_t i = 0; i < n_req; ++i) {
+            for (uint64_t i = 0; i < n_req && !halt.load(std::memory_order_relaxed); ++i) {
                 const auto due = t0 + std::chrono::nanoseconds((long long)(arrival_us[i] * 1000.0));
                 while (Clock::now() < due) {
                 }
-                if (egtb_serve_submit(S, books[i], pool + offsets[i], sizes[i], values4 + 4 * offsets[i],
-                                      valid ? valid + offsets[i] : nullptr, &tickets[i]) != EGTB_OK) {
+                if (serve_submit_at(S, books[i], pool + offsets[i], sizes[i], values4 + 4 * offsets[i],
+                                    valid ? valid + offsets[i] : nullptr, &tickets[i], &due) != EGTB_OK) {
                     failed = true;
                     break;
                 }
@@ -434,10 +461,20 @@ extern "C" int egtb_serve_replay(egtb_server *S, const uint64_t *pool, const dou
             }
             latency_us[answered] = lat;
         }
+        if (timed_out) {
+            // stop submitting, then give what was submitted a bounded time to
+            // finish: the registered ranges are unregistered (by Unreg) only
+            // once no request uses them, since the GPU writes answers there
+            halt = true;
+            driver.join();
+            const uint64_t n_sub = submitted.load(std::memory_order_acquire);
+            for (uint64_t i = answered; i < n_sub; ++i)
+                if (egtb_serve_wait(S, tickets[i], 60000, nullptr) != EGTB_OK) break;
+            throw Error(EGTB_ERR_TIMEOUT, "replay: request " + std::to_string(answered) + " not answered" +
+                                              " (ranges still used by unanswered requests stay registered)");
+        }
         driver.join();
         if (failed) throw Error(EGTB_ERR_ARG, "replay: a request was rejected");
-        if (timed_out)
-            throw Error(EGTB_ERR_TIMEOUT, "replay: request " + std::to_string(answered) + " not answered");
         if (wall_us) *wall_us = std::chrono::duration<double, std::micro>(Clock::now() - t0).count();
     });
 }

@@ -11,8 +11,11 @@
 // them as layer L of the arena (same look-back scheme for the output offset)
 // and closes the layer (length, next offset, capacity check).
 //
-// Every wait on another block is bounded: after kSpinLimit polls the kernel
-// flags kErrTimeout and carries on (the host reports EGTB_ERR_TIMEOUT). A tile
+// Every wait on another block is bounded: after spin_limit polls (a kernel
+// argument; kSpinLimit unless the host set another limit) the kernel flags
+// kErrTimeout and carries on with the counts it has seen, which only moves
+// its writes to lower positions inside the same layer (the host reports
+// EGTB_ERR_TIMEOUT and the result is not used). A tile
 // id is only ever held by a running block, which publishes its own counts
 // before it waits, so the waits always end.
 #pragma once
@@ -27,7 +30,6 @@ constexpr unsigned kErrTimeout = 8u;
 constexpr unsigned long long kFlagAgg = 1ull << 32;
 constexpr unsigned long long kFlagPrefix = 2ull << 32;
 constexpr unsigned long long kFlagMask = 3ull << 32;
-constexpr unsigned kSpinLimit = 1u << 22;
 constexpr int kMaxPasses = 8;
 constexpr int kCounterUnique = 15;  // tile counter slot of the unique kernel
 
@@ -60,7 +62,8 @@ constexpr int kLookWindow = 4;
 // base[j * stride]; kLookWindow predecessors are read at once, so a chain of
 // tiles that all started together is walked kLookWindow tiles per round trip.
 __device__ __forceinline__ unsigned long long look_back(const unsigned long long *base, unsigned long long stride,
-                                                        long long tile, unsigned epoch, DevCtl *ctl) {
+                                                        long long tile, unsigned epoch, unsigned spin_limit,
+                                                        DevCtl *ctl) {
     const unsigned long long want = (unsigned long long)(epoch & 0x3FFFFFFFu);
     unsigned long long excl = 0;
     long long j = tile - 1;
@@ -83,7 +86,7 @@ __device__ __forceinline__ unsigned long long look_back(const unsigned long long
         if (done) return excl;
         j -= used;
         if (used == 0) {
-            if (++spins > kSpinLimit) {
+            if (++spins > spin_limit) {
                 atomicOr(&ctl->err, kErrTimeout);
                 return excl;
             }
@@ -153,7 +156,8 @@ constexpr int kSweepKeys = kTileKeys / kSweepThreads;  // keys per thread
 static __global__ void __launch_bounds__(kSweepThreads, 2)
 onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, const unsigned long long *n_ptr,
                 unsigned long long cap, SortPlan sp, int p, const unsigned *__restrict__ hist,
-                unsigned *__restrict__ counters, unsigned long long *__restrict__ status, unsigned epoch, DevCtl *ctl) {
+                unsigned *__restrict__ counters, unsigned long long *__restrict__ status, unsigned epoch, DevCtl *ctl,
+                unsigned spin_limit) {
     __shared__ uint64_t tkeys[kTileKeys];
     __shared__ unsigned short wcnt[kSweepWarps][256];
     __shared__ unsigned loff[256];
@@ -217,7 +221,7 @@ onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, co
                 publish_status(my, status_word(epoch, kFlagPrefix, cnt));
             } else {
                 publish_status(my, status_word(epoch, kFlagAgg, cnt));
-                excl = look_back(status + d, 256, (long long)tile, epoch, ctl);
+                excl = look_back(status + d, 256, (long long)tile, epoch, spin_limit, ctl);
                 publish_status(my, status_word(epoch, kFlagPrefix, (unsigned)(excl + cnt)));
             }
             gbase[d] = (unsigned long long)ghist[d] + excl;
@@ -359,7 +363,7 @@ seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst
                     const unsigned long long *__restrict__ layer_len, unsigned ntiles,
                     const unsigned short *__restrict__ seg_nib, int p, const unsigned *__restrict__ hist_l,
                     unsigned *__restrict__ counters,
-                    unsigned long long *__restrict__ status, unsigned epoch, DevCtl *ctl) {
+                    unsigned long long *__restrict__ status, unsigned epoch, DevCtl *ctl, unsigned spin_limit) {
     __shared__ uint64_t tkeys[kTileKeys];
     __shared__ unsigned short wcnt[kSweepWarps][256];
     __shared__ unsigned loff[256];
@@ -421,7 +425,7 @@ seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst
             } else {
                 publish_status(my, status_word(epoch, kFlagAgg, cnt));
                 // stops at the first prefix: at the latest the layer's first tile
-                excl = look_back(status + d, 256, (long long)tile, epoch, ctl);
+                excl = look_back(status + d, 256, (long long)tile, epoch, spin_limit, ctl);
                 publish_status(my, status_word(epoch, kFlagPrefix, (unsigned)(excl + cnt)));
             }
             gbase[d] = layer_off[t.layer] + ghist_d + excl;
@@ -467,7 +471,7 @@ unique_layer_kernel(const uint64_t *__restrict__ keys, int x, unsigned long long
                     unsigned long long *__restrict__ layer_off, unsigned long long *__restrict__ layer_len, int L,
                     unsigned long long arena_cap, unsigned *__restrict__ counters,
                     unsigned long long *__restrict__ ustatus, unsigned epoch, unsigned *__restrict__ hist,
-                    DevCtl *ctl, unsigned *progress) {
+                    DevCtl *ctl, unsigned *progress, unsigned spin_limit) {
     __shared__ unsigned long long sm[33];
     __shared__ unsigned tile_sh;
     __shared__ unsigned long long excl_sh;
@@ -520,7 +524,7 @@ unique_layer_kernel(const uint64_t *__restrict__ keys, int x, unsigned long long
                 publish_status(my, status_word(epoch, kFlagPrefix, (unsigned)tile_total));
             } else {
                 publish_status(my, status_word(epoch, kFlagAgg, (unsigned)tile_total));
-                excl = look_back(ustatus, 1, (long long)tile, epoch, ctl);
+                excl = look_back(ustatus, 1, (long long)tile, epoch, spin_limit, ctl);
                 publish_status(my, status_word(epoch, kFlagPrefix, (unsigned)(excl + tile_total)));
             }
             excl_sh = excl;

@@ -89,19 +89,20 @@ static void enqueue_sort_unique_u64(const uint64_t *d_in, size_t n, uint64_t *d_
     else
         EGTB_CUDA(cudaMemcpyAsync(&s.ctl->cand_count[0], &nn, sizeof nn, cudaMemcpyHostToDevice, st));
     const SortPlan sp = full_key_plan();
+    const unsigned spin_limit = look_back_spin_limit();
     sort_hist_kernel<<<grid, kHistThreads, 0, st>>>(d_in, &s.ctl->cand_count[0], n, sp, s.hist, s.counters, s.ctl);
     // 8 passes: in -> out -> tmp -> out ... -> tmp, then unique tmp -> out
     const uint64_t *src = d_in;
     for (int p = 0; p < sp.passes; ++p) {
         uint64_t *dst = (p % 2 == 0) ? d_out : s.tmp;
         onesweep_kernel<<<grid, kSweepThreads, 0, st>>>(src, dst, &s.ctl->cand_count[0], n, sp, p, s.hist, s.counters,
-                                                       s.status, (unsigned)(p + 1), s.ctl);
+                                                       s.status, (unsigned)(p + 1), s.ctl, spin_limit);
         src = dst;
     }
     // the output "arena" is d_out; its capacity check rounds up to a 16-key line
     const unsigned long long cap16 = (n + 15) & ~15ull;
     unique_layer_kernel<<<grid, kSortThreads, 0, st>>>(src, 0, n, d_out, s.layer_off, d_n_out, 0, cap16, s.counters,
-                                                       s.ustatus, 9u, s.hist, s.ctl, nullptr);
+                                                       s.ustatus, 9u, s.hist, s.ctl, nullptr, spin_limit);
     EGTB_CUDA(cudaGetLastError());
 }
 

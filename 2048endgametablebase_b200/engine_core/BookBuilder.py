@@ -2,15 +2,17 @@
 path: resolves a pattern name into PatternSpec / RunOptions and runs the
 build on the GPU through the drop-in formation_core.
 
-Same entry points and semantics as the reference: start_build(pattern,
-target, pathname) (:264-317), _steps_and_docheck (:124-128),
-save_config_to_txt (:131-146), the one resume-retry on the
-"length multiplier" message (:237-261).
+Same entry points and behaviour as the reference's module: start_build(pattern,
+target, pathname) (:264-317), save_config_to_txt (:131-146), the seeds of
+free patterns (generate_free_inits, :149-182) and one resumed retry after the
+"length multiplier" capacity failure (:237-261). The build itself is planned
+here as a BuildPlan (catalog entry -> PatternSpec, RunOptions, seeds).
 """
 from __future__ import annotations
 
 import logging
 import os
+from dataclasses import dataclass
 
 import numpy as np
 
@@ -20,102 +22,143 @@ from .config import SingletonConfig
 
 logger = logging.getLogger("debug_logger")
 
-_SYMM_MODE_BY_NAME = {name: formation_core.SymmMode(v) for name, v in patterns.SYMM_MODES.items()}
+# RunOptions fields taken from the configuration: field -> (config key,
+# default, conversion). The reference's BookBuilder fills the same fields
+# from SingletonConfig with these defaults (engine_core/BookBuilder.py:44-73).
+_CONFIG_OPTIONS = {
+    "success_rate_dtype": ("success_rate_dtype", "uint32", str),
+    "deletion_threshold": ("deletion_threshold", 0.0, float),
+    "compress": ("compress", False, bool),
+    "compress_temp_files": ("compress_temp_files", False, bool),
+    "optimal_branch_only": ("optimal_branch_only", False, bool),
+    "chunked_solve": ("chunked_solve", False, bool),
+    "direct_io": ("direct_io", True, bool),
+    "direct_io_queue_depth": ("direct_io_queue_depth", 16, int),
+    "direct_io_chunk_mib": ("direct_io_chunk_mib", 8, int),
+}
+
+# config.txt keys, in the order the reference writes them (BookBuilder.py:131-146)
+_CONFIG_TXT_KEYS = ("compress", "optimal_branch_only", "compress_temp_files", "advanced_algo", "direct_io",
+                    "direct_io_queue_depth", "direct_io_chunk_mib", "deletion_threshold", "4_spawn_rate",
+                    "success_rate_dtype")
+
+# what run_pattern_build raises when the table outgrows its buffers; the
+# reference retries such a build once, resuming from its files
+_CAPACITY_MESSAGE = formation_core.CAPACITY_MESSAGE
+_CAPACITY_PREFIX = "length multiplier "
 
 
 def _symm_mode_value(name: str) -> int:
-    return int(_SYMM_MODE_BY_NAME.get(name, formation_core.SymmMode.Identity).value)
+    """Integer symmetry mode of a catalog "canonical mode" name (identity if unknown)."""
+    return int(patterns.SYMM_MODES.get(name, int(formation_core.SymmMode.Identity)))
 
 
-def _build_native_run_options(target, steps, pathname, docheck_step, is_free, is_variant, spawn_rate4):
-    """_build_native_run_options, engine_core/BookBuilder.py:44-73"""
-    config = SingletonConfig().config
-    options = formation_core.RunOptions()
-    options.target = int(target)
-    options.steps = int(steps)
-    options.docheck_step = int(docheck_step)
-    options.pathname = str(pathname)
-    options.is_free = bool(is_free)
-    options.is_variant = bool(is_variant)
-    options.spawn_rate4 = float(spawn_rate4)
-    options.success_rate_dtype = str(config.get("success_rate_dtype", "uint32"))
-    options.deletion_threshold = float(config.get("deletion_threshold", 0.0))
-    options.compress = bool(config.get("compress", False))
-    options.compress_temp_files = bool(config.get("compress_temp_files", False))
-    options.optimal_branch_only = bool(config.get("optimal_branch_only", False))
-    options.chunked_solve = bool(config.get("chunked_solve", False))
-    options.direct_io = bool(config.get("direct_io", True))
-    options.direct_io_queue_depth = int(config.get("direct_io_queue_depth", 16))
-    options.direct_io_chunk_mib = int(config.get("direct_io_chunk_mib", 8))
-    options.num_threads = int(max(4, min(32, os.cpu_count() or 2)))
-    return options
+@dataclass
+class BuildPlan:
+    """Everything one classic build needs, resolved from the catalog."""
+    pattern: str
+    target: int
+    pathname: str
+    seeds: np.ndarray
+    steps: int
+    docheck_step: int
+    is_free: bool
+    is_variant: bool
+    spawn_rate4: float
+
+    def spec(self):
+        meta = patterns.pattern_catalog[self.pattern]
+        s = formation_core.PatternSpec()
+        s.name = self.pattern
+        s.pattern_masks = [int(m) for m in meta.get("pattern_masks", ())]
+        s.success_shifts = [int(x) for x in meta.get("success_shifts", ())]
+        s.symm_mode = _symm_mode_value(meta.get("canonical_mode", "identity"))
+        return s
+
+    def options(self):
+        config = SingletonConfig().config
+        o = formation_core.RunOptions()
+        o.target, o.steps, o.docheck_step = int(self.target), int(self.steps), int(self.docheck_step)
+        o.pathname = str(self.pathname)
+        o.is_free, o.is_variant = bool(self.is_free), bool(self.is_variant)
+        o.spawn_rate4 = float(self.spawn_rate4)
+        for field_name, (key, default, conv) in _CONFIG_OPTIONS.items():
+            setattr(o, field_name, conv(config.get(key, default)))
+        o.num_threads = max(4, min(32, os.cpu_count() or 2))
+        return o
+
+    def run(self) -> None:
+        formation_core.run_pattern_build(np.asarray(self.seeds, dtype=np.uint64), self.spec(), self.options())
 
 
-def _build_native_pattern_spec(pattern: str):
-    """_build_native_pattern_spec, engine_core/BookBuilder.py:76-88"""
-    meta = patterns.pattern_catalog.get(pattern)
-    if meta is None:
-        raise KeyError(f"Unknown pattern: {pattern}")
-    spec = formation_core.PatternSpec()
-    spec.name = pattern
-    spec.pattern_masks = list(meta.get("pattern_masks", ()))
-    spec.success_shifts = list(meta.get("success_shifts", ()))
-    spec.symm_mode = _symm_mode_value(meta.get("canonical_mode", "identity"))
-    return spec
-
-
-def _resolve_build_meta(pattern: str):
-    """_resolve_build_meta, engine_core/BookBuilder.py:111-121"""
-    meta = patterns.pattern_catalog.get(pattern)
-    if meta is None:
-        raise KeyError(f"Unknown pattern: {pattern}")
-    tile_sum = -int(meta.get("nums_adjust", 0))
-    seed_boards = np.asarray(meta.get("seed_boards", ()), dtype=np.uint64)
-    if seed_boards.size == 0:
-        raise ValueError(f"Pattern {pattern} has no seed boards")
-    extra_steps = int(meta.get("extra_steps", 36))
-    return meta, tile_sum, seed_boards, extra_steps
-
-
-_steps_and_docheck = patterns.steps_and_docheck
+def _steps_and_docheck(tile_sum: int, target: int, extra_steps: int):
+    return patterns.steps_and_docheck(tile_sum, target, extra_steps)
 
 
 def save_config_to_txt(output_path: str) -> None:
-    """save_config_to_txt, engine_core/BookBuilder.py:131-146"""
-    keys = ["compress", "optimal_branch_only", "compress_temp_files", "advanced_algo", "direct_io",
-            "direct_io_queue_depth", "direct_io_chunk_mib", "deletion_threshold", "4_spawn_rate",
-            "success_rate_dtype"]
+    """config.txt beside the books: one "key: value" line per build setting."""
+    config = SingletonConfig().config
     with open(output_path, "w", encoding="utf-8") as f:
-        for key in keys:
-            f.write(f"{key}: {str(SingletonConfig().config.get(key, '?'))}\n")
-
-
-def _run_classic_build(pattern, arr_init, target, steps, pathname, docheck_step, is_free, is_variant, spawn_rate4):
-    spec = _build_native_pattern_spec(pattern)
-    options = _build_native_run_options(target, steps, pathname, docheck_step, is_free, is_variant, spawn_rate4)
-    formation_core.run_pattern_build(np.asarray(arr_init, dtype=np.uint64), spec, options)
+        f.writelines(f"{k}: {config.get(k, '?')}\n" for k in _CONFIG_TXT_KEYS)
 
 
 def _should_retry_build_resume(exc: Exception) -> bool:
-    message = str(exc).strip()
-    if not message:
-        return False
-    if message == "The length multiplier is not big enough. Please restart.":
-        return True
-    return message.startswith("length multiplier ")
+    """True for the capacity failure that a resumed second attempt can fix."""
+    text = str(exc).strip()
+    return bool(text) and (text == _CAPACITY_MESSAGE or text.startswith(_CAPACITY_PREFIX))
 
 
-def _run_with_single_resume_retry(build_label: str, build_fn) -> None:
-    retried = False
-    while True:
+def _build_with_one_resume(label: str, build) -> None:
+    """Run build(); after a capacity failure run it once more (it resumes from
+    the layer files already written). Any other failure, or a second one,
+    propagates."""
+    for attempt in (1, 2):
         try:
-            build_fn()
+            build()
             return
         except Exception as exc:  # noqa: BLE001
-            if retried or not _should_retry_build_resume(exc):
+            if attempt == 2 or not _should_retry_build_resume(exc):
                 raise
-            retried = True
-            logger.warning("%s interrupted (%s); re-entering build once.", build_label, exc)
+            logger.warning("%s interrupted (%s); re-entering build once.", label, exc)
+
+
+def _free_pattern_seeds(seeds: np.ndarray, tile_sum: int) -> np.ndarray:
+    """A free pattern's start layer: generated (generate_free_inits) when its
+    extra tiles are 2s that fit the free cells, else its catalog seeds."""
+    first = int(seeds[0])
+    walls = sum((first >> (4 * k)) & 0xF == 0xF for k in range(16))
+    extra = tile_sum - 32768 * walls
+    return generate_free_inits(walls, extra // 2) if extra <= (15 - walls) * 2 else seeds
+
+
+def _counts_as_free(pattern: str, tile_sum: int) -> bool:
+    """A catalog pattern whose masks pin fewer than four cells in common
+    (and whose start sum is small) is built with is_free set."""
+    masks = patterns.pattern_catalog[pattern]["pattern_masks"]
+    if not masks:
+        return tile_sum < 180000
+    common = 0xFFFFFFFFFFFFFFFF
+    for m in masks:
+        common &= int(m)
+    return len(patterns.find_f_nibble_positions(common)) < 4 and tile_sum < 180000
+
+
+def plan_build(pattern: str, target: int, pathname: str) -> BuildPlan:
+    """Resolve a catalog pattern and target into a BuildPlan."""
+    meta = patterns.pattern_catalog.get(pattern)
+    if meta is None:
+        raise KeyError(f"Unknown pattern: {pattern}")
+    seeds = np.asarray(meta.get("seed_boards", ()), dtype=np.uint64)
+    if seeds.size == 0:
+        raise ValueError(f"Pattern {pattern} has no seed boards")
+    tile_sum = -int(meta.get("nums_adjust", 0))
+    steps, docheck = _steps_and_docheck(tile_sum, target, int(meta.get("extra_steps", 36)))
+    free = pattern.startswith("free")
+    return BuildPlan(pattern, int(target), pathname,
+                     _free_pattern_seeds(seeds, tile_sum) if free else seeds, steps, docheck,
+                     True if free else _counts_as_free(pattern, tile_sum),
+                     pattern in patterns.category_info.get("variant", []),
+                     float(SingletonConfig().config["4_spawn_rate"]))
 
 
 def generate_free_inits(t32ks: int, t2s: int) -> np.ndarray:
@@ -158,36 +201,12 @@ def generate_free_inits(t32ks: int, t2s: int) -> np.ndarray:
 
 
 def start_build(pattern: str, target: int, pathname: str) -> bool:
-    """start_build, engine_core/BookBuilder.py:264-317 (classic algorithm)."""
-    config = SingletonConfig().config
-    if config.get("advanced_algo", False):
+    """start_build (reference engine_core/BookBuilder.py:264-317), classic
+    algorithm: write config.txt, then build the table through the drop-in
+    formation_core, resuming once after a capacity failure."""
+    if SingletonConfig().config.get("advanced_algo", False):
         raise RuntimeError("the advanced (masked-board) algorithm is not built")
-    spawn_rate4 = float(config["4_spawn_rate"])
-    _, tile_sum, seed_boards, extra_steps = _resolve_build_meta(pattern)
-    steps, docheck_step = _steps_and_docheck(tile_sum, target, extra_steps)
-    is_variant = pattern in patterns.category_info.get("variant", [])
+    plan = plan_build(pattern, target, pathname)
     save_config_to_txt(pathname + "config.txt")
-    if pattern.startswith("free"):
-        # BookBuilder.py:275-283: the seeds of a free pattern are generated
-        # when its extra tiles are all 2s that fit the free cells
-        seed = int(seed_boards[0])
-        num_32k = sum(1 for k in range(16) if (seed >> (4 * k)) & 0xF == 0xF)
-        extra = tile_sum - 32768 * num_32k
-        arr_init = generate_free_inits(num_32k, extra // 2) if extra <= (15 - num_32k) * 2 else seed_boards
-        is_free = True
-    else:
-        arr_init = seed_boards
-        masks = patterns.pattern_catalog[pattern]["pattern_masks"]
-        inter = 0
-        if masks:
-            inter = ~0 & 0xFFFFFFFFFFFFFFFF
-            for m in masks:
-                inter &= int(m)
-        fixed = patterns.find_f_nibble_positions(inter) if masks else []
-        is_free = (len(fixed) < 4) and (tile_sum < 180000)
-    _run_with_single_resume_retry(
-        f"Classic build {pattern}_{2 ** target}",
-        lambda: _run_classic_build(pattern, arr_init, target, steps, pathname, docheck_step, is_free, is_variant,
-                                   spawn_rate4),
-    )
+    _build_with_one_resume(f"Classic build {pattern}_{2 ** int(target)}", plan.run)
     return True

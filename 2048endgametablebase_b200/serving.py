@@ -249,6 +249,13 @@ def request_stream(books: list[Book], n_requests: int, rate_per_s: float, seed: 
     return RequestStream(pool, arrival.astype(np.float64), sizes, offsets, book_of)
 
 
+def at_rate(rs: RequestStream, rate_per_s: float, recorded_rate_per_s: float) -> RequestStream:
+    """The same requests with their arrival times rescaled from the recorded
+    rate to another offered rate (Poisson gaps scale with 1/rate)."""
+    return RequestStream(rs.pool, rs.arrival_us * (recorded_rate_per_s / rate_per_s), rs.sizes, rs.offsets,
+                         rs.book_of)
+
+
 def latency_summary(lat_us: np.ndarray) -> dict:
     lat = np.asarray(lat_us, dtype=np.float64)
     return {"p50_us": float(np.percentile(lat, 50)), "p99_us": float(np.percentile(lat, 99)),

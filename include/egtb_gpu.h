@@ -151,6 +151,16 @@ EGTB_API int egtb_set_stream(int device, void *stream);
 EGTB_API int egtb_profile(int device, int enable);
 EGTB_API int egtb_profile_read(int device, egtb_kernel_time *out, int max_kinds, int *n_kinds);
 
+/* Number of polls a bounded device wait (the sort's look-back on another
+ * block's counts) makes before it gives up; 0 restores the default 2^22.
+ * Process-wide, read at each launch. A wait that gives up makes the call
+ * return EGTB_ERR_TIMEOUT (egtb_build, egtb_generate, egtb_solve,
+ * egtb_build_batch) instead of hanging; the library stays usable. No
+ * reference counterpart (the reference's CPU sort has no cross-block waits);
+ * meant for tests of the timeout path and for callers that want a shorter
+ * bound. */
+EGTB_API int egtb_set_spin_limit(uint32_t polls);
+
 /* ---------------------------------------------------------- progress ---- */
 
 /* get_build_progress / reset_build_progress,
@@ -368,10 +378,15 @@ EGTB_API int egtb_serve_submit(egtb_server *server, int32_t book, const uint64_t
  * writes its answers there, with no staging copy on the host.
  * egtb_serve_replay registers its own buffers. */
 EGTB_API int egtb_serve_register(egtb_server *server, void *ptr, uint64_t bytes);
+/* Refused (EGTB_ERR_ARG) while a request answered in place that is not done
+ * yet (queued or on the GPU) has its positions, values4 or valid_mask in the
+ * range: the GPU still reads or writes it there. */
 EGTB_API int egtb_serve_unregister(egtb_server *server, void *ptr);
 
 /* Wait for a ticket (timeout_ms < 0: one hour); *latency_us = submit to
- * answer. Every ticket must be waited for once. */
+ * answer. Every ticket must be waited for once. On EGTB_ERR_TIMEOUT the
+ * request is still live and its buffers stay in use until it is answered:
+ * wait for the ticket again before freeing or unregistering them. */
 EGTB_API int egtb_serve_wait(egtb_server *server, uint64_t ticket, int32_t timeout_ms, double *latency_us);
 
 EGTB_API int egtb_serve_stats(egtb_server *server, uint64_t *requests, uint64_t *positions, uint64_t *batches,
@@ -380,8 +395,12 @@ EGTB_API int egtb_serve_stats(egtb_server *server, uint64_t *requests, uint64_t 
 /* Replay a recorded request stream: request i arrives arrival_us[i]
  * microseconds after the call, reads sizes[i] positions at pool + offsets[i]
  * for books[book_of[i]] and answers into values4 + 4*offsets[i] and
- * valid + offsets[i] (valid may be NULL); latency_us[i] gets its latency and
- * *wall_us the time until the last answer. */
+ * valid + offsets[i] (valid may be NULL); latency_us[i] gets its latency,
+ * measured from its scheduled arrival (time the submitting thread fell
+ * behind the schedule counts as queueing), and *wall_us the time until the
+ * last answer. On a timeout the replay stops submitting and waits (bounded)
+ * for what it submitted; buffers of requests still unanswered stay
+ * registered (the GPU may still write them). */
 EGTB_API int egtb_serve_replay(egtb_server *server, const uint64_t *pool, const double *arrival_us,
                                const uint32_t *sizes, const uint64_t *offsets, const int32_t *book_of, uint64_t n_req,
                                float *values4, uint8_t *valid, double *latency_us, double *wall_us);

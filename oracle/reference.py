@@ -28,7 +28,11 @@ def available() -> bool:
     return bool(glob.glob(os.path.join(REF_DIR, "formation_core*.so")))
 
 
-def build(ref_root: str = "/root/reference") -> bool:
+# the reference's source tree (only in the container that compiles it)
+REF_ROOT = os.environ.get("EGTB_REFERENCE_ROOT", "/root/reference")
+
+
+def build(ref_root: str = REF_ROOT) -> bool:
     """Compile the reference's classic path from its sources (only where they exist)."""
     if not os.path.isdir(ref_root):
         return available()

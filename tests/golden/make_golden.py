@@ -16,8 +16,9 @@ fixtures are outputs of the reference itself, run in this container:
 
 Usage:  python tests/golden/make_golden.py            # small cases
         python tests/golden/make_golden.py --full     # + full-size L3-256, 442-512
-Reads the reference's pattern catalog from /root/reference (this container
-only); the fixtures carry every input, so nothing reads /root/reference later.
+Reads the reference's pattern catalog from the reference's source tree
+($EGTB_REFERENCE_ROOT, default /root/reference; this container only); the
+fixtures carry every input, so nothing reads the reference tree later.
 """
 from __future__ import annotations
 
@@ -35,7 +36,8 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import reference as R  # noqa: E402
 
 GOLDEN = os.path.dirname(os.path.abspath(__file__))
-REF_CATALOG = "/root/reference/docs_and_configs/patterns_config.json"
+REF_ROOT = os.environ.get("EGTB_REFERENCE_ROOT", "/root/reference")
+REF_CATALOG = os.path.join(REF_ROOT, "docs_and_configs", "patterns_config.json")
 WORK = os.environ.get("GOLDEN_WORK", "/dev/shm/egtb_golden")
 
 
@@ -100,6 +102,14 @@ FULL_CASES = [("L3", 8, "float32"), ("442", 9, "float32")]
 # the 13-cell diagonal table (config-2 family) at the largest target the
 # reference can build here (2.25e9 boards, ~45 GB of files, ~10 min)
 HUGE_CASES = [("4432", 7, "float32")]
+# forward prefixes of tables too large to build here: the first `steps` steps of
+# run_pattern_generate at the table's own docheck_step (the 13-cell diagonal
+# table at 1024: 560 steps, ~1 TB of raw layers). No success check happens
+# before docheck_step (504), so these raw layers are the whole table's.
+PREFIX_CASES = [("4432", 10, 130)]
+# float32 tables against the float64 build of the same pattern (the reference's
+# own builds): the largest and mean |r32 - r64| over every book entry
+FP64_CASES = [("L3", 8), ("442", 9)]
 
 
 def sha(path: str) -> str:
@@ -155,6 +165,51 @@ def run_case(catalog, pat, target, dtype, deletion=0.0, optimal=False, variant=F
         import shutil
         shutil.rmtree(gdir, ignore_errors=True)
     return case, bdir
+
+
+def run_prefix(catalog, pat, target, steps):
+    masks, shifts, symm, seeds, full_steps, docheck, s0 = R.pattern_params(catalog[pat], target)
+    T = 2 ** target
+    name = f"{pat}_{T}"
+    gdir = R.fresh_dir(os.path.join(WORK, f"{name}_prefix{steps}", "gen") + "/")
+    spec, o = R.make_spec_options(masks, shifts, symm, target, steps, docheck, gdir + name + "_", "float32")
+    started, last0, last1 = R.run_generate(seeds, spec, o)
+    raw_len, raw_sha = [], []
+    for t in range(steps - 2):
+        p = gdir + f"{name}_{t}"
+        raw_len.append(os.path.getsize(p) // 8)
+        raw_sha.append(sha(p))
+        os.remove(p)
+    import shutil
+    shutil.rmtree(os.path.dirname(gdir.rstrip("/")), ignore_errors=True)
+    return {
+        "pattern": pat, "target": target, "dtype": "float32", "spawn_rate4": 0.1,
+        "masks": [hex(m) for m in masks], "shifts": shifts, "symm_mode": symm,
+        "seeds": [hex(int(s)) for s in seeds], "steps": steps, "full_steps": full_steps,
+        "docheck_step": docheck, "tile_sum0": s0, "pattern_full": name,
+        "raw_len": raw_len, "raw_sha256": raw_sha,
+        "partial_len": [int(last0.size), int(last1.size)],
+        "size_class": "prefix",
+    }
+
+
+def run_fp64_error(catalog, pat, target):
+    import importlib
+    sys.path.insert(0, ROOT)
+    P = importlib.import_module("2048endgametablebase_b200.precision")
+    masks, shifts, symm, seeds, steps, docheck, s0 = R.pattern_params(catalog[pat], target)
+    name = f"{pat}_{2 ** target}"
+    books = {}
+    for dtype in ("float32", "float64"):
+        bdir = R.fresh_dir(os.path.join(WORK, f"{name}_{dtype}_fp64err") + "/")
+        spec, o = R.make_spec_options(masks, shifts, symm, target, steps, docheck, bdir + name + "_", dtype)
+        R.run_build(seeds, spec, o)
+        books[dtype] = [open(bdir + f"{name}_{t}.book", "rb").read() for t in range(steps)]
+        import shutil
+        shutil.rmtree(bdir, ignore_errors=True)
+    r = P.compare_books(books["float32"], "float32", books["float64"], "float64")
+    r["board"] = hex(r["board"])
+    return r
 
 
 def prims_fixture():
@@ -256,18 +311,23 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--full", action="store_true", help="also the full-size L3-256 and 442-512 builds")
     ap.add_argument("--huge", action="store_true", help="also the 4432-128 build (needs ~45 GB of disk in GOLDEN_WORK)")
+    ap.add_argument("--prefix", action="store_true",
+                    help="also the forward prefix of the 13-cell diagonal table at 1024 (~30 GB in GOLDEN_WORK)")
+    ap.add_argument("--fp64", action="store_true",
+                    help="also the float32-vs-float64 rate error of the full-size L3-256 and 442-512 tables")
     ap.add_argument("--only", default="", help="comma-separated case keys to (re)generate")
     args = ap.parse_args()
-    R.build()
+    R.build(REF_ROOT)
     catalog = json.load(open(REF_CATALOG))
     catalog.update(custom_patterns())
-    prims_fixture()
+    only = set(filter(None, args.only.split(",")))
+    if not only or "prims" in only:
+        prims_fixture()
     cases_path = os.path.join(GOLDEN, "cases.json")
     cases = json.load(open(cases_path)) if os.path.exists(cases_path) else {}
     reader = {}
     rng = np.random.default_rng(7)
     todo = SMALL_CASES + (FULL_CASES if args.full else []) + (HUGE_CASES if args.huge else [])
-    only = set(filter(None, args.only.split(",")))
     for pat, target, dtype in todo:
         key = f"{pat}_{2 ** target}_{dtype}"
         if only and key not in only:
@@ -288,6 +348,18 @@ def main():
                 raw = bdir + f"free5_32_{t}.book"
                 data[f"book_{t}"] = np.fromfile(raw, dtype=np.uint8)
             np.savez_compressed(os.path.join(GOLDEN, "free5_32.npz"), **data)
+    for pat, target, steps in (PREFIX_CASES if args.prefix else []):
+        key = f"{pat}_{2 ** target}_prefix{steps}"
+        if only and key not in only:
+            continue
+        print("case", key, flush=True)
+        cases[key] = run_prefix(catalog, pat, target, steps)
+    for pat, target in (FP64_CASES if args.fp64 else []):
+        key = f"{pat}_{2 ** target}_fp64_error"
+        if only and key not in only:
+            continue
+        print("case", key, flush=True)
+        cases[key] = dict(run_fp64_error(catalog, pat, target), pattern=pat, target=target, size_class="fp64_error")
     for pat, target, dtype, thr in DELETION_CASES:
         key = f"{pat}_{2 ** target}_{dtype}_del{thr}"
         if only and key not in only:

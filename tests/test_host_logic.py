@@ -141,3 +141,19 @@ def test_variant_catalog_entries_match_golden_cases(key):
     steps, docheck = P.steps_and_docheck(case["tile_sum0"], case["target"], meta["extra_steps"])
     assert (steps, docheck) == (case["steps"], case["docheck_step"])
     assert case.get("is_variant") is True
+
+
+def test_compare_books_counts_missing_keys_as_zero():
+    import importlib
+    P = importlib.import_module("2048endgametablebase_b200.precision")
+
+    def book(pairs, dt):
+        rec = np.dtype([("key", "<u8"), ("rate", dt)])
+        return np.array(pairs, dtype=rec).tobytes()
+
+    a = [book([(1, 0.5), (3, 0.25)], "<f4"), book([], "<f4")]
+    b = [book([(1, 0.5), (2, 0.125), (3, 0.2500001)], "<f8"), book([(7, 1e-9)], "<f8")]
+    r = P.compare_books(a, "float32", b, "float64")
+    assert r["entries"] == 4 and r["only_in_b"] == 2 and r["only_in_a"] == 0
+    assert r["max_abs_err"] == 0.125 and r["layer"] == 0 and r["board"] == 2
+    assert r["rate_a"] == 0.0 and r["rate_b"] == 0.125
