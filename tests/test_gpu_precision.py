@@ -10,8 +10,9 @@ import pytest
 import helpers as H
 
 # largest |r32 - r64| over every entry of the L3-256 and 442-512 books
+# (3.06e-7 and 2.78e-7; means 1.7e-8 and 1.6e-8)
 # (the reference's builds give the same figures; see the golden cases)
-MAX_ABS_ERR_BOUND = 1e-6
+MAX_ABS_ERR_BOUND = 4e-7
 
 
 def _P():
