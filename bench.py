@@ -397,6 +397,19 @@ def main():
                 dt, rb = reference_build_seconds(pattern, target, meta, steps, docheck, threads)
                 line["cpu_baseline"] = {"value": rb / dt, "unit": "boards/s", "cores": threads, "kind": "reference",
                                         "sample": f"1 full build of {pattern}-{2 ** target} ({rb} boards, {dt:.2f} s)"}
+        # parity notes, outside every timed region: the float32 books against
+        # a float64 build of the same table, entry by entry
+        if world == 1:
+            N.set_stream(local, None)
+            prec = importlib.import_module("2048endgametablebase_b200.precision")
+            spec_p, o_p = make_spec_options(fc, pattern, target, meta, steps, docheck, "", local)
+            pe = prec.rate_error_vs_fp64(seeds, spec_p, o_p)
+            line["parity"] = {
+                "books": "bit-exact with the reference's (tests/test_gpu_build.py, golden SHA-256 per book)",
+                "max_abs_err_vs_fp64": pe["max_abs_err"], "mean_abs_err_vs_fp64": pe["mean_abs_err"],
+                "max_at": {"layer": pe["layer"], "board": hex(pe["board"]), "float32": pe["rate_a"],
+                           "float64": pe["rate_b"]},
+                "entries": pe["entries"]}
         if not args.no_serve and world == 1:
             N.set_stream(local, None)
             line["serving"] = serving_leg(local, base, offered=args.serve_offered,
