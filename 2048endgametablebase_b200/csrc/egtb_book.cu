@@ -3,6 +3,7 @@
 // answers move_on_dic for many positions at once (the reader side of the
 // reference, native_core/src/ReaderRuntime.cpp:739-840 and 1050-1133).
 #include <cuda_runtime.h>
+#include <sys/stat.h>
 
 #include <algorithm>
 #include <cmath>
@@ -11,11 +12,13 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
 #include "egtb_host.h"
 #include "egtb_device.cuh"
+#include "egtb_trie.h"
 
 namespace egtb {
 
@@ -28,6 +31,14 @@ struct BookLayer {
     unsigned long long n = 0;
     int state = 0;  // 0 not looked at, 1 loaded, 2 file missing
     int sorted = 1;
+    // compressed layer (<name>_<t>.z): its trie levels and block table; the
+    // decoded entries' low 32 bits in `low`, their rates in `rates`
+    int compressed = 0;
+    uint8_t *i_key = nullptr, *ii_key = nullptr;
+    uint32_t *i_next = nullptr, *seg_index = nullptr, *low = nullptr;
+    uint16_t *ii_next = nullptr;
+    unsigned long long *block_end = nullptr;
+    unsigned long long n_i = 0, n_ii = 0, n_seg = 0;
 };
 
 // Layer descriptor read by the lookup kernel.
@@ -40,6 +51,12 @@ struct LayerDesc {
     unsigned long long n;
     int exists;
     int sorted;
+    int compressed;
+    const uint8_t *i_key, *ii_key;
+    const uint32_t *i_next, *seg_index, *low;
+    const uint16_t *ii_next;
+    const unsigned long long *block_end;
+    unsigned long long n_i, n_ii, n_seg;
 };
 
 // ------------------------------------------------------ layer hash index ---
@@ -163,7 +180,47 @@ __global__ void split_records_kernel(const unsigned char *__restrict__ recs, uns
     }
 }
 
-// Load layer `nums` from its .book file (state 2 when the file is missing).
+template <typename V>
+static V *upload(const std::vector<V> &h, cudaStream_t s) {
+    V *d = nullptr;
+    EGTB_CUDA(cudaMalloc(&d, std::max<size_t>(h.size(), 1) * sizeof(V)));
+    if (!h.empty()) EGTB_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice, s));
+    return d;
+}
+
+// Load a compressed layer: every xz block decoded on the host (threads), the
+// trie levels, block table and decoded entries uploaded as they are; the
+// lookup kernel searches them the way the reference's reader does.
+static bool load_compressed_layer(egtb_book &b, BookLayer &L, long long nums) {
+    const std::string zdir = b.dir + "/" + b.pattern_full + "_" + std::to_string(nums) + ".z";
+    struct stat st;
+    if (::stat(zdir.c_str(), &st) != 0 || !S_ISDIR(st.st_mode)) return false;
+    TrieLayer z;
+    const size_t es = dtype_size(b.dtype);
+    const int threads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (!read_compressed_book(zdir, b.pattern_full + "_" + std::to_string(nums) + ".", es, z, threads)) return false;
+    cudaStream_t s = b.stream;
+    L.i_key = upload(z.i_key, s);
+    L.i_next = upload(z.i_next, s);
+    L.ii_key = upload(z.ii_key, s);
+    L.ii_next = upload(z.ii_next, s);
+    L.seg_index = upload(z.seg_index, s);
+    std::vector<unsigned long long> be(z.block_end.begin(), z.block_end.end());
+    L.block_end = upload(be, s);
+    L.low = upload(z.low, s);
+    L.rates = upload(z.rates, s);
+    L.n_i = z.i_key.size();
+    L.n_ii = z.ii_key.size();
+    L.n_seg = z.seg_index.size();
+    L.n = z.low.size();
+    L.compressed = 1;
+    L.sorted = 1;
+    EGTB_CUDA(cudaStreamSynchronize(s));
+    return true;
+}
+
+// Load layer `nums` from its .book file, else from its compressed .z
+// directory (state 2 when neither is there).
 static void load_layer(egtb_book &b, long long nums) {
     if (nums < 0) return;
     if ((long long)b.layers.size() <= nums) b.layers.resize(nums + 1);
@@ -171,7 +228,7 @@ static void load_layer(egtb_book &b, long long nums) {
     const std::string path = layer_path(b, nums);
     if (L.state == 1) return;
     if (!file_exists(path)) {
-        L.state = 2;
+        L.state = load_compressed_layer(b, L, nums) ? 1 : 2;
         b.desc_dirty = true;
         return;
     }
@@ -252,7 +309,9 @@ static void upload_desc(egtb_book &b) {
     std::vector<LayerDesc> h(std::max(n, 1));
     for (int i = 0; i < n; ++i) {
         const BookLayer &L = b.layers[i];
-        h[i] = {L.keys, L.rates, L.split, L.index, L.index_mask, L.n, L.state == 1 ? 1 : 0, L.sorted};
+        h[i] = {L.keys, L.rates, L.split, L.index, L.index_mask, L.n, L.state == 1 ? 1 : 0, L.sorted,
+                L.compressed, L.i_key, L.ii_key, L.i_next, L.seg_index, L.low, L.ii_next, L.block_end,
+                L.n_i, L.n_ii, L.n_seg};
     }
     if (n) EGTB_CUDA(cudaMemcpyAsync(b.d_desc, h.data(), sizeof(LayerDesc) * n, cudaMemcpyHostToDevice, b.stream));
     EGTB_CUDA(cudaStreamSynchronize(b.stream));
@@ -292,6 +351,106 @@ __device__ __forceinline__ bool probe_unsorted(const uint64_t *keys, const T *ra
         }
     }
     return false;
+}
+
+// Search of a compressed layer, step for step as trie_search_with_context
+// (ReaderRuntime.cpp:318-477) runs it over the files: three binary searches
+// down the byte-7/6/5 levels of i, one over the byte-4 groups in ii, the
+// block whose s entry is the first at or after the group, then a lower-bound
+// search of the low 32 bits inside the range the group's neighbours give.
+// The reference's range rules are kept as they are, including its reading of
+// a relative `next` of 0 and its first-entry check, so every answer (hit,
+// miss, or the entry those rules land on) is the reference's. *out = the
+// rate found, or zero.
+template <typename T>
+__device__ __forceinline__ void trie_find(const LayerDesc &L, uint64_t board, T zero, T &out) {
+    out = zero;
+    if (L.n_i < 2 || L.n_seg < 2) return;
+    unsigned long long low = 2, high = (unsigned long long)L.i_next[1] - 1ull;
+    for (int level = 0; level < 3; ++level) {
+        const uint8_t want = (uint8_t)(board >> (56 - 8 * level));
+        if (high >= L.n_i) high = L.n_i - 1;  // stays inside i (a well-formed file never needs it)
+        bool found = false;
+        unsigned long long mid = low;
+        while (low <= high) {
+            mid = (low + high) / 2;
+            const uint8_t k = L.i_key[mid];
+            if (k == want) {
+                found = true;
+                break;
+            }
+            if (k < want) {
+                low = mid + 1;
+            } else {
+                if (mid == 0) break;
+                high = mid - 1;
+            }
+        }
+        if (!found) return;
+        low = (unsigned long long)L.i_next[mid - 1] + 1ull;
+        high = L.i_next[mid];
+    }
+    // ii entries low-1 .. high: the groups under the byte-5 entry and the one before
+    const unsigned long long first = low - 1, count = high - low + 2;
+    if (count <= 1 || first + count > L.n_ii) return;
+    const uint8_t want4 = (uint8_t)(board >> 32);
+    unsigned long long lo = 1, hi = count - 1, pos = 0;
+    bool found = false;
+    while (lo <= hi) {
+        const unsigned long long mid = (lo + hi) / 2;
+        const uint8_t k = L.ii_key[first + mid];
+        if (k == want4) {
+            pos = mid - 1;
+            found = true;
+            break;
+        }
+        if (k < want4) {
+            lo = mid + 1;
+        } else {
+            if (mid == 0) break;
+            hi = mid - 1;
+        }
+    }
+    if (!found) return;
+    // the block: the first s entry at or after ii index pos + low
+    const unsigned long long target = pos + low;
+    long long blk = -1;
+    {
+        unsigned long long a = 0, c = L.n_seg - 1;
+        while (a <= c) {
+            const unsigned long long mid = (a + c) / 2;
+            if ((unsigned long long)L.seg_index[mid] < target) {
+                a = mid + 1;
+            } else {
+                blk = (long long)mid;
+                if (mid == 0) break;
+                c = mid - 1;
+            }
+        }
+    }
+    unsigned long long base = 0, size = 0;
+    if (blk >= 1) {
+        base = L.block_end[blk - 1];
+        size = L.block_end[blk] - base;
+    }
+    const T *rates = (const T *)L.rates;
+    const uint32_t t32 = (uint32_t)board;
+    unsigned long long sub_low = L.ii_next[first + pos], sub_high = (unsigned long long)L.ii_next[first + pos + 1] + 1;
+    if (sub_high == 1) {
+        if (size != 0 && t32 == L.low[base]) {
+            out = rates[base];
+            return;
+        }
+        sub_high = size;
+    }
+    if (sub_low != 0) ++sub_low;
+    if (sub_high > size) sub_high = size;  // stays inside the block (a well-formed file never needs it)
+    while (sub_low < sub_high) {
+        const unsigned long long mid = (sub_low + sub_high) / 2;
+        if (L.low[base + mid] < t32) sub_low = mid + 1;
+        else sub_high = mid;
+    }
+    if (sub_low < size && L.low[base + sub_low] == t32) out = rates[base + sub_low];
 }
 
 // normalize_raw_value + maybe_round_value (ReaderRuntime.cpp:208-214,271-277):
@@ -364,7 +523,13 @@ __device__ __forceinline__ void lookup_position(const LayerDesc *__restrict__ de
             live |= 1u << d;
         }
         T r[4];
-        if (L.sorted && L.index) {
+        if (L.compressed) {
+#pragma unroll
+            for (int d = 0; d < 4; ++d) {
+                r[d] = zero;
+                if (live >> d & 1u) trie_find<T>(L, key[d], zero, r[d]);
+            }
+        } else if (L.sorted && L.index) {
             index_lookup4<T>(L.index, L.index_mask, key, live, zero, r);
         } else {
 #pragma unroll
@@ -583,10 +748,10 @@ extern "C" int egtb_book_close(egtb_book *b) {
         cudaSetDevice(b->device);
         cudaStreamSynchronize(b->stream);
         for (auto &L : b->layers) {
-            if (L.keys) cudaFree(L.keys);
-            if (L.rates) cudaFree(L.rates);
-            if (L.split) cudaFree(L.split);
-            if (L.index) cudaFree(L.index);
+            for (void *p : {(void *)L.keys, L.rates, (void *)L.split, (void *)L.index, (void *)L.i_key, (void *)L.ii_key,
+                            (void *)L.i_next, (void *)L.seg_index, (void *)L.low, (void *)L.ii_next,
+                            (void *)L.block_end})
+                if (p) cudaFree(p);
         }
         if (b->d_desc) cudaFree(b->d_desc);
         if (b->d_pos) cudaFree(b->d_pos);

@@ -32,6 +32,7 @@
 #include "egtb_host.h"
 #include "egtb_kernels.cuh"
 #include "egtb_sort.cuh"
+#include "egtb_trie.h"
 
 namespace egtb {
 
@@ -1282,6 +1283,15 @@ static int first_step_to_run(const egtb_run_options &o, int rec) {
     return o.steps - 1;  // every step on disk
 }
 
+// compress: the books the reference's solve compresses (CompressionBridge.cpp:41-59,
+// called for layer i+2 after layer i is solved, BookSolver.cpp:596-597, and by
+// the optimal-branch pass, :720-728) become trie + xz directories, once every
+// pass that rewrites books (deletion threshold, optimal branches) is done.
+static void compress_books_if_asked(const egtb_run_options &o) {
+    if (!o.compress || !o.write_files) return;
+    compress_table_books(o.pathname, o.steps, dtype_size(o.success_rate_dtype), writer_threads(o));
+}
+
 static std::vector<uint64_t> read_u64_file(const std::string &path) {
     const uint64_t sz = file_size(path);
     std::vector<uint64_t> v(sz / 8);
@@ -1293,7 +1303,11 @@ static void check_common(const uint64_t *seeds, size_t n_seeds, const egtb_patte
                          const egtb_run_options *o) {
     if (!spec || !o) throw Error(EGTB_ERR_ARG, "spec and options are required");
     if (n_seeds && !seeds) throw Error(EGTB_ERR_ARG, "seeds pointer is NULL");
-    if (o->compress) throw Error(EGTB_ERR_UNSUPPORTED, "compressed books (compress) are not built");
+    if (o->compress) {
+        if (!o->write_files) throw Error(EGTB_ERR_UNSUPPORTED, "compressed books (compress) are files: build with write_files");
+        std::string why;
+        if (!xz_available(&why)) throw Error(EGTB_ERR_UNSUPPORTED, "compressed books need liblzma: " + why);
+    }
     dtype_size(o->success_rate_dtype);
     if (o->steps > (1 << 20)) throw Error(EGTB_ERR_ARG, "steps out of range");
 }
@@ -2002,6 +2016,7 @@ extern "C" int egtb_solve(const void *d1_records, size_t n1, const void *d2_reco
             using T = decltype(z);
             solve_files<T>(E, d1_records, n1, d2_records, n2, *spec, *options, stats);
             if (options->optimal_branch_only) optimal_branch_files<T>(E, *spec, *options);  // run_pattern_solve_impl
+            compress_books_if_asked(*options);
         });
     });
 }
@@ -2037,6 +2052,7 @@ extern "C" int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_patt
                 try {
                     fused_build<T>(E, seeds, n_seeds, *spec, *options, stats);
                     if (options->optimal_branch_only) optimal_branch_files<T>(E, *spec, *options);
+                    compress_books_if_asked(*options);
                     return;
                 } catch (const Error &e) {
                     // the table does not fit in device memory: with files, build it
@@ -2054,6 +2070,7 @@ extern "C" int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_patt
                 generate_files<T>(E, seeds, n_seeds, *spec, *options, &st, &g, streamed);
                 solve_files<T>(E, nullptr, 0, nullptr, 0, *spec, *options, stats);
                 if (options->optimal_branch_only) optimal_branch_files<T>(E, *spec, *options);
+                compress_books_if_asked(*options);
                 if (stats) {
                     stats->forward_ms = g.forward_ms;
                     stats->candidates = g.candidates;

@@ -399,6 +399,15 @@ class Reader:
         self.prefer_max = bool(prefer_max)
         self.last_op = 0
 
+    def _trie_lookup(self, zdir: str, stem: str, dtype: str):
+        import ztrie
+        layer = ztrie.TrieLayer.from_dir(zdir, stem, dtype)
+
+        def lookup(key):
+            raw = layer.search(key)
+            return _present(_DTYPE_INFO[dtype][1] if raw is None else raw, dtype)
+        return lookup
+
     def move_on_dic(self, board, path_list, pattern_full: str, nums_adjust: int):
         if not path_list:
             return [("?", "?")], ""
@@ -411,8 +420,13 @@ class Reader:
         ops = [0] if self.variant else [self.last_op] + list(range(8))  # operation_sequence, :171-182
         for directory, dtype in path_list:
             path = os.path.join(directory, f"{pattern_full}_{nums}.book")
-            if not os.path.exists(directory) or best > 0.0 or not os.path.exists(path):
+            zdir = os.path.join(directory, f"{pattern_full}_{nums}.z")
+            # a .book first, else its compressed .z directory (make_classic_lookup_context,
+            # ReaderRuntime.cpp:478-497; find_classic_value_with_context, :520-545)
+            if not os.path.exists(directory) or best > 0.0 or not (os.path.exists(path) or os.path.isdir(zdir)):
                 continue
+            lookup = (lambda key, p=path, dt=dtype: _file_lookup(p, key, dt)) if os.path.exists(path) else \
+                self._trie_lookup(zdir, f"{pattern_full}_{nums}.", dtype)
             for op in ops:
                 enc = _encode(_apply_operation(board, op))
                 if not _is_pattern(np.array([enc], dtype=np.uint64), self.masks)[0]:
@@ -425,7 +439,7 @@ class Reader:
                     if m == enc or not _is_pattern(np.array([m], dtype=np.uint64), self.masks)[0]:
                         continue
                     key = int(canonical(np.array([m], dtype=np.uint64), self.symm)[0])
-                    values[slot_of_move[d]] = _file_lookup(path, key, dtype)
+                    values[slot_of_move[d]] = lookup(key)
                 entries = [(_adjust_direction(op, k), values[i]) for i, k in enumerate(_ORDERED_KEYS)]
                 numeric = [e for e in entries if e[1] is not None]
                 others = [e for e in entries if e[1] is None]

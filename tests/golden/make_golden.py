@@ -107,6 +107,10 @@ HUGE_CASES = [("4432", 7, "float32")]
 # table at 1024: 560 steps, ~1 TB of raw layers). No success check happens
 # before docheck_step (504), so these raw layers are the whole table's.
 PREFIX_CASES = [("4432", 10, 130)]
+# builds with compress=True: books over 2 MiB (layers 3 and up) become trie +
+# xz-block directories <name>_<t>.z (TrieCompression.cpp:326-354, called from
+# BookSolver.cpp:596-597 and CompressionBridge.cpp:41-59)
+COMPRESS_CASES = [("442", 9, "float32"), ("442", 9, "uint32")]
 # float32 tables against the float64 build of the same pattern (the reference's
 # own builds): the largest and mean |r32 - r64| over every book entry
 FP64_CASES = [("L3", 8), ("442", 9)]
@@ -212,6 +216,48 @@ def run_fp64_error(catalog, pat, target):
     return r
 
 
+def run_compress_case(catalog, pat, target, dtype, rng):
+    """A compressed build by the reference: per layer, the .book digest or the
+    digests of the four files of its .z directory; plus move_on_dic answers on
+    the compressed table for positions sampled from the uncompressed books
+    (their answers on the uncompressed table are recorded beside them)."""
+    import shutil
+    case, plain_dir = run_case(catalog, pat, target, dtype)
+    masks, shifts, symm, seeds, steps, docheck, s0 = R.pattern_params(catalog[pat], target)
+    name = f"{pat}_{2 ** target}"
+    zdir = R.fresh_dir(os.path.join(WORK, f"{name}_{dtype}_compressed", "build") + "/")
+    spec, o = R.make_spec_options(masks, shifts, symm, target, steps, docheck, zdir + name + "_", dtype)
+    o.compress = True
+    R.run_build(seeds, spec, o)
+    layers = []
+    for t in range(steps):
+        b = zdir + f"{name}_{t}.book"
+        z = zdir + f"{name}_{t}.z"
+        if os.path.isdir(z):
+            stem = f"{name}_{t}."
+            layers.append({"kind": "z", "sha256": {sfx: sha(os.path.join(z, stem + sfx)) for sfx in ("i", "ii", "s", "z")}})
+        else:
+            layers.append({"kind": "book", "sha256": sha(b) if os.path.exists(b) else None})
+    case = dict(case, compress=True, size_class="compressed", layers=layers)
+    answers = reader_fixture(case, plain_dir, rng, n_pos=400)
+    fc = R.module()
+    sp = fc.PatternSpec()
+    sp.name = pat
+    sp.pattern_masks = [int(m, 16) for m in case["masks"]]
+    sp.success_shifts = case["shifts"]
+    sp.symm_mode = case["symm_mode"]
+    reader = fc.ClassicBookReader(sp, False)
+    differ = 0
+    for a in answers:
+        res, dt = reader.move_on_dic(a["board"], [(zdir, dtype)], name, -case["tile_sum0"])
+        got = [[k, v] for k, v in res.items()]
+        differ += got != a["result"]
+        a["result"], a["dtype"] = got, dt
+    case["reader_answers_differing_from_uncompressed"] = differ
+    shutil.rmtree(os.path.dirname(zdir.rstrip("/")), ignore_errors=True)
+    return case, answers
+
+
 def prims_fixture():
     L = ctypes.CDLL(os.path.join(R.REF_DIR, "libref_prims.so"))
     rng = np.random.default_rng(2048)
@@ -313,6 +359,8 @@ def main():
     ap.add_argument("--huge", action="store_true", help="also the 4432-128 build (needs ~45 GB of disk in GOLDEN_WORK)")
     ap.add_argument("--prefix", action="store_true",
                     help="also the forward prefix of the 13-cell diagonal table at 1024 (~30 GB in GOLDEN_WORK)")
+    ap.add_argument("--compress", action="store_true",
+                    help="also the compressed (trie + xz) builds of 442-512")
     ap.add_argument("--fp64", action="store_true",
                     help="also the float32-vs-float64 rate error of the full-size L3-256 and 442-512 tables")
     ap.add_argument("--only", default="", help="comma-separated case keys to (re)generate")
@@ -354,6 +402,12 @@ def main():
             continue
         print("case", key, flush=True)
         cases[key] = run_prefix(catalog, pat, target, steps)
+    for pat, target, dtype in (COMPRESS_CASES if args.compress else []):
+        key = f"{pat}_{2 ** target}_{dtype}_compressed"
+        if only and key not in only:
+            continue
+        print("case", key, flush=True)
+        cases[key], reader[key] = run_compress_case(catalog, pat, target, dtype, np.random.default_rng(17))
     for pat, target in (FP64_CASES if args.fp64 else []):
         key = f"{pat}_{2 ** target}_fp64_error"
         if only and key not in only:

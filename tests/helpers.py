@@ -65,6 +65,7 @@ def spec_options(case: dict, pathname: str):
     o.success_rate_dtype = case["dtype"]
     o.spawn_rate4 = case["spawn_rate4"]
     o.is_variant = bool(case.get("is_variant", False))
+    o.compress = bool(case.get("compress", False))
     return spec, o
 
 

@@ -144,9 +144,14 @@ def test_invalid_options_raise(tmp_root):
     F = H.fc()
     case = H.cases()["44_64_float32"]
     spec, o = H.spec_options(case, os.path.join(tmp_root, "bad_"))
+    # compressed books are files: a device-only build asking for them is refused
+    import ctypes
+    N = H.pkg()._native
     o.compress = True
-    with pytest.raises(RuntimeError, match="compress"):
-        F.run_pattern_build(H.seeds(case), spec, o)
+    seeds = H.seeds(case)
+    c_spec, c_opt = spec.to_c(), o.to_c(write_files=False)
+    rc = N.lib().egtb_build(seeds.ctypes.data, len(seeds), ctypes.byref(c_spec), ctypes.byref(c_opt), None)
+    assert rc == -7 and "compress" in N.last_error()
     o.compress = False
     spec.symm_mode = 7
     with pytest.raises(RuntimeError, match="symmetry"):

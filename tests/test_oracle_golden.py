@@ -111,3 +111,61 @@ def test_oracle_reader_answers(key, tmp_path):
         res, dt = reader.move_on_dic(entry["board"], [(str(tmp_path), case["dtype"])], name, -case["tile_sum0"])
         assert [[k, v] for k, v in res] == entry["result"], (key, i, entry["board"])
         assert dt == entry["dtype"], (key, i)
+
+
+# ------------------------------------------------- compressed books (.z) ----
+
+COMPRESSED_CASES = sorted(k for k, v in H.cases().items() if v.get("size_class") == "compressed")
+
+
+def test_compression_rule_selects_the_reference_layers():
+    """Layers 3 and up whose book passes 2 MiB are the ones the reference
+    compressed (CompressionBridge.cpp:41-59)."""
+    import ztrie
+    for key in COMPRESSED_CASES:
+        case = H.cases()[key]
+        rec = 12 if case["dtype"] in ("uint32", "float32") else 16
+        for t, layer in enumerate(case["layers"]):
+            name = f"{case['pattern_full']}_{t}.book"
+            assert ztrie.wants_compression(name, case["book_len"][t] * rec) == (layer["kind"] == "z"), (key, t)
+
+
+@pytest.fixture(scope="module")
+def oracle_442():
+    case = H.cases()["442_512_float32"]
+    b = _build(case)
+    return b
+
+
+@pytest.mark.parametrize("dtype", ["float32", "uint32"])
+def test_oracle_compressed_layers_equal_the_reference(oracle_442, dtype):
+    """The oracle's restatement of the trie + xz format, on the oracle's own
+    442-512 books, writes the reference's .z files byte for byte (smallest,
+    middle and last compressed layers)."""
+    import ztrie
+    case = H.cases()[f"442_512_{dtype}_compressed"]
+    oracle_442.solve(dtype, 0.1)
+    zl = [t for t, layer in enumerate(case["layers"]) if layer["kind"] == "z"]
+    for t in (zl[0], zl[len(zl) // 2], zl[-1]):
+        book = oracle_442.book(t, dtype)
+        assert H.sha_bytes(book) == case["book_sha256"][t]
+        stem = f"{case['pattern_full']}_{t}."
+        files = ztrie.compress_book(book, dtype, stem)
+        for sfx, want in case["layers"][t]["sha256"].items():
+            assert H.sha_bytes(files[stem + sfx]) == want, (dtype, t, sfx)
+
+
+def test_oracle_trie_search_finds_every_entry(oracle_442):
+    """The restated reader search over a compressed layer returns each book
+    entry's rate, and a miss for boards that are not in the layer."""
+    import ztrie
+    oracle_442.solve("float32", 0.1)
+    case = H.cases()["442_512_float32_compressed"]
+    t = [t for t, layer in enumerate(case["layers"]) if layer["kind"] == "z"][0]
+    book = oracle_442.book(t, "float32")
+    stem = f"{case['pattern_full']}_{t}."
+    layer = ztrie.TrieLayer(ztrie.compress_book(book, "float32", stem), stem, "float32")
+    rec = np.frombuffer(book, dtype=[("key", "<u8"), ("rate", "<f4")])
+    for i in range(0, len(rec), 97):
+        assert layer.search(int(rec["key"][i])) == rec["rate"][i].item(), i
+    assert layer.search(int(rec["key"][0]) - 1) is None
