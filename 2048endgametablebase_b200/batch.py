@@ -225,3 +225,51 @@ def batch_mismatches(tables: list[Table], dtype: str = "float32", device: int = 
                 bad.append(t.name)
                 break
     return bad
+
+
+# ------------------------------------------------ batches across GPUs ----
+#
+# The tables of a batch are independent: across N GPUs each rank builds its
+# own share of them as one batch, with no collective on the data path (the
+# reference builds every table in its own run, engine_core/BookBuilder.py:264).
+
+
+def table_weight(t: Table) -> float:
+    """Work estimate used to balance tables over GPUs: a table's boards grow
+    about sixfold per free cell and with its number of steps."""
+    return (6.0 ** len(t.cells)) * t.steps
+
+
+def shard_tables(tables: list[Table], world: int) -> list[list[int]]:
+    """Indexes of the tables each of `world` ranks builds: heaviest first,
+    each to the rank with the least work so far (ties to the lowest rank);
+    every table goes to exactly one rank, in ascending order within a rank."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    load = [0.0] * world
+    share: list[list[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(tables)), key=lambda i: (-table_weight(tables[i]), i)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        share[r].append(i)
+        load[r] += table_weight(tables[i])
+    return [sorted(s) for s in share]
+
+
+def build_shard(tables: list[Table], rank: int, world: int, dtype: str = "float32", device: int = 0,
+                params: dict | None = None):
+    """Build this rank's share of `tables` as one batch on `device`. Returns
+    (the share's table indexes, per-table stats, batch stats); the share's
+    books are the device's last batch, table k of the share as batch table k."""
+    mine = shard_tables(tables, world)[rank]
+    if not mine:
+        return mine, [], {"raw_boards": 0, "kernel_launches": 0}
+    ts, bs = build_batch([tables[i] for i in mine], dtype, device, params)
+    return mine, ts, bs
+
+
+def shard_digests(tables: list[Table], mine: list[int], device: int = 0) -> dict:
+    """{table name: SHA-256 of every book layer} of the device's last batch,
+    built from the tables listed in `mine` (as build_shard did)."""
+    import hashlib
+    return {tables[i].name: [hashlib.sha256(batch_book(k, L, device)).hexdigest() for L in range(tables[i].steps)]
+            for k, i in enumerate(mine)}

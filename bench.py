@@ -294,6 +294,14 @@ def main():
         shutil.rmtree(work, ignore_errors=True)
         return
     if args.batch_only:
+        if world > 1:
+            line = batch_shard_leg(local, world, rank, pg, max(1, args.steps), max(1, args.warmup))
+            if rank == 0:
+                print(json.dumps(line), flush=True)
+            shutil.rmtree(work, ignore_errors=True)
+            pg.barrier()
+            pg.destroy_process_group()
+            return
         print(json.dumps({"batched": batch_leg(local, cpu_reference=not args.no_cpu_baseline)}), flush=True)
         shutil.rmtree(work, ignore_errors=True)
         return
@@ -609,6 +617,55 @@ def batch_leg(local: int, steps: int = 3, cpu_reference: bool = True) -> dict:
         if ref:
             out["cpu_reference"] = ref
     return out
+
+
+def batch_shard_leg(local: int, world: int, rank: int, pg, steps: int, warmup: int, build_shard=None,
+                    device_timer=None) -> dict:
+    """The 64-table batch spread over the ranks by table (batch.shard_tables:
+    heaviest first onto the least-loaded rank), each rank building its share
+    as one batch; no collective on the data path. Time = the slowest rank's
+    device time per build (CUDA events on its stream); value = every rank's
+    boards over that time (strong scaling: the 64 tables are fixed).
+    build_shard / device_timer stand in for the GPU in host-only tests."""
+    B = importlib.import_module("2048endgametablebase_b200.batch")
+    tables = B.random_tables(64)
+    if build_shard is None:
+        build_shard = lambda: B.build_shard(tables, rank, world, device=local)  # noqa: E731
+    if device_timer is None:
+        import torch
+
+        N = importlib.import_module("2048endgametablebase_b200._native")
+        stream = torch.cuda.current_stream(local)
+        N.set_stream(local, stream.cuda_stream)
+
+        def device_timer(fn, k):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(k):
+                r = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return r, e0.elapsed_time(e1) / k
+    # the scalars the ranks exchange live where the backend wants them
+    dev = "cpu" if pg.get_backend() == "gloo" else f"cuda:{local}"
+    for _ in range(warmup):
+        build_shard()
+    pg.barrier()
+    (mine, ts, bs), ms = device_timer(build_shard, steps)
+    pg.barrier()
+    ms_max = max_over_ranks(pg, ms, dev)
+    import torch
+
+    tot = torch.tensor([float(bs["raw_boards"]), float(len(mine))], dtype=torch.float64, device=dev)
+    pg.all_reduce(tot)
+    boards = int(tot[0].item())
+    return {"metric": "batched table-build boards/s", "value": boards / (ms_max / 1e3), "unit": "boards/s",
+            "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": ms_max, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "u64 keys, f64 fma accumulate, float32 rates",
+            "data": "synthetic (64 seeded random tables)",
+            "config": {"workload": "64 random tables, 6-10 free cells, targets 64..512, split over ranks by table",
+                       "boards": boards, "tables": int(tot[1].item()), "parallelism": f"tables over {world} ranks"}}
 
 
 def serving_leg(local: int, base: str | None, seconds: float = 0.5, offered: float = 3e8,

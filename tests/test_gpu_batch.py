@@ -148,3 +148,59 @@ def test_benchmark_batch_of_64_equals_plain_builds():
     big = [i for i, t in enumerate(tables) if len(t.cells) == 10 and t.target == 9]
     assert big, "the workload holds 10-cell target-512 tables"
     assert sum(ts[i]["raw_boards"] for i in big) > bs["raw_boards"] // 2
+
+
+def _shard_rank(rank, world, port, q):
+    """One rank of a 2-process batch split (both on GPU 0, gloo for the
+    host-side exchange): build this rank's share, report its digests."""
+    import datetime
+    import sys
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    sys.path.insert(0, H.ROOT)
+    import torch.distributed as dist
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    B = importlib.import_module("2048endgametablebase_b200.batch")
+    tables = B.random_tables(64)
+    mine, ts, bs = B.build_shard(tables, rank, world, device=0)
+    dig = B.shard_digests(tables, mine, device=0)
+    got = [None] * world
+    dist.all_gather_object(got, dig)
+    q.put((rank, got))
+    dist.destroy_process_group()
+
+
+@pytest.mark.slow
+def test_tables_split_over_two_ranks_equal_the_single_batch():
+    """The 64-table benchmark batch split over two ranks by table: the
+    union of the ranks' books equals the books of the whole batch built in
+    one process, table by table."""
+    import socket
+
+    import torch.multiprocessing as mp
+    B = _B()
+    tables = B.random_tables(64)
+    B.build_batch(tables)
+    whole = {t.name: d for t, d in zip(tables, _batch_digests(tables))}
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_shard_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    try:
+        got = [q.get(timeout=900) for _ in procs]
+    finally:
+        for p in procs:
+            p.join(timeout=120)
+            if p.is_alive():
+                p.kill()
+    assert all(p.exitcode == 0 for p in procs)
+    for rank, gathered in got:
+        merged = {}
+        for part in gathered:
+            assert not set(part) & set(merged)  # no table on two ranks
+            merged.update(part)
+        assert merged == whole, rank
