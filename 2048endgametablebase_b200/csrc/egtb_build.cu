@@ -236,8 +236,8 @@ struct Engine {
         EGTB_CUDA(cudaMalloc(&counters, sizeof(unsigned) * 16));
         int per_sm = 0;
         EGTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel, kSweepThreads, 0));
-        EGTB_CUDA(cudaFuncSetAttribute(expand_dedup_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
-        EGTB_CUDA(cudaFuncSetAttribute(expand_dedup_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
+        EGTB_CUDA(cudaFuncSetAttribute(expand_gen_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
+        EGTB_CUDA(cudaFuncSetAttribute(expand_gen_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
         sweep_grid = sm_count * std::max(1, per_sm);
         progress_device_ptr();
     }

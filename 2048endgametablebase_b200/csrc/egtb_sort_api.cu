@@ -161,7 +161,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 // Device address of g_noalloc_scratch per device. In host code the array's
 // name only stands in for the symbol, so the address is asked for once per
-// device, with that device current.
+// device, with that device current. It stays valid while the device's
+// context lives: a cudaDeviceReset ends that, and the entry point is not to
+// be called on that device afterwards (documented in egtb_gpu.h).
 static std::mutex g_noalloc_mu;
 static unsigned char *g_noalloc_ptr[64] = {};
 static int g_noalloc_grid[64] = {};

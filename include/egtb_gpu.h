@@ -91,7 +91,7 @@ typedef struct egtb_run_options {
     double spawn_rate4;
     int32_t success_rate_dtype; /* enum egtb_dtype */
     double deletion_threshold;
-    int32_t compress;
+    int32_t compress;     /* books of layer 3+ over 2 MiB -> <pathname><t>.z trie + xz directories (needs write_files) */
     int32_t compress_temp_files;
     int32_t optimal_branch_only;
     int32_t chunked_solve;
@@ -232,7 +232,10 @@ EGTB_API int egtb_sort_unique_u64(int device, const uint64_t *d_keys, size_t n, 
  * scratch is a static device array of about 8.6 MB that every GPU loading
  * the library holds until exit; the first call on a device looks up that
  * array's address, so make the first call before any stream capture. All
- * calls share the array: calls that overlap on the GPU race. */
+ * calls share the array: calls that overlap on the GPU race. The address is
+ * kept for the life of the process: after a cudaDeviceReset of a device
+ * (which unloads the library's device code there) do not call this entry
+ * point on that device again. */
 EGTB_API int egtb_sort_unique_u64_noalloc(int device, const uint64_t *d_keys, size_t n, uint64_t *d_out,
                                           uint64_t *d_n_out, void *stream);
 
@@ -244,7 +247,12 @@ typedef struct egtb_book egtb_book;
  * resident in device memory as sorted keys + rates (the reader side of
  * ClassicBookReader, native_core/src/ReaderRuntime.cpp:1050-1067).
  * nums_adjust is the pattern's -(seed tile sum) (Config.py:265). Layers
- * are loaded on first use; max_layers bounds the layer index scanned. */
+ * are loaded on first use; max_layers bounds the layer index scanned. A
+ * layer without a .book file is read from its compressed directory
+ * <pattern_full>_<t>.z when there is one (trie + xz blocks,
+ * TrieCompression.cpp:326-354): its blocks are decoded on the host and
+ * searched on the device as trie_search_with_context does
+ * (ReaderRuntime.cpp:318-477). */
 EGTB_API int egtb_book_open(const char *dir, const char *pattern_full, int32_t dtype, const egtb_pattern_spec *spec,
                    int64_t nums_adjust, int32_t device, egtb_book **out);
 EGTB_API int egtb_book_close(egtb_book *book);
