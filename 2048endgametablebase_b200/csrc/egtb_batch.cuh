@@ -37,7 +37,7 @@ struct BatchTable {
     uint64_t *set[2];              // exact dedup sets by layer parity
     unsigned long long set_mask;
     uint64_t *filter;
-    ulonglong2 *index[4];          // rate index planes: layer L in index[L % 4], tagged by tile sum
+    ulonglong2 *index[4];          // rate index planes: layer L in index[L % 4], zeroed by step L+1
     unsigned long long index_mask;
 };
 
@@ -247,11 +247,9 @@ __device__ __forceinline__ void grid_zero16(void *p, unsigned long long words) {
 // ------------------------------------------------------------ backward ----
 //
 // Four rate-index planes per table (layer L in plane L % 4), all zeroed before
-// the backward pass; the solve of step t inserts layer t into plane t % 4.
-// Planes are tagged by tile sum (index_insert_tagged): a slot whose key has
-// another tile sum than the layer searched (layer t+4's, which used the
-// plane before, or 0) is empty, so no step clears a plane. A probe stops at
-// such a slot.
+// the backward pass; the solve of step t inserts layer t into plane t % 4 and
+// zeroes plane (t-1) % 4, whose last layer (t+3) was read by steps t+1 and
+// t+2, for the inserts of step t-1. A probe stops at a zero key.
 
 // Layers steps-2 and steps-1 of every table: success -> max, else zero
 // (final_situation_process, native_core/src/BookSolver.cpp:237-261); live
@@ -296,11 +294,12 @@ batch_solve_kernel(const BatchTable *__restrict__ TB, BatchCtl *C, int n_tables,
                    unsigned progress_value) {
     __shared__ unsigned long long pre[kMaxBatchTables + 1];
     __shared__ unsigned long long scan_sm[33];
-    __shared__ unsigned bsum[256];
-    init_byte_sums(bsum);
     seg_prefix(n_tables, pre, scan_sm, [&](int i) -> unsigned long long {
         return t <= TB[i].steps - 3 ? layer_len[TB[i].lbase + t] : 0ull;
     });
+    if (t >= 2)
+        for (int i = 0; i < n_tables; ++i)
+            if (t <= TB[i].steps - 3) grid_zero16(TB[i].index[(t - 1) % 4], TB[i].index_mask + 1);
     if (progress && blockIdx.x == 0 && threadIdx.x == 0) *(volatile unsigned *)progress = progress_value;
     const unsigned long long total = pre[n_tables];
     unsigned long long looks = 0;
@@ -356,9 +355,8 @@ batch_solve_kernel(const BatchTable *__restrict__ TB, BatchCtl *C, int n_tables,
                             if (sl.x == key[j]) {
                                 got[j] = rate_from_bits<T>(sl.y);
                                 pend &= ~(1u << j);
-                            } else if (sl.x == 0ull ||
-                                       board_tile_sum(sl.x, bsum) != tb.s0 + 2ll * (t + (j < 4 ? 1 : 2))) {
-                                pend &= ~(1u << j);  // an empty slot: the key is not in the layer
+                            } else if (sl.x == 0ull) {
+                                pend &= ~(1u << j);
                             } else {
                                 h[j] = (h[j] + 1) & m;
                             }
@@ -381,8 +379,7 @@ batch_solve_kernel(const BatchTable *__restrict__ TB, BatchCtl *C, int n_tables,
             r = nempty > 0 ? cast_rate<T>(acc / (double)nempty) : zero;
         }
         rates[o] = r;
-        if (t > 0 && r > zero)
-            index_insert_tagged<T>(tb.index[t % 4], tb.index_mask, b, r, tb.s0 + 2ll * t, bsum, &C[i].err);
+        if (t > 0 && r > zero) index_insert_zero<T>(tb.index[t % 4], tb.index_mask, b, r, &C[i].err);
     }
     for (int o = 16; o > 0; o >>= 1) looks += __shfl_xor_sync(0xFFFFFFFFu, looks, o);
     if ((threadIdx.x & 31) == 0 && looks) atomicAdd(&sync->lookups, looks);

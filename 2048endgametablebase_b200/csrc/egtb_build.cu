@@ -177,9 +177,6 @@ struct Engine {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_sorted = nullptr, ev_copied = nullptr;
     uint64_t *cand[2] = {nullptr, nullptr};
-    // a step's children, repeats included, for layers t+1 and t+2 (expand_gen_kernel)
-    uint64_t *gen[2] = {nullptr, nullptr};
-    unsigned long long gen_cap = 0;
     uint64_t *tmp = nullptr;
     unsigned *hist = nullptr;               // digit histograms, kMaxPasses x 256
     unsigned *counters = nullptr;           // tile counters of the sort passes and the unique kernel
@@ -236,8 +233,8 @@ struct Engine {
         EGTB_CUDA(cudaMalloc(&counters, sizeof(unsigned) * 16));
         int per_sm = 0;
         EGTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel, kSweepThreads, 0));
-        EGTB_CUDA(cudaFuncSetAttribute(expand_gen_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
-        EGTB_CUDA(cudaFuncSetAttribute(expand_gen_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
+        EGTB_CUDA(cudaFuncSetAttribute(expand_dedup_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
+        EGTB_CUDA(cudaFuncSetAttribute(expand_dedup_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
         sweep_grid = sm_count * std::max(1, per_sm);
         progress_device_ptr();
     }
@@ -384,17 +381,6 @@ struct Engine {
         ensure_comp_tiles();
     }
 
-    void ensure_gen(unsigned long long cap) {
-        if (cap <= gen_cap) return;
-        release(gen[0]);
-        release(gen[1]);
-        gen_cap = cap;
-        grow(gen_cap, [&] {
-            alloc_or_throw((void **)&gen[0], sizeof(uint64_t) * gen_cap, "step children");
-            alloc_or_throw((void **)&gen[1], sizeof(uint64_t) * gen_cap, "step children");
-        });
-    }
-
     void ensure_comp_tiles() {
         const unsigned long long need = std::max(arena_cap, cand_cap) / kTileKeys + 2;
         if (need <= comp_tiles) return;
@@ -531,8 +517,8 @@ struct ForwardPlan {
 // The expand and solve kernels come in two builds: with the variant boards'
 // symmetry modes (min33/min24/min34) and without; a table takes the one its
 // mode needs, so the classic tables' kernels carry no variant code.
-static auto expand_gen_kernel_for(const DevSpec &spec) {
-    return spec.symm >= 4 ? expand_gen_kernel<true> : expand_gen_kernel<false>;
+static auto expand_kernel_for(const DevSpec &spec) {
+    return spec.symm >= 4 ? expand_dedup_kernel<true> : expand_dedup_kernel<false>;
 }
 
 template <typename T>
@@ -544,30 +530,19 @@ static auto solve_kernel_for(const DevSpec &spec) {
 // kernel each) and close the last two layers. Preconditions on the device:
 // layer first_step-1 in its staging buffer, layer first_step's keys so far in
 // its staging buffer and set, layer_off[first_step-1] set.
-// One forward step: expand layer t (children with repeats into the step
-// buffers), then the exact-set inserts. arena == nullptr: streamed layers.
-static void enqueue_expand_step(Engine &E, const ForwardPlan &P, int i, uint64_t *arena, unsigned long long arena_cap,
-                                unsigned *progress) {
-    cudaStream_t s = E.stream;
-    uint64_t *stage[3] = {E.cand[0], E.cand[1], E.tmp};
-    const int t = i - 1;
-    const auto gen = expand_gen_kernel_for(P.spec);
-    EGTB_LAUNCH(E, gen<<<E.sm_count, kExpandThreads, kRowSmemBytes, s>>>(
-                       stage[t % 3], t % 3, arena, E.layer_off, E.layer_len, arena_cap, t, P.spec,
-                       i > P.docheck ? 1 : 0, E.tab, E.gen[0], E.gen[1], E.gen_cap, E.dset[t % 3], E.dset_cap - 1,
-                       E.ctl));
-    EGTB_LAUNCH(E, expand_insert_kernel<<<E.sm_count * 8, kInsertThreads, 0, s>>>(
-                       E.gen[0], E.gen[1], stage[(t + 1) % 3], stage[(t + 2) % 3], t % 3, (t + 1) % 3, (t + 2) % 3,
-                       E.dset[(t + 1) % 3], E.dset[(t + 2) % 3], E.dset_cap - 1, E.cand_cap, E.ctl, progress,
-                       (unsigned)i));
-}
-
 static void enqueue_forward(Engine &E, const ForwardPlan &P, unsigned *progress) {
     cudaStream_t s = E.stream;
+    const int g_exp = E.sm_count;  // one 1024-thread block per SM (the row table fills its shared memory)
     uint64_t *stage[3] = {E.cand[0], E.cand[1], E.tmp};
+    const auto expand = expand_kernel_for(P.spec);
     for (int i = P.first_step; i < P.steps - 1; ++i) {
+        const int t = i - 1;
         const int pe = E.prof_begin(K_EXPAND);
-        enqueue_expand_step(E, P, i, E.arena, E.arena_cap, progress);
+        EGTB_LAUNCH(E, expand<<<g_exp, kExpandThreads, kRowSmemBytes, s>>>(
+                           stage[t % 3], stage[(t + 1) % 3], stage[(t + 2) % 3], t % 3, (t + 1) % 3, (t + 2) % 3,
+                           E.arena, E.layer_off, E.layer_len, E.arena_cap, t, P.spec, i > P.docheck ? 1 : 0, E.tab,
+                           E.dset[(t + 1) % 3], E.dset[(t + 2) % 3], E.dset_cap - 1, E.cand_cap, E.filter,
+                           E.filter_bits, E.dset[t % 3], E.ctl, progress, (unsigned)i));
         E.prof_end(pe);
     }
     for (int L = std::max(P.first_step, P.steps - 2); L < P.steps; ++L)
@@ -692,9 +667,6 @@ static int run_forward(Engine &E, const ForwardPlan &P, const uint64_t *base, si
     unsigned long long set_need = init_set;
     while (set_need < 4 * std::max<unsigned long long>(n_partial, 1)) set_need <<= 1;
     E.ensure_dedup(std::max(E.dset_cap, set_need));
-    // a step's children with repeats: ~6 per parent on the catalog's tables
-    static const unsigned long long init_gen = env_keys("EGTB_INIT_GEN_KEYS", 1ull << 24);
-    E.ensure_gen(std::max(E.gen_cap, std::max(init_gen, 8 * std::max<unsigned long long>(n_base, n_partial))));
     unsigned *progress = progress_device_ptr();
     for (;;) {
         stage_start(E, P, base, n_base, partial, n_partial);
@@ -723,7 +695,6 @@ static int run_forward(Engine &E, const ForwardPlan &P, const uint64_t *base, si
         if (c.err & kErrCandOverflow) E.ensure_cand(E.cand_cap * 2);
         if (c.err & kErrArenaOverflow) E.ensure_arena(E.arena_cap + E.arena_cap / 2);
         if (c.err & kErrDedupOverflow) E.ensure_dedup(E.dset_cap * 2);
-        if (c.err & kErrGenOverflow) E.ensure_gen(E.gen_cap * 2);
     }
 }
 
@@ -797,7 +768,6 @@ static int run_forward_streamed(Engine &E, const ForwardPlan &P, const uint64_t 
     });
     for (;;) {
         E.ensure_sort_bufs(E.cand_cap);
-        E.ensure_gen(std::max(E.gen_cap, 4 * E.cand_cap));
         E.ensure_status();
         stage_start(E, P, base, n_base, partial, n_partial);
         unsigned char *pin = E.ensure_pinned(2 * E.cand_cap * sizeof(uint64_t));
@@ -842,10 +812,15 @@ static int run_forward_streamed(Engine &E, const ForwardPlan &P, const uint64_t 
                 }
             });
         };
+        const auto expand = expand_kernel_for(P.spec);
         for (int i = P.first_step; i < steps - 1 && !err; ++i) {
             const int t = i - 1;
             const int pe = E.prof_begin(K_EXPAND);
-            enqueue_expand_step(E, P, i, nullptr, 0, progress);
+            EGTB_LAUNCH(E, expand<<<E.sm_count, kExpandThreads, kRowSmemBytes, s>>>(
+                               stage[t % 3], stage[(t + 1) % 3], stage[(t + 2) % 3], t % 3, (t + 1) % 3, (t + 2) % 3,
+                               nullptr, E.layer_off, E.layer_len, 0, t, P.spec, i > P.docheck ? 1 : 0, E.tab,
+                               E.dset[(t + 1) % 3], E.dset[(t + 2) % 3], E.dset_cap - 1, E.cand_cap, E.filter,
+                               E.filter_bits, E.dset[t % 3], E.ctl, progress, (unsigned)i));
             E.prof_end(pe);
             if (pending >= 0) {  // ship the layer sorted last step while this step runs
                 ship(pending, pending_buf);
@@ -903,7 +878,6 @@ static int run_forward_streamed(Engine &E, const ForwardPlan &P, const uint64_t 
         if (retries > 24) throw Error(EGTB_ERR_CAPACITY, "forward pass did not fit after repeated regrowth");
         if (err & kErrCandOverflow) E.ensure_cand(E.cand_cap * 4);
         if (err & kErrDedupOverflow) E.ensure_dedup(E.dset_cap * 4);
-        if (err & kErrGenOverflow) E.ensure_gen(E.gen_cap * 4);
     }
 }
 
@@ -963,7 +937,6 @@ struct BackwardPlan {
     int steps, docheck, dtype;
     double p4;
     DevSpec spec;
-    long long s0;  // tile sum of layer 0 (layer L: s0 + 2L), the rate indexes' tag
 };
 
 // Slots of the rate index of a layer of n entries: a power of two >= 2n.
@@ -1050,21 +1023,22 @@ static void enqueue_backward(Engine &E, const BackwardPlan &B, const std::vector
     const int pf = E.prof_begin(K_FINAL);
     for (int t = B.steps - 2; t < B.steps; ++t)
         if (t >= 0) EGTB_LAUNCH(E, final_layer_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec, zero, maxv));
-    // keys of another table's build must not pass for this one's: the four
-    // index buffers start empty; within the build the tile-sum tags keep
-    // the layers that share a buffer apart, so no launch clears an index
-    for (auto *ix : E.index) EGTB_CUDA(cudaMemsetAsync(ix, 0, sizeof(ulonglong2) * E.index_cap, s));
     for (int t = B.steps - 1; t >= B.steps - 2 && t >= 1; --t) enqueue_index<T>(E, t, len[t], zero);
+    // the solve of layer t reads the indexes of t+1 and t+2, fills layer t's
+    // (L % 4, cleared by the launch before) and clears the one of layer t-1
+    if (B.steps - 3 >= 1)
+        EGTB_CUDA(cudaMemsetAsync(E.index[(B.steps - 3) % 4], 0, sizeof(ulonglong2) * index_slots(len[B.steps - 3]), s));
     E.prof_end(pf);
-    // the solve of layer t reads the indexes of t+1 and t+2 and fills layer t's (L % 4)
     for (int t = B.steps - 3; t >= 0; --t) {
         const int ps = E.prof_begin(K_SOLVE);
         ulonglong2 *idx0 = t >= 1 ? E.index[t % 4] : nullptr;
+        ulonglong2 *clear = t >= 2 ? E.index[(t - 1) % 4] : nullptr;
         EGTB_LAUNCH(E, solve_kernel_for<T>(B.spec)<<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec,
                                                          t > B.docheck ? 1 : 0, E.tab, B.p4, zero, maxv,
                                                          E.index[(t + 1) % 4], index_slots(len[t + 1]) - 1,
                                                          E.index[(t + 2) % 4], index_slots(len[t + 2]) - 1, E.ctl,
-                                                         B.s0, idx0, index_slots(len[t]) - 1, progress,
+                                                         idx0, index_slots(len[t]) - 1, clear,
+                                                         t >= 2 ? index_slots(len[t - 1]) : 0, progress,
                                                          total - (unsigned)t - 2u));
         E.prof_end(ps);
     }
@@ -1124,8 +1098,9 @@ static void backward_write_books(Engine &E, const BackwardPlan &B, const std::ve
     const int pf = E.prof_begin(K_FINAL);
     for (int t = steps - 2; t < steps; ++t)
         if (t >= 0) EGTB_LAUNCH(E, final_layer_kernel<T><<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec, zero, maxv));
-    for (auto *ix : E.index) EGTB_CUDA(cudaMemsetAsync(ix, 0, sizeof(ulonglong2) * E.index_cap, s));
     for (int t = steps - 1; t >= steps - 2 && t >= 1; --t) enqueue_index<T>(E, t, len[t], zero);
+    if (steps - 3 >= 1)
+        EGTB_CUDA(cudaMemsetAsync(E.index[(steps - 3) % 4], 0, sizeof(ulonglong2) * index_slots(len[steps - 3]), s));
     E.prof_end(pf);
     close_group(std::max(0, steps - 2), steps);
     constexpr int kGroup = 16;  // layers per packed group
@@ -1133,11 +1108,13 @@ static void backward_write_books(Engine &E, const BackwardPlan &B, const std::ve
     for (int t = steps - 3; t >= 0; --t) {
         const int ps = E.prof_begin(K_SOLVE);
         ulonglong2 *idx0 = t >= 1 ? E.index[t % 4] : nullptr;
+        ulonglong2 *clear = t >= 2 ? E.index[(t - 1) % 4] : nullptr;
         EGTB_LAUNCH(E, solve_kernel_for<T>(B.spec)<<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec,
                                                          t > B.docheck ? 1 : 0, E.tab, B.p4, zero, maxv,
                                                          E.index[(t + 1) % 4], index_slots(len[t + 1]) - 1,
                                                          E.index[(t + 2) % 4], index_slots(len[t + 2]) - 1, E.ctl,
-                                                         B.s0, idx0, index_slots(len[t]) - 1, progress,
+                                                         idx0, index_slots(len[t]) - 1, clear,
+                                                         t >= 2 ? index_slots(len[t - 1]) : 0, progress,
                                                          total - (unsigned)t - 2u));
         E.prof_end(ps);
         if (hi - t == kGroup || t == 0) {
@@ -1392,7 +1369,7 @@ static void fused_build(Engine &E, const uint64_t *seeds, size_t n_seeds, const 
     const int retries = run_forward(E, P, seeds, n_seeds, nullptr, 0, &fwd_ms);
     std::vector<unsigned long long> off = d2h_u64(E, E.layer_off, steps + 1);
     std::vector<unsigned long long> len = d2h_u64(E, E.layer_len, steps + 1);
-    BackwardPlan B{steps, o.docheck_step, o.success_rate_dtype, o.spawn_rate4, P.spec, P.s0};
+    BackwardPlan B{steps, o.docheck_step, o.success_rate_dtype, o.spawn_rate4, P.spec};
     E.ensure_rates(sizeof(T));
     std::vector<unsigned long long> blen, maxb;
     if (o.write_files) {
@@ -1665,13 +1642,10 @@ static void solve_files(Engine &E, const void *d1_recs, size_t n1, const void *d
             enqueue_index_at<T>(E, 2, dlen2, zero, E.index[idx_of[2]]);
             index_fresh = true;
         }
-        // the kernel's layer 0 is layer i here: its tile sum tags the lookups
-        // (the indexes of i+1 and i+2 were cleared before their inserts)
-        const long long s_i = n0 ? seed_tile_sum(raw[0]) : 0;
         EGTB_LAUNCH(E, solve_kernel_for<T>(ds)<<<E.sm_count * 8, 256, 0, s>>>(
                            E.arena, rates, E.layer_off, E.layer_len, 0, ds, i > o.docheck_step ? 1 : 0, E.tab,
                            o.spawn_rate4, zero, maxv, E.index[idx_of[1]], index_slots(dlen1) - 1, E.index[idx_of[2]],
-                           index_slots(dlen2) - 1, E.ctl, s_i, nullptr, 0, nullptr, 0));
+                           index_slots(dlen2) - 1, E.ctl, nullptr, 0, nullptr, 0, nullptr, 0));
         if (i > 0) enqueue_index_at<T>(E, 0, n0, zero, E.index[idx_of[0]]);
         EGTB_LAUNCH(E, splitters_kernel<<<E.sm_count, 256, 0, s>>>(k0, n0, E.split + slot_of[0] * slot / kSplitStride));
         enqueue_pack<T>(E, 0, zero);

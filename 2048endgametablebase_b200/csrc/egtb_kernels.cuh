@@ -17,7 +17,6 @@ constexpr unsigned kErrArenaOverflow = 2u;
 constexpr unsigned kErrBookOverflow = 4u;
 constexpr unsigned kErrDedupOverflow = 16u;
 constexpr unsigned kErrIndexOverflow = 32u;
-constexpr unsigned kErrGenOverflow = 64u;
 
 constexpr int kTileKeys = 4096;     // keys per sort / compaction tile
 constexpr int kSortThreads = 256;   // 8 warps x 16 keys x 32 lanes
@@ -33,7 +32,6 @@ struct DevCtl {
     unsigned long long candidates;      // statistics: keys that reached a sort
     unsigned long long lookups;         // statistics: exact searches in the backward pass
     unsigned long long expand_next;     // next 32-parent chunk of the running expand launch
-    unsigned long long gen_count[2];    // candidates of the running step for layers t+1, t+2 (expand_gen_kernel)
     unsigned int err;
     unsigned int pad;
 };
@@ -134,15 +132,14 @@ __device__ __forceinline__ unsigned spawn_children(const Rows &rows, const MoveC
 
 // Flush a warp's staging buffer to its candidate stream.
 __device__ __forceinline__ void stage_flush(uint64_t *stage, int &count, uint64_t *__restrict__ out,
-                                            unsigned long long *cnt, unsigned long long cap, unsigned *err,
-                                            unsigned overflow_flag = kErrCandOverflow) {
+                                            unsigned long long *cnt, unsigned long long cap, unsigned *err) {
     const int lane = threadIdx.x & 31;
     if (count == 0) return;
     unsigned long long base = 0;
     if (lane == 0) base = atomicAdd(cnt, (unsigned long long)count);
     base = __shfl_sync(0xFFFFFFFFu, base, 0);
     if (base + (unsigned long long)count > cap) {
-        if (lane == 0) atomicOr(err, overflow_flag);
+        if (lane == 0) atomicOr(err, kErrCandOverflow);
     } else {
         for (int i = lane; i < count; i += 32) out[base + i] = stage[i];
     }
@@ -424,192 +421,6 @@ expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ sta
     }
 }
 
-// ------------------------------------------ expand in two kernels --------
-//
-// One forward step (gen_boards_*, native_core/src/BookGenerator.cpp:472-760,
-// with sort + unique + merge, :1059-1078, done by the sets) as two launches:
-//
-// expand_gen_kernel: every parent of layer t, one per lane, into its kept
-// children (every empty nibble ascending, spawn 2 then 4, the four moves; a
-// child is kept when it moved and matches the pattern, canonicalised),
-// appended with their repeats to two candidate buffers, spawn 2 -> layer
-// t+1, spawn 4 -> layer t+2. Only arithmetic and row lookups in shared
-// memory; the one memory round trip is an append per 32 staged keys. The
-// same launch copies layer t into the arena and closes it, and zeroes layer
-// t's set, which layer t+3 fills next (sets rotate, layer L in set L % 3).
-//
-// expand_insert_kernel: every candidate into its layer's exact set (a CAS on
-// a zero slot), four candidates per thread with their CASes in flight
-// together; the keys that are new go to the layer's staging buffer (warp-
-// aggregated appends). Its last block resets the step's counters and frees
-// layer t's staging buffer.
-//
-// Splitting the dependent set round trips out of the per-parent loop lets
-// every thread keep several of them in flight, where the fused form waited
-// on them one cell after another.
-template <bool kVariantModes>
-__global__ void __launch_bounds__(kExpandThreads, 1)
-expand_gen_kernel(const uint64_t *__restrict__ stage_par, int si_par, uint64_t *__restrict__ arena,
-                  unsigned long long *__restrict__ layer_off, unsigned long long *__restrict__ layer_len,
-                  unsigned long long arena_cap, int t, DevSpec spec, int do_check, const uint32_t *__restrict__ tab,
-                  uint64_t *__restrict__ gen1, uint64_t *__restrict__ gen2, unsigned long long gen_cap,
-                  uint64_t *__restrict__ clear_set, unsigned long long set_mask, DevCtl *ctl) {
-    __shared__ uint64_t stage[kExpandThreads / 32][2][kStage];
-    extern __shared__ uint16_t srows[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    stage_rows(tab, srows);
-    const SharedRows rows{srows};
-    {
-        uint4 *z = reinterpret_cast<uint4 *>(clear_set);
-        const unsigned long long nz = (set_mask + 1) / 2;
-        for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < nz;
-             i += (unsigned long long)gridDim.x * blockDim.x)
-            z[i] = make_uint4(0u, 0u, 0u, 0u);
-    }
-    // once this pass has overflowed a buffer it will be re-run: skip the work
-    const unsigned long long n =
-        (ctl->err & (kErrCandOverflow | kErrDedupOverflow | kErrGenOverflow)) ? 0 : ctl->stage_count[si_par];
-    const unsigned long long off = layer_off[t];
-    // arena == nullptr: layers stream out of the device (the host sorts and
-    // ships layer t after this step); only the layer's length is recorded
-    const bool fits = arena && !(ctl->err & kErrArenaOverflow) && off + n <= arena_cap;
-    if (!arena && blockIdx.x == 0 && threadIdx.x == 0) {
-        layer_len[t] = n;
-        layer_off[t + 1] = 0;
-    } else if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const unsigned long long next = (off + n + kSplitStride - 1) & ~(unsigned long long)(kSplitStride - 1);
-        if (!fits || next > arena_cap) {
-            atomicOr(&ctl->err, kErrArenaOverflow);
-            layer_len[t] = 0;
-            layer_off[t + 1] = off;
-        } else {
-            layer_len[t] = n;
-            layer_off[t + 1] = next;
-        }
-    }
-    __syncthreads();
-    int cnt[2] = {0, 0};
-    unsigned long long kept_total = 0;
-    const unsigned long long warps = (unsigned long long)gridDim.x * (kExpandThreads / 32);
-    for (unsigned long long base = ((unsigned long long)blockIdx.x * (kExpandThreads / 32) + warp) * 32; base < n;
-         base += warps * 32) {
-        const unsigned long long p = base + lane;
-        bool active = p < n;
-        const uint64_t b = active ? stage_par[p] : 0;
-        if (active && fits) arena[off + p] = b;
-        if (active && do_check && is_success(b, spec)) active = false;
-        uint64_t empt = active ? empty_nibbles(b) : 0;
-        MoveCtx mc;
-        move_ctx_init(rows, b, mc);
-        while (__ballot_sync(0xFFFFFFFFu, empt != 0)) {
-            int k = -1;
-            if (empt) {
-                k = (__ffsll((long long)empt) - 1) >> 2;
-                empt &= empt - 1;
-            }
-#pragma unroll
-            for (int v = 1; v <= 2; ++v) {
-                uint64_t mv[4], sb = 0;
-                if (k >= 0) spawn_moves(rows, mc, k, (uint64_t)v, sb, mv);
-#pragma unroll
-                for (int d = 0; d < 4; ++d) {
-                    const bool keep = k >= 0 && mv[d] != sb && is_pattern(mv[d], spec);
-                    const uint64_t key = keep ? canonical<kVariantModes>(mv[d], spec.symm) : 0;
-                    const unsigned m = __ballot_sync(0xFFFFFFFFu, keep);
-                    if (!m) continue;
-                    uint64_t *sbuf = stage[warp][v - 1];
-                    if (keep) sbuf[cnt[v - 1] + __popc(m & ((1u << lane) - 1u))] = key;
-                    cnt[v - 1] += __popc(m);
-                    kept_total += keep;
-                    __syncwarp();
-                    if (cnt[v - 1] > kStage - 32)
-                        stage_flush(sbuf, cnt[v - 1], v == 1 ? gen1 : gen2, &ctl->gen_count[v - 1], gen_cap,
-                                    &ctl->err, kErrGenOverflow);
-                }
-            }
-        }
-    }
-    stage_flush(stage[warp][0], cnt[0], gen1, &ctl->gen_count[0], gen_cap, &ctl->err, kErrGenOverflow);
-    stage_flush(stage[warp][1], cnt[1], gen2, &ctl->gen_count[1], gen_cap, &ctl->err, kErrGenOverflow);
-    for (int o = 16; o > 0; o >>= 1) kept_total += __shfl_xor_sync(0xFFFFFFFFu, kept_total, o);
-    if (lane == 0 && kept_total) atomicAdd(&ctl->candidates, kept_total);
-}
-
-constexpr int kInsertThreads = 256;
-constexpr int kInsertPer = 4;  // candidates per thread per round, their CASes in flight together
-
-// Append the lanes' fresh keys (flag) to a staging buffer: one atomic per warp.
-__device__ __forceinline__ void warp_append(bool flag, uint64_t key, uint64_t *__restrict__ out,
-                                            unsigned long long *cnt, unsigned long long cap, unsigned long long half,
-                                            unsigned *err) {
-    const int lane = threadIdx.x & 31;
-    const unsigned m = __ballot_sync(0xFFFFFFFFu, flag);
-    if (!m) return;
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(cnt, (unsigned long long)__popc(m));
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base + __popc(m) > cap) {
-        if (lane == 0) atomicOr(err, kErrCandOverflow);
-    } else if (flag) {
-        out[base + __popc(m & ((1u << lane) - 1u))] = key;
-    }
-    if (lane == 0 && base + __popc(m) > half) atomicOr(err, kErrDedupOverflow);
-}
-
-static __global__ void __launch_bounds__(kInsertThreads)
-expand_insert_kernel(const uint64_t *__restrict__ gen1, const uint64_t *__restrict__ gen2,
-                     uint64_t *__restrict__ stage1, uint64_t *__restrict__ stage2, int si_par, int si1, int si2,
-                     uint64_t *set1, uint64_t *set2, unsigned long long set_mask, unsigned long long stage_cap,
-                     DevCtl *ctl, unsigned *progress, unsigned progress_value) {
-    __shared__ int last_block;
-    const bool skip = (ctl->err & (kErrCandOverflow | kErrDedupOverflow | kErrGenOverflow)) != 0;
-    const unsigned long long n1 = skip ? 0 : ctl->gen_count[0], n = skip ? 0 : n1 + ctl->gen_count[1];
-    const unsigned long long half = (set_mask + 1) / 2;
-    const unsigned long long threads = (unsigned long long)gridDim.x * kInsertThreads;
-    const unsigned long long tid = (unsigned long long)blockIdx.x * kInsertThreads + threadIdx.x;
-    // rounds of kInsertPer candidates per thread; items of one round are
-    // `threads` apart, so each of the kInsertPer loads is coalesced
-    for (unsigned long long r0 = 0; r0 < n; r0 += threads * kInsertPer) {
-        uint64_t key[kInsertPer];
-        unsigned long long h[kInsertPer], prev[kInsertPer];
-        uint64_t *set[kInsertPer];
-#pragma unroll
-        for (int j = 0; j < kInsertPer; ++j) {
-            const unsigned long long g = r0 + (unsigned long long)j * threads + tid;
-            key[j] = g < n ? (g < n1 ? gen1[g] : gen2[g - n1]) : 0;
-            set[j] = g < n1 ? set1 : set2;
-            h[j] = mix64(key[j]) & set_mask;
-        }
-#pragma unroll
-        for (int j = 0; j < kInsertPer; ++j)
-            prev[j] = key[j] ? atomicCAS((unsigned long long *)set[j] + h[j], 0ull, (unsigned long long)key[j]) : 1ull;
-#pragma unroll
-        for (int j = 0; j < kInsertPer; ++j) {
-            const unsigned long long g = r0 + (unsigned long long)j * threads + tid;
-            bool fresh = key[j] && prev[j] == 0ull;
-            if (key[j] && prev[j] != 0ull && prev[j] != key[j])
-                fresh = dedup_insert_zero_from(set[j], set_mask, key[j], h[j], &ctl->err) != 0;
-            // a warp's items of one round can straddle the two layers
-            const bool to1 = g < n1;
-            warp_append(fresh && to1, key[j], stage1, &ctl->stage_count[si1], stage_cap, half, &ctl->err);
-            warp_append(fresh && !to1, key[j], stage2, &ctl->stage_count[si2], stage_cap, half, &ctl->err);
-        }
-    }
-    // the last block to finish empties layer t's staging buffer and the step's counters
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0)
-        last_block = atomicAdd(&ctl->blocks_done, 1ull) == (unsigned long long)gridDim.x - 1;
-    __syncthreads();
-    if (last_block && threadIdx.x == 0) {
-        ctl->stage_count[si_par] = 0;
-        ctl->gen_count[0] = 0;
-        ctl->gen_count[1] = 0;
-        ctl->blocks_done = 0;
-        if (progress) *(volatile unsigned *)progress = progress_value;
-    }
-}
-
 // Copy a finished layer from its staging buffer into the arena and close it
 // (the last two layers, which no expand step reads).
 static __global__ void __launch_bounds__(256)
@@ -752,70 +563,41 @@ __device__ __forceinline__ void index_insert_zero(ulonglong2 *slots, unsigned lo
     atomicOr(err, kErrIndexOverflow);
 }
 
-// {key, rate} into the index of the layer whose keys have tile sum `want`:
-// a slot holding a key of another tile sum (an older layer that used the
-// same buffer, or 0) is free, so the buffer is never cleared between layers.
-// The "occupied" mark is the key word itself, so a CAS that claims a slot
-// leaves no window in which another insert could take it back. A key placed
-// at slot p only passed slots of its own layer, which stay until the layer's
-// last reader is done, so a lookup from the key's home reaches p.
-template <typename T>
-__device__ __forceinline__ void index_insert_tagged(ulonglong2 *slots, unsigned long long mask, uint64_t key, T r,
-                                                    long long want, const unsigned *bsum, unsigned *err) {
-    unsigned long long h = mix64(key) & mask;
-    for (int probe = 0; probe < kMaxProbe * 32; ++probe) {
-        unsigned long long cur = __ldcg(&slots[h].x);
-        for (;;) {
-            if (cur == key || board_tile_sum(cur, bsum) != want) {
-                const unsigned long long prev = cur == key ? cur : atomicCAS(&slots[h].x, cur, (unsigned long long)key);
-                if (prev == cur) {
-                    slots[h].y = rate_bits<T>(r);
-                    return;
-                }
-                cur = prev;
-                continue;
-            }
-            break;
-        }
-        h = (h + 1) & mask;
-    }
-    atomicOr(err, kErrIndexOverflow);
-}
-
 // Backward solve of layer t (recalculate_layer, native_core/src/BookSolver.cpp:
 // 413-470). Per board: success with do_check -> max; else for every empty
 // nibble ascending, best2 = max of layer t+1 rates over the kept moves of the
 // spawn-2 board, acc = fma(best2, 1-p4, acc); best4 likewise from layer t+2,
 // acc = fma(best4, p4, acc); rate = T(acc / #empty). The two fma() are the
 // reference's `+=` statements as its -Ofast x86-64-v3 build contracts them.
-// The indexes are tagged by tile sum (index_insert_tagged): a slot whose key
-// has another tile sum than the layer searched is empty, so no launch clears
-// an index; s0 is the tile sum of layer 0 (layer L has s0 + 2L). With idx0,
-// layer t's live entries also enter its rate index (mask m0) for the solves
-// of layers t-1 and t-2.
+// With idx0, layer t's live entries also enter its rate index (mask m0) for
+// the solves of layers t-1 and t-2; with clear_idx, this launch zeroes
+// clear_slots slots of another (unused) index for the next launch's inserts.
 template <typename T, bool kVariantModes>
 __global__ void __launch_bounds__(256, 4)
 solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
              const unsigned long long *__restrict__ layer_off, const unsigned long long *__restrict__ layer_len,
              int t, DevSpec spec, int do_check, const uint32_t *__restrict__ tab, double p4, T zero, T maxv,
              const ulonglong2 *__restrict__ idx1, unsigned long long m1, const ulonglong2 *__restrict__ idx2,
-             unsigned long long m2, DevCtl *ctl, long long s0, ulonglong2 *__restrict__ idx0 = nullptr,
-             unsigned long long m0 = 0, unsigned *progress = nullptr, unsigned progress_value = 0) {
-    __shared__ unsigned bsum[256];
-    init_byte_sums(bsum);
-    __syncthreads();
+             unsigned long long m2, DevCtl *ctl, ulonglong2 *__restrict__ idx0 = nullptr, unsigned long long m0 = 0,
+             ulonglong2 *__restrict__ clear_idx = nullptr, unsigned long long clear_slots = 0,
+             unsigned *progress = nullptr, unsigned progress_value = 0) {
     const GlobalRows rows{tab};
     const unsigned long long n0 = layer_len[t], o0 = layer_off[t];
     const double w2 = 1.0 - p4;
-    const long long want0 = s0 + 2ll * t, want1 = want0 + 2, want2 = want0 + 4;
     unsigned long long looks = 0;
     if (progress && blockIdx.x == 0 && threadIdx.x == 0) *(volatile unsigned *)progress = progress_value;
+    if (clear_idx) {
+        uint4 *z = reinterpret_cast<uint4 *>(clear_idx);
+        for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < clear_slots;
+             i += (unsigned long long)gridDim.x * blockDim.x)
+            z[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
     for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n0;
          i += (unsigned long long)gridDim.x * blockDim.x) {
         const uint64_t b = arena[o0 + i];
         if (do_check && is_success(b, spec)) {
             rates[o0 + i] = maxv;
-            if (idx0 && maxv > zero) index_insert_tagged<T>(idx0, m0, b, maxv, want0, bsum, &ctl->err);
+            if (idx0 && maxv > zero) index_insert_zero<T>(idx0, m0, b, maxv, &ctl->err);
             continue;
         }
         MoveCtx mc;
@@ -849,11 +631,7 @@ solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
                 got[j] = zero;
                 h[j] = mix64(key[j]) & (j < 4 ? m1 : m2);
             }
-            for (int guard = 0; pend; ++guard) {
-                if (guard > kMaxProbe * 32) {  // an index over its load bound: flagged, never walked forever
-                    atomicOr(&ctl->err, kErrIndexOverflow);
-                    break;
-                }
+            while (pend) {
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     if (pend >> j & 1u) {
@@ -861,8 +639,8 @@ solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
                         if (sl.x == key[j]) {
                             got[j] = rate_from_bits<T>(sl.y);
                             pend &= ~(1u << j);
-                        } else if (sl.x == 0ull || board_tile_sum(sl.x, bsum) != (j < 4 ? want1 : want2)) {
-                            pend &= ~(1u << j);  // an empty slot: the key is not in the layer
+                        } else if (sl.x == 0ull) {
+                            pend &= ~(1u << j);
                         } else {
                             h[j] = (h[j] + 1) & (j < 4 ? m1 : m2);
                         }
@@ -880,7 +658,7 @@ solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
         }
         const T r = nempty > 0 ? cast_rate<T>(acc / (double)nempty) : zero;
         rates[o0 + i] = r;
-        if (idx0 && r > zero) index_insert_tagged<T>(idx0, m0, b, r, want0, bsum, &ctl->err);
+        if (idx0 && r > zero) index_insert_zero<T>(idx0, m0, b, r, &ctl->err);
     }
     // warp-aggregated statistics
     for (int o = 16; o > 0; o >>= 1) looks += __shfl_xor_sync(0xFFFFFFFFu, looks, o);
