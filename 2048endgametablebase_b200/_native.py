@@ -143,6 +143,7 @@ _SIGS = {
     "egtb_profile_read": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(KernelTimeC), ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_int)]),
     "egtb_set_spin_limit": (ctypes.c_int, [ctypes.c_uint32]),
+    "egtb_release": (ctypes.c_int, [ctypes.c_int32]),
     "egtb_get_build_progress": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
     "egtb_reset_build_progress": (ctypes.c_int, [ctypes.c_uint32]),
     "egtb_build": (ctypes.c_int, [_P, ctypes.c_size_t, ctypes.POINTER(PatternSpecC), ctypes.POINTER(RunOptionsC),
@@ -233,6 +234,11 @@ def profile_read(device: int) -> dict[str, tuple[int, float]]:
     n = ctypes.c_int(0)
     check(lib().egtb_profile_read(int(device), arr, 16, ctypes.byref(n)))
     return {arr[i].name.decode(): (int(arr[i].launches), float(arr[i].total_ms)) for i in range(n.value)}
+
+
+def release(device: int = 0) -> None:
+    """Free the buffers the library keeps on a device between builds (egtb_release)."""
+    check(lib().egtb_release(int(device)))
 
 
 def set_stream(device: int, stream_ptr: int | None) -> None:

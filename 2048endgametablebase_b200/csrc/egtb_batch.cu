@@ -56,6 +56,11 @@ struct DevBuf {
         bytes = sz;
     }
     template <typename T> T *as() const { return (T *)p; }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
     ~DevBuf() {
         if (p) cudaFree(p);
     }
@@ -795,6 +800,33 @@ void apply_memory(BatchEngine &B, std::vector<TablePlan> &tp, egtb_batch_params 
 }
 
 }  // namespace
+
+// egtb_release: free the batch buffers of a device (the caller holds the
+// device's build lock). Captured graphs name the old buffers: dropped too.
+void batch_release_buffers(int device) {
+    BatchEngine *B = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_batch_mu);
+        if (device < (int)g_batch.size()) B = g_batch[device].get();
+    }
+    if (!B) return;
+    B->fwd.reset();
+    B->bwd.reset();
+    for (DevBuf *d : {&B->arena, &B->rates, &B->stage, &B->sets, &B->filters, &B->index, &B->book, &B->comp,
+                      &B->status, &B->seeds, &B->layer_off, &B->layer_len, &B->book_len, &B->layer_max,
+                      &B->first_tile, &B->tile_cnt, &B->tile_off, &B->tables, &B->ctl, &B->seed_at, &B->seg_tab,
+                      &B->seg_hist})
+        d->release();
+    if (B->pinned) cudaFreeHost(B->pinned);
+    B->pinned = nullptr;
+    B->pinned_cap = 0;
+    B->last_lbase.clear();
+    B->last_steps.clear();
+    B->last_off.clear();
+    B->last_blen.clear();
+    B->last_book_bytes = 0;
+}
+
 }  // namespace egtb
 
 using namespace egtb;

@@ -245,6 +245,38 @@ struct Engine {
         p = nullptr;
     }
 
+    // egtb_release: every buffer that grows with the tables built (arena,
+    // rates, books, sets, indexes, sort buffers, pinned staging); the next
+    // build allocates again. The books of the last build go with them.
+    void release_buffers() {
+        for (auto *p : {&arena, &split, &tmp, &sort_buf[0], &sort_buf[1], &cand[0], &cand[1], &dset[0], &dset[1],
+                        &dset[2]})
+            release(*p);
+        release(rates);
+        release(book);
+        for (auto &p : index) release(p);
+        release(status);
+        release(ustatus);
+        release(tile_cnt);
+        release(tile_off);
+        release(seg_tab);
+        release(seg_hist);
+        release(layer_off);
+        release(layer_len);
+        release(book_len);
+        release(layer_max);
+        release(first_tile);
+        if (pinned) cudaFreeHost(pinned);
+        pinned = nullptr;
+        pinned_cap = 0;
+        arena_cap = cand_cap = rates_bytes = sort_cap = sort_tiles = comp_tiles = dset_cap = 0;
+        seg_tab_cap = seg_hist_cap = book_cap_bytes = index_cap = 0;
+        steps_cap = 0;
+        last_steps = 0;
+        last_off.clear();
+        last_blen.clear();
+    }
+
     void alloc_or_throw(void **p, size_t bytes, const char *what) {
         // EGTB_MAX_ALLOC_BYTES: refuse larger single allocations, as a smaller
         // device would (exercises the streamed fallback on any GPU)
@@ -2077,6 +2109,18 @@ extern "C" int egtb_build(const uint64_t *seeds, size_t n_seeds, const egtb_patt
                 }
             }
         });
+    });
+}
+
+extern "C" int egtb_release(int32_t device) {
+    return guarded([&] {
+        Engine &E = engine_for(device);
+        std::lock_guard<std::mutex> lk(E.mu);
+        EGTB_CUDA(cudaSetDevice(E.device));
+        EGTB_CUDA(cudaStreamSynchronize(E.stream));
+        if (E.copy_stream) EGTB_CUDA(cudaStreamSynchronize(E.copy_stream));
+        E.release_buffers();
+        batch_release_buffers(E.device);
     });
 }
 

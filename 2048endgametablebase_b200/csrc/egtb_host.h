@@ -101,6 +101,8 @@ struct EngineRef {
     int sweep_grid;
 };
 EngineRef engine_ref(int device);
+// Free the batched build's buffers on a device (egtb_release; the caller holds the build lock).
+void batch_release_buffers(int device);
 // Nibbles that are 0xF in every canonical key of the pattern.
 uint64_t pattern_pinned_nibbles(const egtb_pattern_spec &s);
 // Build progress (get_build_progress): the mapped word kernels write, and the host setter.

@@ -364,7 +364,10 @@ class ClassicBookReader:
         for directory, dtype in path_list:
             if not os.path.exists(directory) or best > 0.0:
                 continue
-            if not os.path.exists(os.path.join(directory, f"{pattern_full}_{nums}.book")):
+            # the layer's .book, or its compressed directory (make_classic_lookup_context,
+            # ReaderRuntime.cpp:478-497: book_exists || compressed_exists)
+            if not (os.path.exists(os.path.join(directory, f"{pattern_full}_{nums}.book")) or
+                    os.path.isdir(os.path.join(directory, f"{pattern_full}_{nums}.z"))):
                 continue
             book = self._book(directory, pattern_full, dtype, nums_adjust)
             if not self.prefer_max_result_:

@@ -151,6 +151,16 @@ EGTB_API int egtb_set_stream(int device, void *stream);
 EGTB_API int egtb_profile(int device, int enable);
 EGTB_API int egtb_profile_read(int device, egtb_kernel_time *out, int max_kinds, int *n_kinds);
 
+/* Free the device (and pinned host) memory the library keeps on `device`
+ * between builds: the layer arena, sets, rate indexes, sort buffers and the
+ * books of the last egtb_build / egtb_build_batch (egtb_book_layer_copy and
+ * egtb_batch_book_copy have nothing to copy afterwards). Buffers grow to the
+ * largest table built and stay for the next build otherwise. Open books and
+ * servers keep theirs. No reference counterpart (the reference's buffers
+ * live for one call); for long-lived processes that build tables of very
+ * different sizes. */
+EGTB_API int egtb_release(int32_t device);
+
 /* Number of polls a bounded device wait (the sort's look-back on another
  * block's counts) makes before it gives up; 0 restores the default 2^22.
  * Process-wide, read at each launch. A wait that gives up makes the call

@@ -169,3 +169,33 @@ def test_oracle_trie_search_finds_every_entry(oracle_442):
     for i in range(0, len(rec), 97):
         assert layer.search(int(rec["key"][i])) == rec["rate"][i].item(), i
     assert layer.search(int(rec["key"][0]) - 1) is None
+
+
+def test_oracle_reader_on_the_compressed_table(oracle_442, tmp_path):
+    """The oracle's reader over the oracle's own 442-512 table laid out as the
+    reference's compressed build left it (171 layers as .z directories, the
+    rest as .book files) gives the reference reader's answers on that build."""
+    import ztrie
+    key = "442_512_float32_compressed"
+    case = H.cases()[key]
+    oracle_442.solve("float32", 0.1)
+    name = case["pattern_full"]
+    answers = H.reader_cases()[key]
+    # the layers the positions read (a position's layer is its tile sum's)
+    wanted = {(sum(v for row in e["board"] for v in row) - case["tile_sum0"]) // 2 for e in answers}
+    for t, layer in enumerate(case["layers"]):
+        if t not in wanted:
+            continue
+        book = oracle_442.book(t, "float32")
+        if layer["kind"] == "z":
+            zdir = tmp_path / f"{name}_{t}.z"
+            zdir.mkdir()
+            for fname, data in ztrie.compress_book(book, "float32", f"{name}_{t}.").items():
+                (zdir / fname).write_bytes(data)
+        else:
+            (tmp_path / f"{name}_{t}.book").write_bytes(book)
+    reader = O.Reader([int(m, 16) for m in case["masks"]], case["symm_mode"])
+    for i, entry in enumerate(answers):
+        res, dt = reader.move_on_dic(entry["board"], [(str(tmp_path), case["dtype"])], name, -case["tile_sum0"])
+        assert [[k, v] for k, v in res] == entry["result"], (i, entry["board"])
+        assert dt == entry["dtype"]
