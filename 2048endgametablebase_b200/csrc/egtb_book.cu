@@ -142,6 +142,7 @@ struct egtb_book {
     egtb::LayerDesc *d_desc = nullptr;
     int d_desc_cap = 0;
     bool desc_dirty = true;
+    bool any_compressed = false;  // some loaded layer is a compressed (.z) one
     cudaStream_t stream = nullptr;
     std::mutex mu;
     // scratch for host-buffer lookups
@@ -215,6 +216,7 @@ static bool load_compressed_layer(egtb_book &b, BookLayer &L, long long nums) {
     L.n = z.low.size();
     L.compressed = 1;
     L.sorted = 1;
+    b.any_compressed = true;
     EGTB_CUDA(cudaStreamSynchronize(s));
     return true;
 }
@@ -485,7 +487,9 @@ __device__ __forceinline__ int adjusted_slot(int op, int m) {
 // move_on_dic of one position (evaluate_classic_result_candidates,
 // native_core/src/ReaderRuntime.cpp:739-840): four values in direction order
 // up, right, down, left, the mask of directions with a value, and the op used.
-template <typename T, typename OutT, bool kVariantModes>
+// kTrie: the build that also searches compressed layers (taken only for books
+// that have some; the plain build keeps the registers of the hash search).
+template <typename T, typename OutT, bool kVariantModes, bool kTrie>
 __device__ __forceinline__ void lookup_position(const LayerDesc *__restrict__ desc, int n_desc, uint64_t board,
                                                 long long nums_adjust, const DevSpec &spec,
                                                 const uint32_t *__restrict__ tab, int op_mode, double scale,
@@ -523,7 +527,7 @@ __device__ __forceinline__ void lookup_position(const LayerDesc *__restrict__ de
             live |= 1u << d;
         }
         T r[4];
-        if (L.compressed) {
+        if (kTrie && L.compressed) {
 #pragma unroll
             for (int d = 0; d < 4; ++d) {
                 r[d] = zero;
@@ -562,7 +566,7 @@ __device__ __forceinline__ void lookup_position(const LayerDesc *__restrict__ de
     }
 }
 
-template <typename T, typename OutT, bool kVariantModes>
+template <typename T, typename OutT, bool kVariantModes, bool kTrie>
 __global__ void __launch_bounds__(256)
 lookup_kernel(const LayerDesc *__restrict__ desc, int n_desc, const uint64_t *__restrict__ pos, size_t n,
               long long nums_adjust, DevSpec spec, const uint32_t *__restrict__ tab, int op_mode, double scale,
@@ -571,7 +575,7 @@ lookup_kernel(const LayerDesc *__restrict__ desc, int n_desc, const uint64_t *__
         OutT out[4];
         uint8_t mask;
         int used;
-        lookup_position<T, OutT, kVariantModes>(desc, n_desc, pos[i], nums_adjust, spec, tab, op_mode, scale, round9, zero, out,
+        lookup_position<T, OutT, kVariantModes, kTrie>(desc, n_desc, pos[i], nums_adjust, spec, tab, op_mode, scale, round9, zero, out,
                                  mask, used);
 #pragma unroll
         for (int d = 0; d < 4; ++d) values4[4 * i + d] = out[d];
@@ -583,7 +587,7 @@ lookup_kernel(const LayerDesc *__restrict__ desc, int n_desc, const uint64_t *__
 // The same over a list of requests whose positions and answers live in
 // caller memory the device can address (registered host memory): request r
 // covers work items prefix[r] .. prefix[r+1]-1.
-template <typename T, bool kVariantModes>
+template <typename T, bool kVariantModes, bool kTrie>
 __global__ void __launch_bounds__(256)
 lookup_requests_kernel(const LayerDesc *__restrict__ desc, int n_desc, const ServeReq *__restrict__ reqs, int n_req,
                        long long nums_adjust, DevSpec spec, const uint32_t *__restrict__ tab, int op_mode,
@@ -601,7 +605,7 @@ lookup_requests_kernel(const LayerDesc *__restrict__ desc, int n_desc, const Ser
         float out[4];
         uint8_t mask;
         int used;
-        lookup_position<T, float, kVariantModes>(desc, n_desc, q.pos[i], nums_adjust, spec, tab, op_mode, scale, round9, zero, out,
+        lookup_position<T, float, kVariantModes, kTrie>(desc, n_desc, q.pos[i], nums_adjust, spec, tab, op_mode, scale, round9, zero, out,
                                   mask, used);
         reinterpret_cast<float4 *>(q.out)[i] = make_float4(out[0], out[1], out[2], out[3]);
         if (q.valid) q.valid[i] = mask;
@@ -632,30 +636,38 @@ static void launch_lookup(egtb_book &b, const uint64_t *d_pos, size_t n, int op_
     const double scale = scale_for(b.dtype);
     const int r9 = round9_for(b.dtype) ? 1 : 0;
     const int nd = (int)b.layers.size();
-    // the kernel build with the variant symmetry modes only for tables that use them
-    auto run = [&](auto variant_modes) {
+    // the kernel build with the variant symmetry modes only for tables that use
+    // them, the one with the compressed-layer search only for books that have such layers
+    auto run = [&](auto variant_modes, auto trie) {
         constexpr bool W = decltype(variant_modes)::value;
+        constexpr bool Z = decltype(trie)::value;
         switch (b.dtype) {
             case EGTB_DTYPE_UINT32:
-                lookup_kernel<uint32_t, OutT, W><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
+                lookup_kernel<uint32_t, OutT, W, Z><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
                                                                    scale, r9, 0u, d_vals, d_valid, d_op);
                 break;
             case EGTB_DTYPE_UINT64:
-                lookup_kernel<uint64_t, OutT, W><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
+                lookup_kernel<uint64_t, OutT, W, Z><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
                                                                    scale, r9, 0ull, d_vals, d_valid, d_op);
                 break;
             case EGTB_DTYPE_FLOAT32: case EGTB_DTYPE_1_FLOAT32:
-                lookup_kernel<float, OutT, W><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
+                lookup_kernel<float, OutT, W, Z><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
                                                                 scale, r9, (float)dtype_zero(b.dtype), d_vals, d_valid, d_op);
                 break;
             default:
-                lookup_kernel<double, OutT, W><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
+                lookup_kernel<double, OutT, W, Z><<<grid, 256, 0, s>>>(b.d_desc, nd, d_pos, n, b.nums_adjust, b.spec, tab, op_mode,
                                                                  scale, r9, dtype_zero(b.dtype), d_vals, d_valid, d_op);
                 break;
         }
     };
-    if (b.spec.symm >= 4) run(std::true_type{});
-    else run(std::false_type{});
+    const bool trie = b.any_compressed;
+    if (b.spec.symm >= 4) {
+        if (trie) run(std::true_type{}, std::true_type{});
+        else run(std::true_type{}, std::false_type{});
+    } else {
+        if (trie) run(std::false_type{}, std::true_type{});
+        else run(std::false_type{}, std::false_type{});
+    }
     EGTB_CUDA(cudaGetLastError());
 }
 
@@ -862,29 +874,36 @@ void book_lookup_requests(egtb_book *b, const ServeReq *d_reqs, int n_req, unsig
     const double scale = scale_for(b->dtype);
     const int r9 = round9_for(b->dtype) ? 1 : 0;
     const int nd = (int)b->layers.size();
-    auto run = [&](auto variant_modes) {
+    auto run = [&](auto variant_modes, auto trie) {
         constexpr bool W = decltype(variant_modes)::value;
+        constexpr bool Z = decltype(trie)::value;
         switch (b->dtype) {
             case EGTB_DTYPE_UINT32:
-                lookup_requests_kernel<uint32_t, W><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
+                lookup_requests_kernel<uint32_t, W, Z><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
                                                                      tab, op_mode, scale, r9, 0u);
                 break;
             case EGTB_DTYPE_UINT64:
-                lookup_requests_kernel<uint64_t, W><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
+                lookup_requests_kernel<uint64_t, W, Z><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
                                                                      tab, op_mode, scale, r9, 0ull);
                 break;
             case EGTB_DTYPE_FLOAT32: case EGTB_DTYPE_1_FLOAT32:
-                lookup_requests_kernel<float, W><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
+                lookup_requests_kernel<float, W, Z><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
                                                                   tab, op_mode, scale, r9, (float)dtype_zero(b->dtype));
                 break;
             default:
-                lookup_requests_kernel<double, W><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
+                lookup_requests_kernel<double, W, Z><<<grid, 256, 0, s>>>(b->d_desc, nd, d_reqs, n_req, b->nums_adjust, b->spec,
                                                                    tab, op_mode, scale, r9, dtype_zero(b->dtype));
                 break;
         }
     };
-    if (b->spec.symm >= 4) run(std::true_type{});
-    else run(std::false_type{});
+    const bool trie = b->any_compressed;
+    if (b->spec.symm >= 4) {
+        if (trie) run(std::true_type{}, std::true_type{});
+        else run(std::true_type{}, std::false_type{});
+    } else {
+        if (trie) run(std::false_type{}, std::true_type{});
+        else run(std::false_type{}, std::false_type{});
+    }
     EGTB_CUDA(cudaGetLastError());
 }
 }  // namespace egtb

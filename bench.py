@@ -247,6 +247,8 @@ def main():
     ap.add_argument("--batch-only", action="store_true", help="run the batched-build leg alone and print its JSON")
     ap.add_argument("--serve-only", action="store_true", help="run the serving leg alone and print its JSON")
     ap.add_argument("--serve-offered", type=float, default=3e8, help="offered lookups/s of the serving leg")
+    ap.add_argument("--profile-lookup", action="store_true",
+                    help="build and open the 442-512 books, one lookup launch of 2^22 positions, nothing else (for ncu)")
     ap.add_argument("--profile-sort", type=int, default=0,
                     help="one egtb_sort_unique_u64 of this many seeded random keys and nothing else (for ncu)")
     args = ap.parse_args()
@@ -292,6 +294,26 @@ def main():
         torch.cuda.synchronize()
         print(json.dumps({"profile_sort": args.profile_sort, "unique": int(cnt.item())}))
         shutil.rmtree(work, ignore_errors=True)
+        return
+    if args.profile_lookup:
+        S = importlib.import_module("2048endgametablebase_b200.serving")
+        d = tempfile.mkdtemp(prefix="egtb_lookup_", dir=base)
+        try:
+            spec_b, full, adj = S.build_book("442", 9, os.path.join(d, "442_512"), device=local)
+            book = S.open_book(os.path.join(d, "442_512"), full, "float32", spec_b, adj, local)
+            rng = np.random.default_rng(5)
+            pos = S.perturb(S.sample_positions(book, 1 << 22, rng), 0.05, rng)
+            d_pos = torch.from_numpy(pos.view(np.int64)).cuda(local)
+            d_val = torch.empty((len(pos), 4), dtype=torch.float32, device=f"cuda:{local}")
+            d_ok = torch.empty(len(pos), dtype=torch.uint8, device=f"cuda:{local}")
+            N.check(N.lib().egtb_book_lookup_device(book.handle, d_pos.data_ptr(), len(pos), 0, d_val.data_ptr(),
+                                                    d_ok.data_ptr(), stream.cuda_stream))
+            torch.cuda.synchronize()
+            print(json.dumps({"profile_lookup": len(pos), "answered": int((d_ok != 0).sum().item())}))
+            book.close()
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+            shutil.rmtree(work, ignore_errors=True)
         return
     if args.batch_only:
         if world > 1:
