@@ -146,14 +146,15 @@ sort_hist_kernel(const uint64_t *__restrict__ keys, const unsigned long long *n_
     }
 }
 
-// One pass: src -> dst ordered by digit p, stable. 512 threads per 4096-key
-// tile (16 warps x 8 rounds of 32 keys); threads 0..255 own one digit each
-// for the look-back.
-constexpr int kSweepThreads = 512;
+// One pass: src -> dst ordered by digit p, stable. 256 threads per 4096-key
+// tile (8 warps x 16 rounds of 32 keys), four blocks per SM; each thread owns
+// one digit for the look-back. (Two 512-thread blocks per SM measured 4-5 %
+// slower: their barriers held more of the SM's warps at once.)
+constexpr int kSweepThreads = 256;
 constexpr int kSweepWarps = kSweepThreads / 32;
 constexpr int kSweepKeys = kTileKeys / kSweepThreads;  // keys per thread
 
-static __global__ void __launch_bounds__(kSweepThreads, 2)
+static __global__ void __launch_bounds__(kSweepThreads, 4)
 onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, const unsigned long long *n_ptr,
                 unsigned long long cap, SortPlan sp, int p, const unsigned *__restrict__ hist,
                 unsigned *__restrict__ counters, unsigned long long *__restrict__ status, unsigned epoch, DevCtl *ctl,
@@ -357,7 +358,7 @@ seg_hist_kernel(const uint64_t *__restrict__ keys, const int *__restrict__ tile_
 
 // One pass of the per-layer sort: src -> dst (same layout) ordered by digit p
 // within every layer, stable. The same tile work as onesweep_kernel.
-static __global__ void __launch_bounds__(kSweepThreads, 2)
+static __global__ void __launch_bounds__(kSweepThreads, 4)
 seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, const int *__restrict__ tile_layer,
                     const int *__restrict__ layer_tile0, const unsigned long long *__restrict__ layer_off,
                     const unsigned long long *__restrict__ layer_len, unsigned ntiles,
