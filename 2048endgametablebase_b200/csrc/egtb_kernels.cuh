@@ -631,6 +631,10 @@ solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
                 got[j] = zero;
                 h[j] = mix64(key[j]) & (j < 4 ? m1 : m2);
             }
+            // ends: an index holds at most half as many keys as it has slots
+            // (capacity >= 2 x the layer, cleared before its inserts), so every
+            // probe chain meets an empty slot (a counter here measured 3-5 %
+            // slower)
             while (pend) {
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
