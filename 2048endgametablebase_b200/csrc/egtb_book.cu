@@ -39,6 +39,17 @@ struct BookLayer {
     uint16_t *ii_next = nullptr;
     unsigned long long *block_end = nullptr;
     unsigned long long n_i = 0, n_ii = 0, n_seg = 0;
+    struct TrieDesc *d_trie = nullptr;  // the device copy of the above (TrieDesc)
+};
+
+// A compressed layer as the lookup kernel reads it (one per such layer, in
+// device memory, pointed to by its LayerDesc).
+struct TrieDesc {
+    const uint8_t *i_key, *ii_key;
+    const uint32_t *i_next, *seg_index, *low;
+    const uint16_t *ii_next;
+    const unsigned long long *block_end;
+    unsigned long long n_i, n_ii, n_seg;
 };
 
 // Layer descriptor read by the lookup kernel.
@@ -51,12 +62,7 @@ struct LayerDesc {
     unsigned long long n;
     int exists;
     int sorted;
-    int compressed;
-    const uint8_t *i_key, *ii_key;
-    const uint32_t *i_next, *seg_index, *low;
-    const uint16_t *ii_next;
-    const unsigned long long *block_end;
-    unsigned long long n_i, n_ii, n_seg;
+    const TrieDesc *trie;  // compressed layer (keys / split / index unused), else null
 };
 
 // ------------------------------------------------------ layer hash index ---
@@ -213,6 +219,9 @@ static bool load_compressed_layer(egtb_book &b, BookLayer &L, long long nums) {
     L.n_i = z.i_key.size();
     L.n_ii = z.ii_key.size();
     L.n_seg = z.seg_index.size();
+    const TrieDesc td{L.i_key, L.ii_key, L.i_next, L.seg_index, L.low, L.ii_next, L.block_end, L.n_i, L.n_ii, L.n_seg};
+    EGTB_CUDA(cudaMalloc(&L.d_trie, sizeof(TrieDesc)));
+    EGTB_CUDA(cudaMemcpyAsync(L.d_trie, &td, sizeof td, cudaMemcpyHostToDevice, s));
     L.n = z.low.size();
     L.compressed = 1;
     L.sorted = 1;
@@ -312,8 +321,7 @@ static void upload_desc(egtb_book &b) {
     for (int i = 0; i < n; ++i) {
         const BookLayer &L = b.layers[i];
         h[i] = {L.keys, L.rates, L.split, L.index, L.index_mask, L.n, L.state == 1 ? 1 : 0, L.sorted,
-                L.compressed, L.i_key, L.ii_key, L.i_next, L.seg_index, L.low, L.ii_next, L.block_end,
-                L.n_i, L.n_ii, L.n_seg};
+                L.compressed ? L.d_trie : nullptr};
     }
     if (n) EGTB_CUDA(cudaMemcpyAsync(b.d_desc, h.data(), sizeof(LayerDesc) * n, cudaMemcpyHostToDevice, b.stream));
     EGTB_CUDA(cudaStreamSynchronize(b.stream));
@@ -365,7 +373,7 @@ __device__ __forceinline__ bool probe_unsorted(const uint64_t *keys, const T *ra
 // miss, or the entry those rules land on) is the reference's. *out = the
 // rate found, or zero.
 template <typename T>
-__device__ __forceinline__ void trie_find(const LayerDesc &L, uint64_t board, T zero, T &out) {
+__device__ __forceinline__ void trie_find(const TrieDesc &L, const T *__restrict__ rates, uint64_t board, T zero, T &out) {
     out = zero;
     if (L.n_i < 2 || L.n_seg < 2) return;
     unsigned long long low = 2, high = (unsigned long long)L.i_next[1] - 1ull;
@@ -435,7 +443,6 @@ __device__ __forceinline__ void trie_find(const LayerDesc &L, uint64_t board, T 
         base = L.block_end[blk - 1];
         size = L.block_end[blk] - base;
     }
-    const T *rates = (const T *)L.rates;
     const uint32_t t32 = (uint32_t)board;
     unsigned long long sub_low = L.ii_next[first + pos], sub_high = (unsigned long long)L.ii_next[first + pos + 1] + 1;
     if (sub_high == 1) {
@@ -527,11 +534,12 @@ __device__ __forceinline__ void lookup_position(const LayerDesc *__restrict__ de
             live |= 1u << d;
         }
         T r[4];
-        if (kTrie && L.compressed) {
+        if (kTrie && L.trie) {
+            const TrieDesc Z = *L.trie;
 #pragma unroll
             for (int d = 0; d < 4; ++d) {
                 r[d] = zero;
-                if (live >> d & 1u) trie_find<T>(L, key[d], zero, r[d]);
+                if (live >> d & 1u) trie_find<T>(Z, rates, key[d], zero, r[d]);
             }
         } else if (L.sorted && L.index) {
             index_lookup4<T>(L.index, L.index_mask, key, live, zero, r);
@@ -761,7 +769,7 @@ extern "C" int egtb_book_close(egtb_book *b) {
         cudaStreamSynchronize(b->stream);
         for (auto &L : b->layers) {
             for (void *p : {(void *)L.keys, L.rates, (void *)L.split, (void *)L.index, (void *)L.i_key, (void *)L.ii_key,
-                            (void *)L.i_next, (void *)L.seg_index, (void *)L.low, (void *)L.ii_next,
+                            (void *)L.i_next, (void *)L.seg_index, (void *)L.low, (void *)L.ii_next, (void *)L.d_trie,
                             (void *)L.block_end})
                 if (p) cudaFree(p);
         }
