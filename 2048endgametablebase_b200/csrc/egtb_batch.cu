@@ -520,8 +520,10 @@ struct Run {
                                                                   ntiles, passes, seg_nib, hist, B.counters.as<unsigned>());
         ++launches;
         uint64_t *src = B.arena.as<uint64_t>(), *dst = B.comp.as<uint64_t>();
+        // this file's copy of the kernel (it is static in the header) needs its own attribute
+        EGTB_CUDA(cudaFuncSetAttribute(seg_onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSegSweepSmem));
         for (int q = 0; q < passes; ++q) {
-            seg_onesweep_kernel<<<R.sweep_grid, kSweepThreads, 0, s()>>>(src, dst, tile_layer, layer_tile0, loff, llen,
+            seg_onesweep_kernel<<<R.seg_grid, kSweepThreads, kSegSweepSmem, s()>>>(src, dst, tile_layer, layer_tile0, loff, llen,
                                                                         ntiles, seg_nib, q, hist,
                                                                         B.counters.as<unsigned>(),
                                                                         B.status.as<unsigned long long>(), B.epoch++, dc,

@@ -184,6 +184,7 @@ struct Engine {
     unsigned long long *ustatus = nullptr;  // look-back words of the unique kernel, sort_tiles
     unsigned epoch = 1;                     // tags the look-back words of one kernel launch
     int sweep_grid = 0;                     // resident blocks of the onesweep kernel
+    int seg_grid = 0;                       // resident blocks of the per-layer onesweep kernel
     unsigned *tile_cnt = nullptr;
     unsigned long long *tile_off = nullptr;
     unsigned long long sort_tiles = 0, comp_tiles = 0;
@@ -236,6 +237,9 @@ struct Engine {
         EGTB_CUDA(cudaFuncSetAttribute(expand_dedup_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
         EGTB_CUDA(cudaFuncSetAttribute(expand_dedup_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmemBytes));
         sweep_grid = sm_count * std::max(1, per_sm);
+        EGTB_CUDA(cudaFuncSetAttribute(seg_onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSegSweepSmem));
+        EGTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, seg_onesweep_kernel, kSweepThreads, kSegSweepSmem));
+        seg_grid = sm_count * std::max(1, per_sm);
         progress_device_ptr();
     }
 
@@ -669,7 +673,7 @@ static void enqueue_sort_layers(Engine &E, const ForwardPlan &P, const std::vect
     uint64_t *src = E.arena, *dst = (uint64_t *)E.book;  // the book buffer is free until the solve
     for (int q = 0; q < passes; ++q) {
         const int pi = E.prof_begin(K_SORT_PASS);
-        EGTB_LAUNCH(E, seg_onesweep_kernel<<<E.sweep_grid, kSweepThreads, 0, s>>>(
+        EGTB_LAUNCH(E, seg_onesweep_kernel<<<E.seg_grid, kSweepThreads, kSegSweepSmem, s>>>(
                            src, dst, tile_layer, layer_tile0, E.layer_off, E.layer_len, ntiles, seg_nib, q, E.seg_hist,
                            E.counters, E.status, E.epoch++, E.ctl, look_back_spin_limit()));
         E.prof_end(pi);
@@ -1916,7 +1920,7 @@ static void run_prim(int device, const uint64_t *boards, size_t n, size_t out_pe
 EngineRef engine_ref(int device) {
     Engine &E = engine_for(device);
     // the batched build moves every table with the classic rule
-    return EngineRef{&E.mu, E.device, &E.stream, E.classic_tab, E.sm_count, E.sweep_grid};
+    return EngineRef{&E.mu, E.device, &E.stream, E.classic_tab, E.sm_count, E.sweep_grid, E.seg_grid};
 }
 
 uint64_t pattern_pinned_nibbles(const egtb_pattern_spec &s) { return pinned_nibbles(s); }

@@ -99,6 +99,7 @@ struct EngineRef {
     const uint32_t *tab;
     int sm_count;
     int sweep_grid;
+    int seg_grid;  // resident blocks of the per-layer onesweep kernel (kSegSweepSmem of shared memory each)
 };
 EngineRef engine_ref(int device);
 // Free the batched build's buffers on a device (egtb_release; the caller holds the build lock).

@@ -356,25 +356,102 @@ seg_hist_kernel(const uint64_t *__restrict__ keys, const int *__restrict__ tile_
     if (cur >= 0) flush();
 }
 
+// ---------------------------------------------- bulk copies into smem ----
+//
+// The per-layer sort reads each tile with one bulk asynchronous copy
+// (cp.async.bulk into this block's own shared memory, no tensor map) completed on an mbarrier, so
+// the next tile's keys arrive while the block writes out the current one.
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Orders this thread's shared-memory accesses before later bulk copies (and
+// an mbarrier's initialisation before the copies that complete on it).
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bytes (a multiple of 16) from global src (16-byte aligned) into shared dst
+// (16-byte aligned), counted on bar.
+__device__ __forceinline__ void bulk_load_smem(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Polls of an mbarrier wait for a bulk copy; a copy of one tile lands within
+// microseconds, so running out means the copy engine failed: kErrTimeout.
+constexpr unsigned kBulkWaitPolls = 1u << 24;
+
+__device__ __forceinline__ void mbar_wait_bounded(unsigned long long *bar, unsigned parity, DevCtl *ctl) {
+    for (unsigned spins = 0; !mbar_try_wait(bar, parity);) {
+        if (++spins == kBulkWaitPolls) atomicOr(&ctl->err, kErrTimeout);
+        if (spins >= 2 * kBulkWaitPolls) return;  // the result is not used (the host reports the timeout)
+    }
+}
+
+// Dynamic shared memory of seg_onesweep_kernel: the tile as read, the tile in digit order.
+constexpr int kSegSweepSmem = 2 * kTileKeys * (int)sizeof(uint64_t);
+
 // One pass of the per-layer sort: src -> dst (same layout) ordered by digit p
-// within every layer, stable. The same tile work as onesweep_kernel.
-static __global__ void __launch_bounds__(kSweepThreads, 4)
+// within every layer, stable. The same tile work as onesweep_kernel, with
+// the keys read into shared memory by a bulk copy that is issued as soon as
+// the previous tile's keys are scattered (a tile of n keys reads n rounded up
+// to even keys: layer regions start 16-key aligned and are padded to 16 keys,
+// so the rounded read stays inside the tile's layer region).
+static __global__ void __launch_bounds__(kSweepThreads, 3)
 seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst, const int *__restrict__ tile_layer,
                     const int *__restrict__ layer_tile0, const unsigned long long *__restrict__ layer_off,
                     const unsigned long long *__restrict__ layer_len, unsigned ntiles,
                     const unsigned short *__restrict__ seg_nib, int p, const unsigned *__restrict__ hist_l,
                     unsigned *__restrict__ counters,
                     unsigned long long *__restrict__ status, unsigned epoch, DevCtl *ctl, unsigned spin_limit) {
-    __shared__ uint64_t tkeys[kTileKeys];
+    extern __shared__ __align__(128) uint64_t seg_smem[];
+    uint64_t *const in = seg_smem, *const tkeys = seg_smem + kTileKeys;
     __shared__ unsigned short wcnt[kSweepWarps][256];
     __shared__ unsigned loff[256];
     __shared__ unsigned long long gbase[256];
     __shared__ unsigned long long sm[33];
     __shared__ unsigned tile_sh;
+    __shared__ __align__(8) unsigned long long full;  // completes when a tile's keys are in `in`
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int d = threadIdx.x;  // digit owned by this thread when d < 256
+    // thread 0: claim the next tile and start reading its keys
+    auto claim = [&]() {
+        const unsigned tile = atomicAdd(&counters[p], 1u);
+        tile_sh = tile;
+        if (tile < ntiles) {
+            const SegTile t = seg_tile(tile, tile_layer, layer_tile0, layer_off, layer_len);
+            const unsigned bytes = ((t.n + 1u) & ~1u) * (unsigned)sizeof(uint64_t);
+            mbar_arrive_expect_tx(&full, bytes);
+            bulk_load_smem(in, src + t.first, bytes, &full);
+        }
+    };
+    if (threadIdx.x == 0) {
+        mbar_init(&full, 1);
+        fence_proxy_async_smem();
+        claim();
+    }
+    unsigned parity = 0;
     for (;;) {
-        if (threadIdx.x == 0) tile_sh = atomicAdd(&counters[p], 1u);
         for (int i = threadIdx.x; i < kSweepWarps * 256; i += kSweepThreads) (&wcnt[0][0])[i] = 0;
         __syncthreads();
         const unsigned tile = tile_sh;
@@ -388,19 +465,15 @@ seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst
             const unsigned long long hd = d < 256 ? hist_l[((size_t)t.layer * kMaxPasses + p) * 256 + d] : 0ull;
             ghist_d = block_excl_scan<unsigned long long>(hd, sm, &tot);
         }
+        mbar_wait_bounded(&full, parity, ctl);
+        parity ^= 1u;
         const unsigned base = (unsigned)warp * (kTileKeys / kSweepWarps);
-        uint64_t k[kSweepKeys];
         unsigned rd[kSweepKeys];  // rank in the warp (low 16 bits) | digit << 16 (256 = no key)
 #pragma unroll
         for (int r = 0; r < kSweepKeys; ++r) {
             const unsigned idx = base + (unsigned)r * 32 + lane;
-            k[r] = idx < t.n ? src[t.first + idx] : 0;
-        }
-#pragma unroll
-        for (int r = 0; r < kSweepKeys; ++r) {
-            const unsigned idx = base + (unsigned)r * 32 + lane;
             const bool valid = idx < t.n;
-            const unsigned dg = valid ? seg_digit(k[r], nib2) : 256u;
+            const unsigned dg = valid ? seg_digit(in[idx], nib2) : 256u;
             const unsigned peers = __match_any_sync(0xFFFFFFFFu, dg);
             const unsigned before = __popc(peers & ((1u << lane) - 1u));
             unsigned c = 0;
@@ -440,15 +513,19 @@ seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst
 #pragma unroll
         for (int r = 0; r < kSweepKeys; ++r) {
             const unsigned dg = rd[r] >> 16;
-            if (dg < 256u) tkeys[loff[dg] + wcnt[warp][dg] + (rd[r] & 0xFFFFu)] = k[r];
+            if (dg < 256u) tkeys[loff[dg] + wcnt[warp][dg] + (rd[r] & 0xFFFFu)] = in[base + (unsigned)r * 32 + lane];
         }
         __syncthreads();
+        // `in` is free: the next tile's keys load while this one is written out
+        if (threadIdx.x == 0) {
+            fence_proxy_async_smem();
+            claim();
+        }
         for (unsigned i = threadIdx.x; i < t.n; i += kSweepThreads) {
             const uint64_t key = tkeys[i];
             const unsigned dg = seg_digit(key, nib2);
             dst[gbase[dg] + (i - loff[dg])] = key;
         }
-        __syncthreads();
     }
 }
 
