@@ -408,8 +408,9 @@ __device__ __forceinline__ void mbar_wait_bounded(unsigned long long *bar, unsig
     }
 }
 
-// Dynamic shared memory of seg_onesweep_kernel: the tile as read, the tile in digit order.
-constexpr int kSegSweepSmem = 2 * kTileKeys * (int)sizeof(uint64_t);
+// Dynamic shared memory of seg_onesweep_kernel: the tile as read, the tile in
+// digit order and the digit of every key of the latter.
+constexpr int kSegSweepSmem = 2 * kTileKeys * (int)sizeof(uint64_t) + kTileKeys;
 
 // One pass of the per-layer sort: src -> dst (same layout) ordered by digit p
 // within every layer, stable. The same tile work as onesweep_kernel, with
@@ -426,9 +427,10 @@ seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst
                     unsigned long long *__restrict__ status, unsigned epoch, DevCtl *ctl, unsigned spin_limit) {
     extern __shared__ __align__(128) uint64_t seg_smem[];
     uint64_t *const in = seg_smem, *const tkeys = seg_smem + kTileKeys;
+    unsigned char *const tdig = reinterpret_cast<unsigned char *>(seg_smem + 2 * kTileKeys);
+    // per warp and digit: the warp's count, then the tile position of its first key of the digit
     __shared__ unsigned short wcnt[kSweepWarps][256];
-    __shared__ unsigned loff[256];
-    __shared__ unsigned long long gbase[256];
+    __shared__ unsigned long long gdelta[256];  // destination of tile position i (digit d): gdelta[d] + i
     __shared__ unsigned long long sm[33];
     __shared__ unsigned tile_sh;
     __shared__ __align__(8) unsigned long long full;  // completes when a tile's keys are in `in`
@@ -502,18 +504,26 @@ seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst
                 excl = look_back(status + d, 256, (long long)tile, epoch, spin_limit, ctl);
                 publish_status(my, status_word(epoch, kFlagPrefix, (unsigned)(excl + cnt)));
             }
-            gbase[d] = layer_off[t.layer] + ghist_d + excl;
         }
         {
             unsigned long long tot;
             const unsigned long long lo = block_excl_scan<unsigned long long>((unsigned long long)cnt, sm, &tot);
-            if (d < 256) loff[d] = (unsigned)lo;
+            if (d < 256) {
+                // modular: gdelta[d] + i for i >= lo is the key's destination
+                gdelta[d] = layer_off[t.layer] + ghist_d + excl - lo;
+#pragma unroll
+                for (int w = 0; w < kSweepWarps; ++w) wcnt[w][d] = (unsigned short)(wcnt[w][d] + lo);
+            }
         }
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < kSweepKeys; ++r) {
             const unsigned dg = rd[r] >> 16;
-            if (dg < 256u) tkeys[loff[dg] + wcnt[warp][dg] + (rd[r] & 0xFFFFu)] = in[base + (unsigned)r * 32 + lane];
+            if (dg < 256u) {
+                const unsigned pos = wcnt[warp][dg] + (rd[r] & 0xFFFFu);
+                tkeys[pos] = in[base + (unsigned)r * 32 + lane];
+                tdig[pos] = (unsigned char)dg;
+            }
         }
         __syncthreads();
         // `in` is free: the next tile's keys load while this one is written out
@@ -521,11 +531,7 @@ seg_onesweep_kernel(const uint64_t *__restrict__ src, uint64_t *__restrict__ dst
             fence_proxy_async_smem();
             claim();
         }
-        for (unsigned i = threadIdx.x; i < t.n; i += kSweepThreads) {
-            const uint64_t key = tkeys[i];
-            const unsigned dg = seg_digit(key, nib2);
-            dst[gbase[dg] + (i - loff[dg])] = key;
-        }
+        for (unsigned i = threadIdx.x; i < t.n; i += kSweepThreads) dst[gdelta[tdig[i]] + i] = tkeys[i];
     }
 }
 
