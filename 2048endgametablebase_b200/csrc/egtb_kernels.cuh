@@ -847,45 +847,65 @@ book_write_all_kernel(const uint64_t *__restrict__ arena, const T *__restrict__ 
                       const unsigned long long *__restrict__ first_tile, int n_layers, unsigned long long n_tiles, T zero,
                       const unsigned long long *__restrict__ tile_off, unsigned char *__restrict__ book,
                       unsigned long long book_cap_bytes, DevCtl *ctl) {
-    __shared__ unsigned long long sm[33];
+    // tile entry w * kTileKeys/8 + r * 32 + lane for warp w, round r: every
+    // load is coalesced, and a warp's live entries of one round go to
+    // consecutive records
+    constexpr int kWarps = kSortThreads / 32, kRounds = kTileKeys / kSortThreads;
+    __shared__ unsigned wbase[kWarps + 1];
     constexpr int rec = 8 + (int)sizeof(T);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
     for (unsigned long long g = blockIdx.x; g < n_tiles; g += gridDim.x) {
         const int L = layer_of_tile(first_tile, n_layers, g);
         const unsigned long long n = layer_len[L], o = layer_off[L];
-        const unsigned long long base = (g - first_tile[L]) * kTileKeys + (unsigned long long)threadIdx.x * kKeysPerThread;
-        unsigned live = 0, c = 0;
+        const unsigned long long base =
+            (g - first_tile[L]) * kTileKeys + (unsigned long long)warp * (kTileKeys / kWarps) + lane;
+        unsigned live = 0, wcount = 0;
 #pragma unroll
-        for (int i = 0; i < kKeysPerThread; ++i) {
-            const unsigned long long idx = base + i;
+        for (int r = 0; r < kRounds; ++r) {
+            const unsigned long long idx = base + (unsigned long long)r * 32;
             const bool l = idx < n && rates[o + idx] > zero;
-            live |= (unsigned)l << i;
-            c += l;
+            live |= (unsigned)l << r;
+            wcount += __popc(__ballot_sync(0xFFFFFFFFu, l));
         }
-        unsigned long long tot;
-        unsigned long long pos = tile_off[g] - tile_off[first_tile[L]] +
-                                 block_excl_scan<unsigned long long>(c, sm, &tot);
+        if (lane == 0) wbase[warp] = wcount;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned run = 0;
+            for (int w = 0; w < kWarps; ++w) {
+                const unsigned c = wbase[w];
+                wbase[w] = run;
+                run += c;
+            }
+        }
+        __syncthreads();
+        unsigned long long pos = tile_off[g] - tile_off[first_tile[L]] + wbase[warp];
         const unsigned long long book0 = o * rec;
-        for (int i = 0; i < kKeysPerThread; ++i) {
-            if (live >> i & 1u) {
-                const unsigned long long byte = book0 + pos * rec;
+#pragma unroll 4
+        for (int r = 0; r < kRounds; ++r) {
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, live >> r & 1u);
+            if (live >> r & 1u) {
+                const unsigned long long idx = base + (unsigned long long)r * 32;
+                const unsigned long long byte = book0 + (pos + __popc(m & below)) * rec;
                 if (byte + rec <= book_cap_bytes) {
-                    const uint64_t key = arena[o + base + i];
-                    const T r = rates[o + base + i];
+                    const uint64_t key = arena[o + idx];
+                    const T rt = rates[o + idx];
                     if constexpr (rec == 16) {
                         *reinterpret_cast<uint64_t *>(book + byte) = key;
-                        *reinterpret_cast<T *>(book + byte + 8) = r;
+                        *reinterpret_cast<T *>(book + byte + 8) = rt;
                     } else {
                         uint32_t *w = reinterpret_cast<uint32_t *>(book + byte);
                         w[0] = (uint32_t)key;
                         w[1] = (uint32_t)(key >> 32);
-                        w[2] = *reinterpret_cast<const uint32_t *>(&r);
+                        w[2] = *reinterpret_cast<const uint32_t *>(&rt);
                     }
                 } else {
                     atomicOr(&ctl->err, kErrBookOverflow);
                 }
-                ++pos;
             }
+            pos += __popc(m);
         }
+        __syncthreads();  // wbase is rewritten by the next tile
     }
 }
 
