@@ -106,18 +106,22 @@ struct Engine {
     cudaStream_t stream = nullptr;      // stream in use
     cudaStream_t own_stream = nullptr;  // the library's stream
     unsigned long long launches = 0;
-    // per-kind device timing
+    // per-kind device timing: one event pair around a run of `count`
+    // consecutive launches of one kind (a whole layer loop is one run, so the
+    // timing adds two events per loop, not two per launch; a run's time
+    // includes the gaps between its launches)
     bool prof = false;
     struct ProfPair {
         int kind;
         cudaEvent_t a, b;
+        unsigned long long count;
     };
     std::vector<ProfPair> prof_pending;
     std::vector<cudaEvent_t> prof_pool;
     unsigned long long prof_launches[K_NKINDS] = {};
     double prof_ms[K_NKINDS] = {};
 
-    int prof_begin(int kind) {
+    int prof_begin(int kind, unsigned long long count = 1) {
         if (!prof) return -1;
         cudaEvent_t a, b;
         if (prof_pool.size() >= 2) {
@@ -130,7 +134,7 @@ struct Engine {
             EGTB_CUDA(cudaEventCreate(&b));
         }
         EGTB_CUDA(cudaEventRecord(a, stream));
-        prof_pending.push_back({kind, a, b});
+        prof_pending.push_back({kind, a, b, count});
         return (int)prof_pending.size() - 1;
     }
     void prof_end(int idx) {
@@ -143,7 +147,7 @@ struct Engine {
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
                 prof_ms[p.kind] += ms;
-                prof_launches[p.kind] += 1;
+                prof_launches[p.kind] += p.count;
             } else {
                 cudaGetLastError();
             }
@@ -571,16 +575,16 @@ static void enqueue_forward(Engine &E, const ForwardPlan &P, unsigned *progress)
     const int g_exp = E.sm_count;  // one 1024-thread block per SM (the row table fills its shared memory)
     uint64_t *stage[3] = {E.cand[0], E.cand[1], E.tmp};
     const auto expand = expand_kernel_for(P.spec);
+    const int pe = E.prof_begin(K_EXPAND, (unsigned long long)std::max(0, P.steps - 1 - P.first_step));
     for (int i = P.first_step; i < P.steps - 1; ++i) {
         const int t = i - 1;
-        const int pe = E.prof_begin(K_EXPAND);
         EGTB_LAUNCH(E, expand<<<g_exp, kExpandThreads, kRowSmemBytes, s>>>(
                            stage[t % 3], stage[(t + 1) % 3], stage[(t + 2) % 3], t % 3, (t + 1) % 3, (t + 2) % 3,
                            E.arena, E.layer_off, E.layer_len, E.arena_cap, t, P.spec, i > P.docheck ? 1 : 0, E.tab,
                            E.dset[(t + 1) % 3], E.dset[(t + 2) % 3], E.dset_cap - 1, E.cand_cap, E.filter,
                            E.filter_bits, E.dset[t % 3], E.ctl, progress, (unsigned)i));
-        E.prof_end(pe);
     }
+    E.prof_end(pe);
     for (int L = std::max(P.first_step, P.steps - 2); L < P.steps; ++L)
         EGTB_LAUNCH(E, flush_layer_kernel<<<E.sm_count * 2, 256, 0, s>>>(stage[L % 3], L % 3, E.arena, E.layer_off,
                                                                           E.layer_len, E.arena_cap, L, E.ctl));
@@ -1065,8 +1069,8 @@ static void enqueue_backward(Engine &E, const BackwardPlan &B, const std::vector
     if (B.steps - 3 >= 1)
         EGTB_CUDA(cudaMemsetAsync(E.index[(B.steps - 3) % 4], 0, sizeof(ulonglong2) * index_slots(len[B.steps - 3]), s));
     E.prof_end(pf);
+    const int ps = E.prof_begin(K_SOLVE, (unsigned long long)std::max(0, B.steps - 2));
     for (int t = B.steps - 3; t >= 0; --t) {
-        const int ps = E.prof_begin(K_SOLVE);
         ulonglong2 *idx0 = t >= 1 ? E.index[t % 4] : nullptr;
         ulonglong2 *clear = t >= 2 ? E.index[(t - 1) % 4] : nullptr;
         EGTB_LAUNCH(E, solve_kernel_for<T>(B.spec)<<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec,
@@ -1076,8 +1080,8 @@ static void enqueue_backward(Engine &E, const BackwardPlan &B, const std::vector
                                                          idx0, index_slots(len[t]) - 1, clear,
                                                          t >= 2 ? index_slots(len[t - 1]) : 0, progress,
                                                          total - (unsigned)t - 2u));
-        E.prof_end(ps);
     }
+    E.prof_end(ps);
     const int pp = E.prof_begin(K_PACK);
     enqueue_pack_all<T>(E, B.steps, len, zero);
     E.prof_end(pp);

@@ -811,11 +811,14 @@ def roofline(prof, st, k, layer_boards, peak, peak_kind, pattern):
     out = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
            "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
            "algorithmic_bytes_per_launch": bytes_total / count,
-           "launches_per_step": count / k, "avg_launch_us": total / count * 1e3}
+           "launches_per_step": count / k, "avg_launch_us": total / count * 1e3,
+           "launch_timing": "CUDA events around each layer loop in the timed builds (two events per loop), "
+                            "divided by its launches: the gaps between launches count"}
     out["limit"] = {
-        "expand": "latency of L2 round trips (repeat filter, set CAS): ncu long_scoreboard stalls, DRAM 3 %",
-        "solve": "latency of L2 index probes: ncu long_scoreboard stalls",
-        "sort_pass": "issue and barrier bound at ~1.6 TB/s; DRAM traffic equals the algorithmic bytes",
+        "expand": "instruction issue of one warp per 32 parents (about 140 warp instructions per parent at 42 % "
+                  "issue) and the latency of L2 round trips (repeat filter, set CAS); DRAM 3 %",
+        "solve": "latency of L2 index probes and row lookups: ncu long_scoreboard stalls",
+        "sort_pass": "issue and shared-memory bank conflicts at ~2.2 TB/s; DRAM traffic equals the algorithmic bytes",
     }.get(name, "")
     cap = NCU_TRAFFIC.get((pattern, name))
     if cap:

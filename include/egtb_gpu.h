@@ -147,7 +147,10 @@ EGTB_API int egtb_set_stream(int device, void *stream);
 /* Per-kernel-kind device timing with CUDA events on the launching stream
  * (no reference counterpart; the reference logs phase fractions through
  * Config.logger, BookGenerator.cpp:129-146). egtb_profile(device, 1) clears
- * and enables it; egtb_profile_read fills up to max_kinds entries. */
+ * and enables it; egtb_profile_read fills up to max_kinds entries. The layer
+ * loops of the forward expand and of the solve are timed as one run each
+ * (two events per loop, the gaps between their launches included, launches =
+ * the loop's kernel count); other kinds one event pair per launch. */
 EGTB_API int egtb_profile(int device, int enable);
 EGTB_API int egtb_profile_read(int device, egtb_kernel_time *out, int max_kinds, int *n_kinds);
 
