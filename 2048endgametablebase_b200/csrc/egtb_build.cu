@@ -179,6 +179,7 @@ struct Engine {
     uint64_t *sort_buf[2] = {nullptr, nullptr};
     unsigned long long sort_cap = 0;
     cudaStream_t copy_stream = nullptr;
+    cudaStream_t pack_stream = nullptr;  // book packing of finished layer groups, beside the solve
     cudaEvent_t ev_sorted = nullptr, ev_copied = nullptr;
     uint64_t *cand[2] = {nullptr, nullptr};
     uint64_t *tmp = nullptr;
@@ -434,6 +435,7 @@ struct Engine {
     void ensure_copy_stream() {
         if (copy_stream) return;
         EGTB_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+        EGTB_CUDA(cudaStreamCreateWithFlags(&pack_stream, cudaStreamNonBlocking));
         EGTB_CUDA(cudaEventCreateWithFlags(&ev_sorted, cudaEventDisableTiming));
         EGTB_CUDA(cudaEventCreateWithFlags(&ev_copied, cudaEventDisableTiming));
     }
@@ -1026,8 +1028,8 @@ static void enqueue_pack_all(Engine &E, int steps, const std::vector<unsigned lo
 
 // Pack the books of layers l0 .. l1-1 (the same kernels over a range of layers).
 template <typename T>
-static void enqueue_pack_range(Engine &E, int l0, int l1, const std::vector<unsigned long long> &len, T zero) {
-    cudaStream_t s = E.stream;
+static void enqueue_pack_range(Engine &E, int l0, int l1, const std::vector<unsigned long long> &len, T zero,
+                               cudaStream_t s) {
     const int nl = l1 - l0;
     std::vector<unsigned long long> ft(nl + 1, 0);
     for (int k = 0; k < nl; ++k) ft[k + 1] = ft[k] + (len[l0 + k] + kTileKeys - 1) / kTileKeys;
@@ -1090,9 +1092,10 @@ static void enqueue_backward(Engine &E, const BackwardPlan &B, const std::vector
 static int writer_threads(const egtb_run_options &o);
 
 // The same solve, with the books packed in groups of layers as the solve
-// finishes them: while the device solves the next layers, the host copies
-// each finished group (second stream) into pinned memory and writer threads
-// write its .book files. Returns the book lengths and rate maxima.
+// finishes them: while the device solves the next layers, a pack stream packs
+// each finished group, the host copies it (copy stream) into pinned memory and
+// writer threads write its .book files. Returns the book lengths and rate
+// maxima.
 template <typename T>
 static void backward_write_books(Engine &E, const BackwardPlan &B, const std::vector<unsigned long long> &len,
                                  const std::vector<unsigned long long> &off, const egtb_run_options &o,
@@ -1115,23 +1118,30 @@ static void backward_write_books(Engine &E, const BackwardPlan &B, const std::ve
     E.ensure_copy_stream();
     struct Group {
         int l0, l1;
-        cudaEvent_t packed;
+        cudaEvent_t solved, packed;
     };
     std::vector<Group> groups;
     struct GroupGuard {
         std::vector<Group> &v;
         ~GroupGuard() {
-            for (auto &q : v) cudaEventDestroy(q.packed);
+            for (auto &q : v) {
+                cudaEventDestroy(q.solved);
+                cudaEventDestroy(q.packed);
+            }
         }
     } gguard{groups};
+    // a group's layers are solved once the build stream reaches this point;
+    // they are packed on the pack stream while the solve goes on (the packing
+    // reads only their rates and writes only their book regions)
     auto close_group = [&](int l0, int l1) {
-        const int pp = E.prof_begin(K_PACK);
-        enqueue_pack_range<T>(E, l0, l1, len, zero);
-        E.prof_end(pp);
-        cudaEvent_t ev;
-        EGTB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        EGTB_CUDA(cudaEventRecord(ev, s));
-        groups.push_back({l0, l1, ev});
+        Group q{l0, l1, nullptr, nullptr};
+        EGTB_CUDA(cudaEventCreateWithFlags(&q.solved, cudaEventDisableTiming));
+        EGTB_CUDA(cudaEventCreateWithFlags(&q.packed, cudaEventDisableTiming));
+        groups.push_back(q);
+        EGTB_CUDA(cudaEventRecord(q.solved, s));
+        EGTB_CUDA(cudaStreamWaitEvent(E.pack_stream, q.solved, 0));
+        enqueue_pack_range<T>(E, l0, l1, len, zero, E.pack_stream);
+        EGTB_CUDA(cudaEventRecord(q.packed, E.pack_stream));
     };
     EGTB_CUDA(cudaEventRecord(E.ev[2], s));
     EGTB_CUDA(cudaMemsetAsync(E.layer_max, 0, sizeof(unsigned long long) * steps, s));
@@ -1204,6 +1214,7 @@ static void backward_write_books(Engine &E, const BackwardPlan &B, const std::ve
     }
     pool.wait();
     EGTB_CUDA(cudaStreamSynchronize(E.copy_stream));
+    EGTB_CUDA(cudaStreamSynchronize(E.pack_stream));
     EGTB_CUDA(cudaStreamSynchronize(s));
     EGTB_CUDA(cudaGetLastError());
     EGTB_CUDA(cudaEventElapsedTime(bwd_ms, E.ev[2], E.ev[3]));
