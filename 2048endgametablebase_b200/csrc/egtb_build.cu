@@ -15,6 +15,7 @@
 // Backward solve runs layer by layer on the same arena, then every layer is
 // packed into .book records on the device and written by a thread pool.
 #include <cuda_runtime.h>
+#include <dirent.h>
 
 #include <algorithm>
 #include <atomic>
@@ -1301,14 +1302,29 @@ static void write_ranges(Engine &E, const unsigned char *dev, const std::vector<
 // ------------------------------------------------------------- restart ----
 
 static bool any_layer_file(const egtb_run_options &o) {
+    // one pass over the directory instead of five stat() calls per layer (a
+    // fresh 304-step build otherwise spends ~2 ms in 1525 failed lookups)
     const std::string p = o.pathname;
-    for (int i = 0; i < o.steps + 1; ++i) {
-        const std::string b = p + std::to_string(i);
-        if (file_exists(b) || file_exists(b + ".book") || file_exists(b + ".z") || file_exists(b + ".book.7z") ||
-            file_exists(b + ".7z"))
-            return true;
+    const size_t slash = p.find_last_of('/');
+    const std::string dir = slash == std::string::npos ? "." : (slash == 0 ? "/" : p.substr(0, slash));
+    const std::string stem = slash == std::string::npos ? p : p.substr(slash + 1);
+    DIR *dp = opendir(dir.c_str());
+    if (!dp) return false;
+    bool found = false;
+    for (struct dirent *e = readdir(dp); e && !found; e = readdir(dp)) {
+        const char *name = e->d_name;
+        if (std::strncmp(name, stem.c_str(), stem.size()) != 0) continue;
+        // <stem><i> with i in 0..steps, alone or with one of the suffixes
+        const char *q = name + stem.size();
+        if (*q < '0' || *q > '9') continue;
+        char *end = nullptr;
+        const unsigned long long i = std::strtoull(q, &end, 10);
+        if (i > (unsigned long long)o.steps || (q[0] == '0' && end != q + 1)) continue;
+        const std::string suffix = end;
+        found = suffix.empty() || suffix == ".book" || suffix == ".z" || suffix == ".book.7z" || suffix == ".7z";
     }
-    return false;
+    closedir(dp);
+    return found;
 }
 
 // handle_restart, native_core/src/BookGenerator.cpp:384-430: the first step
