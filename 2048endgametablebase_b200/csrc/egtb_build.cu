@@ -93,6 +93,25 @@ static unsigned long long align16(unsigned long long x) { return (x + 15ull) & ~
         ++(E).launches;      \
     } while (0)
 
+// Launch a kernel that may start while the kernel before it in the stream
+// finishes (programmatic stream serialization). The kernel calls pdl_wait()
+// before it reads anything the launch before wrote.
+template <typename Eng, typename Kernel, typename... Args>
+static void launch_dependent(Eng &E, Kernel kernel, int grid, int block, size_t smem, cudaStream_t s, Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    EGTB_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+    ++E.launches;
+}
+
 static const char *kKindNames[] = {"expand", "sort_pass", "layer_sort", "solve", "book_pack", "final_layers",
                                    "rate_index"};
 enum { K_EXPAND = 0, K_SORT_PASS, K_UNIQUE, K_SOLVE, K_PACK, K_FINAL, K_INDEX, K_NKINDS };
@@ -581,11 +600,12 @@ static void enqueue_forward(Engine &E, const ForwardPlan &P, unsigned *progress)
     const int pe = E.prof_begin(K_EXPAND, (unsigned long long)std::max(0, P.steps - 1 - P.first_step));
     for (int i = P.first_step; i < P.steps - 1; ++i) {
         const int t = i - 1;
-        EGTB_LAUNCH(E, expand<<<g_exp, kExpandThreads, kRowSmemBytes, s>>>(
-                           stage[t % 3], stage[(t + 1) % 3], stage[(t + 2) % 3], t % 3, (t + 1) % 3, (t + 2) % 3,
-                           E.arena, E.layer_off, E.layer_len, E.arena_cap, t, P.spec, i > P.docheck ? 1 : 0, E.tab,
-                           E.dset[(t + 1) % 3], E.dset[(t + 2) % 3], E.dset_cap - 1, E.cand_cap, E.filter,
-                           E.filter_bits, E.dset[t % 3], E.ctl, progress, (unsigned)i));
+        // consecutive steps overlap: the next step stages its row table while this one finishes
+        launch_dependent(E, expand, g_exp, kExpandThreads, kRowSmemBytes, s, stage[t % 3], stage[(t + 1) % 3],
+                         stage[(t + 2) % 3], t % 3, (t + 1) % 3, (t + 2) % 3, E.arena, E.layer_off, E.layer_len,
+                         E.arena_cap, t, P.spec, i > P.docheck ? 1 : 0, (const uint32_t *)E.tab, E.dset[(t + 1) % 3],
+                         E.dset[(t + 2) % 3], E.dset_cap - 1, E.cand_cap, E.filter, E.filter_bits, E.dset[t % 3],
+                         E.ctl, progress, (unsigned)i);
     }
     E.prof_end(pe);
     for (int L = std::max(P.first_step, P.steps - 2); L < P.steps; ++L)
@@ -1076,13 +1096,14 @@ static void enqueue_backward(Engine &E, const BackwardPlan &B, const std::vector
     for (int t = B.steps - 3; t >= 0; --t) {
         ulonglong2 *idx0 = t >= 1 ? E.index[t % 4] : nullptr;
         ulonglong2 *clear = t >= 2 ? E.index[(t - 1) % 4] : nullptr;
-        EGTB_LAUNCH(E, solve_kernel_for<T>(B.spec)<<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec,
-                                                         t > B.docheck ? 1 : 0, E.tab, B.p4, zero, maxv,
-                                                         E.index[(t + 1) % 4], index_slots(len[t + 1]) - 1,
-                                                         E.index[(t + 2) % 4], index_slots(len[t + 2]) - 1, E.ctl,
-                                                         idx0, index_slots(len[t]) - 1, clear,
-                                                         t >= 2 ? index_slots(len[t - 1]) : 0, progress,
-                                                         total - (unsigned)t - 2u));
+        // consecutive solves overlap: each launch starts as the one before finishes
+        launch_dependent(E, solve_kernel_for<T>(B.spec), g, 256, 0, s, (const uint64_t *)E.arena, rates,
+                         (const unsigned long long *)E.layer_off, (const unsigned long long *)E.layer_len, t, B.spec,
+                         t > B.docheck ? 1 : 0, (const uint32_t *)E.tab, B.p4, zero, maxv,
+                         (const ulonglong2 *)E.index[(t + 1) % 4], index_slots(len[t + 1]) - 1,
+                         (const ulonglong2 *)E.index[(t + 2) % 4], index_slots(len[t + 2]) - 1, E.ctl, idx0,
+                         index_slots(len[t]) - 1, clear, t >= 2 ? index_slots(len[t - 1]) : 0ull, progress,
+                         total - (unsigned)t - 2u);
     }
     E.prof_end(ps);
     const int pp = E.prof_begin(K_PACK);
@@ -1160,13 +1181,14 @@ static void backward_write_books(Engine &E, const BackwardPlan &B, const std::ve
         const int ps = E.prof_begin(K_SOLVE);
         ulonglong2 *idx0 = t >= 1 ? E.index[t % 4] : nullptr;
         ulonglong2 *clear = t >= 2 ? E.index[(t - 1) % 4] : nullptr;
-        EGTB_LAUNCH(E, solve_kernel_for<T>(B.spec)<<<g, 256, 0, s>>>(E.arena, rates, E.layer_off, E.layer_len, t, B.spec,
-                                                         t > B.docheck ? 1 : 0, E.tab, B.p4, zero, maxv,
-                                                         E.index[(t + 1) % 4], index_slots(len[t + 1]) - 1,
-                                                         E.index[(t + 2) % 4], index_slots(len[t + 2]) - 1, E.ctl,
-                                                         idx0, index_slots(len[t]) - 1, clear,
-                                                         t >= 2 ? index_slots(len[t - 1]) : 0, progress,
-                                                         total - (unsigned)t - 2u));
+        // consecutive solves overlap: each launch starts as the one before finishes
+        launch_dependent(E, solve_kernel_for<T>(B.spec), g, 256, 0, s, (const uint64_t *)E.arena, rates,
+                         (const unsigned long long *)E.layer_off, (const unsigned long long *)E.layer_len, t, B.spec,
+                         t > B.docheck ? 1 : 0, (const uint32_t *)E.tab, B.p4, zero, maxv,
+                         (const ulonglong2 *)E.index[(t + 1) % 4], index_slots(len[t + 1]) - 1,
+                         (const ulonglong2 *)E.index[(t + 2) % 4], index_slots(len[t + 2]) - 1, E.ctl, idx0,
+                         index_slots(len[t]) - 1, clear, t >= 2 ? index_slots(len[t - 1]) : 0ull, progress,
+                         total - (unsigned)t - 2u);
         E.prof_end(ps);
         if (hi - t == kGroup || t == 0) {
             close_group(t, hi);

@@ -10,6 +10,15 @@
 
 namespace egtb {
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may start while the kernel before it in the stream finishes.
+// pdl_trigger lets the next such kernel launch (its blocks take SM resources
+// only as this kernel's blocks leave them); pdl_wait blocks until the kernel
+// before this one has completed and its memory operations are visible. Both
+// are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Default number of polls of a bounded wait on another block (sort look-back).
 constexpr unsigned kSpinLimit = 1u << 22;
 

@@ -314,7 +314,11 @@ expand_dedup_kernel(uint64_t *__restrict__ stage_par, uint64_t *__restrict__ sta
     __shared__ int last_block;
     extern __shared__ uint16_t srows[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // the row table does not depend on the step before: it is staged while
+    // that step's last blocks finish (programmatic dependent launch)
+    pdl_trigger();
     stage_rows(tab, srows);
+    pdl_wait();
     const SharedRows rows{srows};
     {
         uint4 *z = reinterpret_cast<uint4 *>(clear_set);
@@ -582,6 +586,8 @@ solve_kernel(const uint64_t *__restrict__ arena, T *__restrict__ rates,
              ulonglong2 *__restrict__ clear_idx = nullptr, unsigned long long clear_slots = 0,
              unsigned *progress = nullptr, unsigned progress_value = 0) {
     const GlobalRows rows{tab};
+    pdl_trigger();
+    pdl_wait();  // launched early (programmatic dependent launch): the launch before must be done
     const unsigned long long n0 = layer_len[t], o0 = layer_off[t];
     const double w2 = 1.0 - p4;
     unsigned long long looks = 0;
