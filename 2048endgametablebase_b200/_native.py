@@ -132,6 +132,30 @@ class BatchStatsC(ctypes.Structure):
         return d
 
 
+class AdParamC(ctypes.Structure):
+    """egtb_ad_param (AdvancedMaskParam)."""
+    _fields_ = [
+        ("pos_fixed_32k_mask", ctypes.c_uint64),
+        ("small_tile_sum_limit", ctypes.c_uint32),
+        ("target", ctypes.c_uint32),
+        ("num_free_32k", ctypes.c_uint32),
+        ("num_fixed_32k", ctypes.c_uint32),
+    ]
+
+
+class AdTileCountC(ctypes.Structure):
+    """egtb_ad_tile_count (TileCountResult / TileCount4Result)."""
+    _fields_ = [
+        ("pos_bitmap", ctypes.c_uint64),
+        ("total_sum", ctypes.c_uint32),
+        ("count_32k", ctypes.c_int32),
+        ("pos_rank", ctypes.c_uint32),
+        ("merged_tile_found", ctypes.c_uint32),
+        ("merged_tile", ctypes.c_uint32),
+        ("is_success", ctypes.c_uint32),
+    ]
+
+
 # every entry point of include/egtb_gpu.h with its ctypes signature
 _P = ctypes.c_void_p
 _SIGS = {
@@ -160,6 +184,13 @@ _SIGS = {
     "egtb_move_all_dir_variant": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, _P]),
     "egtb_canonical": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, ctypes.c_int32, _P]),
     "egtb_apply_sym": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, ctypes.c_int32, _P]),
+    "egtb_ad_move_all_dir": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, _P, _P]),
+    "egtb_ad_mask_board": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, ctypes.c_int32, _P]),
+    "egtb_ad_tile_stats": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, ctypes.POINTER(AdParamC), ctypes.c_int32,
+                                          _P]),
+    "egtb_ad_validate": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, _P, ctypes.POINTER(AdParamC), _P]),
+    "egtb_ad_row_tables": (ctypes.c_int, [_P, _P]),
+    "egtb_ad_tiles_combinations": (ctypes.c_int, [_P, _P]),
     "egtb_book_open": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(PatternSpecC),
                                       ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(_P)]),
     "egtb_book_close": (ctypes.c_int, [_P]),

@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 OUT = os.path.join(OUT_DIR, "libegtb_gpu.so")
 SOURCES = ["egtb_host.cu", "egtb_build.cu", "egtb_book.cu", "egtb_sort_api.cu", "egtb_serve.cu", "egtb_batch.cu",
-           "egtb_trie.cu"]
+           "egtb_trie.cu", "egtb_ad.cu"]
 HEADERS = ["egtb_host.h", "egtb_device.cuh", "egtb_kernels.cuh", "egtb_sort.cuh", "egtb_batch.cuh", "egtb_trie.h"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

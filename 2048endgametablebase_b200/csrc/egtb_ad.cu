@@ -1,0 +1,430 @@
+// Masked-board primitives of the reference's advanced algorithm (namespace
+// FormationAD): the masked mover, the board masker, the tile statistics and
+// the validity test of a masked board. In a masked board every tile of 64 and
+// up is held as a 0xF ("32k") nibble; 0xF never merges, and a merge that
+// makes a tile of 64 or more yields 0xF and raises mask_new_tile.
+//
+//   row rule and mover      native_core/src/BoardMoverAD.cpp:27-89,171-178
+//   mask_board              native_core/src/BoardMaskerAD.cpp:112-121
+//   tile statistics         native_core/src/BoardMaskerAD.cpp:24-50 (per-row
+//                           info), :123-144, :169-190, :219-257
+//   tiles combinations      native_core/src/BoardMaskerAD.cpp:259-289,524-531
+//   validate                native_core/src/BoardMaskerAD.cpp:409-443
+//
+// One thread per board; the row moves come from a 65536-entry table built on
+// the host from the rule, the per-row statistics are computed in registers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "egtb_host.h"
+
+namespace egtb {
+namespace {
+
+constexpr int kAdCombos = 2560;  // tiles-combination entries: a + 256 b, b < 10
+constexpr int kAdComboVals = 16;
+
+// One row moved toward column 0 (reverse = false) or column 3 under the
+// masked rule: slide the tiles, merge each adjacent equal pair once, first
+// pair first; 0xF slides but never merges; a merged tile of 64 or more
+// (nibble 6 and up) is written as 0xF and sets *made_32k.
+uint32_t ad_row_after_move(uint32_t row, bool reverse, bool *made_32k) {
+    int cell[4];
+    for (int i = 0; i < 4; ++i) cell[i] = (row >> (12 - 4 * i)) & 0xF;  // column 0 first
+    if (reverse) {
+        std::swap(cell[0], cell[3]);
+        std::swap(cell[1], cell[2]);
+    }
+    int out[4] = {0, 0, 0, 0};
+    int m = 0, pending = 0;
+    for (int i = 0; i < 4; ++i) {
+        if (!cell[i]) continue;
+        if (pending && pending == cell[i] && pending != 0xF) {
+            int v = pending + 1;
+            if (v >= 6) {
+                v = 0xF;
+                *made_32k = true;
+            }
+            out[m++] = v;
+            pending = 0;
+        } else {
+            if (pending) out[m++] = pending;
+            pending = cell[i];
+        }
+    }
+    if (pending) out[m++] = pending;
+    if (reverse) {
+        std::swap(out[0], out[3]);
+        std::swap(out[1], out[2]);
+    }
+    uint32_t r = 0;
+    for (int i = 0; i < 4; ++i) r |= (uint32_t)out[i] << (12 - 4 * i);
+    return r;
+}
+
+struct AdTables {
+    std::vector<uint32_t> moves;  // left xor | right xor << 16
+    std::vector<uint8_t> flags;   // the left merge made a 32k tile
+    std::vector<uint8_t> lens;    // tiles combinations: entry length
+    std::vector<uint8_t> vals;    // ... and values (log2 of the large tiles, ascending)
+};
+
+// The large tiles a masked board's 32k cells may hold: `count` tiles of 64
+// and up summing to `sum`, taken largest first with the reference's early
+// exits; empty when none fits.
+std::vector<uint8_t> large_tiles_for(uint64_t sum, int count) {
+    std::vector<uint8_t> out;
+    for (int lg = 13; lg >= 6; --lg) {
+        const uint64_t tile = 1ull << lg;
+        if (tile > sum) continue;
+        if (tile == sum) {
+            if (count == 1) {
+                out.push_back((uint8_t)lg);
+                return out;
+            }
+            continue;
+        }
+        if (2 * tile == sum && count == 2) {
+            out.push_back((uint8_t)lg);
+            out.push_back((uint8_t)lg);
+            return out;
+        }
+        if (tile != 64 && sum == 192 && count == 3) {
+            out.push_back(6);
+            out.push_back(6);
+            out.push_back(6);
+            return out;
+        }
+        sum -= tile;
+        --count;
+        out.push_back((uint8_t)lg);
+    }
+    return {};
+}
+
+const AdTables &host_ad_tables() {
+    static const AdTables t = [] {
+        AdTables a;
+        a.moves.resize(65536);
+        a.flags.resize(65536);
+        for (uint32_t r = 0; r < 65536; ++r) {
+            bool made = false, ignored = false;
+            const uint32_t l = ad_row_after_move(r, false, &made) ^ r;
+            const uint32_t rr = ad_row_after_move(r, true, &ignored) ^ r;
+            a.moves[r] = l | (rr << 16);
+            a.flags[r] = made ? 1 : 0;
+        }
+        a.lens.assign(kAdCombos, 0);
+        a.vals.assign((size_t)kAdCombos * kAdComboVals, 0);
+        for (int s = 1; s < 256; ++s)
+            for (int c = 1; c < 10; ++c) {
+                std::vector<uint8_t> v = large_tiles_for((uint64_t)s << 6, c);
+                std::reverse(v.begin(), v.end());
+                const int e = s + 256 * c;
+                a.lens[e] = (uint8_t)v.size();
+                std::copy(v.begin(), v.end(), a.vals.begin() + (size_t)e * kAdComboVals);
+            }
+        return a;
+    }();
+    return t;
+}
+
+struct AdDeviceTables {
+    uint32_t *moves = nullptr;
+    uint8_t *flags = nullptr, *lens = nullptr, *vals = nullptr;
+};
+
+// The tables in device memory, uploaded once per device (kept until exit).
+AdDeviceTables device_ad_tables(int device) {
+    static std::mutex mu;
+    static std::vector<AdDeviceTables> per_device;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)per_device.size() <= device) per_device.resize(device + 1);
+    AdDeviceTables &d = per_device[device];
+    if (!d.moves) {
+        const AdTables &h = host_ad_tables();
+        AdDeviceTables n;
+        EGTB_CUDA(cudaMalloc(&n.moves, h.moves.size() * sizeof(uint32_t)));
+        EGTB_CUDA(cudaMalloc(&n.flags, h.flags.size()));
+        EGTB_CUDA(cudaMalloc(&n.lens, h.lens.size()));
+        EGTB_CUDA(cudaMalloc(&n.vals, h.vals.size()));
+        EGTB_CUDA(cudaMemcpy(n.moves, h.moves.data(), h.moves.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        EGTB_CUDA(cudaMemcpy(n.flags, h.flags.data(), h.flags.size(), cudaMemcpyHostToDevice));
+        EGTB_CUDA(cudaMemcpy(n.lens, h.lens.data(), h.lens.size(), cudaMemcpyHostToDevice));
+        EGTB_CUDA(cudaMemcpy(n.vals, h.vals.data(), h.vals.size(), cudaMemcpyHostToDevice));
+        d = n;
+    }
+    return d;
+}
+
+// ------------------------------------------------------------ device ----
+
+struct AdParamDev {
+    uint64_t fixed;
+    uint32_t small_limit, target, num_free, num_fixed;
+};
+
+__device__ __forceinline__ uint64_t ad_moved_rows(const uint32_t *tab, uint64_t b, int half) {
+    uint64_t x = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) x |= (uint64_t)((__ldg(tab + ((b >> (16 * k)) & 0xFFFFu)) >> (16 * half)) & 0xFFFFu)
+                                    << (16 * k);
+    return b ^ x;
+}
+
+__device__ __forceinline__ uint8_t ad_any_flag(const uint8_t *flags, uint64_t b) {
+    uint8_t f = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) f |= __ldg(flags + ((b >> (16 * k)) & 0xFFFFu));
+    return f;
+}
+
+__global__ void ad_moves_kernel(const uint32_t *tab, const uint8_t *flags, const uint64_t *in, size_t n,
+                                uint64_t *out4, uint8_t *f4) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint64_t b = in[i], t = transpose(b);
+        const uint8_t fh = ad_any_flag(flags, b), fv = ad_any_flag(flags, t);
+        out4[4 * i + 0] = ad_moved_rows(tab, b, 0);
+        out4[4 * i + 1] = ad_moved_rows(tab, b, 1);
+        out4[4 * i + 2] = transpose(ad_moved_rows(tab, t, 0));
+        out4[4 * i + 3] = transpose(ad_moved_rows(tab, t, 1));
+        f4[4 * i + 0] = fh;
+        f4[4 * i + 1] = fh;
+        f4[4 * i + 2] = fv;
+        f4[4 * i + 3] = fv;
+    }
+}
+
+__global__ void ad_mask_kernel(const uint64_t *in, size_t n, long long threshold, uint64_t *out) {
+    const uint64_t th = (uint64_t)threshold;  // compared as the reference compares: unsigned 64-bit
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        uint64_t b = in[i], m = b;
+        for (int k = 0; k < 16; ++k)
+            if (((b >> (4 * k)) & 0xFull) >= th) m |= 0xFull << (4 * k);
+        out[i] = m;
+    }
+}
+
+// Statistics of one 16-bit row, nibbles from the highest: a 32k cell is 0xF
+// (masked_only) or any tile of 64 and up; the other tiles add to a 16-bit sum
+// (it wraps as the reference's uint16_t field does); a 0xF cell met before
+// any non-0xF 32k cell of the row counts toward pos_rank.
+struct AdRowInfo {
+    uint32_t sum16, count, pos, merged_count, merged_xor, rank;
+};
+
+__device__ __forceinline__ AdRowInfo ad_row_info(uint32_t row, bool masked_only) {
+    AdRowInfo r{0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int i = 3; i >= 0; --i) {
+        const uint32_t v = (row >> (4 * i)) & 0xFu;
+        const bool large = masked_only ? v == 0xFu : v > 5u;
+        if (large) {
+            r.pos |= 0xFu << (4 * i);
+            ++r.count;
+            if (v == 0xFu) {
+                if (r.merged_count == 0) ++r.rank;
+            } else {
+                ++r.merged_count;
+                r.merged_xor ^= v;
+            }
+        } else if (v > 0u) {
+            r.sum16 += 1u << v;
+        }
+    }
+    r.sum16 &= 0xFFFFu;
+    return r;
+}
+
+__device__ __forceinline__ egtb_ad_tile_count ad_stats(uint64_t board, const AdParamDev &p, int kind) {
+    board &= ~p.fixed;
+    AdRowInfo r[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) r[k] = ad_row_info((uint32_t)((board >> (16 * k)) & 0xFFFFu), kind == 1);
+    egtb_ad_tile_count s = {};
+    s.total_sum = r[0].sum16 + r[1].sum16 + r[2].sum16 + r[3].sum16;
+    s.count_32k = (int32_t)(r[0].count + r[1].count + r[2].count + r[3].count);
+    s.pos_bitmap = (uint64_t)r[0].pos | ((uint64_t)r[1].pos << 16) | ((uint64_t)r[2].pos << 32) |
+                   ((uint64_t)r[3].pos << 48);
+    if (kind == 4) {
+        s.merged_tile_found = r[0].merged_count + r[1].merged_count + r[2].merged_count + r[3].merged_count;
+        s.merged_tile = r[0].merged_xor ^ r[1].merged_xor ^ r[2].merged_xor ^ r[3].merged_xor;
+        // 0xF cells from the top row down to the row of the first merged tile
+        const uint32_t s3 = r[3].rank, s2 = s3 + r[2].rank, s1 = s2 + r[1].rank, s0 = s1 + r[0].rank;
+        s.pos_rank = r[3].merged_count ? s3 : r[2].merged_count ? s2 : r[1].merged_count ? s1 : s0;
+        s.is_success = (s.merged_tile == (p.target & 0xFFu) && s.merged_tile_found == 1) ? 1u : 0u;
+    }
+    return s;
+}
+
+__global__ void ad_stats_kernel(const uint64_t *in, size_t n, AdParamDev p, int kind, egtb_ad_tile_count *out) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = ad_stats(in[i], p, kind);
+}
+
+__global__ void ad_validate_kernel(const uint64_t *in, const uint32_t *orig, size_t n, AdParamDev p,
+                                   const uint8_t *lens, const uint8_t *vals, uint8_t *out) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const egtb_ad_tile_count s = ad_stats(in[i], p, 2);
+        const int8_t count = (int8_t)s.count_32k, free32k = (int8_t)(uint8_t)p.num_free;
+        uint8_t ok;
+        if (s.total_sum >= p.small_limit + 64u) {
+            ok = 0;
+        } else if (count == free32k) {
+            ok = 1;
+        } else {
+            const uint32_t large = orig[i] - s.total_sum - ((uint32_t)((p.num_free & 0xFFu) + (p.num_fixed & 0xFFu)) << 15);
+            const uint32_t a = (uint8_t)(large >> 6), c = (uint8_t)(count - free32k);
+            const int len = c < 10 ? lens[a + 256 * c] : 0;
+            const uint8_t *v = vals + (size_t)(a + 256 * c) * kAdComboVals;
+            if (len == 0 || v[len - 1] == (uint8_t)p.target) {
+                ok = 0;
+            } else if (count < 2) {
+                ok = 1;
+            } else if (len > 2 && v[0] == v[2]) {
+                ok = s.total_sum >= p.small_limit - 64u ? 0 : 1;
+            } else if (len > 1 && v[0] == v[1]) {
+                ok = s.total_sum >= p.small_limit ? 0 : 1;
+            } else {
+                ok = 1;
+            }
+        }
+        out[i] = ok;
+    }
+}
+
+// -------------------------------------------------------------- host ----
+
+AdParamDev ad_param(const egtb_ad_param *p) {
+    if (!p) throw Error(EGTB_ERR_ARG, "NULL parameter block");
+    return AdParamDev{p->pos_fixed_32k_mask, p->small_tile_sum_limit, p->target, p->num_free_32k, p->num_fixed_32k};
+}
+
+// Device buffers of one call, freed on every exit.
+struct AdBuffers {
+    std::vector<void *> ptrs;
+    void *get(size_t bytes) {
+        void *p = nullptr;
+        EGTB_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+        ptrs.push_back(p);
+        return p;
+    }
+    ~AdBuffers() {
+        for (void *p : ptrs) cudaFree(p);
+    }
+};
+
+template <typename F>
+void on_device(int device, F &&f) {
+    int count = 0;
+    EGTB_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) throw Error(EGTB_ERR_ARG, "device out of range");
+    EGTB_CUDA(cudaSetDevice(device));
+    f();
+    EGTB_CUDA(cudaGetLastError());
+    EGTB_CUDA(cudaDeviceSynchronize());
+}
+
+constexpr int kAdGrid = 148 * 4, kAdBlock = 256;
+
+}  // namespace
+}  // namespace egtb
+
+using namespace egtb;
+
+extern "C" int egtb_ad_move_all_dir(int device, const uint64_t *boards, size_t n, uint64_t *out4, uint8_t *flags4) {
+    return guarded([&] {
+        if (n == 0) return;
+        if (!boards || !out4 || !flags4) throw Error(EGTB_ERR_ARG, "NULL buffer");
+        on_device(device, [&] {
+            const AdDeviceTables t = device_ad_tables(device);
+            AdBuffers buf;
+            auto *din = (uint64_t *)buf.get(n * 8);
+            auto *dout = (uint64_t *)buf.get(n * 32);
+            auto *dfl = (uint8_t *)buf.get(n * 4);
+            EGTB_CUDA(cudaMemcpy(din, boards, n * 8, cudaMemcpyHostToDevice));
+            ad_moves_kernel<<<kAdGrid, kAdBlock>>>(t.moves, t.flags, din, n, dout, dfl);
+            EGTB_CUDA(cudaGetLastError());
+            EGTB_CUDA(cudaMemcpy(out4, dout, n * 32, cudaMemcpyDeviceToHost));
+            EGTB_CUDA(cudaMemcpy(flags4, dfl, n * 4, cudaMemcpyDeviceToHost));
+        });
+    });
+}
+
+extern "C" int egtb_ad_mask_board(int device, const uint64_t *boards, size_t n, int32_t threshold, uint64_t *out) {
+    return guarded([&] {
+        if (n == 0) return;
+        if (!boards || !out) throw Error(EGTB_ERR_ARG, "NULL buffer");
+        on_device(device, [&] {
+            AdBuffers buf;
+            auto *din = (uint64_t *)buf.get(n * 8);
+            auto *dout = (uint64_t *)buf.get(n * 8);
+            EGTB_CUDA(cudaMemcpy(din, boards, n * 8, cudaMemcpyHostToDevice));
+            ad_mask_kernel<<<kAdGrid, kAdBlock>>>(din, n, (long long)threshold, dout);
+            EGTB_CUDA(cudaGetLastError());
+            EGTB_CUDA(cudaMemcpy(out, dout, n * 8, cudaMemcpyDeviceToHost));
+        });
+    });
+}
+
+extern "C" int egtb_ad_tile_stats(int device, const uint64_t *boards, size_t n, const egtb_ad_param *param,
+                                  int32_t kind, egtb_ad_tile_count *out) {
+    return guarded([&] {
+        if (kind != 1 && kind != 2 && kind != 4) throw Error(EGTB_ERR_ARG, "kind must be 1, 2 or 4");
+        const AdParamDev p = ad_param(param);
+        if (n == 0) return;
+        if (!boards || !out) throw Error(EGTB_ERR_ARG, "NULL buffer");
+        on_device(device, [&] {
+            AdBuffers buf;
+            auto *din = (uint64_t *)buf.get(n * 8);
+            auto *dout = (egtb_ad_tile_count *)buf.get(n * sizeof(egtb_ad_tile_count));
+            EGTB_CUDA(cudaMemcpy(din, boards, n * 8, cudaMemcpyHostToDevice));
+            ad_stats_kernel<<<kAdGrid, kAdBlock>>>(din, n, p, kind, dout);
+            EGTB_CUDA(cudaGetLastError());
+            EGTB_CUDA(cudaMemcpy(out, dout, n * sizeof(egtb_ad_tile_count), cudaMemcpyDeviceToHost));
+        });
+    });
+}
+
+extern "C" int egtb_ad_validate(int device, const uint64_t *boards, size_t n, const uint32_t *original_sums,
+                                const egtb_ad_param *param, uint8_t *out) {
+    return guarded([&] {
+        const AdParamDev p = ad_param(param);
+        if (n == 0) return;
+        if (!boards || !original_sums || !out) throw Error(EGTB_ERR_ARG, "NULL buffer");
+        on_device(device, [&] {
+            const AdDeviceTables t = device_ad_tables(device);
+            AdBuffers buf;
+            auto *din = (uint64_t *)buf.get(n * 8);
+            auto *dsum = (uint32_t *)buf.get(n * 4);
+            auto *dout = (uint8_t *)buf.get(n);
+            EGTB_CUDA(cudaMemcpy(din, boards, n * 8, cudaMemcpyHostToDevice));
+            EGTB_CUDA(cudaMemcpy(dsum, original_sums, n * 4, cudaMemcpyHostToDevice));
+            ad_validate_kernel<<<kAdGrid, kAdBlock>>>(din, dsum, n, p, t.lens, t.vals, dout);
+            EGTB_CUDA(cudaGetLastError());
+            EGTB_CUDA(cudaMemcpy(out, dout, n, cudaMemcpyDeviceToHost));
+        });
+    });
+}
+
+extern "C" int egtb_ad_row_tables(uint32_t *moves, uint8_t *flags) {
+    return guarded([&] {
+        if (!moves || !flags) throw Error(EGTB_ERR_ARG, "NULL buffer");
+        const AdTables &t = host_ad_tables();
+        std::memcpy(moves, t.moves.data(), t.moves.size() * sizeof(uint32_t));
+        std::memcpy(flags, t.flags.data(), t.flags.size());
+    });
+}
+
+extern "C" int egtb_ad_tiles_combinations(uint8_t *lens, uint8_t *vals16) {
+    return guarded([&] {
+        if (!lens || !vals16) throw Error(EGTB_ERR_ARG, "NULL buffer");
+        const AdTables &t = host_ad_tables();
+        std::memcpy(lens, t.lens.data(), t.lens.size());
+        std::memcpy(vals16, t.vals.data(), t.vals.size());
+    });
+}

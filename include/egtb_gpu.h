@@ -228,6 +228,60 @@ EGTB_API int egtb_move_all_dir_variant(int device, const uint64_t *boards, size_
 EGTB_API int egtb_canonical(int device, const uint64_t *boards, size_t n, int32_t symm_mode, uint64_t *out);
 EGTB_API int egtb_apply_sym(int device, const uint64_t *boards, size_t n, int32_t symm_index, uint64_t *out);
 
+/* ------------------------- masked-board primitives (advanced algorithm) --- */
+
+/* The masked boards of the reference's advanced algorithm (namespace
+ * FormationAD): tiles of 64 and up are held as 0xF ("32k") nibbles.
+ * AdvancedMaskParam, native_core/include/FormationRuntime.h:98-104. */
+typedef struct egtb_ad_param {
+    uint64_t pos_fixed_32k_mask;   /* 0xF nibbles at the pattern's fixed 32k cells */
+    uint32_t small_tile_sum_limit; /* default 96 */
+    uint32_t target;               /* log2 of the target tile */
+    uint32_t num_free_32k;
+    uint32_t num_fixed_32k;
+} egtb_ad_param;
+
+/* TileCountResult / TileCount4Result, native_core/include/BoardMaskerAD.h:51-79. */
+typedef struct egtb_ad_tile_count {
+    uint64_t pos_bitmap;        /* 0xF at every cell counted as 32k */
+    uint32_t total_sum;         /* sum of the other tiles */
+    int32_t count_32k;
+    uint32_t pos_rank;          /* kind 4 only: 32k cells before the first merged tile */
+    uint32_t merged_tile_found; /* kind 4: large tiles that are not 0xF */
+    uint32_t merged_tile;       /* kind 4: xor of those tiles */
+    uint32_t is_success;        /* kind 4: one merged tile, equal to the target */
+} egtb_ad_tile_count;
+
+/* Masked mover, batched (host buffers): out4[4i..4i+3] = left, right, up,
+ * down of boards[i]; flags4 likewise = 1 where a merge made a tile of 64 or
+ * more, which the masked board holds as 0xF (mask_new_tile; left and right
+ * report the left merge's flag, up and down the up merge's). 0xF never
+ * merges. m_move_all_dir, native_core/src/BoardMoverAD.cpp:171-178, rows by
+ * merge_line, :49-89. */
+EGTB_API int egtb_ad_move_all_dir(int device, const uint64_t *boards, size_t n, uint64_t *out4, uint8_t *flags4);
+/* mask_board, native_core/src/BoardMaskerAD.cpp:112-121: every nibble >=
+ * threshold becomes 0xF (the reference's default threshold is 6). */
+EGTB_API int egtb_ad_mask_board(int device, const uint64_t *boards, size_t n, int32_t threshold, uint64_t *out);
+/* Tile statistics after clearing the fixed 32k cells: kind 1 counts only 0xF
+ * as 32k (tile_sum_and_32k_count, BoardMaskerAD.cpp:123-144), kind 2 counts
+ * every tile of 64 and up (tile_sum_and_32k_count2, :169-190), kind 4 is kind
+ * 2 plus the merged-tile fields (tile_sum_and_32k_count4, :219-257). */
+EGTB_API int egtb_ad_tile_stats(int device, const uint64_t *boards, size_t n, const egtb_ad_param *param,
+                                int32_t kind, egtb_ad_tile_count *out);
+/* validate, native_core/src/BoardMaskerAD.cpp:409-443: out[i] = 1 when
+ * boards[i] (tile sum original_sums[i] before masking) can stand for a real
+ * board of the pattern. The reference reads its tiles-combination table at
+ * (count_32k - num_free_32k) < 10 only; boards past that give 0 here. */
+EGTB_API int egtb_ad_validate(int device, const uint64_t *boards, size_t n, const uint32_t *original_sums,
+                              const egtb_ad_param *param, uint8_t *out);
+/* The host tables behind the two above (no device needed): the masked row
+ * moves (moves[r] = left xor | right xor << 16, flags[r] = mask_new_tile of
+ * the left merge; BoardMoverAD.cpp:27-45) and the tiles-combination table of
+ * init_masker (BoardMaskerAD.cpp:524-531: entry a + 256 b, a < 256, b < 10;
+ * lens[e] values in vals16[16 e ..]). */
+EGTB_API int egtb_ad_row_tables(uint32_t *moves, uint8_t *flags);
+EGTB_API int egtb_ad_tiles_combinations(uint8_t *lens, uint8_t *vals16);
+
 /* Sort the n keys at d_keys (device memory) ascending, drop repeats, write
  * the unique keys to d_out (device, room for n keys, must not alias d_keys)
  * and their count to *d_n_out (device). Enqueued on `stream`

@@ -10,6 +10,11 @@ fixtures are outputs of the reference itself, run in this container:
   prims.npz    board primitives on seeded random boards: move_all_dir (classic
                and variant movers), canonical_by_mode for modes 0-6,
                apply_sym_like 0-7, row tables of both movers
+  ad_prims.npz the advanced algorithm's masked-board primitives on seeded
+               random boards: m_move_all_dir with its mask_new_tile flags,
+               mask_board, tile_sum_and_32k_count / 2 / 4 and validate under
+               four parameter sets, the masked row rule, the tiles-combination
+               table of init_masker
   reader.json  ClassicBookReader.move_on_dic answers on positions sampled from
                the books of the small cases
   free5_32.npz one complete small build (raw layers and books) as data
@@ -296,6 +301,91 @@ def prims_fixture():
     np.savez_compressed(os.path.join(GOLDEN, "prims.npz"), **out)
 
 
+# masked-board parameter sets of the advanced algorithm: (small_tile_sum_limit,
+# target, fixed 32k shifts, num_free_32k)
+AD_PARAMS = [(96, 10, [], 0), (96, 11, [60, 56], 2), (160, 9, [0, 4, 8], 1), (32, 12, [12], 3)]
+
+
+def _pack(cells: np.ndarray) -> np.ndarray:
+    boards = np.zeros(len(cells), dtype=np.uint64)
+    for k in range(16):
+        boards |= cells[:, k].astype(np.uint64) << np.uint64(4 * k)
+    return boards
+
+
+def ad_prims_fixture():
+    """The advanced algorithm's masked-board primitives, from the reference's
+    own BoardMoverAD / BoardMaskerAD (oracle/_ref/libref_ad_prims.so)."""
+    L = ctypes.CDLL(os.path.join(R.REF_DIR, "libref_ad_prims.so"))
+    P, Z, U = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32
+    L.ref_ad_move_all_dir_batch.argtypes = [P, Z, P, P]
+    L.ref_ad_mask_board_batch.argtypes = [P, Z, ctypes.c_int, P]
+    L.ref_ad_tile_stats_batch.argtypes = [P, Z, U, U, P, Z, U, ctypes.c_int, P]
+    L.ref_ad_validate_batch.argtypes = [P, Z, P, U, U, P, Z, U, P]
+    L.ref_ad_tiles_combinations.argtypes = [P, P]
+    rng = np.random.default_rng(4096)
+    n = 4000
+    # mover: small tiles, equal neighbours common (merges into 32 and 64+), some 0xF
+    vals = np.array([0, 1, 2, 3, 4, 5, 6, 7, 15])
+    prob = np.array([0.30, 0.08, 0.08, 0.08, 0.10, 0.14, 0.10, 0.04, 0.08])
+    mover_boards = _pack(rng.choice(vals, size=(n, 16), p=prob))
+    out = {"mover_boards": mover_boards}
+    mv = np.zeros(n * 4, dtype=np.uint64)
+    fl = np.zeros(n * 4, dtype=np.uint8)
+    L.ref_ad_move_all_dir_batch(mover_boards.ctypes.data, ctypes.c_size_t(n), mv.ctypes.data, fl.ctypes.data)
+    out["mover_moves"], out["mover_flags"] = mv.reshape(n, 4), fl.reshape(n, 4)
+    # masker and tile statistics: any nibble
+    boards = _pack(rng.integers(0, 16, size=(n, 16)))
+    out["boards"] = boards
+    for th in (6, 5, 9):
+        m = np.zeros(n, dtype=np.uint64)
+        L.ref_ad_mask_board_batch(boards.ctypes.data, ctypes.c_size_t(n), ctypes.c_int(th), m.ctypes.data)
+        out[f"mask_{th}"] = m
+    for i, (limit, target, fixed, nfree) in enumerate(AD_PARAMS):
+        fx = np.array(fixed, dtype=np.uint8)
+        for kind in (1, 2, 4):
+            st = np.zeros(n * 8, dtype=np.int64)
+            L.ref_ad_tile_stats_batch(boards.ctypes.data, ctypes.c_size_t(n), ctypes.c_uint32(limit),
+                                      ctypes.c_uint32(target), fx.ctypes.data, ctypes.c_size_t(len(fx)),
+                                      ctypes.c_uint32(nfree), ctypes.c_int(kind), st.ctypes.data)
+            out[f"stats_{i}_{kind}"] = st.reshape(n, 8)
+        # validate: boards whose 32k count (tiles of 64 and up outside the fixed
+        # cells) is num_free_32k .. num_free_32k + 9, where the reference's
+        # table lookup stays inside its table; small tiles mostly
+        cells = rng.choice(np.arange(16), size=(4 * n, 16),
+                           p=np.r_[[0.3], np.full(5, 0.5 / 5), np.full(10, 0.2 / 10)])
+        cand = _pack(cells)
+        st = np.zeros(len(cand) * 8, dtype=np.int64)
+        L.ref_ad_tile_stats_batch(cand.ctypes.data, ctypes.c_size_t(len(cand)), ctypes.c_uint32(limit),
+                                  ctypes.c_uint32(target), fx.ctypes.data, ctypes.c_size_t(len(fx)),
+                                  ctypes.c_uint32(nfree), ctypes.c_int(2), st.ctypes.data)
+        st = st.reshape(len(cand), 8)
+        keep = (st[:, 1] >= nfree) & (st[:, 1] <= nfree + 9)
+        vb = cand[keep][:n]
+        small = st[keep][:n, 0].astype(np.int64)
+        large = 64 * rng.integers(0, 300, size=len(vb))
+        orig = (small + ((nfree + len(fixed)) << 15) + large).astype(np.uint32)
+        ok = np.zeros(len(vb), dtype=np.uint8)
+        L.ref_ad_validate_batch(vb.ctypes.data, ctypes.c_size_t(len(vb)), orig.ctypes.data, ctypes.c_uint32(limit),
+                                ctypes.c_uint32(target), fx.ctypes.data, ctypes.c_size_t(len(fx)),
+                                ctypes.c_uint32(nfree), ok.ctypes.data)
+        out[f"validate_{i}_boards"], out[f"validate_{i}_sums"], out[f"validate_{i}"] = vb, orig, ok
+    lens = np.zeros(2560, dtype=np.uint8)
+    vals16 = np.zeros(2560 * 16, dtype=np.uint8)
+    L.ref_ad_tiles_combinations(lens.ctypes.data, vals16.ctypes.data)
+    out["combo_lens"], out["combo_vals"] = lens, vals16.reshape(2560, 16)
+    # the masked row rule: each row alone on an otherwise empty board
+    rows = np.arange(65536, dtype=np.uint64)
+    mv = np.zeros(65536 * 4, dtype=np.uint64)
+    fl = np.zeros(65536 * 4, dtype=np.uint8)
+    L.ref_ad_move_all_dir_batch(rows.ctypes.data, ctypes.c_size_t(65536), mv.ctypes.data, fl.ctypes.data)
+    mv = mv.reshape(65536, 4)
+    out["row_left"] = (mv[:, 0] & np.uint64(0xFFFF)).astype(np.uint16)
+    out["row_right"] = (mv[:, 1] & np.uint64(0xFFFF)).astype(np.uint16)
+    out["row_flag"] = fl.reshape(65536, 4)[:, 0]
+    np.savez_compressed(os.path.join(GOLDEN, "ad_prims.npz"), **out)
+
+
 def decode(board: int):
     return [[(1 << v) if (v := (board >> (4 * ((3 - r) * 4 + (3 - c)))) & 0xF) else 0 for c in range(4)]
             for r in range(4)]
@@ -371,6 +461,8 @@ def main():
     only = set(filter(None, args.only.split(",")))
     if not only or "prims" in only:
         prims_fixture()
+    if not only or "ad_prims" in only:
+        ad_prims_fixture()
     cases_path = os.path.join(GOLDEN, "cases.json")
     cases = json.load(open(cases_path)) if os.path.exists(cases_path) else {}
     reader = {}

@@ -38,6 +38,26 @@ def prims():
     return np.load(os.path.join(GOLDEN, "prims.npz"))
 
 
+def ad_prims():
+    return np.load(os.path.join(GOLDEN, "ad_prims.npz"))
+
+
+def ad():
+    return importlib.import_module("2048endgametablebase_b200.formation_ad")
+
+
+# the masked-board parameter sets of tests/golden/make_golden.py (AD_PARAMS):
+# (small_tile_sum_limit, target, fixed 32k shifts, num_free_32k)
+AD_PARAMS = [(96, 10, [], 0), (96, 11, [60, 56], 2), (160, 9, [0, 4, 8], 1), (32, 12, [12], 3)]
+
+
+def ad_param(i: int):
+    limit, target, fixed, nfree = AD_PARAMS[i]
+    A = ad()
+    return A.build_mask_param(A.AdvancedPatternSpec(num_free_32k=nfree, fixed_32k_shifts=fixed,
+                                                    small_tile_sum_limit=limit, target=target))
+
+
 def sha(path: str) -> str:
     h = hashlib.sha256()
     with open(path, "rb") as f:
