@@ -189,6 +189,8 @@ _SIGS = {
     "egtb_ad_tile_stats": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, ctypes.POINTER(AdParamC), ctypes.c_int32,
                                           _P]),
     "egtb_ad_validate": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, _P, ctypes.POINTER(AdParamC), _P]),
+    "egtb_ad_unmask": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_size_t, _P, ctypes.POINTER(AdParamC), _P, _P,
+                                      ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)]),
     "egtb_ad_row_tables": (ctypes.c_int, [_P, _P]),
     "egtb_ad_tiles_combinations": (ctypes.c_int, [_P, _P]),
     "egtb_book_open": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(PatternSpecC),

@@ -10,6 +10,7 @@
 //                           info), :123-144, :169-190, :219-257
 //   tiles combinations      native_core/src/BoardMaskerAD.cpp:259-289,524-531
 //   validate                native_core/src/BoardMaskerAD.cpp:409-443
+//   permutations, unmask    native_core/src/BoardMaskerAD.cpp:291-358,445-512
 //
 // One thread per board; the row moves come from a 65536-entry table built on
 // the host from the rule, the per-row statistics are computed in registers.
@@ -104,6 +105,42 @@ std::vector<uint8_t> large_tiles_for(uint64_t sum, int count) {
         out.push_back((uint8_t)lg);
     }
     return {};
+}
+
+// The rows of permutation slot (m, n): every way to put the values 0..n-1
+// into n distinct cells of m (row[j] = the cell that gets value j), in the
+// reference's order: by the cells' contents read from cell 0 to cell m-1, a
+// cell left out reading as 15 (resort_permutations, BoardMaskerAD.cpp:291-332).
+std::vector<uint8_t> permutation_rows(int m, int n) {
+    std::vector<std::pair<uint64_t, std::vector<uint8_t>>> rows;
+    std::vector<uint8_t> row((size_t)n);
+    std::vector<bool> used((size_t)m, false);
+    auto fill = [&](auto &&self, int j) -> void {
+        if (j == n) {
+            uint64_t key = 0;
+            for (int c = 0; c < m; ++c) {
+                uint64_t nib = 15;
+                for (int v = 0; v < n; ++v)
+                    if (row[(size_t)v] == c) nib = (uint64_t)v;
+                key = (key << 4) | nib;
+            }
+            rows.emplace_back(key, row);
+            return;
+        }
+        for (int c = 0; c < m; ++c) {
+            if (used[(size_t)c]) continue;
+            used[(size_t)c] = true;
+            row[(size_t)j] = (uint8_t)c;
+            self(self, j + 1);
+            used[(size_t)c] = false;
+        }
+    };
+    fill(fill, 0);
+    std::sort(rows.begin(), rows.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+    std::vector<uint8_t> flat;
+    flat.reserve(rows.size() * (size_t)n);
+    for (const auto &r : rows) flat.insert(flat.end(), r.second.begin(), r.second.end());
+    return flat;
 }
 
 const AdTables &host_ad_tables() {
@@ -297,6 +334,91 @@ __global__ void ad_validate_kernel(const uint64_t *in, const uint32_t *orig, siz
     }
 }
 
+// Permutation slot (m, n) = index (m << 4) + n: its rows in one buffer.
+struct AdPermSlot {
+    unsigned long long off;
+    unsigned rows, cols;
+};
+
+// What unmask_board does with one board: 0 = nothing, 1 = the board itself,
+// 2 = one board per permutation row of slot `slot` (values from combination
+// entry `combo`); pos[] = the 0xF cells (fixed ones excluded), highest first.
+__device__ __forceinline__ int ad_unmask_plan(uint64_t board, uint32_t orig, const AdParamDev &p, const uint8_t *lens,
+                                              int &slot, int &combo, int &npos, uint8_t pos[16]) {
+    const uint64_t masked = board & ~p.fixed;
+    uint32_t total = 0;
+    npos = 0;
+#pragma unroll
+    for (int k = 3; k >= 0; --k) total += ad_row_info((uint32_t)((masked >> (16 * k)) & 0xFFFFu), true).sum16;
+    for (int sh = 60; sh >= 0; sh -= 4)
+        if (((masked >> sh) & 0xFull) == 0xFull) pos[npos++] = (uint8_t)sh;
+    const int8_t count = (int8_t)npos, free32k = (int8_t)(uint8_t)p.num_free;
+    if (count == 0 || count == free32k) return 1;
+    const uint32_t large = orig - total - ((uint32_t)((p.num_free & 0xFFu) + (p.num_fixed & 0xFFu)) << 15);
+    const uint32_t a = (uint8_t)(large >> 6), c = (uint8_t)(count - free32k);
+    if (c >= 10) return 0;  // past the reference's table (its read is out of bounds)
+    combo = (int)(a + 256 * c);
+    if (lens[combo] == 0) return 0;
+    // init_masker builds slots (n + num_free_32k, n) for 1 <= n < target - 4
+    if ((int)c < 1 || (int)c >= (int)(p.target & 0xFFu) - 4 || npos > 15) return 0;
+    slot = (npos << 4) + (int)c;
+    return 2;
+}
+
+__global__ void ad_unmask_count_kernel(const uint64_t *in, const uint32_t *orig, size_t n, AdParamDev p,
+                                       const uint8_t *lens, const uint8_t *vals, const AdPermSlot *slots,
+                                       const uint8_t *rows, uint32_t *counts) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        int slot = 0, combo = 0, npos = 0;
+        uint8_t pos[16];
+        const int plan = ad_unmask_plan(in[i], orig[i], p, lens, slot, combo, npos, pos);
+        uint32_t cnt = plan == 1 ? 1u : 0u;
+        if (plan == 2) {
+            const AdPermSlot s = slots[slot];
+            const uint8_t *v = vals + (size_t)combo * kAdComboVals;
+            if (lens[combo] > 1 && v[0] == v[1]) {
+                // equal first two tiles: only rows with row[1] < row[0]
+                for (unsigned r = 0; r < s.rows; ++r) {
+                    const uint8_t *row = rows + s.off + (size_t)r * s.cols;
+                    cnt += row[1] < row[0];
+                }
+            } else {
+                cnt = s.rows;
+            }
+        }
+        counts[i] = cnt;
+    }
+}
+
+__global__ void ad_unmask_write_kernel(const uint64_t *in, const uint32_t *orig, size_t n, AdParamDev p,
+                                       const uint8_t *lens, const uint8_t *vals, const AdPermSlot *slots,
+                                       const uint8_t *rows, const unsigned long long *offs, uint64_t *out) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint64_t board = in[i];
+        int slot = 0, combo = 0, npos = 0;
+        uint8_t pos[16];
+        const int plan = ad_unmask_plan(board, orig[i], p, lens, slot, combo, npos, pos);
+        unsigned long long o = offs[i];
+        if (plan == 1) out[o] = board;
+        if (plan != 2) continue;
+        const AdPermSlot s = slots[slot];
+        const int len = lens[combo];
+        const uint8_t *v = vals + (size_t)combo * kAdComboVals;
+        const bool ordered = len > 1 && v[0] == v[1];
+        for (unsigned r = 0; r < s.rows; ++r) {
+            const uint8_t *row = rows + s.off + (size_t)r * s.cols;
+            if (ordered && !(row[1] < row[0])) continue;
+            uint64_t clear = 0, set = 0;
+            for (int j = 0; j < len; ++j) {
+                const int sh = pos[row[j]];
+                clear |= 0xFull << sh;
+                set |= (uint64_t)v[j] << sh;
+            }
+            out[o++] = (board & ~clear) | set;
+        }
+    }
+}
+
 // -------------------------------------------------------------- host ----
 
 AdParamDev ad_param(const egtb_ad_param *p) {
@@ -426,5 +548,63 @@ extern "C" int egtb_ad_tiles_combinations(uint8_t *lens, uint8_t *vals16) {
         const AdTables &t = host_ad_tables();
         std::memcpy(lens, t.lens.data(), t.lens.size());
         std::memcpy(vals16, t.vals.data(), t.vals.size());
+    });
+}
+
+extern "C" int egtb_ad_unmask(int device, const uint64_t *boards, size_t n, const uint32_t *original_sums,
+                              const egtb_ad_param *param, uint32_t *counts, uint64_t *out, size_t cap,
+                              uint64_t *total) {
+    return guarded([&] {
+        const AdParamDev p = ad_param(param);
+        if (!total) throw Error(EGTB_ERR_ARG, "NULL total");
+        *total = 0;
+        if (n == 0) return;
+        if (!boards || !original_sums || !counts || (cap && !out)) throw Error(EGTB_ERR_ARG, "NULL buffer");
+        // the permutation slots init_masker builds: (n + num_free_32k, n), 1 <= n < target - 4
+        std::vector<AdPermSlot> slots(256, AdPermSlot{0, 0, 0});
+        std::vector<uint8_t> rows;
+        for (int k = 1; k < (int)(p.target & 0xFFu) - 4; ++k) {
+            const int m = k + (int)(p.num_free & 0xFFu);
+            if (m > 15) break;
+            double perms = 1.0;
+            for (int j = 0; j < k; ++j) perms *= (double)(m - j);
+            if (perms * k > (double)(1u << 28))
+                throw Error(EGTB_ERR_UNSUPPORTED, "permutation table above 256 MiB for this target and num_free_32k");
+            const std::vector<uint8_t> r = permutation_rows(m, k);
+            slots[(size_t)((m << 4) + k)] = AdPermSlot{(unsigned long long)rows.size(), (unsigned)(r.size() / k),
+                                                        (unsigned)k};
+            rows.insert(rows.end(), r.begin(), r.end());
+        }
+        on_device(device, [&] {
+            const AdDeviceTables t = device_ad_tables(device);
+            AdBuffers buf;
+            auto *din = (uint64_t *)buf.get(n * 8);
+            auto *dsum = (uint32_t *)buf.get(n * 4);
+            auto *dcnt = (uint32_t *)buf.get(n * 4);
+            auto *dslots = (AdPermSlot *)buf.get(slots.size() * sizeof(AdPermSlot));
+            auto *drows = (uint8_t *)buf.get(rows.size());
+            EGTB_CUDA(cudaMemcpy(din, boards, n * 8, cudaMemcpyHostToDevice));
+            EGTB_CUDA(cudaMemcpy(dsum, original_sums, n * 4, cudaMemcpyHostToDevice));
+            EGTB_CUDA(cudaMemcpy(dslots, slots.data(), slots.size() * sizeof(AdPermSlot), cudaMemcpyHostToDevice));
+            if (!rows.empty()) EGTB_CUDA(cudaMemcpy(drows, rows.data(), rows.size(), cudaMemcpyHostToDevice));
+            ad_unmask_count_kernel<<<kAdGrid, kAdBlock>>>(din, dsum, n, p, t.lens, t.vals, dslots, drows, dcnt);
+            EGTB_CUDA(cudaGetLastError());
+            EGTB_CUDA(cudaMemcpy(counts, dcnt, n * 4, cudaMemcpyDeviceToHost));
+            std::vector<unsigned long long> offs(n);
+            unsigned long long sum = 0;
+            for (size_t i = 0; i < n; ++i) {
+                offs[i] = sum;
+                sum += counts[i];
+            }
+            *total = sum;
+            if (sum > cap) throw Error(EGTB_ERR_CAPACITY, "unmasked boards exceed the output capacity");
+            if (sum == 0) return;
+            auto *doffs = (unsigned long long *)buf.get(n * 8);
+            auto *dout = (uint64_t *)buf.get(sum * 8);
+            EGTB_CUDA(cudaMemcpy(doffs, offs.data(), n * 8, cudaMemcpyHostToDevice));
+            ad_unmask_write_kernel<<<kAdGrid, kAdBlock>>>(din, dsum, n, p, t.lens, t.vals, dslots, drows, doffs, dout);
+            EGTB_CUDA(cudaGetLastError());
+            EGTB_CUDA(cudaMemcpy(out, dout, sum * 8, cudaMemcpyDeviceToHost));
+        });
     });
 }

@@ -10,6 +10,7 @@ reference's names (namespace FormationAD):
   tile_sum_and_32k_count(2, 4)   native_core/src/BoardMaskerAD.cpp:123-144,
                                  :169-190, :219-257
   validate                       native_core/src/BoardMaskerAD.cpp:409-443
+  unmask_board                   native_core/src/BoardMaskerAD.cpp:445-512
   build_mask_param               native_core/src/BoardMaskerAD.cpp:102-110
 
 There is no CPU fallback: without the library or a device every call raises.
@@ -22,6 +23,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _native as N
+
+_ERR_CAPACITY = -5  # EGTB_ERR_CAPACITY: the output did not fit; counts and total are filled
 
 
 @dataclass
@@ -120,6 +123,29 @@ def validate(boards, original_sums, param: AdvancedMaskParam, device: int = 0) -
     c = param.to_c()
     N.check(N.lib().egtb_ad_validate(device, b.ctypes.data, len(b), s.ctypes.data, ctypes.byref(c), out.ctypes.data))
     return out.astype(bool)
+
+
+def unmask_board(boards, original_sums, param: AdvancedMaskParam, device: int = 0):
+    """(counts, unmasked): every board each masked board stands for, in the
+    reference's order; unmasked holds all boards' results one after another
+    (counts[i] of them for boards[i])."""
+    b = _boards(boards)
+    s = np.ascontiguousarray(np.asarray(original_sums, dtype=np.uint32).reshape(-1))
+    if len(s) != len(b):
+        raise ValueError("one original sum per board")
+    counts = np.zeros(len(b), dtype=np.uint32)
+    c = param.to_c()
+    total = ctypes.c_uint64(0)
+    cap = 16 * max(1, len(b))
+    out = np.zeros(cap, dtype=np.uint64)
+    rc = N.lib().egtb_ad_unmask(device, b.ctypes.data, len(b), s.ctypes.data, ctypes.byref(c), counts.ctypes.data,
+                                out.ctypes.data, cap, ctypes.byref(total))
+    if rc == _ERR_CAPACITY and total.value > cap:
+        out = np.zeros(int(total.value), dtype=np.uint64)
+        rc = N.lib().egtb_ad_unmask(device, b.ctypes.data, len(b), s.ctypes.data, ctypes.byref(c),
+                                    counts.ctypes.data, out.ctypes.data, len(out), ctypes.byref(total))
+    N.check(rc)
+    return counts, out[:int(total.value)]
 
 
 def row_tables():

@@ -274,7 +274,18 @@ EGTB_API int egtb_ad_tile_stats(int device, const uint64_t *boards, size_t n, co
  * (count_32k - num_free_32k) < 10 only; boards past that give 0 here. */
 EGTB_API int egtb_ad_validate(int device, const uint64_t *boards, size_t n, const uint32_t *original_sums,
                               const egtb_ad_param *param, uint8_t *out);
-/* The host tables behind the two above (no device needed): the masked row
+/* unmask_board, native_core/src/BoardMaskerAD.cpp:445-512 (tables of
+ * init_masker, :514-533): every board that masked board boards[i] (tile sum
+ * original_sums[i] before masking) stands for, in the reference's order:
+ * counts[i] of them, all boards' packed one after another into out (room for
+ * cap). *total = their sum; above cap the call fails with EGTB_ERR_CAPACITY
+ * after filling counts and *total, so the caller can size out and call again.
+ * Boards whose 32k count is below num_free_32k or 10 or more above it (where
+ * the reference reads past its tables) give none. */
+EGTB_API int egtb_ad_unmask(int device, const uint64_t *boards, size_t n, const uint32_t *original_sums,
+                            const egtb_ad_param *param, uint32_t *counts, uint64_t *out, size_t cap,
+                            uint64_t *total);
+/* The host tables behind the kernels above (no device needed): the masked row
  * moves (moves[r] = left xor | right xor << 16, flags[r] = mask_new_tile of
  * the left merge; BoardMoverAD.cpp:27-45) and the tiles-combination table of
  * init_masker (BoardMaskerAD.cpp:524-531: entry a + 256 b, a < 256, b < 10;

@@ -97,3 +97,24 @@ REF_API void ref_ad_tiles_combinations(uint8_t *lens, uint8_t *vals) {
         for (size_t j = 0; j < v.size() && j < 16; ++j) vals[16 * e + j] = v[j];
     }
 }
+
+// unmask_board (native_core/src/BoardMaskerAD.cpp:445-512) with init_masker's
+// tables: counts[i] boards for boards[i], packed in order into out (room for
+// cap); returns the total (boards past cap are counted, not written).
+REF_API size_t ref_ad_unmask_batch(const uint64_t *boards, size_t n, const uint32_t *original_sums,
+                                   uint32_t small_limit, uint32_t target, const uint8_t *fixed_shifts, size_t n_fixed,
+                                   uint32_t num_free_32k, uint32_t *counts, uint64_t *out, size_t cap) {
+    const auto ctx = FormationAD::init_masker(make_spec(small_limit, target, fixed_shifts, n_fixed, num_free_32k));
+    size_t total = 0;
+    std::vector<uint64_t> got;
+    for (size_t i = 0; i < n; ++i) {
+        FormationAD::unmask_board_into(boards[i], original_sums[i], ctx.tiles_combination_table,
+                                       ctx.permutation_table, ctx.param, got);
+        counts[i] = (uint32_t)got.size();
+        for (uint64_t b : got) {
+            if (total < cap) out[total] = b;
+            ++total;
+        }
+    }
+    return total;
+}

@@ -12,8 +12,8 @@ fixtures are outputs of the reference itself, run in this container:
                apply_sym_like 0-7, row tables of both movers
   ad_prims.npz the advanced algorithm's masked-board primitives on seeded
                random boards: m_move_all_dir with its mask_new_tile flags,
-               mask_board, tile_sum_and_32k_count / 2 / 4 and validate under
-               four parameter sets, the masked row rule, the tiles-combination
+               mask_board, tile_sum_and_32k_count / 2 / 4, validate and
+               unmask_board under four parameter sets, the masked row rule, the tiles-combination
                table of init_masker
   reader.json  ClassicBookReader.move_on_dic answers on positions sampled from
                the books of the small cases
@@ -323,6 +323,8 @@ def ad_prims_fixture():
     L.ref_ad_tile_stats_batch.argtypes = [P, Z, U, U, P, Z, U, ctypes.c_int, P]
     L.ref_ad_validate_batch.argtypes = [P, Z, P, U, U, P, Z, U, P]
     L.ref_ad_tiles_combinations.argtypes = [P, P]
+    L.ref_ad_unmask_batch.argtypes = [P, Z, P, U, U, P, Z, U, P, P, Z]
+    L.ref_ad_unmask_batch.restype = ctypes.c_size_t
     rng = np.random.default_rng(4096)
     n = 4000
     # mover: small tiles, equal neighbours common (merges into 32 and 64+), some 0xF
@@ -373,6 +375,43 @@ def ad_prims_fixture():
     lens = np.zeros(2560, dtype=np.uint8)
     vals16 = np.zeros(2560 * 16, dtype=np.uint8)
     L.ref_ad_tiles_combinations(lens.ctypes.data, vals16.ctypes.data)
+    # unmask_board: masked boards (small tiles and 0xF cells) whose 32k count is
+    # num_free_32k .. num_free_32k + 4, tile sums mostly of large tiles that a
+    # combination exists for (a few arbitrary ones)
+    for i, (limit, target, fixed, nfree) in enumerate(AD_PARAMS):
+        fx = np.array(fixed, dtype=np.uint8)
+        fmask = 0
+        for sh in fixed:
+            fmask |= 0xF << sh
+        cells = rng.choice(np.r_[np.arange(6), [15]], size=(8 * 400, 16), p=[0.35, 0.1, 0.1, 0.1, 0.1, 0.05, 0.2])
+        cand = _pack(cells)
+        free_f = np.zeros(len(cand), dtype=np.int64)
+        small = np.zeros(len(cand), dtype=np.int64)
+        for k in range(16):
+            nib = (cand >> np.uint64(4 * k)) & np.uint64(0xF)
+            if (fmask >> (4 * k)) & 0xF:
+                continue
+            free_f += (nib == 15)
+            small += np.where((nib > 0) & (nib < 15), 1 << nib.astype(np.int64), 0)
+        c = free_f - nfree
+        keep = (c >= 0) & (c <= 4)
+        ub, small, c = cand[keep][:400], small[keep][:400], c[keep][:400]
+        large = np.zeros(len(ub), dtype=np.int64)
+        for j in range(len(ub)):
+            ok = np.flatnonzero(lens[256 * c[j]: 256 * c[j] + 256]) if c[j] > 0 else np.array([], dtype=np.int64)
+            if len(ok) and rng.random() < 0.85:
+                large[j] = 64 * int(rng.choice(ok)) + int(rng.integers(0, 64))
+            else:
+                large[j] = 64 * int(rng.integers(0, 256))
+        orig = (small + ((nfree + len(fixed)) << 15) + large).astype(np.uint32)
+        counts = np.zeros(len(ub), dtype=np.uint32)
+        total = L.ref_ad_unmask_batch(ub.ctypes.data, len(ub), orig.ctypes.data, limit, target, fx.ctypes.data,
+                                      len(fx), nfree, counts.ctypes.data, None, 0)
+        got = np.zeros(max(1, total), dtype=np.uint64)
+        L.ref_ad_unmask_batch(ub.ctypes.data, len(ub), orig.ctypes.data, limit, target, fx.ctypes.data, len(fx),
+                              nfree, counts.ctypes.data, got.ctypes.data, total)
+        out[f"unmask_{i}_boards"], out[f"unmask_{i}_sums"] = ub, orig
+        out[f"unmask_{i}_counts"], out[f"unmask_{i}"] = counts, got[:total]
     out["combo_lens"], out["combo_vals"] = lens, vals16.reshape(2560, 16)
     # the masked row rule: each row alone on an otherwise empty board
     rows = np.arange(65536, dtype=np.uint64)

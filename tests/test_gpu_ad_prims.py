@@ -59,3 +59,30 @@ def test_empty_and_bad_arguments():
         A._tile_stats(np.zeros(4, dtype=np.uint64), H.ad_param(0), 3, 0)
     with pytest.raises(ValueError):
         A.validate(np.zeros(4, dtype=np.uint64), np.zeros(3, dtype=np.uint32), H.ad_param(0))
+
+
+@pytest.mark.parametrize("i", range(len(H.AD_PARAMS)))
+def test_unmask_board(i):
+    """Every board a masked board stands for, in the reference's permutation order."""
+    g = H.ad_prims()
+    counts, boards = H.ad().unmask_board(g[f"unmask_{i}_boards"], g[f"unmask_{i}_sums"], H.ad_param(i))
+    assert np.array_equal(counts, g[f"unmask_{i}_counts"])
+    assert np.array_equal(boards, g[f"unmask_{i}"])
+    assert counts.max() > 1 and (counts == 0).any()  # expansions and rejections both occur
+
+
+def test_unmask_reports_capacity():
+    """Too small an output: EGTB_ERR_CAPACITY with the counts and total filled."""
+    import ctypes
+    g = H.ad_prims()
+    N = H.pkg()._native
+    b = np.ascontiguousarray(g["unmask_1_boards"])
+    s = np.ascontiguousarray(g["unmask_1_sums"])
+    counts = np.zeros(len(b), dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint64)
+    total = ctypes.c_uint64(0)
+    c = H.ad_param(1).to_c()
+    rc = N.lib().egtb_ad_unmask(0, b.ctypes.data, len(b), s.ctypes.data, ctypes.byref(c), counts.ctypes.data,
+                                out.ctypes.data, 4, ctypes.byref(total))
+    assert rc == -5 and total.value == g["unmask_1_counts"].sum()
+    assert np.array_equal(counts, g["unmask_1_counts"])
