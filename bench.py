@@ -245,6 +245,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-build leg")
     ap.add_argument("--batch-only", action="store_true", help="run the batched-build leg alone and print its JSON")
+    ap.add_argument("--no-ad", action="store_true", help="skip the masked-board primitives leg")
+    ap.add_argument("--ad-only", action="store_true", help="run the masked-board primitives leg alone")
     ap.add_argument("--serve-only", action="store_true", help="run the serving leg alone and print its JSON")
     ap.add_argument("--serve-offered", type=float, default=3e8, help="offered lookups/s of the serving leg")
     ap.add_argument("--profile-lookup", action="store_true",
@@ -330,6 +332,10 @@ def main():
     if args.serve_only:
         print(json.dumps({"serving": serving_leg(local, base, offered=args.serve_offered,
                                                  cpu_reference=not args.no_cpu_baseline)}), flush=True)
+        shutil.rmtree(work, ignore_errors=True)
+        return
+    if args.ad_only:
+        print(json.dumps({"advanced_prims": ad_leg(cpu_reference=not args.no_cpu_baseline)}), flush=True)
         shutil.rmtree(work, ignore_errors=True)
         return
     if args.profile_run:
@@ -446,6 +452,8 @@ def main():
                                           cpu_reference=not args.no_cpu_baseline)
         if not args.no_batch and world == 1:
             line["batched"] = batch_leg(local, cpu_reference=not args.no_cpu_baseline)
+        if not args.no_ad and world == 1:
+            line["advanced_prims"] = ad_leg(cpu_reference=not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)
     shutil.rmtree(work, ignore_errors=True)
     if pg is not None:
@@ -521,6 +529,132 @@ def stream_workload(args, world, rank, local, pg):
 
 
 SERVE_TABLES = (("L3", 8), ("442", 9))
+
+
+def _ad_boards(rng, n: int, vals, prob) -> np.ndarray:
+    cells = rng.choice(np.asarray(vals, dtype=np.uint64), size=(n, 16), p=prob)
+    return np.bitwise_or.reduce(cells << (np.arange(16, dtype=np.uint64) * np.uint64(4)), axis=1)
+
+
+def ad_leg(n: int = 1 << 22, n_unmask: int = 1 << 18, cpu_reference: bool = True) -> dict:
+    """The advanced algorithm's masked-board primitives through the C ABI
+    (host buffers in and out, copies included), boards per second, beside the
+    reference's own BoardMoverAD / BoardMaskerAD code on the same boards
+    (oracle/_ref, one host thread, a bounded sample). Seeded synthetic boards:
+    small tiles with equal neighbours common (mover), boards whose 32k count
+    lies where the masker's tables apply (validate, unmask)."""
+    A = importlib.import_module("2048endgametablebase_b200.formation_ad")
+    rng = np.random.default_rng(99)
+    limit, target, fixed, nfree = 96, 11, [60, 56], 2
+    param = A.build_mask_param(A.AdvancedPatternSpec(num_free_32k=nfree, fixed_32k_shifts=fixed,
+                                                     small_tile_sum_limit=limit, target=target))
+    fmask = np.uint64(param.pos_fixed_32k_mask)
+    mover = _ad_boards(rng, n, [0, 1, 2, 3, 4, 5, 6, 7, 15], [0.30, 0.08, 0.08, 0.08, 0.10, 0.14, 0.10, 0.04, 0.08])
+
+    def nibbles(b):
+        return (b[:, None] >> (np.arange(16, dtype=np.uint64) * np.uint64(4))) & np.uint64(0xF)
+
+    def small_sum(nib, top):
+        return np.where((nib > 0) & (nib < top), np.uint64(1) << nib, np.uint64(0)).sum(axis=1).astype(np.int64)
+
+    free_cells = ((fmask >> (np.arange(16, dtype=np.uint64) * np.uint64(4))) & np.uint64(0xF)) == 0
+    # validate: 32k count (tiles of 64 and up outside the fixed cells) within num_free .. num_free + 9
+    vb = _ad_boards(rng, 2 * n, list(range(16)), np.r_[[0.3], np.full(5, 0.1), np.full(10, 0.02)])
+    nib = nibbles(vb)
+    c32 = ((nib > 5) & free_cells).sum(axis=1)
+    keep = (c32 >= nfree) & (c32 <= nfree + 9)
+    vb = vb[keep][:n]
+    vsum = (small_sum(nib[keep][:n] * free_cells, 6) + ((nfree + len(fixed)) << 15)
+            + 64 * rng.integers(0, 300, size=len(vb))).astype(np.uint32)
+    # unmask: 0xF count num_free .. num_free + 4, large-tile sums a combination exists for
+    ub = _ad_boards(rng, 4 * n_unmask, [0, 1, 2, 3, 4, 5, 15], [0.35, 0.1, 0.1, 0.1, 0.1, 0.05, 0.2])
+    nib = nibbles(ub)
+    cf = ((nib == 15) & free_cells).sum(axis=1) - nfree
+    keep = (cf >= 1) & (cf <= 4)
+    ub, nib, cf = ub[keep][:n_unmask], nib[keep][:n_unmask], cf[keep][:n_unmask]
+    lens, _ = A.tiles_combinations()
+    large = np.zeros(len(ub), dtype=np.int64)
+    for c in range(1, 5):
+        ok = np.flatnonzero(lens[256 * c:256 * c + 256])
+        sel = cf == c
+        if len(ok):
+            large[sel] = 64 * rng.choice(ok, size=int(sel.sum()))
+    usum = (small_sum(nib * free_cells, 15) + ((nfree + len(fixed)) << 15) + large).astype(np.uint32)
+
+    def timed(fn, reps=3):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            r = fn()
+        return (time.perf_counter() - t0) / reps, r
+
+    out = {"workload": f"{n} boards (mover, mask, validate), {len(ub)} boards (unmask); "
+                       f"param small_tile_sum_limit {limit}, target {target}, fixed 32k cells {len(fixed)}, "
+                       f"num_free_32k {nfree}",
+           "path": "formation_ad -> egtb_ad_* (host buffers, copies in the timed call)"}
+    t, _ = timed(lambda: A.m_move_all_dir(mover))
+    out["m_move_all_dir_boards_per_s"] = n / t
+    t, _ = timed(lambda: A.mask_board(mover))
+    out["mask_board_boards_per_s"] = n / t
+    t, ok = timed(lambda: A.validate(vb, vsum, param))
+    out["validate_boards_per_s"] = len(vb) / t
+    out["validate_share_valid"] = float(ok.mean())
+    t, (cnt, got) = timed(lambda: A.unmask_board(ub, usum, param))
+    out["unmask_boards_per_s"] = len(ub) / t
+    out["unmask_outputs_per_s"] = len(got) / t
+    if cpu_reference:
+        ref = reference_ad_rates(mover, vb, vsum, ub, usum, (limit, target, fixed, nfree))
+        if ref:
+            out["cpu_reference"] = ref
+            out["check"] = "unmask output of the sample equals the reference's" if ref.pop("_same") else "MISMATCH"
+    return out
+
+
+def reference_ad_rates(mover, vb, vsum, ub, usum, params) -> dict | None:
+    """The reference's m_move_all_dir / validate / unmask_board (oracle/_ref
+    shim over its own BoardMoverAD.cpp / BoardMaskerAD.cpp) on bounded
+    samples, one host thread (baseline and checker only)."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_ad_prims.so")
+    if not os.path.exists(path):
+        return None
+    L = ctypes.CDLL(path)
+    P, Z, U = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32
+    L.ref_ad_move_all_dir_batch.argtypes = [P, Z, P, P]
+    L.ref_ad_validate_batch.argtypes = [P, Z, P, U, U, P, Z, U, P]
+    L.ref_ad_unmask_batch.argtypes = [P, Z, P, U, U, P, Z, U, P, P, Z]
+    L.ref_ad_unmask_batch.restype = ctypes.c_size_t
+    limit, target, fixed, nfree = params
+    fx = np.array(fixed, dtype=np.uint8)
+    k = 1 << 20
+    b = np.ascontiguousarray(mover[:k])
+    mv, fl = np.zeros(4 * len(b), dtype=np.uint64), np.zeros(4 * len(b), dtype=np.uint8)
+    t0 = time.perf_counter()
+    L.ref_ad_move_all_dir_batch(b.ctypes.data, len(b), mv.ctypes.data, fl.ctypes.data)
+    r = {"m_move_all_dir_boards_per_s": len(b) / (time.perf_counter() - t0)}
+    b, sm = np.ascontiguousarray(vb[:k]), np.ascontiguousarray(vsum[:k])
+    ok = np.zeros(len(b), dtype=np.uint8)
+    t0 = time.perf_counter()
+    L.ref_ad_validate_batch(b.ctypes.data, len(b), sm.ctypes.data, limit, target, fx.ctypes.data, len(fx), nfree,
+                            ok.ctypes.data)
+    r["validate_boards_per_s"] = len(b) / (time.perf_counter() - t0)
+    k = 1 << 14
+    b, sm = np.ascontiguousarray(ub[:k]), np.ascontiguousarray(usum[:k])
+    cnt = np.zeros(len(b), dtype=np.uint32)
+    total = L.ref_ad_unmask_batch(b.ctypes.data, len(b), sm.ctypes.data, limit, target, fx.ctypes.data, len(fx),
+                                  nfree, cnt.ctypes.data, None, 0)
+    got = np.zeros(max(1, total), dtype=np.uint64)
+    t0 = time.perf_counter()
+    L.ref_ad_unmask_batch(b.ctypes.data, len(b), sm.ctypes.data, limit, target, fx.ctypes.data, len(fx), nfree,
+                          cnt.ctypes.data, got.ctypes.data, total)
+    r["unmask_boards_per_s"] = len(b) / (time.perf_counter() - t0)
+    A = importlib.import_module("2048endgametablebase_b200.formation_ad")
+    param = A.build_mask_param(A.AdvancedPatternSpec(num_free_32k=nfree, fixed_32k_shifts=fixed,
+                                                     small_tile_sum_limit=limit, target=target))
+    dc, dg = A.unmask_board(b, sm, param)
+    r["_same"] = bool(np.array_equal(dc, cnt) and np.array_equal(dg, got[:total]))
+    r.update({"cores": 1, "kind": "reference",
+              "sample": "2^20 boards (mover, validate), 2^14 boards (unmask) of the same inputs"})
+    return r
 
 
 def reference_reader_rate(books, positions: np.ndarray, specs) -> dict | None:
