@@ -193,6 +193,9 @@ AdDeviceTables device_ad_tables(int device) {
         EGTB_CUDA(cudaMemcpy(n.flags, h.flags.data(), h.flags.size(), cudaMemcpyHostToDevice));
         EGTB_CUDA(cudaMemcpy(n.lens, h.lens.data(), h.lens.size(), cudaMemcpyHostToDevice));
         EGTB_CUDA(cudaMemcpy(n.vals, h.vals.data(), h.vals.size(), cudaMemcpyHostToDevice));
+        // a copy from pageable memory may still be landing when cudaMemcpy
+        // returns, and the kernels run on another stream: wait once for it
+        EGTB_CUDA(cudaDeviceSynchronize());
         d = n;
     }
     return d;
@@ -426,29 +429,47 @@ AdParamDev ad_param(const egtb_ad_param *p) {
     return AdParamDev{p->pos_fixed_32k_mask, p->small_tile_sum_limit, p->target, p->num_free_32k, p->num_fixed_32k};
 }
 
-// Device buffers of one call, freed on every exit.
+// The stream the primitives of one device run on, created once per device:
+// non-blocking, so a call waits on no other work of the device (a build or a
+// serving loop on the library's own streams) and nothing waits on it.
+cudaStream_t ad_stream(int device) {
+    static std::mutex mu;
+    static std::vector<cudaStream_t> per_device;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)per_device.size() <= device) per_device.resize(device + 1, nullptr);
+    if (!per_device[device]) EGTB_CUDA(cudaStreamCreateWithFlags(&per_device[device], cudaStreamNonBlocking));
+    return per_device[device];
+}
+
+// Device buffers of one call, allocated and freed in the order of the call's
+// stream (no device-wide synchronisation), freed on every exit.
 struct AdBuffers {
+    cudaStream_t s;
     std::vector<void *> ptrs;
+    explicit AdBuffers(cudaStream_t st) : s(st) {}
     void *get(size_t bytes) {
         void *p = nullptr;
-        EGTB_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+        EGTB_CUDA(cudaMallocAsync(&p, std::max<size_t>(bytes, 16), s));
         ptrs.push_back(p);
         return p;
     }
     ~AdBuffers() {
-        for (void *p : ptrs) cudaFree(p);
+        for (void *p : ptrs) cudaFreeAsync(p, s);
     }
 };
 
+// Run f(stream) for one call on `device`; returns once the call's work and
+// copies are done.
 template <typename F>
 void on_device(int device, F &&f) {
     int count = 0;
     EGTB_CUDA(cudaGetDeviceCount(&count));
     if (device < 0 || device >= count) throw Error(EGTB_ERR_ARG, "device out of range");
     EGTB_CUDA(cudaSetDevice(device));
-    f();
+    const cudaStream_t s = ad_stream(device);
+    f(s);
     EGTB_CUDA(cudaGetLastError());
-    EGTB_CUDA(cudaDeviceSynchronize());
+    EGTB_CUDA(cudaStreamSynchronize(s));
 }
 
 constexpr int kAdGrid = 148 * 4, kAdBlock = 256;
@@ -462,17 +483,17 @@ extern "C" int egtb_ad_move_all_dir(int device, const uint64_t *boards, size_t n
     return guarded([&] {
         if (n == 0) return;
         if (!boards || !out4 || !flags4) throw Error(EGTB_ERR_ARG, "NULL buffer");
-        on_device(device, [&] {
+        on_device(device, [&](cudaStream_t s) {
             const AdDeviceTables t = device_ad_tables(device);
-            AdBuffers buf;
+            AdBuffers buf(s);
             auto *din = (uint64_t *)buf.get(n * 8);
             auto *dout = (uint64_t *)buf.get(n * 32);
             auto *dfl = (uint8_t *)buf.get(n * 4);
-            EGTB_CUDA(cudaMemcpy(din, boards, n * 8, cudaMemcpyHostToDevice));
-            ad_moves_kernel<<<kAdGrid, kAdBlock>>>(t.moves, t.flags, din, n, dout, dfl);
+            EGTB_CUDA(cudaMemcpyAsync(din, boards, n * 8, cudaMemcpyHostToDevice, s));
+            ad_moves_kernel<<<kAdGrid, kAdBlock, 0, s>>>(t.moves, t.flags, din, n, dout, dfl);
             EGTB_CUDA(cudaGetLastError());
-            EGTB_CUDA(cudaMemcpy(out4, dout, n * 32, cudaMemcpyDeviceToHost));
-            EGTB_CUDA(cudaMemcpy(flags4, dfl, n * 4, cudaMemcpyDeviceToHost));
+            EGTB_CUDA(cudaMemcpyAsync(out4, dout, n * 32, cudaMemcpyDeviceToHost, s));
+            EGTB_CUDA(cudaMemcpyAsync(flags4, dfl, n * 4, cudaMemcpyDeviceToHost, s));
         });
     });
 }
@@ -481,14 +502,14 @@ extern "C" int egtb_ad_mask_board(int device, const uint64_t *boards, size_t n, 
     return guarded([&] {
         if (n == 0) return;
         if (!boards || !out) throw Error(EGTB_ERR_ARG, "NULL buffer");
-        on_device(device, [&] {
-            AdBuffers buf;
+        on_device(device, [&](cudaStream_t s) {
+            AdBuffers buf(s);
             auto *din = (uint64_t *)buf.get(n * 8);
             auto *dout = (uint64_t *)buf.get(n * 8);
-            EGTB_CUDA(cudaMemcpy(din, boards, n * 8, cudaMemcpyHostToDevice));
-            ad_mask_kernel<<<kAdGrid, kAdBlock>>>(din, n, (long long)threshold, dout);
+            EGTB_CUDA(cudaMemcpyAsync(din, boards, n * 8, cudaMemcpyHostToDevice, s));
+            ad_mask_kernel<<<kAdGrid, kAdBlock, 0, s>>>(din, n, (long long)threshold, dout);
             EGTB_CUDA(cudaGetLastError());
-            EGTB_CUDA(cudaMemcpy(out, dout, n * 8, cudaMemcpyDeviceToHost));
+            EGTB_CUDA(cudaMemcpyAsync(out, dout, n * 8, cudaMemcpyDeviceToHost, s));
         });
     });
 }
@@ -500,14 +521,14 @@ extern "C" int egtb_ad_tile_stats(int device, const uint64_t *boards, size_t n, 
         const AdParamDev p = ad_param(param);
         if (n == 0) return;
         if (!boards || !out) throw Error(EGTB_ERR_ARG, "NULL buffer");
-        on_device(device, [&] {
-            AdBuffers buf;
+        on_device(device, [&](cudaStream_t s) {
+            AdBuffers buf(s);
             auto *din = (uint64_t *)buf.get(n * 8);
             auto *dout = (egtb_ad_tile_count *)buf.get(n * sizeof(egtb_ad_tile_count));
-            EGTB_CUDA(cudaMemcpy(din, boards, n * 8, cudaMemcpyHostToDevice));
-            ad_stats_kernel<<<kAdGrid, kAdBlock>>>(din, n, p, kind, dout);
+            EGTB_CUDA(cudaMemcpyAsync(din, boards, n * 8, cudaMemcpyHostToDevice, s));
+            ad_stats_kernel<<<kAdGrid, kAdBlock, 0, s>>>(din, n, p, kind, dout);
             EGTB_CUDA(cudaGetLastError());
-            EGTB_CUDA(cudaMemcpy(out, dout, n * sizeof(egtb_ad_tile_count), cudaMemcpyDeviceToHost));
+            EGTB_CUDA(cudaMemcpyAsync(out, dout, n * sizeof(egtb_ad_tile_count), cudaMemcpyDeviceToHost, s));
         });
     });
 }
@@ -518,17 +539,17 @@ extern "C" int egtb_ad_validate(int device, const uint64_t *boards, size_t n, co
         const AdParamDev p = ad_param(param);
         if (n == 0) return;
         if (!boards || !original_sums || !out) throw Error(EGTB_ERR_ARG, "NULL buffer");
-        on_device(device, [&] {
+        on_device(device, [&](cudaStream_t s) {
             const AdDeviceTables t = device_ad_tables(device);
-            AdBuffers buf;
+            AdBuffers buf(s);
             auto *din = (uint64_t *)buf.get(n * 8);
             auto *dsum = (uint32_t *)buf.get(n * 4);
             auto *dout = (uint8_t *)buf.get(n);
-            EGTB_CUDA(cudaMemcpy(din, boards, n * 8, cudaMemcpyHostToDevice));
-            EGTB_CUDA(cudaMemcpy(dsum, original_sums, n * 4, cudaMemcpyHostToDevice));
-            ad_validate_kernel<<<kAdGrid, kAdBlock>>>(din, dsum, n, p, t.lens, t.vals, dout);
+            EGTB_CUDA(cudaMemcpyAsync(din, boards, n * 8, cudaMemcpyHostToDevice, s));
+            EGTB_CUDA(cudaMemcpyAsync(dsum, original_sums, n * 4, cudaMemcpyHostToDevice, s));
+            ad_validate_kernel<<<kAdGrid, kAdBlock, 0, s>>>(din, dsum, n, p, t.lens, t.vals, dout);
             EGTB_CUDA(cudaGetLastError());
-            EGTB_CUDA(cudaMemcpy(out, dout, n, cudaMemcpyDeviceToHost));
+            EGTB_CUDA(cudaMemcpyAsync(out, dout, n, cudaMemcpyDeviceToHost, s));
         });
     });
 }
@@ -575,21 +596,22 @@ extern "C" int egtb_ad_unmask(int device, const uint64_t *boards, size_t n, cons
                                                         (unsigned)k};
             rows.insert(rows.end(), r.begin(), r.end());
         }
-        on_device(device, [&] {
+        on_device(device, [&](cudaStream_t s) {
             const AdDeviceTables t = device_ad_tables(device);
-            AdBuffers buf;
+            AdBuffers buf(s);
             auto *din = (uint64_t *)buf.get(n * 8);
             auto *dsum = (uint32_t *)buf.get(n * 4);
             auto *dcnt = (uint32_t *)buf.get(n * 4);
             auto *dslots = (AdPermSlot *)buf.get(slots.size() * sizeof(AdPermSlot));
             auto *drows = (uint8_t *)buf.get(rows.size());
-            EGTB_CUDA(cudaMemcpy(din, boards, n * 8, cudaMemcpyHostToDevice));
-            EGTB_CUDA(cudaMemcpy(dsum, original_sums, n * 4, cudaMemcpyHostToDevice));
-            EGTB_CUDA(cudaMemcpy(dslots, slots.data(), slots.size() * sizeof(AdPermSlot), cudaMemcpyHostToDevice));
-            if (!rows.empty()) EGTB_CUDA(cudaMemcpy(drows, rows.data(), rows.size(), cudaMemcpyHostToDevice));
-            ad_unmask_count_kernel<<<kAdGrid, kAdBlock>>>(din, dsum, n, p, t.lens, t.vals, dslots, drows, dcnt);
+            EGTB_CUDA(cudaMemcpyAsync(din, boards, n * 8, cudaMemcpyHostToDevice, s));
+            EGTB_CUDA(cudaMemcpyAsync(dsum, original_sums, n * 4, cudaMemcpyHostToDevice, s));
+            EGTB_CUDA(cudaMemcpyAsync(dslots, slots.data(), slots.size() * sizeof(AdPermSlot), cudaMemcpyHostToDevice, s));
+            if (!rows.empty()) EGTB_CUDA(cudaMemcpyAsync(drows, rows.data(), rows.size(), cudaMemcpyHostToDevice, s));
+            ad_unmask_count_kernel<<<kAdGrid, kAdBlock, 0, s>>>(din, dsum, n, p, t.lens, t.vals, dslots, drows, dcnt);
             EGTB_CUDA(cudaGetLastError());
-            EGTB_CUDA(cudaMemcpy(counts, dcnt, n * 4, cudaMemcpyDeviceToHost));
+            EGTB_CUDA(cudaMemcpyAsync(counts, dcnt, n * 4, cudaMemcpyDeviceToHost, s));
+            EGTB_CUDA(cudaStreamSynchronize(s));  // the offsets below read the counts
             std::vector<unsigned long long> offs(n);
             unsigned long long sum = 0;
             for (size_t i = 0; i < n; ++i) {
@@ -601,10 +623,10 @@ extern "C" int egtb_ad_unmask(int device, const uint64_t *boards, size_t n, cons
             if (sum == 0) return;
             auto *doffs = (unsigned long long *)buf.get(n * 8);
             auto *dout = (uint64_t *)buf.get(sum * 8);
-            EGTB_CUDA(cudaMemcpy(doffs, offs.data(), n * 8, cudaMemcpyHostToDevice));
-            ad_unmask_write_kernel<<<kAdGrid, kAdBlock>>>(din, dsum, n, p, t.lens, t.vals, dslots, drows, doffs, dout);
+            EGTB_CUDA(cudaMemcpyAsync(doffs, offs.data(), n * 8, cudaMemcpyHostToDevice, s));
+            ad_unmask_write_kernel<<<kAdGrid, kAdBlock, 0, s>>>(din, dsum, n, p, t.lens, t.vals, dslots, drows, doffs, dout);
             EGTB_CUDA(cudaGetLastError());
-            EGTB_CUDA(cudaMemcpy(out, dout, sum * 8, cudaMemcpyDeviceToHost));
+            EGTB_CUDA(cudaMemcpyAsync(out, dout, sum * 8, cudaMemcpyDeviceToHost, s));
         });
     });
 }
