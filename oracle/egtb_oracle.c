@@ -543,3 +543,257 @@ int or_solve(or_build *b, int dtype, double spawn_rate4) {
     }
     return 0;
 }
+
+/* ================================================================ advanced ===
+ * The advanced algorithm's masked-board primitives (namespace FormationAD),
+ * restated on tile values: a masked board holds every tile of 64 and up as
+ * the 0xF ("32k", value 32768) nibble. */
+
+static uint32_t tile_value(int nibble) { return nibble ? 1u << nibble : 0u; }
+
+static int tile_nibble(uint32_t v) {
+    int n = 0;
+    while (v > 1) {
+        v >>= 1;
+        ++n;
+    }
+    return n;
+}
+
+/* One line of four cells moved toward cell 0 (merge_line,
+ * native_core/src/BoardMoverAD.cpp:49-89): 32768 never merges; a merged
+ * value of 64 or more becomes 32768 and sets *made. */
+static void ad_merge_line(int cells[4], int *made) {
+    uint32_t nz[4], out[4] = {0, 0, 0, 0};
+    int k = 0, m = 0;
+    for (int i = 0; i < 4; ++i)
+        if (cells[i]) nz[k++] = tile_value(cells[i]);
+    for (int i = 0; i < k; ++i) {
+        if (i + 1 < k && nz[i] == nz[i + 1] && nz[i] != 32768u) {
+            uint32_t v = nz[i] * 2u;
+            if (v >= 64u) {
+                *made = 1;
+                v = 32768u;
+            }
+            out[m++] = v;
+            ++i;
+        } else {
+            out[m++] = nz[i];
+        }
+    }
+    for (int i = 0; i < 4; ++i) cells[i] = tile_nibble(out[i]);
+}
+
+/* every row of b moved toward column 0 (reverse=0) or column 3 */
+static uint64_t ad_rows(uint64_t b, int reverse, int *made) {
+    uint64_t o = 0;
+    for (int r = 0; r < 4; ++r) {
+        int cells[4];
+        for (int c = 0; c < 4; ++c) cells[reverse ? 3 - c : c] = nib(b, r, c);
+        ad_merge_line(cells, made);
+        for (int c = 0; c < 4; ++c) o |= put(cells[reverse ? 3 - c : c], r, c);
+    }
+    return o;
+}
+
+/* m_move_all_dir, native_core/src/BoardMoverAD.cpp:171-178: {left, right,
+ * up, down}; left and right carry the left merge's flag, up and down the up
+ * merge's */
+void or_ad_move_all_dir_batch(const uint64_t *b, size_t n, uint64_t *out4, uint8_t *flags4) {
+    for (size_t i = 0; i < n; ++i) {
+        int fh = 0, fv = 0, ignored = 0;
+        const uint64_t t = transpose(b[i]);
+        out4[4 * i + 0] = ad_rows(b[i], 0, &fh);
+        out4[4 * i + 1] = ad_rows(b[i], 1, &ignored);
+        out4[4 * i + 2] = transpose(ad_rows(t, 0, &fv));
+        out4[4 * i + 3] = transpose(ad_rows(t, 1, &ignored));
+        flags4[4 * i + 0] = flags4[4 * i + 1] = (uint8_t)fh;
+        flags4[4 * i + 2] = flags4[4 * i + 3] = (uint8_t)fv;
+    }
+}
+
+/* mask_board, native_core/src/BoardMaskerAD.cpp:112-121 */
+uint64_t or_ad_mask_board(uint64_t b, int threshold) {
+    uint64_t m = b;
+    for (int k = 0; k < 16; ++k)
+        if (((b >> (4 * k)) & 0xFull) >= (uint64_t)(int64_t)threshold) m |= 0xFull << (4 * k);
+    return m;
+}
+
+/* Tile statistics after the fixed 32k cells are cleared:
+ * kind 1 tile_sum_and_32k_count (BoardMaskerAD.cpp:123-144, 32k = 0xF only),
+ * kind 2 tile_sum_and_32k_count2 (:169-190, 32k = 64 and up),
+ * kind 4 tile_sum_and_32k_count4 (:219-257). Per 16-bit row as the
+ * reference's info tables hold it (:24-50): a uint16 tile sum, and pos_rank =
+ * the 0xF cells met, from the row's high nibble down, before its first
+ * non-0xF 32k tile. out8: total_sum, count_32k, pos_bitmap low, high,
+ * pos_rank, merged_tile_found, merged_tile, is_success. */
+void or_ad_tile_stats(uint64_t b, const or_ad_param *p, int kind, int64_t out8[8]) {
+    b &= ~p->pos_fixed_32k_mask;
+    uint32_t total = 0, count = 0, found = 0, merged = 0, rank[4], rowfound[4];
+    uint64_t pos = 0;
+    for (int k = 0; k < 4; ++k) {
+        uint16_t sum16 = 0;
+        rank[k] = rowfound[k] = 0;
+        for (int i = 3; i >= 0; --i) {
+            const int sh = 16 * k + 4 * i;
+            const int v = (int)((b >> sh) & 0xF);
+            const int large = kind == 1 ? v == 15 : v > 5;
+            if (large) {
+                pos |= 0xFull << sh;
+                ++count;
+                if (v == 15) {
+                    if (rowfound[k] == 0) ++rank[k];
+                } else {
+                    ++rowfound[k];
+                    merged ^= (uint32_t)v;
+                }
+            } else if (v > 0) {
+                sum16 = (uint16_t)(sum16 + (1u << v));
+            }
+        }
+        total += sum16;
+        found += rowfound[k];
+    }
+    memset(out8, 0, 8 * sizeof(int64_t));
+    out8[0] = total;
+    out8[1] = count;
+    out8[2] = (int64_t)(pos & 0xFFFFFFFFull);
+    out8[3] = (int64_t)(pos >> 32);
+    if (kind == 4) {
+        /* the 0xF cells counted from the top row down to the first row with a merged tile */
+        uint32_t r = 0;
+        for (int k = 3; k >= 0; --k) {
+            r += rank[k];
+            if (rowfound[k]) break;
+        }
+        out8[4] = r;
+        out8[5] = found;
+        out8[6] = merged;
+        out8[7] = (merged == (p->target & 0xFFu) && found == 1) ? 1 : 0;
+    }
+}
+
+/* masked_tiles_combinations (BoardMaskerAD.cpp:259-289), stored ascending as
+ * init_masker stores it (:524-531): count tiles of 64 .. 8192 summing to
+ * sum, largest first, with the reference's early exits; returns the length
+ * (0: none). */
+static int ad_combination(uint32_t sum, int count, uint8_t out[16]) {
+    uint8_t tiles[16];
+    int len = 0;
+    for (uint32_t tile = 8192; tile >= 64; tile >>= 1) {
+        if (tile > sum) continue;
+        if (tile == sum) {
+            if (count == 1) {
+                tiles[len++] = (uint8_t)tile_nibble(tile);
+                goto done;
+            }
+            continue;
+        }
+        if (2 * tile == sum && count == 2) {
+            tiles[len++] = (uint8_t)tile_nibble(tile);
+            tiles[len++] = (uint8_t)tile_nibble(tile);
+            goto done;
+        }
+        if (tile != 64 && sum == 192 && count == 3) {
+            tiles[len++] = 6;
+            tiles[len++] = 6;
+            tiles[len++] = 6;
+            goto done;
+        }
+        sum -= tile;
+        --count;
+        tiles[len++] = (uint8_t)tile_nibble(tile);
+    }
+    return 0;
+done:
+    for (int i = 0; i < len; ++i) out[i] = tiles[len - 1 - i];
+    return len;
+}
+
+/* validate, native_core/src/BoardMaskerAD.cpp:409-443 (boards whose 32k count
+ * is num_free_32k .. num_free_32k + 9, where the reference's table lookup
+ * stays inside its table) */
+int or_ad_validate(uint64_t b, uint32_t original_sum, const or_ad_param *p) {
+    int64_t st[8];
+    or_ad_tile_stats(b, p, 2, st);
+    const uint32_t total = (uint32_t)st[0];
+    const int8_t count = (int8_t)st[1], free32k = (int8_t)p->num_free_32k;
+    if (total >= p->small_tile_sum_limit + 64u) return 0;
+    if (count == free32k) return 1;
+    const uint32_t large = original_sum - total - ((uint32_t)(p->num_free_32k + p->num_fixed_32k) << 15);
+    const uint8_t a = (uint8_t)(large >> 6), c = (uint8_t)(count - free32k);
+    uint8_t tc[16];
+    const int len = (a == 0 || c >= 10) ? 0 : ad_combination((uint32_t)a << 6, c, tc);  /* table: a > 0, c < 10 */
+    if (len == 0) return 0;
+    if (tc[len - 1] == (uint8_t)p->target) return 0;
+    if (count < 2) return 1;
+    if (len > 2 && tc[0] == tc[2]) return total >= p->small_tile_sum_limit - 64u ? 0 : 1;
+    if (len > 1 && tc[0] == tc[1]) return total >= p->small_tile_sum_limit ? 0 : 1;
+    return 1;
+}
+
+/* unmask_board, native_core/src/BoardMaskerAD.cpp:445-512, over the slots
+ * of init_masker (:514-533). The permutation rows of slot (m, n) come in
+ * the order resort_permutations gives them (:291-332): by the cells'
+ * contents read from cell 0 to cell m-1 (value j, or 15 for a cell left
+ * out), produced here directly in that order by a depth-first walk that
+ * tries a cell's values smallest first and "left out" last. */
+typedef struct {
+    uint64_t board;
+    const uint8_t *pos; /* 0xF cells, highest first */
+    const uint8_t *tc;
+    int m, n, len, ordered;
+    uint64_t *out;
+    size_t cap, total;
+} ad_walk;
+
+static void ad_emit(ad_walk *w, const int cell_of[16]) {
+    if (w->ordered && !(cell_of[1] < cell_of[0])) return;
+    uint64_t clear = 0, set = 0;
+    for (int j = 0; j < w->len; ++j) {
+        clear += 0xFull << w->pos[cell_of[j]];
+        set += (uint64_t)w->tc[j] << w->pos[cell_of[j]];
+    }
+    if (w->total < w->cap) w->out[w->total] = (w->board & ~clear) | set;
+    ++w->total;
+}
+
+static void ad_walk_cells(ad_walk *w, int cell, int placed, int used_mask, int cell_of[16]) {
+    if (cell == w->m) {
+        if (placed == w->n) ad_emit(w, cell_of);
+        return;
+    }
+    for (int j = 0; j < w->n; ++j) {
+        if (used_mask >> j & 1) continue;
+        cell_of[j] = cell;
+        ad_walk_cells(w, cell + 1, placed + 1, used_mask | (1 << j), cell_of);
+    }
+    if (w->m - cell - 1 >= w->n - placed) ad_walk_cells(w, cell + 1, placed, used_mask, cell_of);
+}
+
+size_t or_ad_unmask(uint64_t b, uint32_t original_sum, const or_ad_param *p, uint64_t *out, size_t cap) {
+    const uint64_t masked = b & ~p->pos_fixed_32k_mask;
+    int64_t st[8];
+    or_ad_tile_stats(b, p, 1, st);
+    uint8_t pos[16];
+    int npos = 0;
+    for (int sh = 60; sh >= 0; sh -= 4)
+        if (((masked >> sh) & 0xF) == 0xF) pos[npos++] = (uint8_t)sh;
+    const int8_t count = (int8_t)npos, free32k = (int8_t)p->num_free_32k;
+    if (count == 0 || count == free32k) {
+        if (cap) out[0] = b;
+        return 1;
+    }
+    const uint32_t large = (uint32_t)original_sum - (uint32_t)st[0] -
+                           ((uint32_t)(p->num_free_32k + p->num_fixed_32k) << 15);
+    const uint8_t a = (uint8_t)(large >> 6), c = (uint8_t)(count - free32k);
+    uint8_t tc[16];
+    const int len = (a == 0 || c >= 10) ? 0 : ad_combination((uint32_t)a << 6, c, tc);
+    if (len == 0) return 0;
+    if (c < 1 || (int)c >= (int)(p->target & 0xFFu) - 4 || npos > 15) return 0;  /* no slot */
+    ad_walk w = {b, pos, tc, npos, c, len, len > 1 && tc[0] == tc[1], out, cap, 0};
+    int cell_of[16] = {0};
+    ad_walk_cells(&w, 0, 0, 0, cell_of);
+    return w.total;
+}

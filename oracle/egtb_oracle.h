@@ -1,5 +1,6 @@
 /*
- * CPU oracle for the classic endgame-tablebase build and lookup path.
+ * CPU oracle for the classic endgame-tablebase build and lookup path, and
+ * for the advanced algorithm's masked-board primitives.
  *
  * TEST INFRASTRUCTURE ONLY. This is a plain-C restatement of the reference
  * algorithm (game-difficulty/2048EndgameTablebase, native_core/) used by the
@@ -8,8 +9,8 @@
  *
  * Every function cites the reference file:line it restates. Parity of this
  * restatement against the reference's own compiled code is pinned by
- * tests/test_oracle_golden.py (digests produced by the reference itself,
- * tests/golden/make_golden.py).
+ * tests/test_oracle_golden.py and tests/test_oracle_ad.py (digests and
+ * vectors produced by the reference itself, tests/golden/make_golden.py).
  */
 #ifndef EGTB_ORACLE_H
 #define EGTB_ORACLE_H
@@ -52,6 +53,18 @@ void or_row_tables(uint16_t *left_xor, uint16_t *right_xor);
 /* batch wrappers for tests */
 void or_move_all_dir_batch(const uint64_t *b, size_t n, uint64_t *out4);
 void or_canonical_batch(const uint64_t *b, size_t n, int mode, uint64_t *out);
+
+/* the advanced algorithm's masked-board primitives (AdvancedMaskParam,
+ * native_core/include/FormationRuntime.h:98-104) */
+typedef struct {
+    uint64_t pos_fixed_32k_mask;
+    uint32_t small_tile_sum_limit, target, num_free_32k, num_fixed_32k;
+} or_ad_param;
+void or_ad_move_all_dir_batch(const uint64_t *b, size_t n, uint64_t *out4, uint8_t *flags4);
+uint64_t or_ad_mask_board(uint64_t b, int threshold);
+void or_ad_tile_stats(uint64_t b, const or_ad_param *p, int kind, int64_t out8[8]);
+int or_ad_validate(uint64_t b, uint32_t original_sum, const or_ad_param *p);
+size_t or_ad_unmask(uint64_t b, uint32_t original_sum, const or_ad_param *p, uint64_t *out, size_t cap);
 
 /* full build, layer-resident */
 typedef struct or_build or_build;

@@ -122,6 +122,75 @@ def row_tables(variant: bool = False):
     return left, right
 
 
+# ---- the advanced algorithm's masked-board primitives (checker only)
+
+class _AdParam(ctypes.Structure):
+    _fields_ = [("pos_fixed_32k_mask", ctypes.c_uint64), ("small_tile_sum_limit", ctypes.c_uint32),
+                ("target", ctypes.c_uint32), ("num_free_32k", ctypes.c_uint32), ("num_fixed_32k", ctypes.c_uint32)]
+
+
+def ad_param(small_tile_sum_limit: int, target: int, fixed_shifts, num_free_32k: int) -> _AdParam:
+    fixed = 0
+    for sh in fixed_shifts:
+        fixed |= 0xF << int(sh)
+    return _AdParam(fixed, int(small_tile_sum_limit), int(target), int(num_free_32k), len(fixed_shifts))
+
+
+def _ad_lib():
+    L = lib()
+    if not getattr(L, "_ad_ready", False):
+        P = ctypes.c_void_p
+        L.or_ad_move_all_dir_batch.argtypes = [P, ctypes.c_size_t, P, P]
+        L.or_ad_mask_board.argtypes = [ctypes.c_uint64, ctypes.c_int]
+        L.or_ad_mask_board.restype = ctypes.c_uint64
+        L.or_ad_tile_stats.argtypes = [ctypes.c_uint64, ctypes.POINTER(_AdParam), ctypes.c_int, P]
+        L.or_ad_validate.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(_AdParam)]
+        L.or_ad_unmask.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(_AdParam), P, ctypes.c_size_t]
+        L.or_ad_unmask.restype = ctypes.c_size_t
+        L._ad_ready = True
+    return L
+
+
+def ad_move_all_dir(boards: np.ndarray):
+    b = np.ascontiguousarray(boards, dtype=np.uint64)
+    out = np.zeros((len(b), 4), dtype=np.uint64)
+    fl = np.zeros((len(b), 4), dtype=np.uint8)
+    _ad_lib().or_ad_move_all_dir_batch(b.ctypes.data, len(b), out.ctypes.data, fl.ctypes.data)
+    return out, fl
+
+
+def ad_mask_board(boards: np.ndarray, threshold: int) -> np.ndarray:
+    L = _ad_lib()
+    return np.array([L.or_ad_mask_board(int(x), int(threshold)) for x in boards], dtype=np.uint64)
+
+
+def ad_tile_stats(boards: np.ndarray, param: _AdParam, kind: int) -> np.ndarray:
+    L = _ad_lib()
+    out = np.zeros((len(boards), 8), dtype=np.int64)
+    row = np.zeros(8, dtype=np.int64)
+    for i, x in enumerate(boards):
+        L.or_ad_tile_stats(int(x), ctypes.byref(param), int(kind), row.ctypes.data)
+        out[i] = row
+    return out
+
+
+def ad_validate(boards: np.ndarray, sums: np.ndarray, param: _AdParam) -> np.ndarray:
+    L = _ad_lib()
+    return np.array([L.or_ad_validate(int(x), int(s), ctypes.byref(param)) for x, s in zip(boards, sums)],
+                    dtype=np.uint8)
+
+
+def ad_unmask(boards: np.ndarray, sums: np.ndarray, param: _AdParam):
+    L = _ad_lib()
+    counts, out = [], []
+    buf = np.zeros(1 << 16, dtype=np.uint64)
+    for x, s in zip(boards, sums):
+        n = L.or_ad_unmask(int(x), int(s), ctypes.byref(param), buf.ctypes.data, len(buf))
+        counts.append(n)
+        out.append(buf[:min(n, len(buf))].copy())
+    return np.array(counts, dtype=np.uint32), (np.concatenate(out) if out else np.zeros(0, dtype=np.uint64))
+
+
 def expand(parents: np.ndarray, spec: Spec, target: int, do_check: bool):
     p = np.ascontiguousarray(parents, dtype=np.uint64)
     cap = len(p) * 64 + 16
