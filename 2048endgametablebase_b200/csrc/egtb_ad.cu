@@ -458,7 +458,8 @@ struct AdBuffers {
     }
 };
 
-// Run f(stream) for one call on `device`; returns once the call's work and
+// Run f(stream, grid) for one call on `device` (grid: four 256-thread blocks
+// per SM for the grid-stride kernels); returns once the call's work and
 // copies are done.
 template <typename F>
 void on_device(int device, F &&f) {
@@ -466,13 +467,15 @@ void on_device(int device, F &&f) {
     EGTB_CUDA(cudaGetDeviceCount(&count));
     if (device < 0 || device >= count) throw Error(EGTB_ERR_ARG, "device out of range");
     EGTB_CUDA(cudaSetDevice(device));
+    int sms = 0;
+    EGTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     const cudaStream_t s = ad_stream(device);
-    f(s);
+    f(s, 4 * std::max(1, sms));
     EGTB_CUDA(cudaGetLastError());
     EGTB_CUDA(cudaStreamSynchronize(s));
 }
 
-constexpr int kAdGrid = 148 * 4, kAdBlock = 256;
+constexpr int kAdBlock = 256;
 
 }  // namespace
 }  // namespace egtb
@@ -483,14 +486,14 @@ extern "C" int egtb_ad_move_all_dir(int device, const uint64_t *boards, size_t n
     return guarded([&] {
         if (n == 0) return;
         if (!boards || !out4 || !flags4) throw Error(EGTB_ERR_ARG, "NULL buffer");
-        on_device(device, [&](cudaStream_t s) {
+        on_device(device, [&](cudaStream_t s, int grid) {
             const AdDeviceTables t = device_ad_tables(device);
             AdBuffers buf(s);
             auto *din = (uint64_t *)buf.get(n * 8);
             auto *dout = (uint64_t *)buf.get(n * 32);
             auto *dfl = (uint8_t *)buf.get(n * 4);
             EGTB_CUDA(cudaMemcpyAsync(din, boards, n * 8, cudaMemcpyHostToDevice, s));
-            ad_moves_kernel<<<kAdGrid, kAdBlock, 0, s>>>(t.moves, t.flags, din, n, dout, dfl);
+            ad_moves_kernel<<<grid, kAdBlock, 0, s>>>(t.moves, t.flags, din, n, dout, dfl);
             EGTB_CUDA(cudaGetLastError());
             EGTB_CUDA(cudaMemcpyAsync(out4, dout, n * 32, cudaMemcpyDeviceToHost, s));
             EGTB_CUDA(cudaMemcpyAsync(flags4, dfl, n * 4, cudaMemcpyDeviceToHost, s));
@@ -502,12 +505,12 @@ extern "C" int egtb_ad_mask_board(int device, const uint64_t *boards, size_t n, 
     return guarded([&] {
         if (n == 0) return;
         if (!boards || !out) throw Error(EGTB_ERR_ARG, "NULL buffer");
-        on_device(device, [&](cudaStream_t s) {
+        on_device(device, [&](cudaStream_t s, int grid) {
             AdBuffers buf(s);
             auto *din = (uint64_t *)buf.get(n * 8);
             auto *dout = (uint64_t *)buf.get(n * 8);
             EGTB_CUDA(cudaMemcpyAsync(din, boards, n * 8, cudaMemcpyHostToDevice, s));
-            ad_mask_kernel<<<kAdGrid, kAdBlock, 0, s>>>(din, n, (long long)threshold, dout);
+            ad_mask_kernel<<<grid, kAdBlock, 0, s>>>(din, n, (long long)threshold, dout);
             EGTB_CUDA(cudaGetLastError());
             EGTB_CUDA(cudaMemcpyAsync(out, dout, n * 8, cudaMemcpyDeviceToHost, s));
         });
@@ -521,12 +524,12 @@ extern "C" int egtb_ad_tile_stats(int device, const uint64_t *boards, size_t n, 
         const AdParamDev p = ad_param(param);
         if (n == 0) return;
         if (!boards || !out) throw Error(EGTB_ERR_ARG, "NULL buffer");
-        on_device(device, [&](cudaStream_t s) {
+        on_device(device, [&](cudaStream_t s, int grid) {
             AdBuffers buf(s);
             auto *din = (uint64_t *)buf.get(n * 8);
             auto *dout = (egtb_ad_tile_count *)buf.get(n * sizeof(egtb_ad_tile_count));
             EGTB_CUDA(cudaMemcpyAsync(din, boards, n * 8, cudaMemcpyHostToDevice, s));
-            ad_stats_kernel<<<kAdGrid, kAdBlock, 0, s>>>(din, n, p, kind, dout);
+            ad_stats_kernel<<<grid, kAdBlock, 0, s>>>(din, n, p, kind, dout);
             EGTB_CUDA(cudaGetLastError());
             EGTB_CUDA(cudaMemcpyAsync(out, dout, n * sizeof(egtb_ad_tile_count), cudaMemcpyDeviceToHost, s));
         });
@@ -539,7 +542,7 @@ extern "C" int egtb_ad_validate(int device, const uint64_t *boards, size_t n, co
         const AdParamDev p = ad_param(param);
         if (n == 0) return;
         if (!boards || !original_sums || !out) throw Error(EGTB_ERR_ARG, "NULL buffer");
-        on_device(device, [&](cudaStream_t s) {
+        on_device(device, [&](cudaStream_t s, int grid) {
             const AdDeviceTables t = device_ad_tables(device);
             AdBuffers buf(s);
             auto *din = (uint64_t *)buf.get(n * 8);
@@ -547,7 +550,7 @@ extern "C" int egtb_ad_validate(int device, const uint64_t *boards, size_t n, co
             auto *dout = (uint8_t *)buf.get(n);
             EGTB_CUDA(cudaMemcpyAsync(din, boards, n * 8, cudaMemcpyHostToDevice, s));
             EGTB_CUDA(cudaMemcpyAsync(dsum, original_sums, n * 4, cudaMemcpyHostToDevice, s));
-            ad_validate_kernel<<<kAdGrid, kAdBlock, 0, s>>>(din, dsum, n, p, t.lens, t.vals, dout);
+            ad_validate_kernel<<<grid, kAdBlock, 0, s>>>(din, dsum, n, p, t.lens, t.vals, dout);
             EGTB_CUDA(cudaGetLastError());
             EGTB_CUDA(cudaMemcpyAsync(out, dout, n, cudaMemcpyDeviceToHost, s));
         });
@@ -596,7 +599,7 @@ extern "C" int egtb_ad_unmask(int device, const uint64_t *boards, size_t n, cons
                                                         (unsigned)k};
             rows.insert(rows.end(), r.begin(), r.end());
         }
-        on_device(device, [&](cudaStream_t s) {
+        on_device(device, [&](cudaStream_t s, int grid) {
             const AdDeviceTables t = device_ad_tables(device);
             AdBuffers buf(s);
             auto *din = (uint64_t *)buf.get(n * 8);
@@ -608,7 +611,7 @@ extern "C" int egtb_ad_unmask(int device, const uint64_t *boards, size_t n, cons
             EGTB_CUDA(cudaMemcpyAsync(dsum, original_sums, n * 4, cudaMemcpyHostToDevice, s));
             EGTB_CUDA(cudaMemcpyAsync(dslots, slots.data(), slots.size() * sizeof(AdPermSlot), cudaMemcpyHostToDevice, s));
             if (!rows.empty()) EGTB_CUDA(cudaMemcpyAsync(drows, rows.data(), rows.size(), cudaMemcpyHostToDevice, s));
-            ad_unmask_count_kernel<<<kAdGrid, kAdBlock, 0, s>>>(din, dsum, n, p, t.lens, t.vals, dslots, drows, dcnt);
+            ad_unmask_count_kernel<<<grid, kAdBlock, 0, s>>>(din, dsum, n, p, t.lens, t.vals, dslots, drows, dcnt);
             EGTB_CUDA(cudaGetLastError());
             EGTB_CUDA(cudaMemcpyAsync(counts, dcnt, n * 4, cudaMemcpyDeviceToHost, s));
             EGTB_CUDA(cudaStreamSynchronize(s));  // the offsets below read the counts
@@ -624,7 +627,7 @@ extern "C" int egtb_ad_unmask(int device, const uint64_t *boards, size_t n, cons
             auto *doffs = (unsigned long long *)buf.get(n * 8);
             auto *dout = (uint64_t *)buf.get(sum * 8);
             EGTB_CUDA(cudaMemcpyAsync(doffs, offs.data(), n * 8, cudaMemcpyHostToDevice, s));
-            ad_unmask_write_kernel<<<kAdGrid, kAdBlock, 0, s>>>(din, dsum, n, p, t.lens, t.vals, dslots, drows, doffs, dout);
+            ad_unmask_write_kernel<<<grid, kAdBlock, 0, s>>>(din, dsum, n, p, t.lens, t.vals, dslots, drows, doffs, dout);
             EGTB_CUDA(cudaGetLastError());
             EGTB_CUDA(cudaMemcpyAsync(out, dout, sum * 8, cudaMemcpyDeviceToHost, s));
         });
